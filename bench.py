@@ -1,0 +1,386 @@
+"""Solve-phase benchmark: time-to-1e-10 relative residual on one B200 per rank.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl prism|reference]
+
+Workload (default): 3D Poisson 7-point Laplacian 128^3 (n = 2,097,152,
+nnz = 14,581,760; generateLaplacianCSR), b ~ N(0,1) from a fixed seed, x0 = 0,
+flexible CG + threshold incomplete Cholesky ICT(1e-3), relative tolerance
+1e-10, max 1000 iterations.  The preconditioner is set up once on the host
+(outside the timed region); one step is one complete device-resident solve.
+The headline is the mixed-precision solve (FP32 factor values, FP64 Krylov
+vectors and scalars); the same solve with FP64 factor values is timed beside it.
+
+Multi-GPU: replicas only (one independent system per rank, no collective on the
+data path); the process group is used for the barrier and the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "time-to-1e-10 rel. residual (FCG + ICT(1e-3), mixed FP32-factor / FP64-Krylov)"
+SEED = 2024
+
+
+def workload(grid: int, tol: float) -> str:
+    n = grid ** 3
+    nnz = 7 * n - 6 * grid * grid
+    return (f"3D Poisson 7-pt {grid}^3 (n={n}, nnz={nnz}), FCG + ICT(1e-3), tol {tol:g}, "
+            f"b~N(0,1) seed {SEED}")
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="prism", choices=["prism", "reference"])
+    p.add_argument("--grid", type=int, default=128)
+    p.add_argument("--tol", type=float, default=1e-10)
+    p.add_argument("--no-fp64", action="store_true", help="skip the FP64-factor comparison solve")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-sample-s", type=float, default=15.0, help="target seconds of reference CPU work")
+    return p.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out = ""
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak_gbs():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# reference CPU solver (oracle/_ref fast build, else the oracle port)
+# ---------------------------------------------------------------------------
+class CpuReference:
+    """The reference's CG<double> + IncompleteCholesky<float,double> on the host
+    cores (oracle/_ref, built from the reference's sources with its Release
+    flags; 4 OpenMP threads as THREAD_NUM hard-wires), else the oracle port.
+    Setup runs once in the constructor (so the solve's own setup() is a no-op,
+    IncompleteCholesky.cpp:105) and is excluded from the timings."""
+
+    def __init__(self, grid: int, tol: float):
+        from oracle import ref
+        self.tol = tol
+        self.b = np.random.default_rng(SEED).standard_normal(grid ** 3)
+        t0 = time.perf_counter()
+        if ref.available(fast=True):
+            self.A = ref.RefCSR.laplacian(grid, grid, grid, fast=True)
+            self.P = ref.RefPrecond(self.A, ref.KIND_IC, True, 1e-3)
+            self.P.setup()
+            self.cores, self.kind = 4, "reference"
+            self._solve = lambda k: ref.cg_solve(self.A, self.P, self.b, tol=tol, maxit=k, flexible=True)[1]
+        else:
+            import prispack_b200 as PB
+            from oracle import oracle as orc
+            A = PB.CSRMatrix.laplacian(grid, grid, grid)
+            F = PB.HostFactor(A, PB.PRECOND_IC, tol=1e-3, precision=PB.PRISM_FP32)
+            rp, ci, v, _ = F.arrays(0)
+            OP = orc.Precond(1, A.n, (rp, ci, v))
+            self.cores, self.kind = 1, "port"
+            self._solve = lambda k: orc.cg(A.rowptr, A.col, A.val, self.b, OP, tol=tol, maxit=k)[1]
+        self.setup_s = time.perf_counter() - t0
+
+    def run(self, k: int):
+        t = time.perf_counter()
+        it = self._solve(k)
+        return time.perf_counter() - t, it
+
+    def sample(self, sample_s: float, full_iters: int | None):
+        """Times a bounded sample of the solve: maxIter = k iterations for a k taking
+        about `sample_s` seconds, scaled to `full_iters` (None: run to convergence)."""
+        t2, _ = self.run(2)
+        per_iter = max(t2 / 2.0, 1e-6)
+        k = 1000 if full_iters is None else int(max(3, min(sample_s / per_iter, full_iters)))
+        tk, itk = self.run(k)
+        per_iter = tk / max(itk - 1, 1)
+        iters = full_iters or itk
+        return {"value": per_iter * iters * 1e3, "unit": "ms", "cores": self.cores, "kind": self.kind,
+                "iters": itk,
+                "sample": f"{itk - 1} FCG iterations ({tk:.1f} s) of the same solve, scaled to {iters} iterations; "
+                          f"host setup {self.setup_s:.1f} s excluded"}
+
+
+# ---------------------------------------------------------------------------
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        return reference_arm(args, rank, world)
+
+    import torch
+    import prispack_b200 as PB
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    g = args.grid
+    A = PB.CSRMatrix.laplacian(g, g, g)
+    n = A.n
+    b_host = np.random.default_rng(SEED).standard_normal(n)
+    t0 = time.perf_counter()
+    F32 = PB.HostFactor(A, PB.PRECOND_IC, tol=1e-3, precision=PB.PRISM_FP32)
+    setup32_s = time.perf_counter() - t0
+    S = PB.DeviceSystem(A, device=local)
+    stream = torch.cuda.current_stream()
+    S.set_stream(stream.cuda_stream)
+    S.attach(F32)
+    b = torch.tensor(b_host, device="cuda")
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def timed_solves(steps, warm):
+        for _ in range(warm):
+            x.zero_()
+            S.solve(b, x, tol=args.tol, max_iter=1000)
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        launches0 = PB.kernel_launch_count()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        stats = []
+        for _ in range(steps):
+            x.zero_()
+            _, st = S.solve(b, x, tol=args.tol, max_iter=1000)
+            stats.append((st.num_iter, st.true_rel_residual, st.converged, st.device_ms))
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1) / steps
+        return ms, stats, PB.kernel_launch_count() - launches0
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms32, stats32, launches = timed_solves(args.steps, args.warmup)
+    clk = clocks.stop()
+    iters = stats32[-1][0]
+
+    # ---- e2e through the host-buffer C-ABI call (H2D b, x0; D2H x inside the timed region)
+    pin_b = torch.from_numpy(b_host).pin_memory()
+    pin_x = torch.zeros(n, dtype=torch.float64).pin_memory()
+    bnp, xnp = pin_b.numpy(), pin_x.numpy()
+    S.solve(bnp, xnp, tol=args.tol, max_iter=1000)  # warm
+    torch.cuda.synchronize()
+    barrier()
+    e2e = []
+    for _ in range(max(1, args.steps)):
+        xnp[:] = 0.0
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        xs, st = S.solve(bnp, xnp, tol=args.tol, max_iter=1000)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e.append(e0.elapsed_time(e1))
+    e2e_ms = statistics.mean(e2e)
+
+    # ---- dominant kernel: one triangular sweep, timed alone with CUDA events
+    info = S.sweep_info(0)
+    vin = torch.randn(n, dtype=torch.float64, device="cuda")
+    vout = torch.empty_like(vin)
+    reps = 10
+    sweep_ms = []
+    for sw in (0, 1):
+        S.sweep_device(sw, vin, vout, True)
+        torch.cuda.synchronize()
+        tot = 0.0
+        for _ in range(reps):
+            S.sweep_device(sw, vin, vout, True)  # marks out pending (fill kernel), then the sweep
+            s0 = torch.cuda.Event(enable_timing=True)
+            s1 = torch.cuda.Event(enable_timing=True)
+            s0.record(stream)
+            S.sweep_device(sw, vin, vout, False)
+            s1.record(stream)
+            torch.cuda.synchronize()
+            tot += s0.elapsed_time(s1)
+        sweep_ms.append(tot / reps)
+    # algorithmic bytes of one sweep launch: per stored entry a column index (4 B) and a
+    # value (4 B FP32); per row its offset (4 B), position->row map (4 B), diagonal (8 B),
+    # right-hand side read (8 B) and result write (8 B)
+    sweep_bytes = info["nnz"] * (4 + info["value_bytes"]) + n * 32 + 4
+    sweep_avg_ms = statistics.mean(sweep_ms)
+    achieved = sweep_bytes / (sweep_avg_ms * 1e-3) / 1e9
+    peak, peak_src = measured_peak_gbs()
+
+    # ---- SpMV alone (the other bandwidth kernel), for reference
+    spmv_ms = []
+    for _ in range(reps):
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        S.spmv(vin)
+        s1.record(stream)
+        torch.cuda.synchronize()
+        spmv_ms.append(s0.elapsed_time(s1))
+    spmv_bytes = 12 * A.nnz + 20 * n + 4
+    spmv_gbs = spmv_bytes / (statistics.median(spmv_ms) * 1e-3) / 1e9
+
+    # ---- FP64-factor solve beside it
+    fp64 = None
+    if not args.no_fp64:
+        t0 = time.perf_counter()
+        F64 = PB.HostFactor(A, PB.PRECOND_IC, tol=1e-3, precision=PB.PRISM_FP64)
+        setup64_s = time.perf_counter() - t0
+        S.attach(F64)
+        ms64, stats64, _ = timed_solves(max(1, args.steps // 2), 1)
+        fp64 = {"ms": ms64, "iters": stats64[-1][0], "true_rel_residual": stats64[-1][1],
+                "mixed_speedup": ms64 / ms32, "host_setup_s": setup64_s}
+        S.attach(F32)
+
+    # ---- max over ranks
+    vals = torch.tensor([ms32, e2e_ms], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(vals, op=dist.ReduceOp.MAX)
+    ms32, e2e_ms = float(vals[0]), float(vals[1])
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = CpuReference(g, args.tol).sample(args.cpu_sample_s, iters)
+            cpu.pop("iters", None)
+        except Exception as e:  # reported, not fatal
+            cpu = {"value": None, "unit": "ms", "cores": 0, "kind": "unavailable", "sample": str(e)[:200]}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC,
+            "value": round(ms32, 4),
+            "unit": "ms",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": round(ms32, 4),
+            "higher_is_better": False,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64 (Krylov) / f32 (factor values)",
+            "data": "synthetic",
+            "config": {"workload": workload(g, args.tol), "n": n, "nnz": A.nnz, "precond_nnz": F32.info()["mnnz"],
+                       "sweep_levels": [S.sweep_info(0)["levels"], S.sweep_info(1)["levels"]],
+                       "iterations": iters, "true_rel_residual": stats32[-1][1],
+                       "converged": bool(stats32[-1][2]), "host_setup_s": round(setup32_s, 2),
+                       "l2": "inputs larger than L2 (A 216 MB + factor > 600 MB per solve)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "spmv_per_iter": 1},
+            "e2e": {"value": round(e2e_ms, 4), "unit": "ms", "h2d_bytes_per_step": 2 * 8 * n,
+                    "d2h_bytes_per_step": 8 * n},
+            "roofline": {"bound": "hbm", "kernel": "k_sweep<float> (lower+upper avg)",
+                         "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "peak_source": peak_src,
+                         "bytes_per_launch": sweep_bytes, "launch_ms": [round(t, 4) for t in sweep_ms],
+                         "traffic": None},
+            "spmv": {"ms": round(statistics.median(spmv_ms), 4), "bytes": spmv_bytes, "GB/s": round(spmv_gbs, 1),
+                     "frac": round(spmv_gbs / peak, 4)},
+            "fp64_factor": fp64,
+            "cpu_baseline": cpu,
+            "gpu_launches": int(launches / max(args.steps, 1)) * args.steps,
+            "clocks": clk,
+        }
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def reference_arm(args, rank, world):
+    """The reference's own CPU solver on the host cores (rank 0 only)."""
+    if rank != 0:
+        return
+    from oracle import ref
+    R = CpuReference(args.grid, args.tol)
+    full = R.sample(0.0, None)          # one full solve: learns the iteration count (untimed warm-up)
+    full_iters = full["iters"]
+    vals, desc = [], full
+    for i in range(max(0, args.warmup - 1) + args.steps):
+        r = R.sample(args.cpu_sample_s, full_iters)
+        if i >= max(0, args.warmup - 1):
+            vals.append(r["value"])
+        desc = r
+    v = statistics.mean(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "ms", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(v, 3), "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64 (Krylov) / f32 (factor values)",
+            "data": "synthetic", "config": {"workload": workload(args.grid, args.tol)},
+            "cpu_baseline": {"value": round(v, 3), "unit": "ms", "cores": desc["cores"], "kind": desc["kind"],
+                             "sample": desc["sample"]},
+            "e2e": {"value": round(v, 3), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if not ref.available(fast=True):
+        line["note"] = "reference build absent on this host: the oracle port was timed"
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,191 @@
+/*
+ * prism_solve.h -- C ABI of the B200 solve phase for PrisPack.
+ *
+ * One handle = one square CSR operator A resident on one CUDA device, an
+ * optional preconditioner M built on the host and uploaded once, and the
+ * device workspace of the Krylov solvers.  Every handle owns one CUDA stream;
+ * a handle is not thread-safe (the reference's preconditioner objects are not
+ * either: they keep per-object scratch vectors).  No C++ exception crosses
+ * this boundary; every entry point returns a prism_status and, on failure,
+ * leaves a message for prism_last_error() (per calling thread).
+ *
+ * Index and value types follow HOST::CSRMatrix<double>
+ * (include/MatrixClass/CSRMatrix.h:19-30 of the reference): uint32 row
+ * offsets and column indices, sorted columns within each row, double values.
+ *
+ * Entry points and the reference interface each one replaces:
+ *   prism_create / prism_destroy      HOST::CSRMatrix<double> ctor/dtor
+ *                                     (include/MatrixClass/CSRMatrix.h:57)
+ *   prism_spmv*                       CSRMatrix::MatPVec
+ *                                     (include/MatrixClass/CSRMatrix.h:360-395)
+ *   prism_set_precond_ic              IncompleteCholesky(A, threshold) + setup()
+ *                                     (source/Preconditioner/IncompleteCholesky.cpp:11-246)
+ *   prism_set_precond_ildlt           IncompleteLDLT(A, tol) + setup()
+ *                                     (source/Preconditioner/IncompleteLDLT.cpp:39-186)
+ *   prism_set_precond_ilut            IncompleteLU(A, lfill, tol) + setup()
+ *                                     (source/Preconditioner/IncompleteLU.cpp:12-266)
+ *   prism_apply*                      BasePrecondition::MInvSolve(vecIN, vecOUT)
+ *                                     (include/Preconditioner/BasePreconditon.h:110-128,
+ *                                      TriangularPrecondition::MInvSolve :307-358)
+ *   prism_solve* (PRISM_SOLVER_FCG,   CG<double>::solve
+ *                 PRISM_SOLVER_CG)    (source/Solver/CG.cpp:34-83)
+ *   prism_solve* (PRISM_SOLVER_FGMRES,GMRES<double>::solve + setRestart
+ *                 PRISM_SOLVER_GMRES) (source/Solver/GMRES.cpp:60-221)
+ *   prism_laplacian_*                 generateLaplacianCSR
+ *                                     (include/MatrixClass/ModelProblem.h:45-52,
+ *                                      source/MatrixClass/ModelProblem.cpp:68-133)
+ */
+#ifndef PRISM_SOLVE_H
+#define PRISM_SOLVE_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum prism_status {
+    PRISM_OK = 0,
+    PRISM_ERR_ARG = 1,            /* bad argument, size or pointer */
+    PRISM_ERR_CUDA = 2,           /* a CUDA runtime call failed */
+    PRISM_ERR_ZERO_PIVOT = 3,     /* ILUT/ILDLT |pivot| < 1e-15 (reference throws) */
+    PRISM_ERR_NOT_SPD = 4,        /* IC met a non-positive pivot (reference prints and returns) */
+    PRISM_ERR_NOT_READY = 5,      /* apply/solve before a preconditioner was set up */
+    PRISM_ERR_TIMEOUT = 6,        /* a bounded device-side wait ran out (SpTRSV row flags) */
+    PRISM_ERR_NONFINITE = 7,      /* NaN/Inf met in a Krylov scalar */
+    PRISM_ERR_ALLOC = 8,          /* host or device allocation failed */
+    PRISM_ERR_UNSUPPORTED = 9,    /* option not available for this preconditioner/solver */
+    PRISM_ERR_BAD_MATRIX = 10     /* CSR structure invalid (row offsets, column range, order) */
+} prism_status;
+
+typedef enum prism_precision {
+    PRISM_FP64 = 0,               /* factor values stored in double (<double,double> instantiation) */
+    PRISM_FP32 = 1                /* factor values stored in float  (<float,double> instantiation) */
+} prism_precision;
+
+typedef enum prism_precond_kind {
+    PRISM_PRECOND_NONE = 0,
+    PRISM_PRECOND_IC = 1,         /* PreconditionIC    (BasePreconditon.h:12-19) */
+    PRISM_PRECOND_ILUT = 2,       /* PreconditionILUT  */
+    PRISM_PRECOND_ILDLT = 3,      /* PreconditionILDLT */
+    PRISM_PRECOND_GMSLR = 4,      /* PreconditionGMSLR */
+    PRISM_PRECOND_AMSED = 5       /* PreconditionAMSED */
+} prism_precond_kind;
+
+typedef enum prism_solver_kind {
+    PRISM_SOLVER_FCG = 0,         /* CG with CGType FlexibleCG (CG.h:14-18) */
+    PRISM_SOLVER_CG = 1,          /* CG with CGType NormalCG: M^{-1} only at step 0 (CG.cpp:48,65) */
+    PRISM_SOLVER_FGMRES = 2,      /* GMRES with FlexibleGMRES */
+    PRISM_SOLVER_GMRES = 3        /* GMRES with NormalGMRES (no preconditioner applied, GMRES.cpp:164) */
+} prism_solver_kind;
+
+typedef struct prism_solve_opts {
+    int32_t solver;               /* prism_solver_kind */
+    double tol;                   /* relative residual tolerance (CG.cpp:59, GMRES.cpp:194) */
+    uint32_t max_iter;            /* CG: maxIter (CG.cpp:57); GMRES: 500 as MAX_ITER_NUM_SOLVER (config.h:25) */
+    uint32_t restart;             /* GMRES restart m; 0 = no restart (setRestart(false, .)) */
+} prism_solve_opts;
+
+typedef struct prism_solve_stats {
+    int32_t num_iter;             /* getNumIter(): CG m+1 (CG.cpp:81); GMRES k*m+m_final (GMRES.cpp:218) */
+    int32_t converged;            /* getConvergence() */
+    double final_error;           /* getError(): recursive residual (CG) / Givens estimate (GMRES) */
+    double true_rel_residual;     /* ||b - A x||_2 / ||b||_2 recomputed in FP64 at exit */
+    uint32_t precond_applies;     /* number of M^{-1} applications performed */
+    uint32_t spmv_count;          /* number of A x products performed */
+    double device_ms;             /* device time of the solve (CUDA events on the handle's stream) */
+} prism_solve_stats;
+
+typedef struct prism_handle_s* prism_handle;
+
+/* ---- diagnostics ------------------------------------------------------- */
+const char* prism_last_error(void);
+int32_t prism_version(void);
+/* number of kernel launches issued by this library in this process (all handles) */
+uint64_t prism_kernel_launch_count(void);
+
+/* ---- model problems (host) --------------------------------------------- */
+/* sizes of generateLaplacianCSR(nx,ny,nz,...): n = nx*ny*nz, nnz exact */
+int32_t prism_laplacian_dims(int32_t nx, int32_t ny, int32_t nz, uint32_t* n, uint32_t* nnz);
+/* fills caller buffers (rowptr[n+1], col[nnz], val[nnz]) exactly as
+ * generateLaplacianCOO + transCOO2CSR (ModelProblem.cpp:68-133, MatrixTools.h:16-62) */
+int32_t prism_laplacian_fill(int32_t nx, int32_t ny, int32_t nz, double alphax, double alphay,
+                             double alphaz, double shift, uint32_t* rowptr, uint32_t* col, double* val);
+
+/* ---- operator ------------------------------------------------------------ */
+/* Copies the host CSR to device `device`.  The structure is validated
+ * (monotone offsets, columns < n, strictly increasing within a row). */
+int32_t prism_create(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val,
+                     int32_t device, prism_handle* out);
+int32_t prism_destroy(prism_handle h);
+/* Makes the handle issue its work on `stream` (a cudaStream_t) instead of its own stream. */
+int32_t prism_set_stream(prism_handle h, void* stream);
+int32_t prism_dims(prism_handle h, uint32_t* n, uint64_t* nnz);
+
+/* y = A x on device pointers / host pointers */
+int32_t prism_spmv_device(prism_handle h, const double* x_d, double* y_d);
+int32_t prism_spmv(prism_handle h, const double* x, double* y);
+
+/* ---- preconditioners (host setup, bit-exact with the reference; then uploaded) -- */
+int32_t prism_set_precond_none(prism_handle h);
+int32_t prism_set_precond_ic(prism_handle h, double threshold, int32_t precision);
+int32_t prism_set_precond_ildlt(prism_handle h, double tol, int32_t precision);
+int32_t prism_set_precond_ilut(prism_handle h, uint32_t lfill, double tol, int32_t precision);
+/* getPreconditionNonZeroCount() (BasePreconditon.h:134-136) */
+int32_t prism_precond_nnz(prism_handle h, uint64_t* mnnz);
+int32_t prism_precond_type(prism_handle h, int32_t* kind);
+
+/* Factor export for parity checks.  which = 0: first stored triangle
+ * (IC/ILDLT: L^T by rows; ILUT: L), which = 1: second (ILUT: U).
+ * diag receives ILDLT D / ILUT Dinv (may be NULL).  Pass NULL arrays to
+ * query sizes only. */
+int32_t prism_precond_factor(prism_handle h, int32_t which, uint32_t* n, uint64_t* nnz,
+                             uint32_t* rowptr, uint32_t* col, double* val, double* diag);
+/* Dependency depth of each triangular sweep (number of wavefronts of the
+ * exact integer level schedule): sweep 0 = lower, 1 = upper. */
+int32_t prism_precond_levels(prism_handle h, int32_t sweep, uint32_t* num_levels);
+
+/* ---- host-only factors ----------------------------------------------------------
+ * The same incomplete factorisations without a device: for callers that
+ * build once and attach to several handles, and for host-side parity checks.
+ * kind: PRISM_PRECOND_IC (tol = threshold), PRISM_PRECOND_ILUT (lfill, tol),
+ * PRISM_PRECOND_ILDLT (tol). */
+typedef struct prism_factor_s* prism_factor;
+int32_t prism_factor_create(int32_t kind, uint32_t n, const uint32_t* rowptr, const uint32_t* col,
+                            const double* val, double tol, uint32_t lfill, int32_t precision,
+                            prism_factor* out);
+int32_t prism_factor_destroy(prism_factor f);
+/* same layout as prism_precond_factor */
+int32_t prism_factor_get(prism_factor f, int32_t which, uint32_t* n, uint64_t* nnz, uint32_t* rowptr,
+                         uint32_t* col, double* val, double* diag);
+/* getPreconditionNonZeroCount() and the wavefront counts of the two sweeps */
+int32_t prism_factor_info(prism_factor f, uint64_t* mnnz, uint32_t* lower_levels, uint32_t* upper_levels);
+/* attaches a host factor (built for a matrix of the same size) to a handle */
+int32_t prism_set_precond_factor(prism_handle h, prism_factor f);
+
+/* out = M^{-1} in (in == out allowed) */
+int32_t prism_apply_device(prism_handle h, const double* in_d, double* out_d);
+int32_t prism_apply(prism_handle h, const double* in, double* out);
+
+/* One triangular sweep alone (sweep 0 = lower, 1 = upper), on device vectors.
+ * `prepare` != 0 first marks out_d pending (the sweep's readiness encoding);
+ * pass 0 only when the caller did that already.  For timing the sweep kernel
+ * by itself; the preconditioner apply is prism_apply_device.  Also reports the
+ * sweep's stored non-zeros and the bytes its value array takes per entry. */
+int32_t prism_precond_sweep_device(prism_handle h, int32_t sweep, const double* in_d, double* out_d,
+                                   int32_t prepare);
+int32_t prism_precond_sweep_info(prism_handle h, int32_t sweep, uint32_t* n, uint64_t* nnz,
+                                 uint32_t* value_bytes, uint32_t* num_levels);
+
+/* ---- solvers ------------------------------------------------------------- */
+/* x is the in/out initial guess, as BaseSolver::solve (BaseSolver.h:16). */
+int32_t prism_solve_device(prism_handle h, const prism_solve_opts* opts, const double* b_d, double* x_d,
+                           prism_solve_stats* stats);
+int32_t prism_solve(prism_handle h, const prism_solve_opts* opts, const double* b, double* x,
+                    prism_solve_stats* stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PRISM_SOLVE_H */

@@ -1,0 +1,276 @@
+/*
+ * CPU oracle of the PrisPack solve phase -- TEST INFRASTRUCTURE ONLY.
+ * Parity is pinned against the reference's compiled sources (oracle/_ref) and
+ * the golden vectors in tests/golden/.  Never linked into the product.
+ *
+ * Every routine restates one reference routine, in the same operation order,
+ * serially (the reference's OpenMP reductions are order-nondeterministic; the
+ * serial order is its single-thread behaviour).
+ */
+#include "oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* generateLaplacianCOO (source/MatrixClass/ModelProblem.cpp:68-133) followed by
+ * transCOO2CSR's per-row insertion sort (include/MatrixClass/MatrixTools.h:16-62). */
+void orc_laplacian(int nx, int ny, int nz, double ax, double ay, double az, double shift,
+                   uint32_t* rowptr, uint32_t* col, double* val) {
+    int numones = (nx == 1) + (ny == 1) + (nz == 1);
+    double v = -1.0;
+    double vxp = v - ax, vxn = v + ax, vyp = v - ay, vyn = v + ay, vzp = v - az, vzn = v + az;
+    double vd = numones > 0 ? 4.0 : 6.0;
+    vd -= shift;
+    long n = (long)nx * ny * nz, pos = 0;
+    rowptr[0] = 0;
+    for (long ii = 0; ii < n; ii++) {
+        long k = ii / ((long)nx * ny);
+        long i = (ii - k * nx * ny) / nx;
+        long j = ii - k * nx * ny - i * nx;
+        long c[7];
+        double w[7];
+        int m = 0;
+        if (k > 0) { c[m] = ii - (long)nx * ny; w[m++] = vzn; }
+        if (k < nz - 1) { c[m] = ii + (long)nx * ny; w[m++] = vzp; }
+        if (i > 0) { c[m] = ii - nx; w[m++] = vyn; }
+        if (i < ny - 1) { c[m] = ii + nx; w[m++] = vyp; }
+        if (j > 0) { c[m] = ii - 1; w[m++] = vxn; }
+        if (j < nx - 1) { c[m] = ii + 1; w[m++] = vxp; }
+        c[m] = ii; w[m++] = vd;
+        /* sortVectorPair: insertion sort by column (include/VectorClass/VectorTools.h:39-57) */
+        for (int a = 1; a < m; a++) {
+            long key = c[a]; double kv = w[a]; int b = a - 1;
+            while (b >= 0 && c[b] > key) { c[b + 1] = c[b]; w[b + 1] = w[b]; b--; }
+            c[b + 1] = key; w[b + 1] = kv;
+        }
+        for (int a = 0; a < m; a++) { col[pos] = (uint32_t)c[a]; val[pos] = w[a]; pos++; }
+        rowptr[ii + 1] = (uint32_t)pos;
+    }
+}
+
+/* CSRMatrix::MatPVecWithRawPtr (include/MatrixClass/CSRMatrix.h:360-377) */
+void orc_spmv(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val,
+              const double* x, double* y) {
+    for (uint32_t i = 0; i < n; i++) {
+        double s = 0;
+        for (uint32_t j = rowptr[i]; j < rowptr[i + 1]; j++) s += x[col[j]] * val[j];
+        y[i] = s;
+    }
+}
+
+/* TriangularPrecondition::MInvSolve (include/Preconditioner/BasePreconditon.h:307-315):
+ * lower, (ILDLT: diagonal), upper -- in place. */
+void orc_precond_apply(const orc_precond* P, double* vec) {
+    const uint32_t n = P->n;
+    if (P->kind == 1) {
+        /* IncompleteCholesky::MSolveLowerUsePtr (IncompleteCholesky.cpp:249-271): column scatter */
+        for (uint32_t i = 0; i < n; i++) {
+            uint32_t k = P->rp0[i];
+            double t = vec[i] / P->v0[k];
+            vec[i] = t;
+            for (k = P->rp0[i] + 1; k < P->rp0[i + 1]; k++) vec[P->ci0[k]] -= P->v0[k] * t;
+        }
+        /* MSolveUpperUsePtr (IncompleteCholesky.cpp:274-295): row gather */
+        for (uint32_t i = n; i-- > 0;) {
+            double t = vec[i];
+            for (uint32_t k = P->rp0[i] + 1; k < P->rp0[i + 1]; k++) t -= P->v0[k] * vec[P->ci0[k]];
+            vec[i] = t / P->v0[P->rp0[i]];
+        }
+    } else if (P->kind == 3) {
+        /* IncompleteLDLT lower (IncompleteLDLT.cpp:216-233), diagonal (:206-214), upper (:188-204) */
+        for (uint32_t i = 0; i < n; i++)
+            for (uint32_t k = P->rp0[i]; k < P->rp0[i + 1]; k++) vec[P->ci0[k]] -= P->v0[k] * vec[i];
+        for (uint32_t i = 0; i < n; i++) vec[i] /= P->diag[i];
+        for (uint32_t i = n; i-- > 0;)
+            for (uint32_t k = P->rp0[i]; k < P->rp0[i + 1]; k++) vec[i] -= P->v0[k] * vec[P->ci0[k]];
+    } else if (P->kind == 2) {
+        /* IncompleteLU lower (IncompleteLU.cpp:284-297), upper (:268-282) */
+        for (uint32_t i = 0; i < n; i++)
+            for (uint32_t k = P->rp0[i]; k < P->rp0[i + 1]; k++) vec[i] -= P->v0[k] * vec[P->ci0[k]];
+        for (uint32_t i = n; i > 0; i--) {
+            for (uint32_t k = P->rp1[i - 1]; k < P->rp1[i]; k++) vec[i - 1] -= P->v1[k] * vec[P->ci1[k]];
+            vec[i - 1] *= P->diag[i - 1];
+        }
+    }
+}
+
+static double dot(uint32_t n, const double* a, const double* b) {
+    double s = 0.0; /* BaseVector::innerProduct serial branch (BaseVector.h:429-448) */
+    for (uint32_t i = 0; i < n; i++) s += a[i] * b[i];
+    return s;
+}
+
+/* CG<double>::solve (source/Solver/CG.cpp:34-83), including the second
+ * v = A d at the top of every iteration. */
+void orc_cg(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val,
+            const orc_precond* P, int flexible, double tol, uint32_t max_iter,
+            const double* b, double* x, int32_t* num_iter, double* final_error, int32_t* converged) {
+    double* r = calloc(n, sizeof(double));
+    double* v = calloc(n, sizeof(double));
+    double* w = calloc(n, sizeof(double));
+    double* d = calloc(n, sizeof(double));
+    int has_p = P && P->kind != 0;
+    *converged = 0;
+    uint32_t m = max_iter;
+    double norm_b = sqrt(dot(n, b, b)), norm = -1.0, v1, v2;
+    orc_spmv(n, rowptr, col, val, x, r);
+    for (uint32_t i = 0; i < n; i++) w[i] = 1 * b[i] + -1 * r[i];
+    memcpy(r, w, n * sizeof(double));
+    if (has_p) orc_precond_apply(P, w);
+    memcpy(d, w, n * sizeof(double));
+    orc_spmv(n, rowptr, col, val, d, v);
+    v1 = dot(n, d, r);
+    v2 = dot(n, d, v);
+    v1 /= v2;
+    for (uint32_t i = 0; i < n; i++) x[i] = 1 * x[i] + v1 * d[i];
+    for (uint32_t i = 0; i < n; i++) r[i] = 1 * r[i] + -v1 * v[i];
+    for (uint32_t it = 1; it < max_iter; it++) {
+        norm = sqrt(dot(n, r, r)) / norm_b;
+        if (norm < tol) { *converged = 1; m = it; break; }
+        memcpy(w, r, n * sizeof(double));
+        if (flexible && has_p) orc_precond_apply(P, w);
+        orc_spmv(n, rowptr, col, val, d, v);
+        v1 = dot(n, w, v);
+        v2 = dot(n, d, v);
+        v1 = v1 / v2;
+        for (uint32_t i = 0; i < n; i++) d[i] = 1 * w[i] + -v1 * d[i];
+        v1 = dot(n, d, r);
+        orc_spmv(n, rowptr, col, val, d, v);
+        v2 = dot(n, d, v);
+        v1 = v1 / v2;
+        for (uint32_t i = 0; i < n; i++) x[i] = 1 * x[i] + v1 * d[i];
+        for (uint32_t i = 0; i < n; i++) r[i] = 1 * r[i] + -v1 * v[i];
+    }
+    *num_iter = (int32_t)(m + 1);
+    *final_error = norm;
+    free(r); free(v); free(w); free(d);
+}
+
+/* Kahan-compensated Σ x² as BaseVector::sumKahan(start, len, func) (BaseVector.h:635-648) */
+static double sum_sq_kahan(uint32_t n, const double* x) {
+    double s = 0.0, c = 0.0, t, ns;
+    for (uint32_t i = 0; i < n; i++) {
+        t = x[i] * x[i] + c;
+        ns = s + t;
+        c = t - (ns - s);
+        s = ns;
+    }
+    return s + c;
+}
+
+/* GMRES<double>::givensTransform (source/Solver/GMRES.cpp:73-101); H column-major (m+1) x m */
+static void givens(double* H, uint32_t ld, double* c, double* s, double* ksi, uint32_t j) {
+    double val0, val1, val2, tao;
+    for (uint32_t i = 0; i < j; i++) {
+        val1 = H[i + j * ld];
+        val2 = H[i + 1 + j * ld];
+        val0 = c[i] * val2 - s[i] * val1;
+        H[i + 1 + j * ld] = val0;
+        val0 = c[i] * val1 + s[i] * val2;
+        H[i + j * ld] = val0;
+    }
+    val1 = H[j + j * ld];
+    val2 = H[j + 1 + j * ld];
+    if (fabs(val1) > fabs(val2)) {
+        tao = val2 / val1;
+        c[j] = 1 / sqrt(fabs(1.0 + tao * tao));
+        s[j] = c[j] * tao;
+    } else {
+        tao = val1 / val2;
+        s[j] = 1 / sqrt(fabs(1.0 + tao * tao));
+        c[j] = s[j] * tao;
+    }
+    H[j + j * ld] = c[j] * val1 + s[j] * val2;
+    H[j + 1 + j * ld] = 0.0;
+    ksi[j + 1] = -s[j] * ksi[j];
+    ksi[j] = c[j] * ksi[j];
+}
+
+/* GMRES<double>::solve (source/Solver/GMRES.cpp:122-221) with setRestart
+ * (GMRES.cpp:60-70) when restart > 0; MAX_ITER_NUM_SOLVER = 500 (config/config.h:25). */
+void orc_gmres(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val,
+               const orc_precond* P, int flexible, uint32_t restart, double tol,
+               const double* b, double* x, int32_t* num_iter, double* final_error, int32_t* converged) {
+    int32_t max_iter = 500;
+    uint32_t mm = n;
+    if (restart > 0) {
+        mm = restart;
+        max_iter = max_iter / (int32_t)restart;
+        if (restart >= n) mm = n - 1;
+    } else {
+        mm = n - 1;
+    }
+    uint32_t m = mm;
+    double beta, val0, rnorm = 0.0, rel = 0.0;
+    double bnorm = sqrt(sum_sq_kahan(n, b));
+    double* vj = calloc(n, sizeof(double));
+    double* wj = calloc(n, sizeof(double));
+    double* r = calloc(n, sizeof(double));
+    double* ksi = calloc(mm + 1, sizeof(double));
+    double* s = calloc(mm + 1, sizeof(double));
+    double* c = calloc(mm + 1, sizeof(double));
+    double* V = calloc((size_t)n * (mm + 1), sizeof(double));
+    double* H = calloc((size_t)(mm + 1) * mm, sizeof(double));
+    double* Z = flexible ? calloc((size_t)n * (mm + 1), sizeof(double)) : NULL;
+    const uint32_t ld = mm + 1;
+    *converged = 0;
+    orc_spmv(n, rowptr, col, val, x, r);
+    for (uint32_t i = 0; i < n; i++) vj[i] = 1 * b[i] + -1 * r[i];
+    beta = sqrt(sum_sq_kahan(n, vj));
+    int32_t k = -1;
+    while (!*converged && k < max_iter) {
+        ++k;
+        for (uint32_t i = 0; i < n; i++) vj[i] *= 1 / beta;
+        memcpy(V, vj, n * sizeof(double));
+        for (uint32_t i = 0; i < mm; i++) ksi[i] = 0;
+        ksi[0] = beta;
+        for (uint32_t j = 0; j < m; j++) {
+            if (flexible) {
+                if (P && P->kind) orc_precond_apply(P, vj);
+                memcpy(Z + (size_t)j * n, vj, n * sizeof(double));
+            }
+            orc_spmv(n, rowptr, col, val, vj, wj);
+            for (uint32_t i = 0; i < j + 1; i++) {
+                memcpy(vj, V + (size_t)i * n, n * sizeof(double));
+                val0 = dot(n, wj, vj);
+                H[i + j * ld] = val0;
+                for (uint32_t q = 0; q < n; q++) vj[q] *= val0;
+                for (uint32_t q = 0; q < n; q++) wj[q] = wj[q] + -1 * vj[q];
+            }
+            val0 = sqrt(sum_sq_kahan(n, wj));
+            H[j + 1 + j * ld] = val0;
+            if (fabs(val0) == 0) { m = j; break; }
+            memcpy(vj, wj, n * sizeof(double));
+            for (uint32_t q = 0; q < n; q++) vj[q] *= 1 / val0;
+            memcpy(V + (size_t)(j + 1) * n, vj, n * sizeof(double));
+            givens(H, ld, c, s, ksi, j);
+            rnorm = fabs(ksi[j + 1]);
+            rel = rnorm / bnorm;
+            if (rel < tol) { m = j; break; }
+        }
+        /* retrospectiveSolver (GMRES.cpp:103-119) */
+        for (int i = (int)m - 1; i >= 0; --i) {
+            for (int jj = i + 1; jj < (int)m; ++jj) ksi[i] = ksi[i] - H[i + jj * ld] * ksi[jj];
+            ksi[i] = ksi[i] / H[i + i * ld];
+        }
+        ksi[m] = 0;
+        ksi[m] = 0;
+        /* x += Z ksi (flexible) or V ksi: DenseMatrix::MatVec over m+1 columns (DenseMatrix.cpp:208-243) */
+        const double* B = flexible ? Z : V;
+        for (uint32_t q = 0; q < n; q++) wj[q] = 0;
+        for (uint32_t jj = 0; jj < mm + 1; jj++) {
+            double kj = ksi[jj];
+            for (uint32_t q = 0; q < n; q++) wj[q] += B[(size_t)jj * n + q] * kj;
+        }
+        for (uint32_t q = 0; q < n; q++) x[q] = x[q] + 1 * wj[q];
+        *converged = rel < tol;
+        orc_spmv(n, rowptr, col, val, x, r);
+        for (uint32_t i = 0; i < n; i++) vj[i] = 1 * b[i] + -1 * r[i];
+        beta = rnorm;
+    }
+    *final_error = rel;
+    *num_iter = k * (int32_t)mm + (int32_t)m;
+    free(vj); free(wj); free(r); free(ksi); free(s); free(c); free(V); free(H);
+    if (Z) free(Z);
+}

@@ -1,0 +1,40 @@
+/*
+ * CPU oracle of the PrisPack solve phase -- TEST INFRASTRUCTURE ONLY.
+ *
+ * A plain-C restatement of the reference's solve-phase algorithms, used by
+ * tests/, __graft_entry__.smoke() and the cpu_baseline leg of bench.py as the
+ * checker.  The product library never links, loads or calls it.
+ *
+ * Pinning: the restatement is checked against the reference's own compiled
+ * sources (oracle/_ref, built by oracle/Makefile) and against golden vectors
+ * generated from them (tests/golden/, tests/golden/make_golden.py).
+ */
+#ifndef PRISM_ORACLE_H
+#define PRISM_ORACLE_H
+#include <stdint.h>
+
+/* preconditioner described by its stored factor arrays (values widened to double) */
+typedef struct orc_precond {
+    int kind;                 /* 0 none, 1 IC, 2 ILUT, 3 ILDLT */
+    uint32_t n;
+    const uint32_t* rp0;      /* IC/ILDLT: L^T rows; ILUT: L rows */
+    const uint32_t* ci0;
+    const double* v0;
+    const uint32_t* rp1;      /* ILUT: U rows */
+    const uint32_t* ci1;
+    const double* v1;
+    const double* diag;       /* ILDLT: D; ILUT: Dinv */
+} orc_precond;
+
+void orc_laplacian(int nx, int ny, int nz, double ax, double ay, double az, double shift,
+                   uint32_t* rowptr, uint32_t* col, double* val);
+void orc_spmv(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val,
+              const double* x, double* y);
+void orc_precond_apply(const orc_precond* P, double* vec);
+void orc_cg(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val,
+            const orc_precond* P, int flexible, double tol, uint32_t max_iter,
+            const double* b, double* x, int32_t* num_iter, double* final_error, int32_t* converged);
+void orc_gmres(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val,
+               const orc_precond* P, int flexible, uint32_t restart, double tol,
+               const double* b, double* x, int32_t* num_iter, double* final_error, int32_t* converged);
+#endif

@@ -1,0 +1,114 @@
+"""ctypes binding of the C oracle (oracle.c) -- TEST INFRASTRUCTURE ONLY.
+
+Imported by tests/, __graft_entry__.smoke() and the cpu_baseline leg of
+bench.py as the checker; the product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+_u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+
+
+class _Precond(C.Structure):
+    _fields_ = [("kind", C.c_int), ("n", C.c_uint32),
+                ("rp0", C.c_void_p), ("ci0", C.c_void_p), ("v0", C.c_void_p),
+                ("rp1", C.c_void_p), ("ci1", C.c_void_p), ("v1", C.c_void_p),
+                ("diag", C.c_void_p)]
+
+
+def build() -> str:
+    path = os.path.join(_HERE, "liboracle.so")
+    src = [os.path.join(_HERE, f) for f in ("oracle.c", "oracle.h")]
+    if not os.path.exists(path) or any(os.path.getmtime(s) > os.path.getmtime(path) for s in src):
+        subprocess.run(["/usr/bin/gcc", "-std=c11", "-O2", "-ffp-contract=off", "-fPIC", "-shared",
+                        "-o", path, os.path.join(_HERE, "oracle.c"), "-lm"], check=True)
+    return path
+
+
+def lib() -> C.CDLL:
+    global _LIB
+    if _LIB is None:
+        _LIB = C.CDLL(build())
+        _LIB.orc_laplacian.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                       C.c_double, _u32p, _u32p, _f64p]
+        _LIB.orc_spmv.argtypes = [C.c_uint32, _u32p, _u32p, _f64p, _f64p, _f64p]
+        _LIB.orc_precond_apply.argtypes = [C.POINTER(_Precond), _f64p]
+        _LIB.orc_cg.argtypes = [C.c_uint32, _u32p, _u32p, _f64p, C.POINTER(_Precond), C.c_int, C.c_double,
+                                C.c_uint32, _f64p, _f64p, C.POINTER(C.c_int32), C.POINTER(C.c_double),
+                                C.POINTER(C.c_int32)]
+        _LIB.orc_gmres.argtypes = [C.c_uint32, _u32p, _u32p, _f64p, C.POINTER(_Precond), C.c_int, C.c_uint32,
+                                   C.c_double, _f64p, _f64p, C.POINTER(C.c_int32), C.POINTER(C.c_double),
+                                   C.POINTER(C.c_int32)]
+    return _LIB
+
+
+def laplacian(nx, ny, nz, ax=0.0, ay=0.0, az=0.0, shift=0.0):
+    n = nx * ny * nz
+    cap = 7 * n
+    rp = np.zeros(n + 1, np.uint32)
+    ci = np.zeros(cap, np.uint32)
+    v = np.zeros(cap, np.float64)
+    lib().orc_laplacian(nx, ny, nz, ax, ay, az, shift, rp, ci, v)
+    nnz = int(rp[-1])
+    return rp, ci[:nnz].copy(), v[:nnz].copy()
+
+
+def spmv(rp, ci, v, x):
+    y = np.zeros(len(rp) - 1)
+    lib().orc_spmv(len(rp) - 1, rp, ci, v, np.ascontiguousarray(x, np.float64), y)
+    return y
+
+
+class Precond:
+    """Factor arrays in the reference's stored layout (kind 1 IC, 2 ILUT, 3 ILDLT)."""
+
+    def __init__(self, kind, n, f0=None, f1=None, diag=None):
+        self.keep = []
+        s = _Precond()
+        s.kind = kind
+        s.n = n
+
+        def ptr(a, dt):
+            if a is None:
+                return None
+            a = np.ascontiguousarray(a, dt)
+            self.keep.append(a)
+            return a.ctypes.data
+
+        if f0 is not None:
+            s.rp0, s.ci0, s.v0 = ptr(f0[0], np.uint32), ptr(f0[1], np.uint32), ptr(f0[2], np.float64)
+        if f1 is not None:
+            s.rp1, s.ci1, s.v1 = ptr(f1[0], np.uint32), ptr(f1[1], np.uint32), ptr(f1[2], np.float64)
+        s.diag = ptr(diag, np.float64)
+        self.s = s
+
+    def apply(self, vec):
+        out = np.array(vec, np.float64, copy=True)
+        lib().orc_precond_apply(C.byref(self.s), out)
+        return out
+
+
+def cg(rp, ci, v, b, P=None, x0=None, tol=1e-8, maxit=1000, flexible=True):
+    n = len(rp) - 1
+    x = np.zeros(n) if x0 is None else np.array(x0, np.float64, copy=True)
+    it, err, conv = C.c_int32(), C.c_double(), C.c_int32()
+    lib().orc_cg(n, rp, ci, v, C.byref(P.s) if P else None, int(flexible), tol, maxit,
+                 np.ascontiguousarray(b, np.float64), x, C.byref(it), C.byref(err), C.byref(conv))
+    return x, it.value, err.value, bool(conv.value)
+
+
+def gmres(rp, ci, v, b, P=None, x0=None, tol=1e-8, restart=50, flexible=True):
+    n = len(rp) - 1
+    x = np.zeros(n) if x0 is None else np.array(x0, np.float64, copy=True)
+    it, err, conv = C.c_int32(), C.c_double(), C.c_int32()
+    lib().orc_gmres(n, rp, ci, v, C.byref(P.s) if P else None, int(flexible), restart, tol,
+                    np.ascontiguousarray(b, np.float64), x, C.byref(it), C.byref(err), C.byref(conv))
+    return x, it.value, err.value, bool(conv.value)

@@ -1,0 +1,172 @@
+"""ctypes view of the reference's own CPU classes, compiled from its sources.
+
+Test infrastructure only: the parity tests, the golden-fixture generator and
+the CPU-baseline arm of bench.py load this; the product never does.
+
+``oracle/Makefile`` (target ``ref``) compiles PrisPack's CSRMatrix, COOMatrix,
+ModelProblem, IncompleteCholesky, IncompleteLDLT, IncompleteLU, CG and GMRES
+sources together with ``ref_shim/ref_capi.cpp`` into
+
+* ``_ref/libprism_ref.so``       -- parity build (no fast-math, no FMA contraction)
+* ``_ref/libprism_ref_fast.so``  -- the reference's Release flags (timing only)
+
+Both are absent where the reference sources were never available; callers
+check :func:`available` first.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIBS: dict[str, C.CDLL] = {}
+
+_u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+
+KIND_IC, KIND_ILUT, KIND_ILDLT = 1, 2, 3
+
+
+def lib_path(fast: bool = False) -> str:
+    return os.path.join(_HERE, "_ref", "libprism_ref_fast.so" if fast else "libprism_ref.so")
+
+
+def available(fast: bool = False) -> bool:
+    return os.path.exists(lib_path(fast))
+
+
+def load(fast: bool = False) -> C.CDLL:
+    key = "fast" if fast else "parity"
+    if key in _LIBS:
+        return _LIBS[key]
+    lib = C.CDLL(lib_path(fast))
+    vp = C.c_void_p
+    lib.ref_csr_laplacian.restype = vp
+    lib.ref_csr_laplacian.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double]
+    lib.ref_csr_poisson.restype = vp
+    lib.ref_csr_poisson.argtypes = [C.c_uint]
+    lib.ref_csr_from_arrays.restype = vp
+    lib.ref_csr_from_arrays.argtypes = [C.c_uint, _u32p, _u32p, _f64p]
+    lib.ref_csr_dims.argtypes = [vp, C.POINTER(C.c_uint), C.POINTER(C.c_uint)]
+    lib.ref_csr_copy.argtypes = [vp, _u32p, _u32p, _f64p]
+    lib.ref_csr_free.argtypes = [vp]
+    lib.ref_spmv.argtypes = [vp, _f64p, _f64p]
+    lib.ref_precond_create.restype = vp
+    lib.ref_precond_create.argtypes = [vp, C.c_int, C.c_int, C.c_double, C.c_int]
+    lib.ref_precond_setup.argtypes = [vp]
+    lib.ref_precond_free.argtypes = [vp]
+    lib.ref_precond_mnnz.restype = C.c_uint
+    lib.ref_precond_mnnz.argtypes = [vp]
+    lib.ref_precond_factor_dims.argtypes = [vp, C.c_int, C.POINTER(C.c_uint), C.POINTER(C.c_uint)]
+    lib.ref_precond_factor_copy.argtypes = [vp, C.c_int, _u32p, _u32p, _f64p, C.c_void_p]
+    lib.ref_precond_apply.argtypes = [vp, C.c_uint, _f64p]
+    lib.ref_cg_solve.argtypes = [vp, vp, C.c_int, C.c_double, C.c_uint, _f64p, _f64p,
+                                 C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_int)]
+    lib.ref_gmres_solve.argtypes = [vp, vp, C.c_int, C.c_uint, C.c_double, _f64p, _f64p,
+                                    C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_int)]
+    lib.ref_omp_max_threads.restype = C.c_int
+    _LIBS[key] = lib
+    return lib
+
+
+class RefCSR:
+    """HOST::CSRMatrix<double> owned through the shim."""
+
+    def __init__(self, handle: int, lib: C.CDLL):
+        self.h = handle
+        self.lib = lib
+
+    @classmethod
+    def laplacian(cls, nx, ny, nz, ax=0.0, ay=0.0, az=0.0, shift=0.0, fast=False):
+        lib = load(fast)
+        return cls(lib.ref_csr_laplacian(nx, ny, nz, ax, ay, az, shift), lib)
+
+    @classmethod
+    def from_arrays(cls, rowptr, col, val, fast=False):
+        lib = load(fast)
+        n = len(rowptr) - 1
+        return cls(lib.ref_csr_from_arrays(n, np.ascontiguousarray(rowptr, np.uint32),
+                                           np.ascontiguousarray(col, np.uint32),
+                                           np.ascontiguousarray(val, np.float64)), lib)
+
+    def dims(self):
+        n, nnz = C.c_uint(), C.c_uint()
+        self.lib.ref_csr_dims(self.h, C.byref(n), C.byref(nnz))
+        return n.value, nnz.value
+
+    def arrays(self):
+        n, nnz = self.dims()
+        rp = np.zeros(n + 1, np.uint32)
+        ci = np.zeros(nnz, np.uint32)
+        v = np.zeros(nnz, np.float64)
+        self.lib.ref_csr_copy(self.h, rp, ci, v)
+        return rp, ci, v
+
+    def spmv(self, x):
+        n, _ = self.dims()
+        y = np.zeros(n, np.float64)
+        self.lib.ref_spmv(self.h, np.ascontiguousarray(x, np.float64), y)
+        return y
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.ref_csr_free(self.h)
+            self.h = None
+
+
+class RefPrecond:
+    """IncompleteCholesky / IncompleteLU / IncompleteLDLT<low, double> through the shim."""
+
+    def __init__(self, A: RefCSR, kind: int, low_precision: bool, tol: float, lfill: int = 0):
+        self.A = A
+        self.lib = A.lib
+        self.kind = kind
+        self.h = self.lib.ref_precond_create(A.h, kind, int(low_precision), tol, lfill)
+        if not self.h:
+            raise ValueError("bad preconditioner kind")
+
+    def setup(self) -> int:
+        return self.lib.ref_precond_setup(self.h)
+
+    def factor(self, which: int = 0):
+        n, nnz = C.c_uint(), C.c_uint()
+        self.lib.ref_precond_factor_dims(self.h, which, C.byref(n), C.byref(nnz))
+        rp = np.zeros(n.value + 1, np.uint32)
+        ci = np.zeros(nnz.value, np.uint32)
+        v = np.zeros(nnz.value, np.float64)
+        d = np.zeros(n.value, np.float64)
+        self.lib.ref_precond_factor_copy(self.h, which, rp, ci, v, d.ctypes.data_as(C.c_void_p))
+        return rp, ci, v, d
+
+    def apply(self, vec):
+        out = np.array(vec, dtype=np.float64, copy=True)
+        self.lib.ref_precond_apply(self.h, len(out), out)
+        return out
+
+    def mnnz(self) -> int:
+        return self.lib.ref_precond_mnnz(self.h)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.ref_precond_free(self.h)
+            self.h = None
+
+
+def cg_solve(A: RefCSR, P: RefPrecond | None, b, x0=None, tol=1e-8, maxit=1000, flexible=True):
+    n, _ = A.dims()
+    x = np.zeros(n) if x0 is None else np.array(x0, np.float64, copy=True)
+    it, err, conv = C.c_int(), C.c_double(), C.c_int()
+    A.lib.ref_cg_solve(A.h, P.h if P else None, int(flexible), tol, maxit,
+                       np.ascontiguousarray(b, np.float64), x, C.byref(it), C.byref(err), C.byref(conv))
+    return x, it.value, err.value, bool(conv.value)
+
+
+def gmres_solve(A: RefCSR, P: RefPrecond | None, b, x0=None, tol=1e-8, restart=50, flexible=True):
+    n, _ = A.dims()
+    x = np.zeros(n) if x0 is None else np.array(x0, np.float64, copy=True)
+    it, err, conv = C.c_int(), C.c_double(), C.c_int()
+    A.lib.ref_gmres_solve(A.h, P.h if P else None, int(flexible), restart, tol,
+                          np.ascontiguousarray(b, np.float64), x, C.byref(it), C.byref(err), C.byref(conv))
+    return x, it.value, err.value, bool(conv.value)

@@ -1,0 +1,239 @@
+// Test-only C entry points around the reference's own CPU classes.
+//
+// This file is compiled together with the reference's unmodified sources
+// (include/, source/ of PrisPack) by oracle/Makefile into oracle/_ref/.
+// It is the checker's view of the reference: it lets the Python tests and the
+// CPU-baseline arm of bench.py drive HOST::CSRMatrix, HOST::IncompleteCholesky,
+// HOST::IncompleteLDLT, HOST::IncompleteLU, HOST::CG and HOST::GMRES through
+// plain pointers.  Nothing in the product library links against it.
+//
+// The reference keeps factor arrays in private members without getters for
+// ILDLT, so private/protected are opened up for this translation unit only,
+// after every standard header has been included.
+#include "config/headers.h"
+#include <omp.h>
+#include <functional>
+#include <numeric>
+// everything that carries OpenMP pragmas (private(...) clauses) first
+#include "MatrixClass/CSRMatrix.h"
+#include "MatrixClass/DenseMatrix.h"
+#include "MatrixClass/ModelProblem.h"
+#include "VectorClass/VectorTools.h"
+#include "utils/MemoryTools/SharedPtrTools.h"
+#include "utils/TimerTools/CPUtimer.hpp"
+#include "Preconditioner/BasePreconditon.h"
+#define private public
+#define protected public
+#include "Preconditioner/IncompleteCholesky.h"
+#include "Preconditioner/IncompleteLDLT.h"
+#include "Preconditioner/IncompleteLU.h"
+#include "Solver/CG.h"
+#include "Solver/GMRES.h"
+#undef private
+#undef protected
+
+using namespace HOST;
+
+namespace {
+using CSRd = CSRMatrix<FLOAT64>;
+
+struct RefPrecond {
+    int kind;        // 1 = IC, 2 = ILUT, 3 = ILDLT
+    int lowPrecision;  // 1 = factor values stored in FP32
+    std::shared_ptr<BasePrecondition<FLOAT64>> p;
+};
+
+template <typename V>
+void copyVec(const HostVector<V>& src, V* dst, UINT32 n) {
+    for (UINT32 i = 0; i < n; ++i) dst[i] = src[i];
+}
+// Factor export.  which: 0 = first stored triangle (IC/ILDLT: L^T rows; ILUT: L),
+// 1 = second (ILUT: U).  Values are widened to double.
+template <typename Low>
+const CSRMatrix<Low>* factorMat(RefPrecond* r, int which) {
+    if (r->kind == 1) return &*static_cast<IncompleteCholesky<Low, FLOAT64>*>(r->p.get())->m_matTransL;
+    if (r->kind == 3) return &*static_cast<IncompleteLDLT<Low, FLOAT64>*>(r->p.get())->m_matTransL;
+    auto* lu = static_cast<IncompleteLU<Low, FLOAT64>*>(r->p.get());
+    return which == 0 ? &*lu->m_L : &*lu->m_U;
+}
+
+template <typename Low>
+void factorDims(RefPrecond* r, int which, unsigned* n, unsigned* nnz) {
+    const CSRMatrix<Low>* M = factorMat<Low>(r, which);
+    *n = M->getRowNum();
+    *nnz = M->getRowOffsetPtr(0)[M->getRowNum()];
+}
+
+template <typename Low>
+void factorCopy(RefPrecond* r, int which, unsigned* rowptr, unsigned* col, double* val, double* diag) {
+    const CSRMatrix<Low>* M = factorMat<Low>(r, which);
+    UINT32 n = M->getRowNum();
+    const UINT32* rp = M->getRowOffsetPtr(0);
+    for (UINT32 i = 0; i <= n; ++i) rowptr[i] = rp[i];
+    for (UINT32 k = 0; k < rp[n]; ++k) { col[k] = M->getColIndicesPtr(0)[k]; val[k] = (double)M->getCSRValuesPtr(0)[k]; }
+    if (diag) {
+        if (r->kind == 3) {
+            auto* p = static_cast<IncompleteLDLT<Low, FLOAT64>*>(r->p.get());
+            for (UINT32 i = 0; i < n; ++i) diag[i] = (*p->m_diagVals)[i];
+        } else if (r->kind == 2) {
+            auto* p = static_cast<IncompleteLU<Low, FLOAT64>*>(r->p.get());
+            for (UINT32 i = 0; i < n; ++i) diag[i] = (double)(*p->m_diagVals)[i];
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+// ---- CSR -----------------------------------------------------------------
+void* ref_csr_laplacian(int nx, int ny, int nz, double ax, double ay, double az, double shift) {
+    auto* A = new CSRd();
+    generateLaplacianCSR<FLOAT64>(*A, nx, ny, nz, ax, ay, az, shift);
+    return A;
+}
+
+void* ref_csr_poisson(unsigned blk) {
+    auto* A = new CSRd();
+    generatePoissonCSR<FLOAT64>(*A, blk);
+    return A;
+}
+
+void* ref_csr_from_arrays(unsigned n, const unsigned* rowptr, const unsigned* col, const double* val) {
+    UINT32 nnz = rowptr[n];
+    auto* A = new CSRd(n, n, nnz, memoryBase);
+    UINT32* rp = A->getRowOffsetPtr(0);
+    UINT32* ci = A->getColIndicesPtr(0);
+    FLOAT64* v = A->getCSRValuesPtr(0);
+    for (UINT32 i = 0; i <= n; ++i) rp[i] = rowptr[i];
+    for (UINT32 k = 0; k < nnz; ++k) { ci[k] = col[k]; v[k] = val[k]; }
+    return A;
+}
+
+void ref_csr_dims(void* h, unsigned* n, unsigned* nnz) {
+    auto* A = static_cast<CSRd*>(h);
+    *n = A->getRowNum();
+    *nnz = A->getRowOffsetPtr(0)[A->getRowNum()];
+}
+
+void ref_csr_copy(void* h, unsigned* rowptr, unsigned* col, double* val) {
+    auto* A = static_cast<CSRd*>(h);
+    UINT32 n = A->getRowNum();
+    const UINT32* rp = A->getRowOffsetPtr(0);
+    for (UINT32 i = 0; i <= n; ++i) rowptr[i] = rp[i];
+    for (UINT32 k = 0; k < rp[n]; ++k) { col[k] = A->getColIndicesPtr(0)[k]; val[k] = A->getCSRValuesPtr(0)[k]; }
+}
+
+void ref_csr_free(void* h) { delete static_cast<CSRd*>(h); }
+
+void ref_spmv(void* h, const double* x, double* y) {
+    auto* A = static_cast<CSRd*>(h);
+    A->MatPVecWithRawPtr(x, y);
+}
+
+// ---- preconditioners -------------------------------------------------------
+// kind: 1 IC (threshold), 2 ILUT (lfill, tol), 3 ILDLT (tol)
+void* ref_precond_create(void* hA, int kind, int lowPrecision, double tol, int lfill) {
+    auto* A = static_cast<CSRd*>(hA);
+    // the preconditioner keeps a shared_ptr alias; the matrix stays owned by the caller
+    std::shared_ptr<CSRd> sp(A, [](CSRd*) {});
+    auto* r = new RefPrecond{kind, lowPrecision, nullptr};
+    if (kind == 1) {
+        if (lowPrecision) r->p = std::make_shared<IncompleteCholesky<FLOAT32, FLOAT64>>(sp, tol);
+        else r->p = std::make_shared<IncompleteCholesky<FLOAT64, FLOAT64>>(sp, tol);
+    } else if (kind == 2) {
+        if (lowPrecision) r->p = std::make_shared<IncompleteLU<FLOAT32, FLOAT64>>(sp, (UINT32)lfill, tol);
+        else r->p = std::make_shared<IncompleteLU<FLOAT64, FLOAT64>>(sp, (UINT32)lfill, tol);
+    } else if (kind == 3) {
+        if (lowPrecision) r->p = std::make_shared<IncompleteLDLT<FLOAT32, FLOAT64>>(sp, tol);
+        else r->p = std::make_shared<IncompleteLDLT<FLOAT64, FLOAT64>>(sp, tol);
+    } else {
+        delete r;
+        return nullptr;
+    }
+    return r;
+}
+
+int ref_precond_setup(void* h) {
+    auto* r = static_cast<RefPrecond*>(h);
+    try {
+        r->p->setup();
+    } catch (...) {
+        return -1;
+    }
+    return r->p->isReady() ? 0 : -2;
+}
+
+void ref_precond_free(void* h) { delete static_cast<RefPrecond*>(h); }
+
+unsigned ref_precond_mnnz(void* h) { return static_cast<RefPrecond*>(h)->p->getPreconditionNonZeroCount(); }
+
+void ref_precond_factor_dims(void* h, int which, unsigned* n, unsigned* nnz) {
+    auto* r = static_cast<RefPrecond*>(h);
+    if (r->lowPrecision) factorDims<FLOAT32>(r, which, n, nnz);
+    else factorDims<FLOAT64>(r, which, n, nnz);
+}
+
+void ref_precond_factor_copy(void* h, int which, unsigned* rowptr, unsigned* col, double* val, double* diag) {
+    auto* r = static_cast<RefPrecond*>(h);
+    if (r->lowPrecision) factorCopy<FLOAT32>(r, which, rowptr, col, val, diag);
+    else factorCopy<FLOAT64>(r, which, rowptr, col, val, diag);
+}
+
+// vec <- M^{-1} vec (TriangularPrecondition::MInvSolve, in place)
+void ref_precond_apply(void* h, unsigned n, double* vec) {
+    auto* r = static_cast<RefPrecond*>(h);
+    DenseVector<FLOAT64> v(n);
+    for (UINT32 i = 0; i < n; ++i) v[i] = vec[i];
+    r->p->MInvSolve(v);
+    for (UINT32 i = 0; i < n; ++i) vec[i] = v[i];
+}
+
+// ---- solvers ---------------------------------------------------------------
+// cgType: 0 NormalCG, 1 FlexibleCG.  hP may be null.  x is the in/out guess.
+int ref_cg_solve(void* hA, void* hP, int cgType, double tol, unsigned maxIter, const double* b, double* x,
+                 int* numIter, double* finalError, int* converged) {
+    auto* A = static_cast<CSRd*>(hA);
+    UINT32 n = A->getRowNum();
+    DenseVector<FLOAT64> vb(n), vx(n);
+    for (UINT32 i = 0; i < n; ++i) { vb[i] = b[i]; vx[i] = x[i]; }
+    if (hP) {
+        auto* r = static_cast<RefPrecond*>(hP);
+        CG<FLOAT64> s(n, r->p, cgType ? FlexibleCG : NormalCG, tol, maxIter);
+        s.solve(*A, vb, vx);
+        *numIter = s.getNumIter();
+        *finalError = s.getError();
+        *converged = s.getConvergence();
+    } else {
+        CG<FLOAT64> s(n, tol, maxIter);
+        s.solve(*A, vb, vx);
+        *numIter = s.getNumIter();
+        *finalError = s.getError();
+        *converged = s.getConvergence();
+    }
+    for (UINT32 i = 0; i < n; ++i) x[i] = vx[i];
+    return 0;
+}
+
+// gmresType: 0 NormalGMRES, 1 FlexibleGMRES; restart > 0 enables setRestart(true, restart)
+int ref_gmres_solve(void* hA, void* hP, int gmresType, unsigned restart, double tol, const double* b, double* x,
+                    int* numIter, double* finalError, int* converged) {
+    auto* A = static_cast<CSRd*>(hA);
+    UINT32 n = A->getRowNum();
+    DenseVector<FLOAT64> vb(n), vx(n);
+    for (UINT32 i = 0; i < n; ++i) { vb[i] = b[i]; vx[i] = x[i]; }
+    std::shared_ptr<BasePrecondition<FLOAT64>> p;
+    if (hP) p = static_cast<RefPrecond*>(hP)->p;
+    GMRES<FLOAT64> s(n, p, tol, gmresType ? FlexibleGMRES : NormalGMRES);
+    if (restart > 0) s.setRestart(true, restart);
+    s.solve(*A, vb, vx);
+    *numIter = s.getNumIter();
+    *finalError = s.getError();
+    *converged = s.getConvergence();
+    for (UINT32 i = 0; i < n; ++i) x[i] = vx[i];
+    return 0;
+}
+
+int ref_omp_max_threads(void) { return omp_get_max_threads(); }
+
+}  // extern "C"

@@ -1,0 +1,423 @@
+"""B200 solve phase for PrisPack: Python view of the C ABI (include/prism_solve.h).
+
+The classes mirror the reference's C++ interface names and argument meaning
+(HOST::CSRMatrix, IncompleteCholesky, IncompleteLU, IncompleteLDLT, CG, GMRES;
+include/Preconditioner/BasePreconditon.h:34-145, include/Solver/BaseSolver.h:9-17),
+so that code written against the reference reads the same.  All work runs in
+``_lib/libprism_solve.so``; there is no CPU fallback: importing this package
+without the built library raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libprism_solve.so")
+
+# ---- enums (include/prism_solve.h) ------------------------------------------------
+PRISM_FP64, PRISM_FP32 = 0, 1
+PRECOND_NONE, PRECOND_IC, PRECOND_ILUT, PRECOND_ILDLT, PRECOND_GMSLR, PRECOND_AMSED = range(6)
+SOLVER_FCG, SOLVER_CG, SOLVER_FGMRES, SOLVER_GMRES = range(4)
+# reference spellings (include/Solver/CG.h:14-18, include/Solver/GMRES.h:15-18)
+NormalCG, FlexibleCG = "NormalCG", "FlexibleCG"
+NormalGMRES, FlexibleGMRES = "NormalGMRES", "FlexibleGMRES"
+MAX_ITER_NUM_SOLVER = 500  # config/config.h:25
+
+STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_ZERO_PIVOT", 4: "ERR_NOT_SPD", 5: "ERR_NOT_READY",
+          6: "ERR_TIMEOUT", 7: "ERR_NONFINITE", 8: "ERR_ALLOC", 9: "ERR_UNSUPPORTED", 10: "ERR_BAD_MATRIX"}
+
+
+class PrismError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class SolveOpts(C.Structure):
+    _fields_ = [("solver", C.c_int32), ("tol", C.c_double), ("max_iter", C.c_uint32), ("restart", C.c_uint32)]
+
+
+class SolveStats(C.Structure):
+    _fields_ = [("num_iter", C.c_int32), ("converged", C.c_int32), ("final_error", C.c_double),
+                ("true_rel_residual", C.c_double), ("precond_applies", C.c_uint32),
+                ("spmv_count", C.c_uint32), ("device_ms", C.c_double)]
+
+
+_lib = None
+_u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_vp = C.c_void_p
+
+# every exported symbol with its argument types (the C header, one to one)
+_SIGS = {
+    "prism_last_error": (C.c_char_p, []),
+    "prism_version": (C.c_int32, []),
+    "prism_kernel_launch_count": (C.c_uint64, []),
+    "prism_laplacian_dims": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+    "prism_laplacian_fill": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
+                                         C.c_double, _u32p, _u32p, _f64p]),
+    "prism_create": (C.c_int32, [C.c_uint32, _u32p, _u32p, _f64p, C.c_int32, C.POINTER(_vp)]),
+    "prism_destroy": (C.c_int32, [_vp]),
+    "prism_set_stream": (C.c_int32, [_vp, _vp]),
+    "prism_dims": (C.c_int32, [_vp, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]),
+    "prism_spmv_device": (C.c_int32, [_vp, _vp, _vp]),
+    "prism_spmv": (C.c_int32, [_vp, _f64p, _f64p]),
+    "prism_set_precond_none": (C.c_int32, [_vp]),
+    "prism_set_precond_ic": (C.c_int32, [_vp, C.c_double, C.c_int32]),
+    "prism_set_precond_ildlt": (C.c_int32, [_vp, C.c_double, C.c_int32]),
+    "prism_set_precond_ilut": (C.c_int32, [_vp, C.c_uint32, C.c_double, C.c_int32]),
+    "prism_precond_nnz": (C.c_int32, [_vp, C.POINTER(C.c_uint64)]),
+    "prism_precond_type": (C.c_int32, [_vp, C.POINTER(C.c_int32)]),
+    "prism_precond_factor": (C.c_int32, [_vp, C.c_int32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64),
+                                         _vp, _vp, _vp, _vp]),
+    "prism_precond_levels": (C.c_int32, [_vp, C.c_int32, C.POINTER(C.c_uint32)]),
+    "prism_factor_create": (C.c_int32, [C.c_int32, C.c_uint32, _u32p, _u32p, _f64p, C.c_double, C.c_uint32,
+                                        C.c_int32, C.POINTER(_vp)]),
+    "prism_factor_destroy": (C.c_int32, [_vp]),
+    "prism_factor_get": (C.c_int32, [_vp, C.c_int32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64),
+                                     _vp, _vp, _vp, _vp]),
+    "prism_factor_info": (C.c_int32, [_vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+    "prism_set_precond_factor": (C.c_int32, [_vp, _vp]),
+    "prism_precond_sweep_device": (C.c_int32, [_vp, C.c_int32, _vp, _vp, C.c_int32]),
+    "prism_precond_sweep_info": (C.c_int32, [_vp, C.c_int32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64),
+                                             C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+    "prism_apply_device": (C.c_int32, [_vp, _vp, _vp]),
+    "prism_apply": (C.c_int32, [_vp, _f64p, _f64p]),
+    "prism_solve_device": (C.c_int32, [_vp, C.POINTER(SolveOpts), _vp, _vp, C.POINTER(SolveStats)]),
+    "prism_solve": (C.c_int32, [_vp, C.POINTER(SolveOpts), _f64p, _f64p, C.POINTER(SolveStats)]),
+}
+
+
+def load() -> C.CDLL:
+    """Loads the solve-phase library; raises if it was never built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run `python -m prispack_b200.build` (no CPU fallback exists)")
+        lib = C.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def exported_symbols():
+    return list(_SIGS)
+
+
+def _check(rc: int):
+    if rc != 0:
+        raise PrismError(rc, load().prism_last_error().decode())
+
+
+def kernel_launch_count() -> int:
+    return int(load().prism_kernel_launch_count())
+
+
+def _ptr(t) -> int:
+    """Device pointer of a torch CUDA tensor (float64, contiguous)."""
+    import torch
+    assert isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()
+    return t.data_ptr()
+
+
+# =============================================================================
+# CSR matrix (HOST::CSRMatrix<double>) and model problems
+# =============================================================================
+class CSRMatrix:
+    """Host CSR with uint32 offsets/indices and double values, rows sorted."""
+
+    def __init__(self, rowptr, col, val):
+        self.rowptr = np.ascontiguousarray(rowptr, np.uint32)
+        self.col = np.ascontiguousarray(col, np.uint32)
+        self.val = np.ascontiguousarray(val, np.float64)
+
+    @property
+    def n(self) -> int:
+        return len(self.rowptr) - 1
+
+    @property
+    def nnz(self) -> int:
+        return int(self.rowptr[-1])
+
+    def getRowNum(self) -> int:
+        return self.n
+
+    @classmethod
+    def laplacian(cls, nx, ny, nz, alphax=0.0, alphay=0.0, alphaz=0.0, shift=0.0) -> "CSRMatrix":
+        """generateLaplacianCSR (include/MatrixClass/ModelProblem.h:45-52)."""
+        lib = load()
+        n, nnz = C.c_uint32(), C.c_uint32()
+        _check(lib.prism_laplacian_dims(nx, ny, nz, C.byref(n), C.byref(nnz)))
+        rp = np.zeros(n.value + 1, np.uint32)
+        ci = np.zeros(nnz.value, np.uint32)
+        v = np.zeros(nnz.value, np.float64)
+        _check(lib.prism_laplacian_fill(nx, ny, nz, alphax, alphay, alphaz, shift, rp, ci, v))
+        return cls(rp, ci, v)
+
+    def to_scipy(self):
+        import scipy.sparse as sp
+        return sp.csr_matrix((self.val, self.col, self.rowptr), shape=(self.n, self.n))
+
+
+def generateLaplacianCSR(nx, ny, nz, alphax=0.0, alphay=0.0, alphaz=0.0, shift=0.0) -> CSRMatrix:
+    return CSRMatrix.laplacian(nx, ny, nz, alphax, alphay, alphaz, shift)
+
+
+# =============================================================================
+# Host-only incomplete factorisation (no device needed)
+# =============================================================================
+class HostFactor:
+    """prism_factor: an IC / ILUT / ILDLT factor built on the host, bit-exact
+    with the reference's setup(), attachable to any DeviceSystem of the same size."""
+
+    def __init__(self, A: CSRMatrix, kind: int, *, tol: float = 1e-3, lfill: int = 20, precision: int = PRISM_FP64):
+        self.lib = load()
+        self.kind = kind
+        h = _vp()
+        _check(self.lib.prism_factor_create(kind, A.n, A.rowptr, A.col, A.val, tol, lfill, precision, C.byref(h)))
+        self.h = h
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.prism_factor_destroy(self.h)
+            self.h = None
+
+    def arrays(self, which: int = 0):
+        n, nnz = C.c_uint32(), C.c_uint64()
+        _check(self.lib.prism_factor_get(self.h, which, C.byref(n), C.byref(nnz), None, None, None, None))
+        rp = np.zeros(n.value + 1, np.uint32)
+        ci = np.zeros(nnz.value, np.uint32)
+        v = np.zeros(nnz.value, np.float64)
+        d = np.zeros(n.value, np.float64)
+        _check(self.lib.prism_factor_get(self.h, which, C.byref(n), C.byref(nnz), rp.ctypes.data, ci.ctypes.data,
+                                         v.ctypes.data, d.ctypes.data))
+        return rp, ci, v, d
+
+    def info(self):
+        m, lo, up = C.c_uint64(), C.c_uint32(), C.c_uint32()
+        _check(self.lib.prism_factor_info(self.h, C.byref(m), C.byref(lo), C.byref(up)))
+        return {"mnnz": m.value, "lower_levels": lo.value, "upper_levels": up.value}
+
+
+# =============================================================================
+# Device operator: one C-ABI handle (A on the GPU + preconditioner + workspace)
+# =============================================================================
+class DeviceSystem:
+    """A resident on one device, its preconditioner and Krylov workspace."""
+
+    def __init__(self, A: CSRMatrix, device: int = 0):
+        self.lib = load()
+        self.A = A
+        h = _vp()
+        _check(self.lib.prism_create(A.n, A.rowptr, A.col, A.val, device, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.prism_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def n(self) -> int:
+        return self.A.n
+
+    def set_stream(self, stream_ptr: int):
+        _check(self.lib.prism_set_stream(self.h, stream_ptr))
+
+    # y = A x
+    def spmv(self, x):
+        if hasattr(x, "is_cuda"):
+            import torch
+            y = torch.empty_like(x)
+            _check(self.lib.prism_spmv_device(self.h, _ptr(x), _ptr(y)))
+            return y
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.zeros(self.n)
+        _check(self.lib.prism_spmv(self.h, x, y))
+        return y
+
+    # ---- preconditioner -------------------------------------------------------
+    def set_precond(self, kind: int, *, tol: float = 1e-3, lfill: int = 20, precision: int = PRISM_FP64):
+        if kind == PRECOND_NONE:
+            _check(self.lib.prism_set_precond_none(self.h))
+        elif kind == PRECOND_IC:
+            _check(self.lib.prism_set_precond_ic(self.h, tol, precision))
+        elif kind == PRECOND_ILDLT:
+            _check(self.lib.prism_set_precond_ildlt(self.h, tol, precision))
+        elif kind == PRECOND_ILUT:
+            _check(self.lib.prism_set_precond_ilut(self.h, lfill, tol, precision))
+        else:
+            raise PrismError(9, f"preconditioner kind {kind} not available")
+
+    def attach(self, factor: "HostFactor"):
+        _check(self.lib.prism_set_precond_factor(self.h, factor.h))
+
+    def precond_nnz(self) -> int:
+        v = C.c_uint64()
+        _check(self.lib.prism_precond_nnz(self.h, C.byref(v)))
+        return v.value
+
+    def precond_levels(self, sweep: int) -> int:
+        v = C.c_uint32()
+        _check(self.lib.prism_precond_levels(self.h, sweep, C.byref(v)))
+        return v.value
+
+    def precond_factor(self, which: int = 0):
+        """Stored factor arrays in the reference layout: (rowptr, col, val, diag)."""
+        n, nnz = C.c_uint32(), C.c_uint64()
+        _check(self.lib.prism_precond_factor(self.h, which, C.byref(n), C.byref(nnz), None, None, None, None))
+        rp = np.zeros(n.value + 1, np.uint32)
+        ci = np.zeros(nnz.value, np.uint32)
+        v = np.zeros(nnz.value, np.float64)
+        d = np.zeros(n.value, np.float64)
+        _check(self.lib.prism_precond_factor(self.h, which, C.byref(n), C.byref(nnz), rp.ctypes.data,
+                                             ci.ctypes.data, v.ctypes.data, d.ctypes.data))
+        return rp, ci, v, d
+
+    def sweep_device(self, sweep: int, vin, vout, prepare: bool = True):
+        """One triangular sweep alone on torch CUDA tensors (kernel timing)."""
+        _check(self.lib.prism_precond_sweep_device(self.h, sweep, _ptr(vin), _ptr(vout), int(prepare)))
+
+    def sweep_info(self, sweep: int) -> dict:
+        n, nnz, vb, lv = C.c_uint32(), C.c_uint64(), C.c_uint32(), C.c_uint32()
+        _check(self.lib.prism_precond_sweep_info(self.h, sweep, C.byref(n), C.byref(nnz), C.byref(vb), C.byref(lv)))
+        return {"n": n.value, "nnz": nnz.value, "value_bytes": vb.value, "levels": lv.value}
+
+    def apply(self, vec):
+        """out = M^{-1} vec (MInvSolve(vecIN, vecOUT))."""
+        if hasattr(vec, "is_cuda"):
+            import torch
+            out = torch.empty_like(vec)
+            _check(self.lib.prism_apply_device(self.h, _ptr(vec), _ptr(out)))
+            return out
+        vec = np.ascontiguousarray(vec, np.float64)
+        out = np.zeros(self.n)
+        _check(self.lib.prism_apply(self.h, vec, out))
+        return out
+
+    # ---- solve ------------------------------------------------------------------
+    def solve(self, b, x=None, *, solver=SOLVER_FCG, tol=1e-8, max_iter=1000, restart=0) -> tuple:
+        """x (in/out initial guess) solved in place; returns (x, SolveStats)."""
+        opts = SolveOpts(solver, tol, max_iter, restart)
+        st = SolveStats()
+        if hasattr(b, "is_cuda"):
+            import torch
+            if x is None:
+                x = torch.zeros_like(b)
+            _check(self.lib.prism_solve_device(self.h, C.byref(opts), _ptr(b), _ptr(x), C.byref(st)))
+            return x, st
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.zeros(self.n) if x is None else np.array(x, np.float64, copy=True)
+        _check(self.lib.prism_solve(self.h, C.byref(opts), b, x, C.byref(st)))
+        return x, st
+
+
+# =============================================================================
+# Reference-named wrappers (BasePrecondition / BaseSolver mirror)
+# =============================================================================
+class _Triangular:
+    kind = PRECOND_NONE
+
+    def __init__(self, system: DeviceSystem, precision: int = PRISM_FP64):
+        self.system = system
+        self.precision = precision
+        self._ready = False
+
+    def isReady(self) -> bool:
+        return self._ready
+
+    def MInvSolve(self, vec):
+        self.setup()
+        return self.system.apply(vec)
+
+    def getPreconditionNonZeroCount(self) -> int:
+        self.setup()
+        return self.system.precond_nnz()
+
+    def getPreconditionFillinRatio(self) -> float:
+        return self.getPreconditionNonZeroCount() / self.system.A.nnz
+
+
+class IncompleteCholesky(_Triangular):
+    """IncompleteCholesky<Low, double>(A, threshold) (IncompleteCholesky.cpp:11-33)."""
+    kind = PRECOND_IC
+
+    def __init__(self, system, threshold, precision=PRISM_FP64):
+        super().__init__(system, precision)
+        self.threshold = threshold
+
+    def setup(self):
+        if not self._ready:
+            self.system.set_precond(PRECOND_IC, tol=self.threshold, precision=self.precision)
+            self._ready = True
+
+
+class IncompleteLDLT(_Triangular):
+    """IncompleteLDLT<Low, double>(A, tol) (IncompleteLDLT.cpp)."""
+    kind = PRECOND_ILDLT
+
+    def __init__(self, system, tolerance, precision=PRISM_FP64):
+        super().__init__(system, precision)
+        self.tolerance = tolerance
+
+    def setup(self):
+        if not self._ready:
+            self.system.set_precond(PRECOND_ILDLT, tol=self.tolerance, precision=self.precision)
+            self._ready = True
+
+
+class IncompleteLU(_Triangular):
+    """IncompleteLU<Low, double>(A, lfill, tolerance) (IncompleteLU.cpp:12-35)."""
+    kind = PRECOND_ILUT
+
+    def __init__(self, system, lfill, tolerance, precision=PRISM_FP64):
+        super().__init__(system, precision)
+        self.lfill = lfill
+        self.tolerance = tolerance
+
+    def setup(self):
+        if not self._ready:
+            self.system.set_precond(PRECOND_ILUT, tol=self.tolerance, lfill=self.lfill, precision=self.precision)
+            self._ready = True
+
+
+class CG:
+    """CG<double>(n, precond, CGType, tol, maxIter) (source/Solver/CG.cpp:11-31)."""
+
+    def __init__(self, problemSize, precond=None, cgType=FlexibleCG, tol=1e-8, maxIter=1000):
+        self.n = problemSize
+        self.precond = precond
+        self.cgType = cgType
+        self.tol = tol
+        self.maxIter = maxIter
+        self.stats = None
+
+    def solve(self, system: DeviceSystem, b, x):
+        if self.precond is not None:
+            self.precond.setup()
+        else:
+            system.set_precond(PRECOND_NONE)
+        kind = SOLVER_FCG if self.cgType == FlexibleCG else SOLVER_CG
+        x_out, self.stats = system.solve(b, x, solver=kind, tol=self.tol, max_iter=self.maxIter)
+        return x_out
+
+    def getNumIter(self):
+        return self.stats.num_iter
+
+    def getError(self):
+        return self.stats.final_error
+
+    def getConvergence(self):
+        return bool(self.stats.converged)

@@ -1,0 +1,397 @@
+// extern "C" boundary of the solve phase (declared in include/prism_solve.h).
+// Every entry point catches everything: no C++ exception crosses the ABI.
+#include <cstring>
+#include <string>
+
+#include "../../include/prism_solve.h"
+#include "solve.cuh"
+
+using prism::Error;
+using prism::Handle;
+
+namespace {
+thread_local std::string g_last_error;
+
+int fail(int status, const std::string& msg) {
+    g_last_error = msg;
+    return status;
+}
+
+template <typename F>
+int guarded(F&& f) {
+    try {
+        g_last_error.clear();
+        return f();
+    } catch (const Error& e) {
+        return fail(e.status, e.what());
+    } catch (const std::bad_alloc&) {
+        return fail(PRISM_ERR_ALLOC, "host allocation failed");
+    } catch (const std::exception& e) {
+        return fail(PRISM_ERR_ARG, e.what());
+    } catch (...) {
+        return fail(PRISM_ERR_ARG, "unknown error");
+    }
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+}  // namespace
+
+struct prism_handle_s : Handle {};
+
+struct prism_factor_s {
+    std::shared_ptr<const prism::HostFactor> f;
+};
+
+static int32_t set_tri(prism_handle h, int kind, double tol, uint32_t lfill, int32_t precision) {
+    if (!h) return fail(PRISM_ERR_ARG, "null handle");
+    if (precision != PRISM_FP64 && precision != PRISM_FP32) return fail(PRISM_ERR_ARG, "precision must be PRISM_FP64 or PRISM_FP32");
+    return guarded([&]() -> int {
+        DeviceGuard g(h->info.device);
+        h->P.reset();
+        auto f = std::make_shared<prism::HostFactor>();
+        std::string err;
+        int rc = prism::build_triangular(kind, h->A_host, tol, lfill, precision == PRISM_FP32, *f, &err);
+        if (rc) return fail(rc, err);
+        h->P = std::make_unique<prism::TriangularPrecond>(*h, std::move(f));
+        return PRISM_OK;
+    });
+}
+
+extern "C" {
+
+const char* prism_last_error(void) { return g_last_error.c_str(); }
+
+int32_t prism_version(void) { return 100; }
+
+uint64_t prism_kernel_launch_count(void) { return prism::launch_counter().load(); }
+
+int32_t prism_laplacian_dims(int32_t nx, int32_t ny, int32_t nz, uint32_t* n, uint32_t* nnz) {
+    if (!n || !nnz) return fail(PRISM_ERR_ARG, "null output pointer");
+    if (!prism::laplacian_dims(nx, ny, nz, n, nnz)) return fail(PRISM_ERR_ARG, "grid dimensions out of range");
+    return PRISM_OK;
+}
+
+int32_t prism_laplacian_fill(int32_t nx, int32_t ny, int32_t nz, double ax, double ay, double az, double shift,
+                             uint32_t* rowptr, uint32_t* col, double* val) {
+    uint32_t n, nnz;
+    if (!rowptr || !col || !val) return fail(PRISM_ERR_ARG, "null output pointer");
+    if (!prism::laplacian_dims(nx, ny, nz, &n, &nnz)) return fail(PRISM_ERR_ARG, "grid dimensions out of range");
+    return guarded([&]() -> int {
+        prism::laplacian_fill(nx, ny, nz, ax, ay, az, shift, rowptr, col, val);
+        return PRISM_OK;
+    });
+}
+
+int32_t prism_create(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val, int32_t device,
+                     prism_handle* out) {
+    if (!out) return fail(PRISM_ERR_ARG, "null output handle");
+    *out = nullptr;
+    if (n == 0) return fail(PRISM_ERR_ARG, "empty matrix (n == 0)");
+    if (!rowptr || !col || !val) return fail(PRISM_ERR_ARG, "null CSR array");
+    std::string bad = prism::validate_csr(n, rowptr, col);
+    if (!bad.empty()) return fail(PRISM_ERR_BAD_MATRIX, bad);
+    return guarded([&]() -> int {
+        int ndev = 0;
+        PRISM_CUDA(cudaGetDeviceCount(&ndev));
+        if (device < 0 || device >= ndev)
+            return fail(PRISM_ERR_ARG, "device " + std::to_string(device) + " not present (" + std::to_string(ndev) + " devices)");
+        DeviceGuard g(device);
+        auto* h = new prism_handle_s();
+        try {
+            prism::init_device_info(h->info, device);
+            PRISM_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+            h->own_stream = true;
+            PRISM_CUDA(cudaEventCreate(&h->ev0));
+            PRISM_CUDA(cudaEventCreate(&h->ev1));
+            PRISM_CUDA(cudaMallocHost(&h->pinned, prism::kNumScalars * sizeof(double)));
+            const uint64_t nnz = rowptr[n];
+            h->A_host.n = n;
+            h->A_host.rowptr.assign(rowptr, rowptr + n + 1);
+            h->A_host.col.assign(col, col + nnz);
+            h->A_host.val.assign(val, val + nnz);
+            h->A.n = n;
+            h->A.nnz = nnz;
+            h->A.rowptr.upload(rowptr, (size_t)n + 1, h->stream);
+            h->A.col.upload(col, nnz, h->stream);
+            h->A.val.upload(val, nnz, h->stream);
+            h->red.partial.alloc(prism::Reducer::kMaxGrid * 2);
+            h->red.ticket.alloc(1);
+            h->red.scalars.alloc(prism::kNumScalars);
+            h->status.alloc(1);
+            PRISM_CUDA(cudaMemsetAsync(h->red.ticket.get(), 0, sizeof(unsigned), h->stream));
+            PRISM_CUDA(cudaMemsetAsync(h->red.scalars.get(), 0, prism::kNumScalars * sizeof(double), h->stream));
+            PRISM_CUDA(cudaMemsetAsync(h->status.get(), 0, sizeof(int), h->stream));
+            PRISM_CUDA(cudaStreamSynchronize(h->stream));
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+        return PRISM_OK;
+    });
+}
+
+int32_t prism_destroy(prism_handle h) {
+    if (!h) return PRISM_OK;
+    return guarded([&]() -> int {
+        DeviceGuard g(h->info.device);
+        cudaStreamSynchronize(h->stream);
+        delete h;
+        return PRISM_OK;
+    });
+}
+
+int32_t prism_set_stream(prism_handle h, void* stream) {
+    if (!h) return fail(PRISM_ERR_ARG, "null handle");
+    return guarded([&]() -> int {
+        DeviceGuard g(h->info.device);
+        PRISM_CUDA(cudaStreamSynchronize(h->stream));
+        if (h->own_stream) PRISM_CUDA(cudaStreamDestroy(h->stream));
+        h->own_stream = false;
+        h->stream = static_cast<cudaStream_t>(stream);
+        return PRISM_OK;
+    });
+}
+
+int32_t prism_dims(prism_handle h, uint32_t* n, uint64_t* nnz) {
+    if (!h) return fail(PRISM_ERR_ARG, "null handle");
+    if (n) *n = h->A.n;
+    if (nnz) *nnz = h->A.nnz;
+    return PRISM_OK;
+}
+
+int32_t prism_spmv_device(prism_handle h, const double* x_d, double* y_d) {
+    if (!h) return fail(PRISM_ERR_ARG, "null handle");
+    if (!x_d || !y_d) return fail(PRISM_ERR_ARG, "null vector");
+    return guarded([&]() -> int {
+        DeviceGuard g(h->info.device);
+        h->spmv(x_d, y_d);
+        PRISM_CUDA(cudaStreamSynchronize(h->stream));
+        return PRISM_OK;
+    });
+}
+
+int32_t prism_spmv(prism_handle h, const double* x, double* y) {
+    if (!h) return fail(PRISM_ERR_ARG, "null handle");
+    if (!x || !y) return fail(PRISM_ERR_ARG, "null vector");
+    return guarded([&]() -> int {
+        DeviceGuard g(h->info.device);
+        const uint32_t n = h->A.n;
+        if (h->xb.size() < n) { h->xb.alloc(n); h->bb.alloc(n); }
+        PRISM_CUDA(cudaMemcpyAsync(h->xb.get(), x, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        h->spmv(h->xb.get(), h->bb.get());
+        PRISM_CUDA(cudaMemcpyAsync(y, h->bb.get(), n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        PRISM_CUDA(cudaStreamSynchronize(h->stream));
+        return PRISM_OK;
+    });
+}
+
+// ---- preconditioners --------------------------------------------------------
+int32_t prism_set_precond_none(prism_handle h) {
+    if (!h) return fail(PRISM_ERR_ARG, "null handle");
+    h->P.reset();
+    return PRISM_OK;
+}
+
+int32_t prism_set_precond_ic(prism_handle h, double threshold, int32_t precision) {
+    return set_tri(h, PRISM_PRECOND_IC, threshold, 0, precision);
+}
+
+int32_t prism_set_precond_ildlt(prism_handle h, double tol, int32_t precision) {
+    return set_tri(h, PRISM_PRECOND_ILDLT, tol, 0, precision);
+}
+
+int32_t prism_set_precond_ilut(prism_handle h, uint32_t lfill, double tol, int32_t precision) {
+    return set_tri(h, PRISM_PRECOND_ILUT, tol, lfill, precision);
+}
+
+int32_t prism_set_precond_factor(prism_handle h, prism_factor f) {
+    if (!h || !f) return fail(PRISM_ERR_ARG, "null argument");
+    if (f->f->f0.n != h->A.n) return fail(PRISM_ERR_ARG, "factor dimension does not match the operator");
+    return guarded([&]() -> int {
+        DeviceGuard g(h->info.device);
+        h->P.reset();
+        h->P = std::make_unique<prism::TriangularPrecond>(*h, f->f);
+        return PRISM_OK;
+    });
+}
+
+// ---- host-only factors ------------------------------------------------------------
+int32_t prism_factor_create(int32_t kind, uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val,
+                            double tol, uint32_t lfill, int32_t precision, prism_factor* out) {
+    if (!out) return fail(PRISM_ERR_ARG, "null output");
+    *out = nullptr;
+    if (n == 0 || !rowptr || !col || !val) return fail(PRISM_ERR_ARG, "empty or null CSR");
+    if (kind != PRISM_PRECOND_IC && kind != PRISM_PRECOND_ILUT && kind != PRISM_PRECOND_ILDLT)
+        return fail(PRISM_ERR_UNSUPPORTED, "kind must be IC, ILUT or ILDLT");
+    if (precision != PRISM_FP64 && precision != PRISM_FP32) return fail(PRISM_ERR_ARG, "bad precision");
+    std::string bad = prism::validate_csr(n, rowptr, col);
+    if (!bad.empty()) return fail(PRISM_ERR_BAD_MATRIX, bad);
+    return guarded([&]() -> int {
+        prism::CsrHost A;
+        A.n = n;
+        A.rowptr.assign(rowptr, rowptr + n + 1);
+        A.col.assign(col, col + rowptr[n]);
+        A.val.assign(val, val + rowptr[n]);
+        auto f = std::make_shared<prism::HostFactor>();
+        std::string err;
+        int rc = prism::build_triangular(kind, A, tol, lfill, precision == PRISM_FP32, *f, &err);
+        if (rc) return fail(rc, err);
+        *out = new prism_factor_s{std::move(f)};
+        return PRISM_OK;
+    });
+}
+
+int32_t prism_factor_destroy(prism_factor f) {
+    delete f;
+    return PRISM_OK;
+}
+
+int32_t prism_factor_get(prism_factor f, int32_t which, uint32_t* n, uint64_t* nnz, uint32_t* rowptr, uint32_t* col,
+                         double* val, double* diag) {
+    if (!f) return fail(PRISM_ERR_ARG, "null factor");
+    int rc = prism::export_host_factor(*f->f, which, n, nnz, rowptr, col, val, diag);
+    if (rc) return fail(rc, "which must be 0 (or 1 for ILUT)");
+    return PRISM_OK;
+}
+
+int32_t prism_factor_info(prism_factor f, uint64_t* mnnz, uint32_t* lower_levels, uint32_t* upper_levels) {
+    if (!f) return fail(PRISM_ERR_ARG, "null factor");
+    const prism::HostFactor& F = *f->f;
+    if (mnnz) *mnnz = F.mnnz;
+    if (lower_levels) *lower_levels = F.fp32 ? F.lower32.num_levels : F.lower64.num_levels;
+    if (upper_levels) *upper_levels = F.fp32 ? F.upper32.num_levels : F.upper64.num_levels;
+    return PRISM_OK;
+}
+
+int32_t prism_precond_nnz(prism_handle h, uint64_t* mnnz) {
+    if (!h || !mnnz) return fail(PRISM_ERR_ARG, "null argument");
+    if (!h->P) return fail(PRISM_ERR_NOT_READY, "no preconditioner set");
+    *mnnz = h->P->mnnz();
+    return PRISM_OK;
+}
+
+int32_t prism_precond_type(prism_handle h, int32_t* kind) {
+    if (!h || !kind) return fail(PRISM_ERR_ARG, "null argument");
+    *kind = h->P ? h->P->kind() : PRISM_PRECOND_NONE;
+    return PRISM_OK;
+}
+
+int32_t prism_precond_factor(prism_handle h, int32_t which, uint32_t* n, uint64_t* nnz, uint32_t* rowptr,
+                             uint32_t* col, double* val, double* diag) {
+    if (!h) return fail(PRISM_ERR_ARG, "null handle");
+    if (!h->P) return fail(PRISM_ERR_NOT_READY, "no preconditioner set");
+    int rc = h->P->export_factor(which, n, nnz, rowptr, col, val, diag);
+    if (rc) return fail(rc, "factor export not available for this preconditioner/which");
+    return PRISM_OK;
+}
+
+int32_t prism_precond_levels(prism_handle h, int32_t sweep, uint32_t* num_levels) {
+    if (!h || !num_levels) return fail(PRISM_ERR_ARG, "null argument");
+    if (!h->P) return fail(PRISM_ERR_NOT_READY, "no preconditioner set");
+    *num_levels = h->P->levels(sweep);
+    return PRISM_OK;
+}
+
+int32_t prism_apply_device(prism_handle h, const double* in_d, double* out_d) {
+    if (!h) return fail(PRISM_ERR_ARG, "null handle");
+    if (!in_d || !out_d) return fail(PRISM_ERR_ARG, "null vector");
+    if (!h->P) return fail(PRISM_ERR_NOT_READY, "no preconditioner set");
+    return guarded([&]() -> int {
+        DeviceGuard g(h->info.device);
+        h->P->apply(h->stream, in_d, out_d);
+        h->check_status();
+        return PRISM_OK;
+    });
+}
+
+int32_t prism_apply(prism_handle h, const double* in, double* out) {
+    if (!h) return fail(PRISM_ERR_ARG, "null handle");
+    if (!in || !out) return fail(PRISM_ERR_ARG, "null vector");
+    if (!h->P) return fail(PRISM_ERR_NOT_READY, "no preconditioner set");
+    return guarded([&]() -> int {
+        DeviceGuard g(h->info.device);
+        const uint32_t n = h->A.n;
+        if (h->xb.size() < n) { h->xb.alloc(n); h->bb.alloc(n); }
+        PRISM_CUDA(cudaMemcpyAsync(h->bb.get(), in, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        h->P->apply(h->stream, h->bb.get(), h->xb.get());
+        PRISM_CUDA(cudaMemcpyAsync(out, h->xb.get(), n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        h->check_status();
+        return PRISM_OK;
+    });
+}
+
+int32_t prism_precond_sweep_device(prism_handle h, int32_t sweep, const double* in_d, double* out_d,
+                                   int32_t prepare) {
+    if (!h || !in_d || !out_d) return fail(PRISM_ERR_ARG, "null argument");
+    if (sweep != 0 && sweep != 1) return fail(PRISM_ERR_ARG, "sweep must be 0 or 1");
+    if (in_d == out_d) return fail(PRISM_ERR_ARG, "a sweep cannot run in place");
+    if (!h->P) return fail(PRISM_ERR_NOT_READY, "no preconditioner set");
+    return guarded([&]() -> int {
+        DeviceGuard g(h->info.device);
+        if (!h->P->run_sweep(h->stream, sweep, in_d, out_d, prepare != 0))
+            return fail(PRISM_ERR_UNSUPPORTED, "preconditioner has no single sweeps");
+        return PRISM_OK;
+    });
+}
+
+int32_t prism_precond_sweep_info(prism_handle h, int32_t sweep, uint32_t* n, uint64_t* nnz, uint32_t* value_bytes,
+                                 uint32_t* num_levels) {
+    if (!h) return fail(PRISM_ERR_ARG, "null handle");
+    if (!h->P) return fail(PRISM_ERR_NOT_READY, "no preconditioner set");
+    if (!h->P->sweep_info(sweep, n, nnz, value_bytes, num_levels))
+        return fail(PRISM_ERR_UNSUPPORTED, "preconditioner has no single sweeps");
+    return PRISM_OK;
+}
+
+// ---- solvers -------------------------------------------------------------------
+static int check_opts(prism_handle h, const prism_solve_opts* o) {
+    if (!h) return fail(PRISM_ERR_ARG, "null handle");
+    if (!o) return fail(PRISM_ERR_ARG, "null options");
+    if (!(o->tol > 0.0)) return fail(PRISM_ERR_ARG, "tol must be > 0");
+    if (o->solver != PRISM_SOLVER_FCG && o->solver != PRISM_SOLVER_CG) {
+        return fail(PRISM_ERR_UNSUPPORTED, "solver kind not available");
+    }
+    return PRISM_OK;
+}
+
+int32_t prism_solve_device(prism_handle h, const prism_solve_opts* opts, const double* b_d, double* x_d,
+                           prism_solve_stats* stats) {
+    int rc = check_opts(h, opts);
+    if (rc) return rc;
+    if (!b_d || !x_d) return fail(PRISM_ERR_ARG, "null vector");
+    return guarded([&]() -> int {
+        DeviceGuard g(h->info.device);
+        prism::fcg_solve(*h, *opts, b_d, x_d, stats);
+        return PRISM_OK;
+    });
+}
+
+int32_t prism_solve(prism_handle h, const prism_solve_opts* opts, const double* b, double* x,
+                    prism_solve_stats* stats) {
+    int rc = check_opts(h, opts);
+    if (rc) return rc;
+    if (!b || !x) return fail(PRISM_ERR_ARG, "null vector");
+    return guarded([&]() -> int {
+        DeviceGuard g(h->info.device);
+        const uint32_t n = h->A.n;
+        if (h->xb.size() < n) { h->xb.alloc(n); h->bb.alloc(n); }
+        PRISM_CUDA(cudaMemcpyAsync(h->bb.get(), b, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        PRISM_CUDA(cudaMemcpyAsync(h->xb.get(), x, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        prism::fcg_solve(*h, *opts, h->bb.get(), h->xb.get(), stats);
+        PRISM_CUDA(cudaMemcpyAsync(x, h->xb.get(), n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        PRISM_CUDA(cudaStreamSynchronize(h->stream));
+        return PRISM_OK;
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,535 @@
+// Host-side setup: model problems, bit-exact incomplete factorisations and the
+// exact integer level schedules used by the device sweeps.
+#include "host_setup.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+namespace prism {
+
+// ============================================================================
+// Model problems
+// ============================================================================
+bool laplacian_dims(int32_t nx, int32_t ny, int32_t nz, uint32_t* n, uint32_t* nnz) {
+    if (nx <= 0 || ny <= 0 || nz <= 0) return false;
+    uint64_t N = (uint64_t)nx * ny * nz;
+    if (N >= 0xFFFFFFFFull) return false;
+    // every row has a diagonal plus one entry per existing neighbour
+    uint64_t off = 2ull * ((uint64_t)(nx - 1) * ny * nz + (uint64_t)nx * (ny - 1) * nz + (uint64_t)nx * ny * (nz - 1));
+    uint64_t total = N + off;
+    if (total >= 0xFFFFFFFFull) return false;
+    *n = (uint32_t)N;
+    *nnz = (uint32_t)total;
+    return true;
+}
+
+void laplacian_fill(int32_t nx, int32_t ny, int32_t nz, double ax, double ay, double az, double shift,
+                    uint32_t* rowptr, uint32_t* col, double* val) {
+    // Coefficients as generateLaplacianCOO computes them (ModelProblem.cpp:76-93):
+    // a problem is "2D" as soon as one dimension is 1.
+    int ones = (nx == 1) + (ny == 1) + (nz == 1);
+    const double v = -1.0;
+    const double vxp = v - ax, vxn = v + ax, vyp = v - ay, vyn = v + ay, vzp = v - az, vzn = v + az;
+    double vd = ones > 0 ? 4.0 : 6.0;
+    vd -= shift;
+    const int64_t nxy = (int64_t)nx * ny;
+    const int64_t N = nxy * nz;
+    uint32_t pos = 0;
+    rowptr[0] = 0;
+    for (int64_t ii = 0; ii < N; ++ii) {
+        const int64_t k = ii / nxy;
+        const int64_t i = (ii - k * nxy) / nx;
+        const int64_t j = ii - k * nxy - i * nx;
+        // collect (column, value) then order by column, as transCOO2CSR's per-row sort does
+        int64_t c[7];
+        double w[7];
+        int m = 0;
+        if (k > 0) { c[m] = ii - nxy; w[m++] = vzn; }
+        if (k < nz - 1) { c[m] = ii + nxy; w[m++] = vzp; }
+        if (i > 0) { c[m] = ii - nx; w[m++] = vyn; }
+        if (i < ny - 1) { c[m] = ii + nx; w[m++] = vyp; }
+        if (j > 0) { c[m] = ii - 1; w[m++] = vxn; }
+        if (j < nx - 1) { c[m] = ii + 1; w[m++] = vxp; }
+        c[m] = ii;
+        w[m++] = vd;
+        for (int a = 1; a < m; ++a) {  // insertion sort, stable
+            int64_t kc = c[a];
+            double kv = w[a];
+            int b = a - 1;
+            while (b >= 0 && c[b] > kc) { c[b + 1] = c[b]; w[b + 1] = w[b]; --b; }
+            c[b + 1] = kc;
+            w[b + 1] = kv;
+        }
+        for (int a = 0; a < m; ++a) { col[pos] = (uint32_t)c[a]; val[pos] = w[a]; ++pos; }
+        rowptr[ii + 1] = pos;
+    }
+}
+
+std::string validate_csr(uint32_t n, const uint32_t* rowptr, const uint32_t* col) {
+    if (rowptr[0] != 0) return "rowptr[0] must be 0";
+    for (uint32_t i = 0; i < n; ++i) {
+        if (rowptr[i + 1] < rowptr[i]) return "row offsets must be non-decreasing (row " + std::to_string(i) + ")";
+        for (uint32_t k = rowptr[i]; k < rowptr[i + 1]; ++k) {
+            if (col[k] >= n) return "column index out of range in row " + std::to_string(i);
+            if (k > rowptr[i] && col[k] <= col[k - 1])
+                return "columns must be strictly increasing inside row " + std::to_string(i);
+        }
+    }
+    return std::string();
+}
+
+// ============================================================================
+// Threshold incomplete Cholesky (left-looking, column linked lists)
+// ============================================================================
+namespace {
+constexpr uint32_t kNone = 0xFFFFFFFFu;
+
+// Shared driver of the two left-looking threshold factorisations.  The
+// reference keeps, for every finished column k, a cursor (`next`) to its next
+// unconsumed entry and threads k into the list of the row that entry lives in
+// (`link` doubles as list head for rows not yet reached and as list link for
+// finished columns; lists are LIFO).  Column j gathers its updates by walking
+// the list of row j.  `ldlt` selects the IncompleteLDLT variant (no sqrt,
+// pivot kept in D, unit L^T stored without its diagonal).
+template <typename Low, bool ldlt>
+int left_looking(const CsrHost& A, double thr, CsrT<Low>& Lt, std::vector<double>* D, std::string* err) {
+    const uint32_t n = A.n;
+    std::vector<uint8_t> used(n, 0);
+    std::vector<uint32_t> touched(n);
+    std::vector<double> acc(n, 0.0);
+    std::vector<uint32_t> link(n, kNone);
+    std::vector<uint32_t> next(n, 0);
+    Lt.n = n;
+    Lt.rowptr.assign((size_t)n + 1, 0);
+    Lt.col.clear();
+    Lt.val.clear();
+    Lt.col.reserve(A.nnz() * 4);
+    Lt.val.reserve(A.nnz() * 4);
+    if (ldlt) D->assign(n, 0.0);
+
+    for (uint32_t j = 0; j < n; ++j) {
+        uint32_t cnt = 0;
+        double colThr = 0.0;
+        // lower part of column j of A (row j, symmetric storage)
+        for (uint32_t p = A.rowptr[j]; p < A.rowptr[j + 1]; ++p) {
+            const uint32_t i = A.col[p];
+            const double a = A.val[p];
+            if (i >= j) {
+                colThr += std::fabs(a);
+                if (!used[i]) { acc[i] = 0.0; used[i] = 1; touched[cnt++] = i; }
+                acc[i] += a;
+            }
+        }
+        colThr *= thr;
+        // updates from every finished column k with a non-zero in row j
+        uint32_t k = link[j];
+        while (k != kNone) {
+            uint32_t start = next[k];
+            const double Ljk = (double)Lt.val[start];
+            const double dk = ldlt ? (*D)[k] : 0.0;
+            const uint32_t stop = Lt.rowptr[k + 1];
+            for (uint32_t p = start; p < stop; ++p) {
+                const uint32_t i = Lt.col[p];
+                const double Lik = (double)Lt.val[p];
+                if (!used[i]) { used[i] = 1; acc[i] = 0.0; touched[cnt++] = i; }
+                if (ldlt) acc[i] -= Lik * Ljk * dk;
+                else acc[i] -= Lik * Ljk;
+            }
+            ++start;
+            const uint32_t knext = link[k];
+            if (start < stop) {
+                next[k] = start;
+                const uint32_t i = Lt.col[start];
+                link[k] = link[i];
+                link[i] = k;
+            }
+            k = knext;
+        }
+        double piv = acc[j];
+        if (ldlt) {
+            if (std::fabs(piv) < 1e-15) {
+                if (err) *err = "ILDLT: zero diagonal encountered! Zero diagonal row index is: " + std::to_string(j);
+                return SETUP_ZERO_PIVOT;
+            }
+            (*D)[j] = piv;
+            next[j] = (uint32_t)Lt.col.size();
+        } else {
+            if (piv <= 0.0) {
+                if (err) *err = "The original matrix is not positive definite! (column " + std::to_string(j) + ")";
+                return SETUP_NOT_SPD;
+            }
+            piv = std::sqrt(piv);
+            acc[j] = piv;
+            Lt.val.push_back((Low)piv);
+            Lt.col.push_back(j);
+            next[j] = (uint32_t)Lt.col.size();
+        }
+        std::sort(touched.begin(), touched.begin() + cnt);
+        bool first = true;
+        for (uint32_t q = 0; q < cnt; ++q) {
+            const uint32_t i = touched[q];
+            if (i != j) {
+                double Lij = acc[i];
+                if (std::fabs(Lij) >= colThr) {
+                    if (first) {
+                        first = false;
+                        link[j] = link[i];
+                        link[i] = j;
+                    }
+                    Lij = Lij / piv;
+                    Lt.val.push_back((Low)Lij);
+                    Lt.col.push_back(i);
+                }
+            }
+            used[i] = 0;
+        }
+        Lt.rowptr[j + 1] = (uint32_t)Lt.col.size();
+    }
+    return SETUP_OK;
+}
+
+// Selection of the Ncut largest |a| to the front (SPARSKIT qsplit, as used by
+// include/VectorClass/VectorTools.h:160-203); it also reorders the rest, and
+// the reference calls it even when nothing is dropped, so its exact swap
+// sequence fixes the column order of every ILUT row.
+template <typename T>
+void qsplit_select(T* a, int32_t* ind, int32_t n, int32_t ncut_count) {
+    const int32_t ncut = ncut_count - 1;
+    int32_t first = 0, last = n - 1;
+    if (ncut < first || ncut > last) return;
+    int32_t mid;
+    do {
+        mid = first;
+        const double key = std::fabs((double)a[mid]);
+        for (int32_t j = first + 1; j <= last; ++j) {
+            if (std::fabs((double)a[j]) > key) {
+                ++mid;
+                const double tmp = (double)a[mid];
+                const int32_t itmp = ind[mid];
+                a[mid] = a[j];
+                ind[mid] = ind[j];
+                a[j] = (T)tmp;
+                ind[j] = itmp;
+            }
+        }
+        const double tmp = (double)a[mid];
+        a[mid] = a[first];
+        a[first] = (T)tmp;
+        const int32_t itmp = ind[mid];
+        ind[mid] = ind[first];
+        ind[first] = itmp;
+        if (mid == ncut) break;
+        if (mid > ncut) last = mid - 1;
+        else first = mid + 1;
+    } while (mid != ncut);
+}
+}  // namespace
+
+template <typename Low>
+int ict_factor(const CsrHost& A, double threshold, CsrT<Low>& Lt, std::string* err) {
+    return left_looking<Low, false>(A, threshold, Lt, nullptr, err);
+}
+
+template <typename Low>
+int ildlt_factor(const CsrHost& A, double tol, CsrT<Low>& Lt, std::vector<double>& D, std::string* err) {
+    return left_looking<Low, true>(A, tol, Lt, &D, err);
+}
+
+template <typename Low>
+int ilut_factor(const CsrHost& A, uint32_t lfill, double tol, CsrT<Low>& L, CsrT<Low>& U, std::vector<Low>& Dinv,
+                std::string* err) {
+    const int32_t n = (int32_t)A.n;
+    L.n = U.n = A.n;
+    L.rowptr.assign((size_t)n + 1, 0);
+    U.rowptr.assign((size_t)n + 1, 0);
+    L.col.clear(); L.val.clear(); U.col.clear(); U.val.clear();
+    Dinv.assign(n, (Low)0);
+    std::vector<int32_t> iw(n, -1), jbuf(n);
+    std::vector<Low> wn(n), w(n);
+    for (int32_t i = 0; i < n; ++i) {
+        const uint32_t begin = A.rowptr[i], end = A.rowptr[i + 1];
+        const uint32_t nzcount = end - begin;
+        double tnorm = 0.0;
+        for (uint32_t p = begin; p < end; ++p) tnorm += std::fabs(A.val[p]);
+        if (tnorm < 1e-15) {
+            if (err) *err = "ILUT: zero row encountered! (row " + std::to_string(i) + ")";
+            return SETUP_ZERO_PIVOT;
+        }
+        tnorm /= (double)nzcount;
+        const double tolnorm = tol * tnorm;
+        // split row i of A into the work row: L part at [0, lenl), diagonal at i, U part at (i, i+lenu]
+        int32_t lenu = 0, lenl = 0;
+        jbuf[i] = i;
+        w[i] = (Low)0;
+        iw[i] = i;
+        for (uint32_t p = begin; p < end; ++p) {
+            const int32_t c = (int32_t)A.col[p];
+            const Low t = (Low)A.val[p];
+            if (c < i) {
+                iw[c] = lenl; jbuf[lenl] = c; w[lenl] = t; ++lenl;
+            } else if (c == i) {
+                w[i] = t;
+            } else {
+                ++lenu;
+                const int32_t jpos = i + lenu;
+                iw[c] = jpos; jbuf[jpos] = c; w[jpos] = t;
+            }
+        }
+        // eliminate the L part in increasing column order (selection of the smallest remaining column)
+        for (int32_t jj = 0; jj < lenl; ++jj) {
+            int32_t jrow = jbuf[jj];
+            int32_t jpos = jj;
+            for (int32_t q = jj + 1; q < lenl; ++q)
+                if (jbuf[q] < jrow) { jrow = jbuf[q]; jpos = q; }
+            if (jpos != jj) {
+                const int32_t c = jbuf[jj];
+                jbuf[jj] = jbuf[jpos];
+                jbuf[jpos] = c;
+                iw[jrow] = jj;
+                iw[c] = jpos;
+                const Low t = w[jj];
+                w[jj] = w[jpos];
+                w[jpos] = t;
+            }
+            const Low fact = w[jj] * Dinv[jrow];
+            w[jj] = fact;
+            iw[jrow] = -1;
+            for (uint32_t q = U.rowptr[jrow]; q < U.rowptr[jrow + 1]; ++q) {
+                const int32_t c = (int32_t)U.col[q];
+                const int32_t cpos = iw[c];
+                const Low lxu = -fact * U.val[q];
+                if (std::fabs((double)lxu) < tolnorm && cpos == -1) continue;
+                if (c < i) {
+                    if (cpos == -1) {
+                        jbuf[lenl] = c; iw[c] = lenl; w[lenl] = lxu; ++lenl;
+                    } else {
+                        w[cpos] += lxu;
+                    }
+                } else {
+                    if (cpos == -1 && std::fabs((double)lxu) > tolnorm) {
+                        ++lenu;
+                        const int32_t upos = i + lenu;
+                        jbuf[upos] = c; iw[c] = upos; w[upos] = lxu;
+                    } else if (cpos != -1) {
+                        // (|lxu| == tolnorm exactly with no slot: the reference indexes w[-1]; skipped here)
+                        w[cpos] += lxu;
+                    }
+                }
+            }
+        }
+        iw[i] = -1;
+        for (int32_t q = 0; q < lenu; ++q) iw[jbuf[i + q + 1]] = -1;
+        if (std::fabs((double)w[i]) < 1e-15) {
+            if (err) *err = "ILUT: zero diagonal encountered! Zero diagonal row index is: " + std::to_string(i);
+            return SETUP_ZERO_PIVOT;
+        }
+        Dinv[i] = (Low)1 / w[i];
+        // keep the lfill largest of the L part
+        int32_t len = lenl < (int32_t)lfill ? lenl : (int32_t)lfill;
+        for (int32_t q = 0; q < lenl; ++q) { wn[q] = (Low)std::fabs((double)w[q]); iw[q] = q; }
+        qsplit_select(wn.data(), iw.data(), lenl, len);
+        for (int32_t q = 0; q < len; ++q) {
+            const int32_t jpos = iw[q];
+            L.col.push_back((uint32_t)jbuf[jpos]);
+            L.val.push_back(w[jpos]);
+        }
+        L.rowptr[i + 1] = (uint32_t)L.col.size();
+        for (int32_t q = 0; q < lenl; ++q) iw[q] = -1;
+        // keep the lfill largest of the U part
+        len = lenu < (int32_t)lfill ? lenu : (int32_t)lfill;
+        for (int32_t q = 0; q < lenu; ++q) { wn[q] = (Low)std::fabs((double)w[i + q + 1]); iw[q] = i + q + 1; }
+        qsplit_select(wn.data(), iw.data(), lenu, len);
+        for (int32_t q = 0; q < len; ++q) {
+            const int32_t jpos = iw[q];
+            U.col.push_back((uint32_t)jbuf[jpos]);
+            U.val.push_back(w[jpos]);
+        }
+        U.rowptr[i + 1] = (uint32_t)U.col.size();
+        for (int32_t q = 0; q < lenu; ++q) iw[q] = -1;
+    }
+    return SETUP_OK;
+}
+
+// ============================================================================
+// Sweeps and level schedules
+// ============================================================================
+template <typename V>
+void transpose_csr(uint32_t n, const std::vector<uint32_t>& rowptr, const std::vector<uint32_t>& col,
+                   const std::vector<V>& val, std::vector<uint32_t>& trp, std::vector<uint32_t>& tcol,
+                   std::vector<V>& tval) {
+    const uint64_t nnz = rowptr[n];
+    trp.assign((size_t)n + 1, 0);
+    tcol.resize(nnz);
+    tval.resize(nnz);
+    for (uint64_t k = 0; k < nnz; ++k) trp[col[k] + 1]++;
+    for (uint32_t i = 0; i < n; ++i) trp[i + 1] += trp[i];
+    std::vector<uint32_t> fill(trp.begin(), trp.end() - 1);
+    for (uint32_t r = 0; r < n; ++r)
+        for (uint32_t k = rowptr[r]; k < rowptr[r + 1]; ++k) {
+            const uint32_t c = col[k];
+            tcol[fill[c]] = r;
+            tval[fill[c]] = val[k];
+            fill[c]++;
+        }
+}
+
+template <typename Low>
+void build_sweep(uint32_t n, const std::vector<uint32_t>& rowptr, const std::vector<uint32_t>& col,
+                 const std::vector<Low>& val, const std::vector<double>* diag, int op, bool lower,
+                 Sweep<Low>& out) {
+    std::vector<uint32_t> level(n, 0);
+    uint32_t maxLevel = 0;
+    if (lower) {
+        for (uint32_t r = 0; r < n; ++r) {
+            uint32_t l = 0;
+            for (uint32_t k = rowptr[r]; k < rowptr[r + 1]; ++k) l = std::max(l, level[col[k]] + 1);
+            level[r] = l;
+            maxLevel = std::max(maxLevel, l);
+        }
+    } else {
+        for (uint32_t r = n; r-- > 0;) {
+            uint32_t l = 0;
+            for (uint32_t k = rowptr[r]; k < rowptr[r + 1]; ++k) l = std::max(l, level[col[k]] + 1);
+            level[r] = l;
+            maxLevel = std::max(maxLevel, l);
+        }
+    }
+    out.n = n;
+    out.op = op;
+    out.lower = lower;
+    out.num_levels = n ? maxLevel + 1 : 0;
+    out.level_ptr.assign((size_t)out.num_levels + 1, 0);
+    for (uint32_t r = 0; r < n; ++r) out.level_ptr[level[r] + 1]++;
+    for (uint32_t l = 0; l < out.num_levels; ++l) out.level_ptr[l + 1] += out.level_ptr[l];
+    out.order.resize(n);
+    {
+        std::vector<uint32_t> fill(out.level_ptr.begin(), out.level_ptr.end() - 1);
+        for (uint32_t r = 0; r < n; ++r) out.order[fill[level[r]]++] = r;
+    }
+    out.rowptr.assign((size_t)n + 1, 0);
+    for (uint32_t p = 0; p < n; ++p) {
+        const uint32_t r = out.order[p];
+        out.rowptr[p + 1] = out.rowptr[p] + (rowptr[r + 1] - rowptr[r]);
+    }
+    out.col.resize(out.rowptr[n]);
+    out.val.resize(out.rowptr[n]);
+    out.diag.assign(n, 1.0);
+    for (uint32_t p = 0; p < n; ++p) {
+        const uint32_t r = out.order[p];
+        std::copy(col.begin() + rowptr[r], col.begin() + rowptr[r + 1], out.col.begin() + out.rowptr[p]);
+        std::copy(val.begin() + rowptr[r], val.begin() + rowptr[r + 1], out.val.begin() + out.rowptr[p]);
+        if (diag) out.diag[p] = (*diag)[r];
+    }
+}
+
+// ============================================================================
+// Triangular preconditioners in device layout
+// ============================================================================
+namespace {
+template <typename Low>
+void widen_csr(const CsrT<Low>& in, CsrT<double>& out) {
+    out.n = in.n;
+    out.rowptr = in.rowptr;
+    out.col = in.col;
+    out.val.assign(in.val.begin(), in.val.end());
+}
+
+template <typename Low>
+int build_tri_t(int kind, const CsrHost& A, double tol, uint32_t lfill, HostFactor& F, Sweep<Low>& lo,
+                Sweep<Low>& up, std::string* err) {
+    const uint32_t n = A.n;
+    if (kind == 1) {
+        // IC: L^T rows hold the diagonal first.  Lower sweep = gather over L
+        // (transpose of the strictly upper part), upper sweep = gather over L^T.
+        CsrT<Low> Lt;
+        int rc = ict_factor<Low>(A, tol, Lt, err);
+        if (rc) return rc;
+        std::vector<uint32_t> urp(n + 1, 0), ucol;
+        std::vector<Low> uval;
+        std::vector<double> dg(n);
+        ucol.reserve(Lt.nnz());
+        uval.reserve(Lt.nnz());
+        for (uint32_t i = 0; i < n; ++i) {
+            dg[i] = (double)Lt.val[Lt.rowptr[i]];
+            for (uint32_t k = Lt.rowptr[i] + 1; k < Lt.rowptr[i + 1]; ++k) {
+                ucol.push_back(Lt.col[k]);
+                uval.push_back(Lt.val[k]);
+            }
+            urp[i + 1] = (uint32_t)ucol.size();
+        }
+        std::vector<uint32_t> lrp, lcol;
+        std::vector<Low> lval;
+        transpose_csr<Low>(n, urp, ucol, uval, lrp, lcol, lval);
+        build_sweep<Low>(n, lrp, lcol, lval, &dg, SWEEP_DIV, true, lo);
+        build_sweep<Low>(n, urp, ucol, uval, &dg, SWEEP_DIV, false, up);
+        F.mnnz = Lt.nnz() * 2 + n;  // IncompleteCholesky.cpp:245
+        widen_csr(Lt, F.f0);
+        return 0;
+    }
+    if (kind == 3) {
+        // ILDLT: unit L^T without diagonal, D separate; D^{-1} folded into the upper sweep.
+        CsrT<Low> Lt;
+        std::vector<double> D;
+        int rc = ildlt_factor<Low>(A, tol, Lt, D, err);
+        if (rc) return rc;
+        std::vector<uint32_t> lrp, lcol;
+        std::vector<Low> lval;
+        transpose_csr<Low>(n, Lt.rowptr, Lt.col, Lt.val, lrp, lcol, lval);
+        build_sweep<Low>(n, lrp, lcol, lval, nullptr, SWEEP_NONE, true, lo);
+        build_sweep<Low>(n, Lt.rowptr, Lt.col, Lt.val, &D, SWEEP_PREDIV, false, up);
+        F.mnnz = Lt.nnz() * 2 + n;  // IncompleteLDLT.cpp:185
+        widen_csr(Lt, F.f0);
+        F.diag = D;
+        return 0;
+    }
+    if (kind == 2) {
+        CsrT<Low> L, U;
+        std::vector<Low> Dinv;
+        int rc = ilut_factor<Low>(A, lfill, tol, L, U, Dinv, err);
+        if (rc) return rc;
+        std::vector<double> dd(Dinv.begin(), Dinv.end());
+        build_sweep<Low>(n, L.rowptr, L.col, L.val, nullptr, SWEEP_NONE, true, lo);
+        build_sweep<Low>(n, U.rowptr, U.col, U.val, &dd, SWEEP_MUL, false, up);
+        F.mnnz = L.nnz() + U.nnz() + n;  // IncompleteLU.cpp:264
+        widen_csr(L, F.f0);
+        widen_csr(U, F.f1);
+        F.diag = dd;
+        return 0;
+    }
+    if (err) *err = "unknown triangular preconditioner kind " + std::to_string(kind);
+    return SETUP_BAD_INPUT;
+}
+}  // namespace
+
+int build_triangular(int kind, const CsrHost& A, double tol, uint32_t lfill, bool fp32, HostFactor& out,
+                     std::string* err) {
+    out = HostFactor();
+    out.kind = kind;
+    out.fp32 = fp32;
+    if (fp32) return build_tri_t<float>(kind, A, tol, lfill, out, out.lower32, out.upper32, err);
+    return build_tri_t<double>(kind, A, tol, lfill, out, out.lower64, out.upper64, err);
+}
+
+// ---- explicit instantiations ------------------------------------------------
+template int ict_factor<double>(const CsrHost&, double, CsrT<double>&, std::string*);
+template int ict_factor<float>(const CsrHost&, double, CsrT<float>&, std::string*);
+template int ildlt_factor<double>(const CsrHost&, double, CsrT<double>&, std::vector<double>&, std::string*);
+template int ildlt_factor<float>(const CsrHost&, double, CsrT<float>&, std::vector<double>&, std::string*);
+template int ilut_factor<double>(const CsrHost&, uint32_t, double, CsrT<double>&, CsrT<double>&,
+                                 std::vector<double>&, std::string*);
+template int ilut_factor<float>(const CsrHost&, uint32_t, double, CsrT<float>&, CsrT<float>&,
+                                std::vector<float>&, std::string*);
+template void transpose_csr<double>(uint32_t, const std::vector<uint32_t>&, const std::vector<uint32_t>&,
+                                    const std::vector<double>&, std::vector<uint32_t>&, std::vector<uint32_t>&,
+                                    std::vector<double>&);
+template void transpose_csr<float>(uint32_t, const std::vector<uint32_t>&, const std::vector<uint32_t>&,
+                                   const std::vector<float>&, std::vector<uint32_t>&, std::vector<uint32_t>&,
+                                   std::vector<float>&);
+template void build_sweep<double>(uint32_t, const std::vector<uint32_t>&, const std::vector<uint32_t>&,
+                                  const std::vector<double>&, const std::vector<double>*, int, bool, Sweep<double>&);
+template void build_sweep<float>(uint32_t, const std::vector<uint32_t>&, const std::vector<uint32_t>&,
+                                 const std::vector<float>&, const std::vector<double>*, int, bool, Sweep<float>&);
+
+}  // namespace prism

@@ -1,0 +1,297 @@
+// Device-resident operator, triangular preconditioners and the FCG driver.
+#include <cmath>
+#include <cstring>
+
+#include "../../include/prism_solve.h"
+#include "kernels.cuh"
+#include "solve.cuh"
+
+namespace prism {
+
+std::atomic<uint64_t>& launch_counter() {
+    static std::atomic<uint64_t> c{0};
+    return c;
+}
+
+namespace {
+constexpr unsigned long long kWaitNs = 1000000000ull;  // 1 s per dependency wait
+constexpr int kSpmvG = 8;                              // lanes per row in the CSR SpMV
+
+int vec_grid(const Handle& h, uint32_t n) {
+    long want = ((long)n + kBlock - 1) / kBlock;
+    long cap = (long)h.info.sms * 4;
+    if (want < 1) want = 1;
+    return (int)(want < cap ? want : cap);
+}
+
+void launch_fill(cudaStream_t st, const Handle& h, uint32_t n, double* p) {
+    if (!n) return;
+    k_fill_pending<<<vec_grid(h, n), kBlock, 0, st>>>(n, reinterpret_cast<unsigned long long*>(p));
+    PRISM_LAUNCHED();
+}
+
+void launch_sweep(const Handle& h, cudaStream_t st, const DevSweep& s, const double* in, double* out) {
+    if (!s.n) return;
+    long want = ((long)s.n * 32 + kBlock - 1) / kBlock;
+    long cap = (long)h.info.sms * h.info.sweep_blocks_per_sm;
+    int grid = (int)(want < cap ? want : cap);
+    void* fn = nullptr;
+    if (s.fp32) {
+        switch (s.op) {
+            case SWEEP_DIV: fn = (void*)k_sweep<float, OP_DIV>; break;
+            case SWEEP_MUL: fn = (void*)k_sweep<float, OP_MUL>; break;
+            case SWEEP_NONE: fn = (void*)k_sweep<float, OP_NONE>; break;
+            default: fn = (void*)k_sweep<float, OP_PREDIV>; break;
+        }
+    } else {
+        switch (s.op) {
+            case SWEEP_DIV: fn = (void*)k_sweep<double, OP_DIV>; break;
+            case SWEEP_MUL: fn = (void*)k_sweep<double, OP_MUL>; break;
+            case SWEEP_NONE: fn = (void*)k_sweep<double, OP_NONE>; break;
+            default: fn = (void*)k_sweep<double, OP_PREDIV>; break;
+        }
+    }
+    uint32_t n = s.n;
+    const uint32_t* order = s.order.get();
+    const uint32_t* rowptr = s.rowptr.get();
+    const uint32_t* col = s.col.get();
+    const void* val = s.fp32 ? (const void*)s.val32.get() : (const void*)s.val64.get();
+    const double* diag = s.diag.get();
+    int* status = h.status.get();
+    unsigned long long wait = kWaitNs;
+    void* args[] = {&n, &order, &rowptr, &col, &val, &diag, &in, &out, &status, &wait};
+    // Cooperative launch: all blocks co-resident, which the level-order
+    // progress argument of k_sweep relies on.
+    PRISM_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kBlock), args, 0, st));
+    PRISM_LAUNCHED();
+}
+}  // namespace
+
+// ============================================================================
+// Handle
+// ============================================================================
+void init_device_info(DeviceInfo& info, int device) {
+    info.device = device;
+    PRISM_CUDA(cudaDeviceGetAttribute(&info.sms, cudaDevAttrMultiProcessorCount, device));
+    int occ = 0, occ2 = 0;
+    PRISM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_sweep<double, OP_DIV>, kBlock, 0));
+    PRISM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, k_sweep<float, OP_DIV>, kBlock, 0));
+    occ = occ < occ2 ? occ : occ2;
+    // a fraction of the co-resident capacity: enough warps to cover a wavefront,
+    // few enough pollers to leave L2 bandwidth to the producers
+    info.sweep_blocks_per_sm = occ < 4 ? (occ > 0 ? occ : 1) : 4;
+}
+
+Handle::~Handle() {
+    P.reset();
+    if (pinned) cudaFreeHost(pinned);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (own_stream && stream) cudaStreamDestroy(stream);
+}
+
+void Handle::ensure_workspace() {
+    const uint32_t n = A.n;
+    if (r.size() < n) {
+        r.alloc(n); w.alloc(n); d.alloc(n); v.alloc(n); y.alloc(n);
+    }
+}
+
+void Handle::spmv(const double* x, double* yout, int ndot, const double* z, const double* q, int scalar) {
+    const uint32_t n = A.n;
+    if (!n) return;
+    long want = ((long)n * kSpmvG + kBlock - 1) / kBlock;
+    long cap = (long)info.sms * 8;
+    int grid = (int)(want < cap ? want : cap);
+    if (grid > Reducer::kMaxGrid) grid = Reducer::kMaxGrid;
+    ReduceSlot slot = red.slot(scalar);
+    if (ndot == 0)
+        k_spmv<kSpmvG, 0><<<grid, kBlock, 0, stream>>>(n, A.rowptr.get(), A.col.get(), A.val.get(), x, yout, z, q, slot);
+    else if (ndot == 1)
+        k_spmv<kSpmvG, 1><<<grid, kBlock, 0, stream>>>(n, A.rowptr.get(), A.col.get(), A.val.get(), x, yout, z, q, slot);
+    else
+        k_spmv<kSpmvG, 2><<<grid, kBlock, 0, stream>>>(n, A.rowptr.get(), A.col.get(), A.val.get(), x, yout, z, q, slot);
+    PRISM_LAUNCHED();
+}
+
+void Handle::check_status() {
+    int s = 0;
+    PRISM_CUDA(cudaMemcpyAsync(&s, status.get(), sizeof(int), cudaMemcpyDeviceToHost, stream));
+    PRISM_CUDA(cudaStreamSynchronize(stream));
+    if (s != 0) {
+        PRISM_CUDA(cudaMemsetAsync(status.get(), 0, sizeof(int), stream));
+        throw Error(s, "device-side wait ran out of time in a triangular sweep (status " + std::to_string(s) + ")");
+    }
+}
+
+// ============================================================================
+// Sweeps and triangular preconditioners
+// ============================================================================
+template <typename Low>
+void DevSweep::upload(const Sweep<Low>& s, cudaStream_t st) {
+    n = s.n;
+    num_levels = s.num_levels;
+    op = s.op;
+    fp32 = std::is_same<Low, float>::value;
+    order.upload(s.order.data(), s.order.size(), st);
+    rowptr.upload(s.rowptr.data(), s.rowptr.size(), st);
+    col.upload(s.col.data(), s.col.size(), st);
+    diag.upload(s.diag.data(), s.diag.size(), st);
+    if (fp32) val32.upload(reinterpret_cast<const float*>(s.val.data()), s.val.size(), st);
+    else val64.upload(reinterpret_cast<const double*>(s.val.data()), s.val.size(), st);
+    // keep at least one element so kernels always get valid pointers
+    if (col.size() == 0) col.alloc(1);
+    if (fp32 && val32.size() == 0) val32.alloc(1);
+    if (!fp32 && val64.size() == 0) val64.alloc(1);
+    PRISM_CUDA(cudaStreamSynchronize(st));
+}
+
+TriangularPrecond::TriangularPrecond(Handle& h, std::shared_ptr<const HostFactor> f) : h_(h), f_(std::move(f)) {
+    if (f_->fp32) {
+        lower_.upload(f_->lower32, h_.stream);
+        upper_.upload(f_->upper32, h_.stream);
+    } else {
+        lower_.upload(f_->lower64, h_.stream);
+        upper_.upload(f_->upper64, h_.stream);
+    }
+}
+
+void TriangularPrecond::apply(cudaStream_t st, const double* in, double* out) {
+    const uint32_t n = h_.A.n;
+    if (tmp_.size() < n) tmp_.alloc(n);
+    launch_fill(st, h_, n, tmp_.get());
+    if (in != out) launch_fill(st, h_, n, out);
+    launch_sweep(h_, st, lower_, in, tmp_.get());
+    if (in == out) launch_fill(st, h_, n, out);
+    launch_sweep(h_, st, upper_, tmp_.get(), out);
+}
+
+bool TriangularPrecond::run_sweep(cudaStream_t st, int sweep, const double* in, double* out, bool prepare) {
+    const DevSweep& s = sweep == 0 ? lower_ : upper_;
+    if (prepare) launch_fill(st, h_, s.n, out);
+    launch_sweep(h_, st, s, in, out);
+    return true;
+}
+
+bool TriangularPrecond::sweep_info(int sweep, uint32_t* n, uint64_t* nnz, uint32_t* vbytes, uint32_t* levels) const {
+    const DevSweep& s = sweep == 0 ? lower_ : upper_;
+    if (n) *n = s.n;
+    if (nnz) *nnz = s.fp32 ? s.val32.size() : s.val64.size();
+    if (vbytes) *vbytes = s.fp32 ? 4 : 8;
+    if (levels) *levels = s.num_levels;
+    return true;
+}
+
+int export_host_factor(const HostFactor& f, int which, uint32_t* n, uint64_t* nnz, uint32_t* rowptr, uint32_t* col,
+                       double* val, double* diag) {
+    if (which != 0 && !(which == 1 && f.kind == PRISM_PRECOND_ILUT)) return PRISM_ERR_ARG;
+    const CsrT<double>& m = which == 0 ? f.f0 : f.f1;
+    if (n) *n = m.n;
+    if (nnz) *nnz = m.nnz();
+    if (rowptr) std::memcpy(rowptr, m.rowptr.data(), m.rowptr.size() * sizeof(uint32_t));
+    if (col) std::memcpy(col, m.col.data(), m.col.size() * sizeof(uint32_t));
+    if (val) std::memcpy(val, m.val.data(), m.val.size() * sizeof(double));
+    if (diag && !f.diag.empty()) std::memcpy(diag, f.diag.data(), f.diag.size() * sizeof(double));
+    return 0;
+}
+
+int TriangularPrecond::export_factor(int which, uint32_t* n, uint64_t* nnz, uint32_t* rowptr, uint32_t* col,
+                                     double* val, double* diag) const {
+    return export_host_factor(*f_, which, n, nnz, rowptr, col, val, diag);
+}
+
+// ============================================================================
+// Flexible / normal preconditioned CG  (CG<double>::solve, CG.cpp:34-83)
+//
+// Same recurrence, same stopping test on the recursive residual, same
+// iteration count convention (numIter = m + 1).  The reference recomputes
+// v = A d at the top of every iteration (CG.cpp:68) although d has not
+// changed since v = A d at the end of the previous one (CG.cpp:75); the
+// SpMV and the d.v reduction are deterministic here, so that product and its
+// d.v are reused instead of recomputed: one SpMV per iteration, not two.
+// ============================================================================
+void fcg_solve(Handle& h, const prism_solve_opts& o, const double* b, double* x, prism_solve_stats* st) {
+    const uint32_t n = h.A.n;
+    h.ensure_workspace();
+    cudaStream_t s = h.stream;
+    const bool flexible = o.solver == PRISM_SOLVER_FCG;
+    Precond* P = h.P.get();
+    double* r = h.r.get();
+    double* w = h.w.get();
+    double* d = h.d.get();
+    double* v = h.v.get();
+    double* y = h.y.get();
+    double* sc = h.red.scalars.get();
+    const int vg = vec_grid(h, n);
+    uint32_t applies = 0, spmvs = 0;
+
+    PRISM_CUDA(cudaEventRecord(h.ev0, s));
+    // r = b - A x ; Σ b²
+    h.spmv(x, y);
+    ++spmvs;
+    k_residual<<<vg, kBlock, 0, s>>>(n, b, y, r, h.red.slot(SC_BB));
+    PRISM_LAUNCHED();
+    // w = M^{-1} r ; d = w
+    if (P) { P->apply(s, r, w); ++applies; }
+    else PRISM_CUDA(cudaMemcpyAsync(w, r, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    PRISM_CUDA(cudaMemcpyAsync(d, w, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    // v = A d ; Σ v·d , Σ d·r
+    h.spmv(d, v, 2, d, r, SC_DV);
+    ++spmvs;
+    // x += a d ; r -= a v ; Σ r²
+    k_fcg_step<<<vg, kBlock, 0, s>>>(n, x, r, d, v, sc + SC_DR, sc + SC_DV, h.red.slot(SC_RR));
+    PRISM_LAUNCHED();
+
+    PRISM_CUDA(cudaMemcpyAsync(h.pinned, sc, kNumScalars * sizeof(double), cudaMemcpyDeviceToHost, s));
+    h.check_status();
+    const double norm_b = std::sqrt(h.pinned[SC_BB]);
+    uint32_t m = o.max_iter;
+    double norm = -1.0;
+    bool converged = false;
+    for (uint32_t i = 1; i < o.max_iter; ++i) {
+        if (i > 1) {
+            PRISM_CUDA(cudaMemcpyAsync(h.pinned + SC_RR, sc + SC_RR, sizeof(double), cudaMemcpyDeviceToHost, s));
+            h.check_status();
+        }
+        norm = std::sqrt(h.pinned[SC_RR]) / norm_b;
+        if (!std::isfinite(norm)) throw Error(PRISM_ERR_NONFINITE, "non-finite residual norm in CG iteration " + std::to_string(i));
+        if (norm < o.tol) {
+            converged = true;
+            m = i;
+            break;
+        }
+        if (flexible && P) { P->apply(s, r, w); ++applies; }
+        else PRISM_CUDA(cudaMemcpyAsync(w, r, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        // v still holds A d and sc[DV] its d.v: c = (w.v)/(d.v); d = w - c d; Σ d·r
+        k_dot<<<vg, kBlock, 0, s>>>(n, w, v, h.red.slot(SC_WV));
+        PRISM_LAUNCHED();
+        k_fcg_direction<<<vg, kBlock, 0, s>>>(n, w, d, r, sc + SC_WV, sc + SC_DV, h.red.slot(SC_DR2));
+        PRISM_LAUNCHED();
+        // v = A d ; Σ v·d
+        h.spmv(d, v, 1, d, nullptr, SC_DV);
+        ++spmvs;
+        k_fcg_step<<<vg, kBlock, 0, s>>>(n, x, r, d, v, sc + SC_DR2, sc + SC_DV, h.red.slot(SC_RR));
+        PRISM_LAUNCHED();
+    }
+    // true FP64 residual
+    h.spmv(x, y);
+    ++spmvs;
+    k_residual<<<vg, kBlock, 0, s>>>(n, b, y, nullptr, h.red.slot(SC_BB));
+    PRISM_LAUNCHED();
+    PRISM_CUDA(cudaEventRecord(h.ev1, s));
+    PRISM_CUDA(cudaMemcpyAsync(h.pinned, sc, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    h.check_status();
+    float ms = 0.f;
+    PRISM_CUDA(cudaEventElapsedTime(&ms, h.ev0, h.ev1));
+    if (st) {
+        st->num_iter = (int32_t)(m + 1);
+        st->converged = converged;
+        st->final_error = norm;
+        st->true_rel_residual = std::sqrt(h.pinned[SC_RES]) / std::sqrt(h.pinned[SC_BB]);
+        st->precond_applies = applies;
+        st->spmv_count = spmvs;
+        st->device_ms = ms;
+    }
+}
+
+}  // namespace prism

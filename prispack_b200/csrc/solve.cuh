@@ -1,0 +1,142 @@
+// Device-resident operator, preconditioners and Krylov solvers behind the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/prism_solve.h"
+#include "device_common.cuh"
+#include "host_setup.hpp"
+
+namespace prism {
+
+// Per-device launch geometry, looked up once per handle.
+struct DeviceInfo {
+    int device = 0;
+    int sms = 148;
+    int sweep_blocks_per_sm = 1;   // co-resident k_sweep blocks (cooperative launch bound)
+};
+
+// Reduction scratch shared by all kernels of one stream (they run serially).
+struct Reducer {
+    DevBuf<double> partial;     // [kMaxGrid * 2]
+    DevBuf<unsigned> ticket;    // [1]
+    DevBuf<double> scalars;     // [kNumScalars]
+    static constexpr int kMaxGrid = 4096;
+    ReduceSlot slot(int scalar) const { return ReduceSlot{partial.get(), ticket.get(), scalars.get() + scalar}; }
+};
+
+// Scalar slots.
+// Sweep operation codes shared with the kernels.
+
+enum Scalar : int {
+    SC_BB = 0, SC_RES = 1,   // written together by k_residual: Σ b², Σ (b - y)²
+    SC_RR = 2,
+    SC_WV = 3,
+    SC_DV = 4, SC_DR = 5,    // written together by k_spmv<.,2>: Σ v·d, Σ d·r
+    SC_TMP = 6, SC_TMP2 = 7,
+    SC_DR2 = 8,
+    kNumScalars = 16
+};
+
+struct DeviceCsr {
+    uint32_t n = 0;
+    uint64_t nnz = 0;
+    DevBuf<uint32_t> rowptr, col;
+    DevBuf<double> val;
+};
+
+// One triangular sweep resident on the device (see build_sweep for the layout).
+struct DevSweep {
+    uint32_t n = 0, num_levels = 0;
+    int op = SWEEP_NONE;
+    bool fp32 = false;
+    DevBuf<uint32_t> order, rowptr, col;
+    DevBuf<double> val64, diag;
+    DevBuf<float> val32;
+    template <typename Low>
+    void upload(const Sweep<Low>& s, cudaStream_t st);
+};
+
+class Precond {
+  public:
+    virtual ~Precond() = default;
+    virtual int kind() const = 0;
+    virtual uint64_t mnnz() const = 0;
+    // out = M^{-1} in; in != out not required.
+    virtual void apply(cudaStream_t st, const double* in, double* out) = 0;
+    virtual uint32_t levels(int sweep) const { (void)sweep; return 0; }
+    // one sweep alone (diagnostics / kernel timing); returns false if not a sweep-based preconditioner
+    virtual bool run_sweep(cudaStream_t st, int sweep, const double* in, double* out, bool prepare) {
+        (void)st; (void)sweep; (void)in; (void)out; (void)prepare;
+        return false;
+    }
+    virtual bool sweep_info(int sweep, uint32_t* n, uint64_t* nnz, uint32_t* vbytes, uint32_t* levels) const {
+        (void)sweep; (void)n; (void)nnz; (void)vbytes; (void)levels;
+        return false;
+    }
+    // factor export (parity checks)
+    virtual int export_factor(int which, uint32_t* n, uint64_t* nnz, uint32_t* rowptr, uint32_t* col, double* val,
+                              double* diag) const {
+        (void)which; (void)n; (void)nnz; (void)rowptr; (void)col; (void)val; (void)diag;
+        return 9;
+    }
+};
+
+struct Handle;
+
+// IC / ILDLT / ILUT: two sweeps on the device (ILDLT's D^{-1} is folded into
+// its upper sweep).  Built from a host factor, which it keeps for export.
+class TriangularPrecond : public Precond {
+  public:
+    TriangularPrecond(Handle& h, std::shared_ptr<const HostFactor> f);
+    int kind() const override { return f_->kind; }
+    uint64_t mnnz() const override { return f_->mnnz; }
+    void apply(cudaStream_t st, const double* in, double* out) override;
+    uint32_t levels(int sweep) const override { return sweep == 0 ? lower_.num_levels : upper_.num_levels; }
+    int export_factor(int which, uint32_t* n, uint64_t* nnz, uint32_t* rowptr, uint32_t* col, double* val,
+                      double* diag) const override;
+    bool run_sweep(cudaStream_t st, int sweep, const double* in, double* out, bool prepare) override;
+    bool sweep_info(int sweep, uint32_t* n, uint64_t* nnz, uint32_t* vbytes, uint32_t* levels) const override;
+
+  private:
+    Handle& h_;
+    std::shared_ptr<const HostFactor> f_;
+    DevSweep lower_, upper_;
+    DevBuf<double> tmp_;
+};
+
+// Factor export shared by the device preconditioner and the host-only factor object.
+int export_host_factor(const HostFactor& f, int which, uint32_t* n, uint64_t* nnz, uint32_t* rowptr, uint32_t* col,
+                       double* val, double* diag);
+
+struct Handle {
+    DeviceInfo info;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    CsrHost A_host;
+    DeviceCsr A;
+    std::unique_ptr<Precond> P;
+    Reducer red;
+    DevBuf<int> status;            // device status word of the bounded waits
+    DevBuf<double> r, w, d, v, y;  // Krylov workspace (n each)
+    DevBuf<double> xb, bb;         // host-pointer API staging
+    double* pinned = nullptr;      // host mirror of scalars (pinned)
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+    ~Handle();
+    void spmv(const double* x, double* y, int ndot = 0, const double* z = nullptr, const double* q = nullptr,
+              int scalar = 0);
+    void check_status();           // synchronises; throws on a raised device status
+    void ensure_workspace();
+};
+
+// Queries SM count and the co-resident capacity of the sweep kernel.
+void init_device_info(DeviceInfo& info, int device);
+
+void fcg_solve(Handle& h, const prism_solve_opts& o, const double* b, double* x, prism_solve_stats* st);
+
+}  // namespace prism

@@ -1,0 +1,125 @@
+"""Generates the golden fixtures in this directory from the reference itself.
+
+Runs the reference's own CPU classes (compiled from its sources by
+``oracle/Makefile`` target ``ref`` into ``oracle/_ref/libprism_ref.so``, the
+parity build) on seeded model problems and stores their outputs:
+
+* CSR arrays of generateLaplacianCSR,
+* stored factor arrays of IncompleteCholesky / IncompleteLDLT / IncompleteLU
+  (both <double,double> and <float,double>), full arrays for small cases and
+  SHA-256 digests for the 64x64 case,
+* MInvSolve outputs on a seeded vector,
+* CG (FlexibleCG, NormalCG) and GMRES (FlexibleGMRES with restart) results:
+  iteration count, reported error, convergence flag and solution.
+
+Usage (needs the reference sources, i.e. only where oracle/_ref was built):
+    make -C oracle ref && python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.abspath(os.path.join(HERE, "..", "..")))
+
+from oracle import ref  # noqa: E402
+
+# (name, (nx, ny, nz, alphax, alphay, alphaz, shift), symmetric, full arrays?)
+CASES = [
+    ("lap2d_8", (8, 8, 1, 0.0, 0.0, 0.0, 0.0), True, True),
+    ("lap3d_6", (6, 6, 6, 0.0, 0.0, 0.0, 0.0), True, True),
+    ("conv2d_16", (16, 16, 1, 0.3, -0.2, 0.0, 0.0), False, True),
+    ("lap2d_64", (64, 64, 1, 0.0, 0.0, 0.0, 0.0), True, False),
+]
+SEED = 20241116
+
+
+def digest(*arrays) -> str:
+    h = hashlib.sha256()
+    for a in arrays:
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()
+
+
+def rhs(n: int, seed: int) -> np.ndarray:
+    return np.random.default_rng(seed).uniform(-1.0, 1.0, n)
+
+
+def main():
+    if not ref.available():
+        raise SystemExit("oracle/_ref/libprism_ref.so not built: run `make -C oracle ref` where the reference exists")
+    manifest = {}
+    for name, grid, sym, full in CASES:
+        A = ref.RefCSR.laplacian(*grid)
+        rp, ci, v = A.arrays()
+        n = len(rp) - 1
+        b = rhs(n, SEED)
+        probe = rhs(n, SEED + 1)
+        out = {"rowptr": rp, "col": ci, "val": v, "b": b, "probe": probe}
+        meta = {"grid": grid, "n": n, "nnz": int(rp[-1]), "A_sha": digest(rp, ci, v), "precond": {}}
+        precs = []
+        if sym:
+            precs += [("ic_1e-3", ref.KIND_IC, 1e-3, 0), ("ic_1e-2", ref.KIND_IC, 1e-2, 0),
+                      ("ic_0", ref.KIND_IC, 0.0, 0), ("ildlt_1e-3", ref.KIND_ILDLT, 1e-3, 0)]
+        precs += [("ilut_20_1e-2", ref.KIND_ILUT, 1e-2, 20), ("ilut_5_1e-3", ref.KIND_ILUT, 1e-3, 5)]
+        for pname, kind, tol, lfill in precs:
+            for low in (False, True):
+                key = f"{pname}_{'fp32' if low else 'fp64'}"
+                P = ref.RefPrecond(A, kind, low, tol, lfill)
+                rc = P.setup()
+                if rc != 0:
+                    meta["precond"][key] = {"setup_rc": rc}
+                    continue
+                f0 = P.factor(0)
+                entry = {"setup_rc": 0, "mnnz": P.mnnz(), "kind": kind, "tol": tol, "lfill": lfill,
+                         "f0_sha": digest(f0[0], f0[1], f0[2]), "nnz0": int(f0[0][-1])}
+                if kind == ref.KIND_ILDLT:
+                    entry["diag_sha"] = digest(f0[3])
+                if kind == ref.KIND_ILUT:
+                    f1 = P.factor(1)
+                    entry["f1_sha"] = digest(f1[0], f1[1], f1[2])
+                    entry["diag_sha"] = digest(f1[3])
+                    entry["nnz1"] = int(f1[0][-1])
+                if full:
+                    out[f"{key}.f0_rowptr"], out[f"{key}.f0_col"], out[f"{key}.f0_val"] = f0[0], f0[1], f0[2]
+                    if kind == ref.KIND_ILDLT:
+                        out[f"{key}.diag"] = f0[3]
+                    if kind == ref.KIND_ILUT:
+                        out[f"{key}.f1_rowptr"], out[f"{key}.f1_col"], out[f"{key}.f1_val"] = f1[0], f1[1], f1[2]
+                        out[f"{key}.diag"] = f1[3]
+                out[f"{key}.apply"] = P.apply(probe)
+                # solvers
+                if sym and kind in (ref.KIND_IC, ref.KIND_ILDLT):
+                    for flex in (True, False):
+                        x, it, err, conv = ref.cg_solve(A, P, b, tol=1e-8, maxit=1000, flexible=flex)
+                        tag = f"{key}.cg_{'flex' if flex else 'normal'}"
+                        out[f"{tag}.x"] = x
+                        entry[tag] = {"iters": it, "err": err, "conv": conv}
+                x, it, err, conv = ref.gmres_solve(A, P, b, tol=1e-8, restart=20, flexible=True)
+                out[f"{key}.fgmres20.x"] = x
+                entry[f"{key}.fgmres20"] = {"iters": it, "err": err, "conv": conv}
+                meta["precond"][key] = entry
+        # unpreconditioned solvers
+        if sym:
+            x, it, err, conv = ref.cg_solve(A, None, b, tol=1e-8, maxit=1000, flexible=True)
+            out["none.cg.x"] = x
+            meta["none.cg"] = {"iters": it, "err": err, "conv": conv}
+        x, it, err, conv = ref.gmres_solve(A, None, b, tol=1e-8, restart=30, flexible=False)
+        out["none.gmres30.x"] = x
+        meta["none.gmres30"] = {"iters": it, "err": err, "conv": conv}
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+        manifest[name] = meta
+    manifest["_seed"] = SEED
+    manifest["_generator"] = "tests/golden/make_golden.py via oracle/_ref/libprism_ref.so (reference sources, parity flags)"
+    with open(os.path.join(HERE, "manifest.json"), "w") as f:
+        json.dump(manifest, f, indent=1, sort_keys=True)
+    print("wrote", len(CASES), "cases")
+
+
+if __name__ == "__main__":
+    main()
