@@ -85,15 +85,22 @@ __global__ void __launch_bounds__(kBlock) k_spmv(uint32_t n, const uint32_t* __r
                                                  ReduceSlot slot) {
     const int lane = threadIdx.x & (G - 1);
     const uint32_t groups = (gridDim.x * blockDim.x) / G;
+    const uint32_t gid = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+    const uint32_t sub = (threadIdx.x & 31) / G;  // group index inside the warp
     double acc[NDOT > 0 ? NDOT : 1];
 #pragma unroll
     for (int t = 0; t < (NDOT > 0 ? NDOT : 1); ++t) acc[t] = 0.0;
-    for (uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) / G; row < n; row += groups) {
-        const uint32_t beg = __ldg(rowptr + row), end = __ldg(rowptr + row + 1);
+    // the trip count is uniform across the warp (row0 is the warp's first group),
+    // so the full-mask shuffles in group_sum are always reached by all 32 lanes
+    for (uint32_t row0 = gid - sub; row0 < n; row0 += groups) {
+        const uint32_t row = row0 + sub;
         double s = 0.0;
-        for (uint32_t k = beg + lane; k < end; k += G) s += __ldcs(val + k) * __ldg(x + __ldcs(col + k));
+        if (row < n) {
+            const uint32_t beg = __ldg(rowptr + row), end = __ldg(rowptr + row + 1);
+            for (uint32_t k = beg + lane; k < end; k += G) s += __ldcs(val + k) * __ldg(x + __ldcs(col + k));
+        }
         s = group_sum<G>(s);
-        if (lane == 0) {
+        if (lane == 0 && row < n) {
             y[row] = s;
             if (NDOT >= 1) acc[0] += s * z[row];
             if (NDOT >= 2) acc[1] += x[row] * q[row];
