@@ -105,6 +105,14 @@ int32_t prism_version(void);
 /* number of kernel launches issued by this library in this process (all handles) */
 uint64_t prism_kernel_launch_count(void);
 
+/* Failure-detection self test of the bounded device waits: runs, on one warp,
+ * a two-row triangular sweep whose first row waits for a value nothing
+ * produces.  The wait gives up after wait_ns (<= 2 s) and the kernel returns
+ * with status PRISM_ERR_TIMEOUT, which is stored in *device_status; the call
+ * then runs a valid sweep to show the context is still usable.  No reference
+ * counterpart (the reference has no device-side waits). */
+int32_t prism_selftest_wait_timeout(int32_t device, uint64_t wait_ns, int32_t* device_status);
+
 /* ---- model problems (host) --------------------------------------------- */
 /* sizes of generateLaplacianCSR(nx,ny,nz,...): n = nx*ny*nz, nnz exact */
 int32_t prism_laplacian_dims(int32_t nx, int32_t ny, int32_t nz, uint32_t* n, uint32_t* nnz);
@@ -168,15 +176,18 @@ int32_t prism_set_precond_factor(prism_handle h, prism_factor f);
 int32_t prism_apply_device(prism_handle h, const double* in_d, double* out_d);
 int32_t prism_apply(prism_handle h, const double* in, double* out);
 
-/* One triangular sweep alone (sweep 0 = lower, 1 = upper), on device vectors.
- * `prepare` != 0 first marks out_d pending (the sweep's readiness encoding);
- * pass 0 only when the caller did that already.  For timing the sweep kernel
- * by itself; the preconditioner apply is prism_apply_device.  Also reports the
- * sweep's stored non-zeros and the bytes its value array takes per entry. */
+/* One triangular sweep alone (sweep 0 = lower, 1 = upper), on device vectors,
+ * for timing the sweep kernel by itself (the preconditioner apply is
+ * prism_apply_device).  prepare = 1: mark out_d pending (the sweep's readiness
+ * encoding) then sweep; 0: sweep only (the caller marked out_d already);
+ * 2: mark out_d pending only.  prism_precond_sweep_info reports the sweep's
+ * rows, stored non-zeros, bytes per stored value, wavefront count and the
+ * kernel the setup-time autotuner kept (1: level-ordered grid-wide sweep,
+ * 2: slab-blocked sweep with shared-memory dependencies). */
 int32_t prism_precond_sweep_device(prism_handle h, int32_t sweep, const double* in_d, double* out_d,
                                    int32_t prepare);
 int32_t prism_precond_sweep_info(prism_handle h, int32_t sweep, uint32_t* n, uint64_t* nnz,
-                                 uint32_t* value_bytes, uint32_t* num_levels);
+                                 uint32_t* value_bytes, uint32_t* num_levels, uint32_t* kernel);
 
 /* ---- solvers ------------------------------------------------------------- */
 /* x is the in/out initial guess, as BaseSolver::solve (BaseSolver.h:16). */

@@ -56,6 +56,7 @@ _SIGS = {
     "prism_last_error": (C.c_char_p, []),
     "prism_version": (C.c_int32, []),
     "prism_kernel_launch_count": (C.c_uint64, []),
+    "prism_selftest_wait_timeout": (C.c_int32, [C.c_int32, C.c_uint64, C.POINTER(C.c_int32)]),
     "prism_laplacian_dims": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     "prism_laplacian_fill": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
                                          C.c_double, _u32p, _u32p, _f64p]),
@@ -83,7 +84,7 @@ _SIGS = {
     "prism_set_precond_factor": (C.c_int32, [_vp, _vp]),
     "prism_precond_sweep_device": (C.c_int32, [_vp, C.c_int32, _vp, _vp, C.c_int32]),
     "prism_precond_sweep_info": (C.c_int32, [_vp, C.c_int32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64),
-                                             C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+                                             C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     "prism_apply_device": (C.c_int32, [_vp, _vp, _vp]),
     "prism_apply": (C.c_int32, [_vp, _f64p, _f64p]),
     "prism_solve_device": (C.c_int32, [_vp, C.POINTER(SolveOpts), _vp, _vp, C.POINTER(SolveStats)]),
@@ -117,6 +118,13 @@ def _check(rc: int):
 
 def kernel_launch_count() -> int:
     return int(load().prism_kernel_launch_count())
+
+
+def selftest_wait_timeout(device: int = 0, wait_ns: int = 50_000_000) -> int:
+    """Runs the bounded-wait self test; returns the device status the wait raised (6 = timeout)."""
+    st = C.c_int32(-1)
+    _check(load().prism_selftest_wait_timeout(device, wait_ns, C.byref(st)))
+    return st.value
 
 
 def _ptr(t) -> int:
@@ -286,14 +294,17 @@ class DeviceSystem:
                                              ci.ctypes.data, v.ctypes.data, d.ctypes.data))
         return rp, ci, v, d
 
-    def sweep_device(self, sweep: int, vin, vout, prepare: bool = True):
-        """One triangular sweep alone on torch CUDA tensors (kernel timing)."""
+    def sweep_device(self, sweep: int, vin, vout, prepare: int = 1):
+        """One triangular sweep alone on torch CUDA tensors (kernel timing).
+        prepare: 1 mark pending + sweep, 0 sweep only, 2 mark pending only."""
         _check(self.lib.prism_precond_sweep_device(self.h, sweep, _ptr(vin), _ptr(vout), int(prepare)))
 
     def sweep_info(self, sweep: int) -> dict:
-        n, nnz, vb, lv = C.c_uint32(), C.c_uint64(), C.c_uint32(), C.c_uint32()
-        _check(self.lib.prism_precond_sweep_info(self.h, sweep, C.byref(n), C.byref(nnz), C.byref(vb), C.byref(lv)))
-        return {"n": n.value, "nnz": nnz.value, "value_bytes": vb.value, "levels": lv.value}
+        n, nnz, vb, lv, kk = C.c_uint32(), C.c_uint64(), C.c_uint32(), C.c_uint32(), C.c_uint32()
+        _check(self.lib.prism_precond_sweep_info(self.h, sweep, C.byref(n), C.byref(nnz), C.byref(vb), C.byref(lv),
+                                                 C.byref(kk)))
+        return {"n": n.value, "nnz": nnz.value, "value_bytes": vb.value, "levels": lv.value,
+                "kernel": {1: "level-order", 2: "slab"}.get(kk.value, "?")}
 
     def apply(self, vec):
         """out = M^{-1} vec (MInvSolve(vecIN, vecOUT))."""

@@ -74,6 +74,18 @@ int32_t prism_version(void) { return 100; }
 
 uint64_t prism_kernel_launch_count(void) { return prism::launch_counter().load(); }
 
+int32_t prism_selftest_wait_timeout(int32_t device, uint64_t wait_ns, int32_t* device_status) {
+    if (!device_status) return fail(PRISM_ERR_ARG, "null output");
+    if (wait_ns == 0 || wait_ns > 2000000000ull) return fail(PRISM_ERR_ARG, "wait_ns must be in (0, 2 s]");
+    return guarded([&]() -> int {
+        int s = -1;
+        DeviceGuard g(device);
+        prism::selftest_wait_timeout(device, wait_ns, &s);
+        *device_status = s;
+        return PRISM_OK;
+    });
+}
+
 int32_t prism_laplacian_dims(int32_t nx, int32_t ny, int32_t nz, uint32_t* n, uint32_t* nnz) {
     if (!n || !nnz) return fail(PRISM_ERR_ARG, "null output pointer");
     if (!prism::laplacian_dims(nx, ny, nz, n, nnz)) return fail(PRISM_ERR_ARG, "grid dimensions out of range");
@@ -338,17 +350,18 @@ int32_t prism_precond_sweep_device(prism_handle h, int32_t sweep, const double* 
     if (!h->P) return fail(PRISM_ERR_NOT_READY, "no preconditioner set");
     return guarded([&]() -> int {
         DeviceGuard g(h->info.device);
-        if (!h->P->run_sweep(h->stream, sweep, in_d, out_d, prepare != 0))
+        if (prepare < 0 || prepare > 2) return fail(PRISM_ERR_ARG, "prepare must be 0, 1 or 2");
+        if (!h->P->run_sweep(h->stream, sweep, in_d, out_d, prepare))
             return fail(PRISM_ERR_UNSUPPORTED, "preconditioner has no single sweeps");
         return PRISM_OK;
     });
 }
 
 int32_t prism_precond_sweep_info(prism_handle h, int32_t sweep, uint32_t* n, uint64_t* nnz, uint32_t* value_bytes,
-                                 uint32_t* num_levels) {
+                                 uint32_t* num_levels, uint32_t* kernel) {
     if (!h) return fail(PRISM_ERR_ARG, "null handle");
     if (!h->P) return fail(PRISM_ERR_NOT_READY, "no preconditioner set");
-    if (!h->P->sweep_info(sweep, n, nnz, value_bytes, num_levels))
+    if (!h->P->sweep_info(sweep, n, nnz, value_bytes, num_levels, kernel))
         return fail(PRISM_ERR_UNSUPPORTED, "preconditioner has no single sweeps");
     return PRISM_OK;
 }

@@ -408,6 +408,7 @@ void build_sweep(uint32_t n, const std::vector<uint32_t>& rowptr, const std::vec
         std::vector<uint32_t> fill(out.level_ptr.begin(), out.level_ptr.end() - 1);
         for (uint32_t r = 0; r < n; ++r) out.order[fill[level[r]]++] = r;
     }
+    out.level = level;
     out.rowptr.assign((size_t)n + 1, 0);
     for (uint32_t p = 0; p < n; ++p) {
         const uint32_t r = out.order[p];
@@ -421,6 +422,47 @@ void build_sweep(uint32_t n, const std::vector<uint32_t>& rowptr, const std::vec
         std::copy(col.begin() + rowptr[r], col.begin() + rowptr[r + 1], out.col.begin() + out.rowptr[p]);
         std::copy(val.begin() + rowptr[r], val.begin() + rowptr[r + 1], out.val.begin() + out.rowptr[p]);
         if (diag) out.diag[p] = (*diag)[r];
+    }
+}
+
+template <typename Low>
+void slab_layout(const Sweep<Low>& s, uint32_t num_ctas, uint32_t rows_per_cta, std::vector<uint32_t>& cta_pos,
+                 Sweep<Low>& out) {
+    const uint32_t n = s.n;
+    cta_pos.assign((size_t)num_ctas + 1, 0);
+    for (uint32_t r = 0; r < n; ++r) cta_pos[std::min<uint32_t>(r / rows_per_cta, num_ctas - 1) + 1]++;
+    for (uint32_t b = 0; b < num_ctas; ++b) cta_pos[b + 1] += cta_pos[b];
+    // the global (level, row) order, bucketed by owning CTA, stays (level, row) ordered per CTA
+    std::vector<uint32_t> fill(cta_pos.begin(), cta_pos.end() - 1);
+    std::vector<uint32_t> newpos_of_old(n);
+    for (uint32_t p = 0; p < n; ++p) {
+        const uint32_t r = s.order[p];
+        const uint32_t b = std::min<uint32_t>(r / rows_per_cta, num_ctas - 1);
+        newpos_of_old[p] = fill[b]++;
+    }
+    out.n = n;
+    out.op = s.op;
+    out.lower = s.lower;
+    out.num_levels = s.num_levels;
+    out.level_ptr = s.level_ptr;
+    out.level = s.level;
+    out.order.resize(n);
+    out.diag.resize(n);
+    out.rowptr.assign((size_t)n + 1, 0);
+    std::vector<uint32_t> old_of_new(n);
+    for (uint32_t p = 0; p < n; ++p) old_of_new[newpos_of_old[p]] = p;
+    for (uint32_t q = 0; q < n; ++q) {
+        const uint32_t p = old_of_new[q];
+        out.order[q] = s.order[p];
+        out.diag[q] = s.diag[p];
+        out.rowptr[q + 1] = out.rowptr[q] + (s.rowptr[p + 1] - s.rowptr[p]);
+    }
+    out.col.resize(s.col.size());
+    out.val.resize(s.val.size());
+    for (uint32_t q = 0; q < n; ++q) {
+        const uint32_t p = old_of_new[q];
+        std::copy(s.col.begin() + s.rowptr[p], s.col.begin() + s.rowptr[p + 1], out.col.begin() + out.rowptr[q]);
+        std::copy(s.val.begin() + s.rowptr[p], s.val.begin() + s.rowptr[p + 1], out.val.begin() + out.rowptr[q]);
     }
 }
 
@@ -527,6 +569,9 @@ template void transpose_csr<double>(uint32_t, const std::vector<uint32_t>&, cons
 template void transpose_csr<float>(uint32_t, const std::vector<uint32_t>&, const std::vector<uint32_t>&,
                                    const std::vector<float>&, std::vector<uint32_t>&, std::vector<uint32_t>&,
                                    std::vector<float>&);
+template void slab_layout<double>(const Sweep<double>&, uint32_t, uint32_t, std::vector<uint32_t>&,
+                                  Sweep<double>&);
+template void slab_layout<float>(const Sweep<float>&, uint32_t, uint32_t, std::vector<uint32_t>&, Sweep<float>&);
 template void build_sweep<double>(uint32_t, const std::vector<uint32_t>&, const std::vector<uint32_t>&,
                                   const std::vector<double>&, const std::vector<double>*, int, bool, Sweep<double>&);
 template void build_sweep<float>(uint32_t, const std::vector<uint32_t>&, const std::vector<uint32_t>&,

@@ -92,7 +92,16 @@ struct Sweep {
     std::vector<uint32_t> col;         // dependency rows (original numbering)
     std::vector<Low> val;
     std::vector<double> diag;          // by position (unused for SWEEP_NONE)
+    std::vector<uint32_t> level;       // by row: wavefront index
 };
+
+// Slab layout of a sweep for the blocked device kernel: CTA b owns the
+// contiguous rows [b*rows_per_cta, (b+1)*rows_per_cta) and visits them in
+// (level, row) order.  Positions are renumbered so that CTA b's rows occupy
+// positions [cta_pos[b], cta_pos[b+1]); rowptr/col/val/diag/order follow.
+template <typename Low>
+void slab_layout(const Sweep<Low>& s, uint32_t num_ctas, uint32_t rows_per_cta, std::vector<uint32_t>& cta_pos,
+                 Sweep<Low>& out);
 
 // Builds a sweep from a gather-form CSR (row r lists its dependencies and
 // coefficients, in the order the reference accumulates them) plus optional

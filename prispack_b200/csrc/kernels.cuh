@@ -120,19 +120,23 @@ __global__ void __launch_bounds__(kBlock) k_spmv(uint32_t n, const uint32_t* __r
 //   out[r] = post( pre(in[r]) - Σ_k val[k] * out[col[k]] )
 //
 // Readiness is carried by the value itself: before the sweep every out[] slot
-// holds kPending, a signalling-NaN bit pattern that no arithmetic result can
-// take (results that are NaN are canonicalised).  A row polls its
-// dependencies' slots until they differ from kPending -- one 8-byte
-// single-copy-atomic word carries both the flag and the value, so no fence or
-// second load is needed on the critical path.
+// holds kPending, a signalling-NaN bit pattern that no arithmetic result takes
+// (NaN results are canonicalised).  One 8-byte single-copy-atomic word carries
+// both the flag and the value, so no fence and no second load sits on the
+// critical path.
 //
 // Rows are visited in level order: warp w takes positions w, w+W, w+2W, ...
-// and a row only depends on rows of earlier levels, i.e. earlier positions,
-// held by warps that are resident (the grid never exceeds the number of
-// co-resident warps).  The lowest unfinished position therefore never waits,
-// so the sweep always progresses.  Every wait is still bounded: after
-// `wait_ns` without progress the warp raises *status = 6 (timeout), and all
-// waiters leave as soon as they see a non-zero status.
+// A row depends only on rows of earlier levels, i.e. earlier positions, held
+// by warps that are resident (cooperative launch), so the lowest unfinished
+// position never waits and the sweep always progresses.
+//
+// Latency hiding: while a row waits, the warp has already loaded the next
+// row's offsets, column indices, values, diagonal, right-hand side and the
+// current value of every dependency (all independent of the wait).  When the
+// warp turns to that row, only the dependencies that were still pending are
+// polled, by their own lanes; the others cost nothing more.  Every wait is
+// bounded: after `wait_ns` without progress the warp raises *status = 6
+// (timeout) and every waiter leaves as soon as it sees a non-zero status.
 // ---------------------------------------------------------------------------
 constexpr unsigned long long kPending = 0x7FF4DEADBEEF5EEDull;
 constexpr unsigned long long kCanonicalNaN = 0x7FF8000000000000ull;
@@ -141,6 +145,89 @@ enum : int { OP_DIV = 0, OP_MUL = 1, OP_NONE = 2, OP_PREDIV = 3 };
 
 __global__ void k_fill_pending(uint32_t n, unsigned long long* __restrict__ p) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = kPending;
+}
+
+// One row of a sweep as a warp holds it: lane k owns the k-th stored entry
+// (rows longer than 32 entries continue in a loop); `bits` is the value of the
+// lane's dependency as last seen (kPending if not produced yet).
+struct SweepRow {
+    uint32_t beg, end, r;
+    uint32_t c;                 // this lane's dependency row (first 32 entries)
+    double a;                   // its coefficient
+    unsigned long long bits;    // its value, loaded when the row was prefetched
+    double d, v;                // diagonal and right-hand side (lane 0)
+};
+
+// Loads a row's offsets, entries, diagonal, right-hand side and -- already --
+// the current value of each dependency; all of it is independent of the
+// wait, so it overlaps the previous row's wait.  `dep` is a callable loading
+// a dependency's current bits.
+template <typename Low, typename Dep>
+__device__ __forceinline__ void prefetch_row(SweepRow& m, uint32_t p, int lane, const uint32_t* __restrict__ order,
+                                             const uint32_t* __restrict__ rowptr, const uint32_t* __restrict__ col,
+                                             const Low* __restrict__ val, const double* __restrict__ diag,
+                                             const double* __restrict__ in, Dep&& dep) {
+    m.beg = __ldg(rowptr + p);
+    m.end = __ldg(rowptr + p + 1);
+    m.r = __ldg(order + p);
+    m.c = 0;
+    m.a = 0.0;
+    m.bits = 0ull;
+    if (m.beg + lane < m.end) {
+        m.c = __ldcs(col + m.beg + lane);
+        m.a = (double)__ldcs(val + m.beg + lane);
+        m.bits = dep(m.c);
+    }
+    if (lane == 0) {
+        m.d = __ldg(diag + p);
+        m.v = __ldg(in + m.r);
+    }
+}
+
+// Finishes a prefetched row: polls only the dependencies that were still
+// pending, reduces, and returns the row's value in lane 0 (false: a wait ran out).
+template <typename Low, int OP, typename Wait>
+__device__ __forceinline__ bool finish_row(const SweepRow& m, int lane, const uint32_t* __restrict__ col,
+                                           const Low* __restrict__ val, Wait&& wait, unsigned long long& out_bits) {
+    bool ok = true;
+    double s = 0.0;
+    if (m.beg + lane < m.end) {
+        unsigned long long bits = m.bits;
+        if (bits == kPending) ok = wait(m.c, bits);
+        s = m.a * __longlong_as_double((long long)bits);
+    }
+    for (uint32_t k = m.beg + 32 + lane; ok && k < m.end; k += 32) {  // rows longer than a warp
+        unsigned long long bits;
+        ok = wait(__ldcs(col + k), bits);
+        s += (double)__ldcs(val + k) * __longlong_as_double((long long)bits);
+    }
+    if (!__all_sync(0xffffffffu, ok)) return false;
+    s = group_sum<32>(s);
+    double res;
+    if (OP == OP_DIV) res = (m.v - s) / m.d;
+    else if (OP == OP_MUL) res = (m.v - s) * m.d;
+    else if (OP == OP_NONE) res = m.v - s;
+    else res = m.v / m.d - s;
+    out_bits = (unsigned long long)__double_as_longlong(res);
+    if (res != res) out_bits = kCanonicalNaN;
+    return true;
+}
+
+// Spin on a word until it is no longer kPending; false when the wait gave up.
+template <typename Load>
+__device__ __forceinline__ bool spin_ready(Load&& load, unsigned long long& bits, const int* status,
+                                           unsigned long long wait_ns) {
+    bits = load();
+    if (bits != kPending) return true;
+    const unsigned long long t0 = globaltimer_ns();
+    unsigned spins = 0;
+    do {
+        if ((++spins & 255u) == 0u) {
+            if (ld_relaxed_s32(status) != 0 || globaltimer_ns() - t0 > wait_ns) return false;
+        }
+        bits = load();
+    } while (bits == kPending);
+    return true;
 }
 
 template <typename Low, int OP>
@@ -152,47 +239,106 @@ __global__ void __launch_bounds__(kBlock) k_sweep(uint32_t n, const uint32_t* __
     const int lane = threadIdx.x & 31;
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t p = warp; p < n; p += nwarps) {
-        const uint32_t beg = __ldg(rowptr + p), end = __ldg(rowptr + p + 1);
-        double s = 0.0;
-        bool failed = false;
-        for (uint32_t k = beg + lane; k < end; k += 32) {
-            const uint32_t c = __ldg(col + k);
-            const double a = (double)__ldg(val + k);
-            unsigned long long bits = ld_relaxed_u64(out + c);
-            if (bits == kPending) {
-                const unsigned long long t0 = globaltimer_ns();
-                unsigned spins = 0;
-                do {
-                    if ((++spins & 255u) == 0u) {
-                        if (ld_relaxed_s32(status) != 0 || globaltimer_ns() - t0 > wait_ns) {
-                            failed = true;
-                            break;
-                        }
-                    }
-                    bits = ld_relaxed_u64(out + c);
-                } while (bits == kPending);
-            }
-            if (failed) break;
-            s += a * __longlong_as_double((long long)bits);
-        }
-        if (__any_sync(0xffffffffu, failed)) {
+    auto dep = [&](uint32_t c) { return ld_relaxed_u64(out + c); };
+    auto wait = [&](uint32_t c, unsigned long long& bits) {
+        return spin_ready([&] { return ld_relaxed_u64(out + c); }, bits, status, wait_ns);
+    };
+    uint32_t p = warp;
+    if (p >= n) return;
+    SweepRow cur, nxt;
+    prefetch_row<Low>(cur, p, lane, order, rowptr, col, val, diag, in, dep);
+    while (true) {
+        const uint32_t pn = p + nwarps;
+        if (pn < n) prefetch_row<Low>(nxt, pn, lane, order, rowptr, col, val, diag, in, dep);
+        unsigned long long rb;
+        if (!finish_row<Low, OP>(cur, lane, col, val, wait, rb)) {
             if (lane == 0) atomicCAS(status, 0, 6);
             return;
         }
-        s = group_sum<32>(s);
-        if (lane == 0) {
-            const uint32_t r = __ldg(order + p);
-            const double v = in[r];
-            double res;
-            if (OP == OP_DIV) res = (v - s) / diag[p];
-            else if (OP == OP_MUL) res = (v - s) * diag[p];
-            else if (OP == OP_NONE) res = v - s;
-            else res = v / diag[p] - s;
-            unsigned long long bits = (unsigned long long)__double_as_longlong(res);
-            if (res != res) bits = kCanonicalNaN;
-            st_relaxed_u64(out + r, bits);
+        if (lane == 0) st_relaxed_u64(out + cur.r, rb);
+        if (pn >= n) break;
+        cur = nxt;
+        p = pn;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Slab-blocked sync-free sweep.
+//
+// CTA b owns the contiguous rows [rb, re) = [b*rows_per_cta, ...) and visits
+// them in (level, row) order (positions [cta_pos[b], cta_pos[b+1]) of the slab
+// layout); its warps take those positions round-robin.  The CTA keeps the
+// values of its own rows in shared memory (the first `smem_rows` of them), so
+// a dependency produced inside the slab is a shared-memory poll of a few tens
+// of cycles; only dependencies owned by other slabs poll global memory.  Each
+// finished row is written to both.  Readiness uses the same kPending encoding
+// as k_sweep, in shared memory (initialised by the CTA itself) and in global
+// memory (initialised by k_fill_pending before the launch).
+//
+// Progress: take the unfinished row of lowest level.  Its dependencies are
+// finished; in its CTA every earlier position has a level no higher than its
+// own, so those rows can finish too, and the warp that owns the position
+// reaches it.  All CTAs are co-resident (cooperative launch), so no CTA waits
+// for one that is not running.  Waits are bounded as in k_sweep.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long ld_shared_u64(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.volatile.shared.u64 %0, [%1];" : "=l"(v) : "r"((unsigned)__cvta_generic_to_shared(p)) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_shared_u64(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.volatile.shared.u64 [%0], %1;" ::"r"((unsigned)__cvta_generic_to_shared(p)), "l"(v) : "memory");
+}
+
+template <typename Low, int OP>
+__global__ void __launch_bounds__(1024) k_sweep_slab(uint32_t n, uint32_t rows_per_cta, uint32_t smem_rows,
+                                                     const uint32_t* __restrict__ cta_pos,
+                                                     const uint32_t* __restrict__ order,
+                                                     const uint32_t* __restrict__ rowptr,
+                                                     const uint32_t* __restrict__ col, const Low* __restrict__ val,
+                                                     const double* __restrict__ diag, const double* __restrict__ in,
+                                                     double* out, int* status, unsigned long long wait_ns) {
+    extern __shared__ unsigned long long xs[];
+    const uint32_t b = blockIdx.x;
+    const uint32_t rb = b * rows_per_cta;
+    const uint32_t re = min(n, rb + rows_per_cta);
+    const uint32_t owned = re > rb ? re - rb : 0;
+    const uint32_t local_rows = min(owned, smem_rows);
+    for (uint32_t i = threadIdx.x; i < local_rows; i += blockDim.x) xs[i] = kPending;
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const uint32_t wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const uint32_t p0 = cta_pos[b], p1 = cta_pos[b + 1];
+    auto load = [&](uint32_t c) {
+        const uint32_t lc = c - rb;  // wraps for c < rb
+        return lc < local_rows ? ld_shared_u64(xs + lc) : ld_relaxed_u64(out + c);
+    };
+    auto wait = [&](uint32_t c, unsigned long long& bits) {
+        return spin_ready([&] { return load(c); }, bits, status, wait_ns);
+    };
+    // Dependency values are not read ahead here: inside a slab most of them are
+    // produced by neighbouring positions and would still be pending.
+    auto later = [](uint32_t) { return kPending; };
+    uint32_t p = p0 + wid;
+    if (p >= p1) return;
+    SweepRow cur, nxt;
+    prefetch_row<Low>(cur, p, lane, order, rowptr, col, val, diag, in, later);
+    while (true) {
+        const uint32_t pn = p + nw;
+        if (pn < p1) prefetch_row<Low>(nxt, pn, lane, order, rowptr, col, val, diag, in, later);
+        unsigned long long rbits;
+        if (!finish_row<Low, OP>(cur, lane, col, val, wait, rbits)) {
+            if (lane == 0) atomicCAS(status, 0, 6);
+            return;
         }
+        if (lane == 0) {
+            const uint32_t lr = cur.r - rb;
+            if (lr < local_rows) st_shared_u64(xs + lr, rbits);
+            st_relaxed_u64(out + cur.r, rbits);
+        }
+        if (pn >= p1) break;
+        cur = nxt;
+        p = pn;
     }
 }
 

@@ -1,5 +1,6 @@
 // Device-resident operator, triangular preconditioners and the FCG driver.
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "../../include/prism_solve.h"
@@ -30,8 +31,44 @@ void launch_fill(cudaStream_t st, const Handle& h, uint32_t n, double* p) {
     PRISM_LAUNCHED();
 }
 
+void* slab_kernel(bool fp32, int op) {
+    if (fp32) {
+        switch (op) {
+            case SWEEP_DIV: return (void*)k_sweep_slab<float, OP_DIV>;
+            case SWEEP_MUL: return (void*)k_sweep_slab<float, OP_MUL>;
+            case SWEEP_NONE: return (void*)k_sweep_slab<float, OP_NONE>;
+            default: return (void*)k_sweep_slab<float, OP_PREDIV>;
+        }
+    }
+    switch (op) {
+        case SWEEP_DIV: return (void*)k_sweep_slab<double, OP_DIV>;
+        case SWEEP_MUL: return (void*)k_sweep_slab<double, OP_MUL>;
+        case SWEEP_NONE: return (void*)k_sweep_slab<double, OP_NONE>;
+        default: return (void*)k_sweep_slab<double, OP_PREDIV>;
+    }
+}
+
+constexpr int kSlabThreads = 1024;
+
 void launch_sweep(const Handle& h, cudaStream_t st, const DevSweep& s, const double* in, double* out) {
     if (!s.n) return;
+    if (s.num_ctas > 0) {
+        void* fn = slab_kernel(s.fp32, s.op);
+        uint32_t n = s.n, rpc = s.rows_per_cta, smem_rows = s.smem_rows;
+        const uint32_t* cta_pos = s.cta_pos.get();
+        const uint32_t* order = s.order.get();
+        const uint32_t* rowptr = s.rowptr.get();
+        const uint32_t* col = s.col.get();
+        const void* val = s.fp32 ? (const void*)s.val32.get() : (const void*)s.val64.get();
+        const double* diag = s.diag.get();
+        int* status = h.status.get();
+        unsigned long long wait = kWaitNs;
+        void* args[] = {&n, &rpc, &smem_rows, &cta_pos, &order, &rowptr, &col, &val, &diag, &in, &out, &status, &wait};
+        PRISM_CUDA(cudaLaunchCooperativeKernel(fn, dim3(s.num_ctas), dim3(kSlabThreads), args,
+                                               (size_t)s.smem_rows * sizeof(double), st));
+        PRISM_LAUNCHED();
+        return;
+    }
     long want = ((long)s.n * 32 + kBlock - 1) / kBlock;
     long cap = (long)h.info.sms * h.info.sweep_blocks_per_sm;
     int grid = (int)(want < cap ? want : cap);
@@ -68,6 +105,56 @@ void launch_sweep(const Handle& h, cudaStream_t st, const DevSweep& s, const dou
 }  // namespace
 
 // ============================================================================
+// Bounded-wait self test: a two-row sweep whose first position depends on the
+// second one, run by a single warp.  The warp reaches position 0 first, so the
+// value it waits for is never produced; the wait must run out after wait_ns,
+// raise status 6 and return, leaving the context usable (checked by a normal
+// sweep afterwards).
+// ============================================================================
+int selftest_wait_timeout(int device, unsigned long long wait_ns, int* device_status) {
+    PRISM_CUDA(cudaSetDevice(device));
+    cudaStream_t st;
+    PRISM_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    // position 0 = row 0 (depends on row 1), position 1 = row 1 (no dependency)
+    const uint32_t h_order[2] = {0, 1}, h_rowptr[3] = {0, 1, 1}, h_col[1] = {1};
+    const double h_val[1] = {0.5}, h_diag[2] = {1.0, 1.0}, h_in[2] = {1.0, 2.0};
+    DevBuf<uint32_t> order(2), rowptr(3), col(1);
+    DevBuf<double> val(1), diag(2), in(2), out(2);
+    DevBuf<int> status(1);
+    order.upload(h_order, 2, st); rowptr.upload(h_rowptr, 3, st); col.upload(h_col, 1, st);
+    val.upload(h_val, 1, st); diag.upload(h_diag, 2, st); in.upload(h_in, 2, st);
+    PRISM_CUDA(cudaMemsetAsync(status.get(), 0, sizeof(int), st));
+    k_fill_pending<<<1, 32, 0, st>>>(2, reinterpret_cast<unsigned long long*>(out.get()));
+    PRISM_LAUNCHED();
+    k_sweep<double, OP_NONE><<<1, 32, 0, st>>>(2, order.get(), rowptr.get(), col.get(), val.get(), diag.get(),
+                                               in.get(), out.get(), status.get(), wait_ns);
+    PRISM_LAUNCHED();
+    int s = -1;
+    PRISM_CUDA(cudaMemcpyAsync(&s, status.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
+    PRISM_CUDA(cudaStreamSynchronize(st));
+    *device_status = s;
+    // the context is still usable: the same rows in a valid order solve normally
+    const uint32_t g_order[2] = {1, 0}, g_rowptr[3] = {0, 0, 1};
+    order.upload(g_order, 2, st); rowptr.upload(g_rowptr, 3, st);
+    PRISM_CUDA(cudaMemsetAsync(status.get(), 0, sizeof(int), st));
+    k_fill_pending<<<1, 32, 0, st>>>(2, reinterpret_cast<unsigned long long*>(out.get()));
+    PRISM_LAUNCHED();
+    k_sweep<double, OP_NONE><<<1, 32, 0, st>>>(2, order.get(), rowptr.get(), col.get(), val.get(), diag.get(),
+                                               in.get(), out.get(), status.get(), wait_ns);
+    PRISM_LAUNCHED();
+    double h_out[2] = {0, 0};
+    int s2 = -1;
+    PRISM_CUDA(cudaMemcpyAsync(h_out, out.get(), sizeof(h_out), cudaMemcpyDeviceToHost, st));
+    PRISM_CUDA(cudaMemcpyAsync(&s2, status.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
+    PRISM_CUDA(cudaStreamSynchronize(st));
+    PRISM_CUDA(cudaStreamDestroy(st));
+    // row 1 = 2, row 0 = 1 - 0.5 * 2 = 0
+    if (s2 != 0 || h_out[0] != 0.0 || h_out[1] != 2.0)
+        throw Error(PRISM_ERR_CUDA, "context unusable after a timed-out wait");
+    return 0;
+}
+
+// ============================================================================
 // Handle
 // ============================================================================
 void init_device_info(DeviceInfo& info, int device) {
@@ -79,7 +166,22 @@ void init_device_info(DeviceInfo& info, int device) {
     occ = occ < occ2 ? occ : occ2;
     // a fraction of the co-resident capacity: enough warps to cover a wavefront,
     // few enough pollers to leave L2 bandwidth to the producers
-    info.sweep_blocks_per_sm = occ < 4 ? (occ > 0 ? occ : 1) : 4;
+    int want = 4;
+    if (const char* e = std::getenv("PRISM_SWEEP_BLOCKS_PER_SM")) want = std::atoi(e);
+    if (want < 1) want = 1;
+    info.sweep_blocks_per_sm = occ < want ? (occ > 0 ? occ : 1) : want;
+    PRISM_CUDA(cudaDeviceGetAttribute(&info.max_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+    if (const char* e = std::getenv("PRISM_SWEEP_KERNEL")) {
+        const std::string k(e);
+        info.sweep_kernel = k == "global" ? 1 : (k == "slab" ? 2 : 0);
+    }
+    if (const char* e = std::getenv("PRISM_SLAB_MIN_ROWS")) info.slab_min_rows = (uint32_t)std::atoi(e);
+    if (info.slab_min_rows < 32) info.slab_min_rows = 32;
+    // the slab kernel runs one 1024-thread CTA per SM with up to the whole opt-in shared memory
+    for (bool f32 : {false, true})
+        for (int op = 0; op < 4; ++op)
+            PRISM_CUDA(cudaFuncSetAttribute(slab_kernel(f32, op), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            info.max_smem_optin));
 }
 
 Handle::~Handle() {
@@ -128,17 +230,33 @@ void Handle::check_status() {
 // Sweeps and triangular preconditioners
 // ============================================================================
 template <typename Low>
-void DevSweep::upload(const Sweep<Low>& s, cudaStream_t st) {
-    n = s.n;
-    num_levels = s.num_levels;
-    op = s.op;
+void DevSweep::upload(const Sweep<Low>& s0, const DeviceInfo& info, bool slab_layout_wanted, cudaStream_t st) {
+    n = s0.n;
+    num_levels = s0.num_levels;
+    op = s0.op;
     fp32 = std::is_same<Low, float>::value;
-    order.upload(s.order.data(), s.order.size(), st);
-    rowptr.upload(s.rowptr.data(), s.rowptr.size(), st);
-    col.upload(s.col.data(), s.col.size(), st);
-    diag.upload(s.diag.data(), s.diag.size(), st);
-    if (fp32) val32.upload(reinterpret_cast<const float*>(s.val.data()), s.val.size(), st);
-    else val64.upload(reinterpret_cast<const double*>(s.val.data()), s.val.size(), st);
+    const Sweep<Low>* s = &s0;
+    Sweep<Low> slab;
+    std::vector<uint32_t> cpos;
+    num_ctas = rows_per_cta = smem_rows = 0;
+    if (slab_layout_wanted && n > 0) {
+        uint32_t ctas = (uint32_t)info.sms;
+        uint32_t want = (n + info.slab_min_rows - 1) / info.slab_min_rows;
+        if (want < ctas) ctas = want;
+        if (ctas < 1) ctas = 1;
+        rows_per_cta = (n + ctas - 1) / ctas;
+        num_ctas = (n + rows_per_cta - 1) / rows_per_cta;
+        smem_rows = std::min<uint32_t>(rows_per_cta, (uint32_t)(info.max_smem_optin / sizeof(double)));
+        slab_layout<Low>(s0, num_ctas, rows_per_cta, cpos, slab);
+        s = &slab;
+        cta_pos.upload(cpos.data(), cpos.size(), st);
+    }
+    order.upload(s->order.data(), s->order.size(), st);
+    rowptr.upload(s->rowptr.data(), s->rowptr.size(), st);
+    col.upload(s->col.data(), s->col.size(), st);
+    diag.upload(s->diag.data(), s->diag.size(), st);
+    if (fp32) val32.upload(reinterpret_cast<const float*>(s->val.data()), s->val.size(), st);
+    else val64.upload(reinterpret_cast<const double*>(s->val.data()), s->val.size(), st);
     // keep at least one element so kernels always get valid pointers
     if (col.size() == 0) col.alloc(1);
     if (fp32 && val32.size() == 0) val32.alloc(1);
@@ -146,13 +264,58 @@ void DevSweep::upload(const Sweep<Low>& s, cudaStream_t st) {
     PRISM_CUDA(cudaStreamSynchronize(st));
 }
 
+namespace {
+// Sweep-kernel autotuner: uploads the sweep in the plain level order and in
+// the slab layout in turn, times a few launches of each on a random
+// right-hand side with CUDA events, and keeps the faster one.  Which kernel
+// wins depends on how many rows a wavefront holds and how far dependencies
+// reach (the slab kernel pays off when most of them stay inside a slab).
+template <typename Low>
+void tune_sweep(Handle& h, DevSweep& d, const Sweep<Low>& s) {
+    const int mode = h.info.sweep_kernel;
+    if (mode != 0 || s.n == 0) {
+        d.upload(s, h.info, mode == 2, h.stream);
+        return;
+    }
+    DevBuf<double> in(s.n), out(s.n);
+    std::vector<double> rhs(s.n);
+    for (uint32_t i = 0; i < s.n; ++i) rhs[i] = 1.0 + (double)(i % 7) * 0.125;
+    in.upload(rhs.data(), s.n, h.stream);
+    cudaEvent_t e0, e1;
+    PRISM_CUDA(cudaEventCreate(&e0));
+    PRISM_CUDA(cudaEventCreate(&e1));
+    float best = 0.f;
+    bool best_slab = false;
+    for (bool slab : {false, true}) {
+        d.upload(s, h.info, slab, h.stream);
+        float tot = 0.f;
+        for (int it = 0; it < 4; ++it) {
+            launch_fill(h.stream, h, s.n, out.get());
+            PRISM_CUDA(cudaEventRecord(e0, h.stream));
+            launch_sweep(h, h.stream, d, in.get(), out.get());
+            PRISM_CUDA(cudaEventRecord(e1, h.stream));
+            PRISM_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            PRISM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            if (it > 0) tot += ms;  // first launch is a warm-up
+        }
+        h.check_status();
+        if (!slab || tot < best) { best = tot; best_slab = slab; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (!best_slab) d.upload(s, h.info, false, h.stream);
+    d.tuned_ms = best / 3.f;
+}
+}  // namespace
+
 TriangularPrecond::TriangularPrecond(Handle& h, std::shared_ptr<const HostFactor> f) : h_(h), f_(std::move(f)) {
     if (f_->fp32) {
-        lower_.upload(f_->lower32, h_.stream);
-        upper_.upload(f_->upper32, h_.stream);
+        tune_sweep(h_, lower_, f_->lower32);
+        tune_sweep(h_, upper_, f_->upper32);
     } else {
-        lower_.upload(f_->lower64, h_.stream);
-        upper_.upload(f_->upper64, h_.stream);
+        tune_sweep(h_, lower_, f_->lower64);
+        tune_sweep(h_, upper_, f_->upper64);
     }
 }
 
@@ -166,15 +329,17 @@ void TriangularPrecond::apply(cudaStream_t st, const double* in, double* out) {
     launch_sweep(h_, st, upper_, tmp_.get(), out);
 }
 
-bool TriangularPrecond::run_sweep(cudaStream_t st, int sweep, const double* in, double* out, bool prepare) {
+bool TriangularPrecond::run_sweep(cudaStream_t st, int sweep, const double* in, double* out, int prepare) {
     const DevSweep& s = sweep == 0 ? lower_ : upper_;
-    if (prepare) launch_fill(st, h_, s.n, out);
-    launch_sweep(h_, st, s, in, out);
+    if (prepare != 0) launch_fill(st, h_, s.n, out);
+    if (prepare != 2) launch_sweep(h_, st, s, in, out);
     return true;
 }
 
-bool TriangularPrecond::sweep_info(int sweep, uint32_t* n, uint64_t* nnz, uint32_t* vbytes, uint32_t* levels) const {
+bool TriangularPrecond::sweep_info(int sweep, uint32_t* n, uint64_t* nnz, uint32_t* vbytes, uint32_t* levels,
+                                   uint32_t* kernel) const {
     const DevSweep& s = sweep == 0 ? lower_ : upper_;
+    if (kernel) *kernel = s.num_ctas > 0 ? 2 : 1;
     if (n) *n = s.n;
     if (nnz) *nnz = s.fp32 ? s.val32.size() : s.val64.size();
     if (vbytes) *vbytes = s.fp32 ? 4 : 8;

@@ -18,6 +18,9 @@ struct DeviceInfo {
     int device = 0;
     int sms = 148;
     int sweep_blocks_per_sm = 1;   // co-resident k_sweep blocks (cooperative launch bound)
+    int max_smem_optin = 0;        // bytes of dynamic shared memory one block may opt into
+    int sweep_kernel = 0;          // 0: autotune per sweep, 1: global level order, 2: slab-blocked
+    uint32_t slab_min_rows = 2048; // smallest slab (small systems use fewer CTAs)
 };
 
 // Reduction scratch shared by all kernels of one stream (they run serially).
@@ -54,11 +57,14 @@ struct DevSweep {
     uint32_t n = 0, num_levels = 0;
     int op = SWEEP_NONE;
     bool fp32 = false;
-    DevBuf<uint32_t> order, rowptr, col;
+    // slab layout (k_sweep_slab) when num_ctas > 0, plain level order (k_sweep) otherwise
+    uint32_t num_ctas = 0, rows_per_cta = 0, smem_rows = 0;
+    DevBuf<uint32_t> order, rowptr, col, cta_pos;
     DevBuf<double> val64, diag;
     DevBuf<float> val32;
     template <typename Low>
-    void upload(const Sweep<Low>& s, cudaStream_t st);
+    void upload(const Sweep<Low>& s, const DeviceInfo& info, bool slab, cudaStream_t st);
+    float tuned_ms = 0.f;          // time of the chosen kernel at setup (0: not tuned)
 };
 
 class Precond {
@@ -70,12 +76,13 @@ class Precond {
     virtual void apply(cudaStream_t st, const double* in, double* out) = 0;
     virtual uint32_t levels(int sweep) const { (void)sweep; return 0; }
     // one sweep alone (diagnostics / kernel timing); returns false if not a sweep-based preconditioner
-    virtual bool run_sweep(cudaStream_t st, int sweep, const double* in, double* out, bool prepare) {
+    virtual bool run_sweep(cudaStream_t st, int sweep, const double* in, double* out, int prepare) {
         (void)st; (void)sweep; (void)in; (void)out; (void)prepare;
         return false;
     }
-    virtual bool sweep_info(int sweep, uint32_t* n, uint64_t* nnz, uint32_t* vbytes, uint32_t* levels) const {
-        (void)sweep; (void)n; (void)nnz; (void)vbytes; (void)levels;
+    virtual bool sweep_info(int sweep, uint32_t* n, uint64_t* nnz, uint32_t* vbytes, uint32_t* levels,
+                            uint32_t* kernel) const {
+        (void)sweep; (void)n; (void)nnz; (void)vbytes; (void)levels; (void)kernel;
         return false;
     }
     // factor export (parity checks)
@@ -99,8 +106,9 @@ class TriangularPrecond : public Precond {
     uint32_t levels(int sweep) const override { return sweep == 0 ? lower_.num_levels : upper_.num_levels; }
     int export_factor(int which, uint32_t* n, uint64_t* nnz, uint32_t* rowptr, uint32_t* col, double* val,
                       double* diag) const override;
-    bool run_sweep(cudaStream_t st, int sweep, const double* in, double* out, bool prepare) override;
-    bool sweep_info(int sweep, uint32_t* n, uint64_t* nnz, uint32_t* vbytes, uint32_t* levels) const override;
+    bool run_sweep(cudaStream_t st, int sweep, const double* in, double* out, int prepare) override;
+    bool sweep_info(int sweep, uint32_t* n, uint64_t* nnz, uint32_t* vbytes, uint32_t* levels,
+                    uint32_t* kernel) const override;
 
   private:
     Handle& h_;
@@ -133,6 +141,9 @@ struct Handle {
     void check_status();           // synchronises; throws on a raised device status
     void ensure_workspace();
 };
+
+// Runs the bounded-wait self test (see solve.cu); returns the device status the wait raised.
+int selftest_wait_timeout(int device, unsigned long long wait_ns, int* device_status);
 
 // Queries SM count and the co-resident capacity of the sweep kernel.
 void init_device_info(DeviceInfo& info, int device);

@@ -131,3 +131,17 @@ def test_launch_counter_moves():
     S = P.DeviceSystem(A)
     S.spmv(np.ones(A.n))
     assert P.kernel_launch_count() > before
+
+
+def test_bounded_wait_times_out_and_context_survives():
+    """A sweep row waits for a value nothing produces: the wait runs out (50 ms),
+    the kernel reports PRISM_ERR_TIMEOUT, and the context keeps working."""
+    import time
+    t = time.time()
+    assert P.selftest_wait_timeout(0, 50_000_000) == 6
+    assert time.time() - t < 10
+    A = P.CSRMatrix.laplacian(8, 8, 1)
+    S = P.DeviceSystem(A)
+    S.set_precond(P.PRECOND_IC, tol=1e-3)
+    x, st = S.solve(np.ones(A.n), tol=1e-8)
+    assert st.converged
