@@ -432,3 +432,38 @@ class CG:
 
     def getConvergence(self):
         return bool(self.stats.converged)
+
+
+class GMRES:
+    """GMRES<double>(n, precond, tol, GMRESType) + setRestart (source/Solver/GMRES.cpp:11-70)."""
+
+    def __init__(self, problemSize, precond=None, tolerance=1e-7, gmresType=FlexibleGMRES):
+        self.n = problemSize
+        self.precond = precond
+        self.tol = tolerance
+        self.gmresType = gmresType
+        self.restart = 0
+        self.stats = None
+
+    def setRestart(self, restart: bool, m: int):
+        self.restart = m if restart else 0
+
+    def solve(self, system: DeviceSystem, b, x):
+        if self.precond is not None:
+            self.precond.setup()
+        elif self.gmresType == FlexibleGMRES:
+            raise PrismError(5, "FlexibleGMRES must use a preconditioner")
+        else:
+            system.set_precond(PRECOND_NONE)
+        kind = SOLVER_FGMRES if self.gmresType == FlexibleGMRES else SOLVER_GMRES
+        x_out, self.stats = system.solve(b, x, solver=kind, tol=self.tol, restart=self.restart)
+        return x_out
+
+    def getNumIter(self):
+        return self.stats.num_iter
+
+    def getError(self):
+        return self.stats.final_error
+
+    def getConvergence(self):
+        return bool(self.stats.converged)

@@ -124,7 +124,7 @@ int32_t prism_create(uint32_t n, const uint32_t* rowptr, const uint32_t* col, co
             h->own_stream = true;
             PRISM_CUDA(cudaEventCreate(&h->ev0));
             PRISM_CUDA(cudaEventCreate(&h->ev1));
-            PRISM_CUDA(cudaMallocHost(&h->pinned, prism::kNumScalars * sizeof(double)));
+            PRISM_CUDA(cudaMallocHost(&h->pinned, prism::Handle::kScalarCapacity * sizeof(double)));
             const uint64_t nnz = rowptr[n];
             h->A_host.n = n;
             h->A_host.rowptr.assign(rowptr, rowptr + n + 1);
@@ -137,10 +137,11 @@ int32_t prism_create(uint32_t n, const uint32_t* rowptr, const uint32_t* col, co
             h->A.val.upload(val, nnz, h->stream);
             h->red.partial.alloc(prism::Reducer::kMaxGrid * 2);
             h->red.ticket.alloc(1);
-            h->red.scalars.alloc(prism::kNumScalars);
+            h->red.scalars.alloc(prism::Handle::kScalarCapacity);
             h->status.alloc(1);
             PRISM_CUDA(cudaMemsetAsync(h->red.ticket.get(), 0, sizeof(unsigned), h->stream));
-            PRISM_CUDA(cudaMemsetAsync(h->red.scalars.get(), 0, prism::kNumScalars * sizeof(double), h->stream));
+            PRISM_CUDA(cudaMemsetAsync(h->red.scalars.get(), 0, prism::Handle::kScalarCapacity * sizeof(double),
+                                       h->stream));
             PRISM_CUDA(cudaMemsetAsync(h->status.get(), 0, sizeof(int), h->stream));
             PRISM_CUDA(cudaStreamSynchronize(h->stream));
         } catch (...) {
@@ -367,13 +368,19 @@ int32_t prism_precond_sweep_info(prism_handle h, int32_t sweep, uint32_t* n, uin
 }
 
 // ---- solvers -------------------------------------------------------------------
+static void run_solver(prism::Handle& h, const prism_solve_opts& o, const double* b, double* x,
+                       prism_solve_stats* st) {
+    if (o.solver == PRISM_SOLVER_FCG || o.solver == PRISM_SOLVER_CG) prism::fcg_solve(h, o, b, x, st);
+    else prism::gmres_solve(h, o, b, x, st);
+}
+
 static int check_opts(prism_handle h, const prism_solve_opts* o) {
     if (!h) return fail(PRISM_ERR_ARG, "null handle");
     if (!o) return fail(PRISM_ERR_ARG, "null options");
     if (!(o->tol > 0.0)) return fail(PRISM_ERR_ARG, "tol must be > 0");
-    if (o->solver != PRISM_SOLVER_FCG && o->solver != PRISM_SOLVER_CG) {
-        return fail(PRISM_ERR_UNSUPPORTED, "solver kind not available");
-    }
+    if (o->solver < PRISM_SOLVER_FCG || o->solver > PRISM_SOLVER_GMRES) return fail(PRISM_ERR_ARG, "unknown solver kind");
+    if ((o->solver == PRISM_SOLVER_FGMRES || o->solver == PRISM_SOLVER_GMRES) && o->restart + 2 > prism::Handle::kMaxKrylov)
+        return fail(PRISM_ERR_ARG, "restart length above the Krylov workspace limit (1022)");
     return PRISM_OK;
 }
 
@@ -384,7 +391,7 @@ int32_t prism_solve_device(prism_handle h, const prism_solve_opts* opts, const d
     if (!b_d || !x_d) return fail(PRISM_ERR_ARG, "null vector");
     return guarded([&]() -> int {
         DeviceGuard g(h->info.device);
-        prism::fcg_solve(*h, *opts, b_d, x_d, stats);
+        run_solver(*h, *opts, b_d, x_d, stats);
         return PRISM_OK;
     });
 }
@@ -400,7 +407,7 @@ int32_t prism_solve(prism_handle h, const prism_solve_opts* opts, const double* 
         if (h->xb.size() < n) { h->xb.alloc(n); h->bb.alloc(n); }
         PRISM_CUDA(cudaMemcpyAsync(h->bb.get(), b, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
         PRISM_CUDA(cudaMemcpyAsync(h->xb.get(), x, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-        prism::fcg_solve(*h, *opts, h->bb.get(), h->xb.get(), stats);
+        run_solver(*h, *opts, h->bb.get(), h->xb.get(), stats);
         PRISM_CUDA(cudaMemcpyAsync(x, h->xb.get(), n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
         PRISM_CUDA(cudaStreamSynchronize(h->stream));
         return PRISM_OK;

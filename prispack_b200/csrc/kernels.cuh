@@ -78,7 +78,7 @@ __device__ __forceinline__ void grid_reduce(double (&v)[NV], ReduceSlot slot) {
 // products for the Krylov loop: Σ y_i z_i and Σ x_i q_i.
 // ---------------------------------------------------------------------------
 template <int G, int NDOT>
-__global__ void __launch_bounds__(kBlock) k_spmv(uint32_t n, const uint32_t* __restrict__ rowptr,
+static __global__ void __launch_bounds__(kBlock) k_spmv(uint32_t n, const uint32_t* __restrict__ rowptr,
                                                  const uint32_t* __restrict__ col, const double* __restrict__ val,
                                                  const double* __restrict__ x, double* __restrict__ y,
                                                  const double* __restrict__ z, const double* __restrict__ q,
@@ -143,7 +143,7 @@ constexpr unsigned long long kCanonicalNaN = 0x7FF8000000000000ull;
 
 enum : int { OP_DIV = 0, OP_MUL = 1, OP_NONE = 2, OP_PREDIV = 3 };
 
-__global__ void k_fill_pending(uint32_t n, unsigned long long* __restrict__ p) {
+static __global__ void k_fill_pending(uint32_t n, unsigned long long* __restrict__ p) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = kPending;
 }
 
@@ -291,7 +291,7 @@ __device__ __forceinline__ void st_shared_u64(unsigned long long* p, unsigned lo
 }
 
 template <typename Low, int OP>
-__global__ void __launch_bounds__(1024) k_sweep_slab(uint32_t n, uint32_t rows_per_cta, uint32_t smem_rows,
+static __global__ void __launch_bounds__(1024) k_sweep_slab(uint32_t n, uint32_t rows_per_cta, uint32_t smem_rows,
                                                      const uint32_t* __restrict__ cta_pos,
                                                      const uint32_t* __restrict__ order,
                                                      const uint32_t* __restrict__ rowptr,
@@ -347,7 +347,7 @@ __global__ void __launch_bounds__(1024) k_sweep_slab(uint32_t n, uint32_t rows_p
 // BaseVector.h:279-530), each with its reduction fused.
 // ---------------------------------------------------------------------------
 // r = b - y (r may be null) ; out = { Σ b_i^2, Σ (b_i - y_i)^2 }
-__global__ void __launch_bounds__(kBlock) k_residual(uint32_t n, const double* __restrict__ b,
+static __global__ void __launch_bounds__(kBlock) k_residual(uint32_t n, const double* __restrict__ b,
                                                      const double* __restrict__ y, double* __restrict__ r,
                                                      ReduceSlot slot) {
     double v[2] = {0.0, 0.0};
@@ -362,7 +362,7 @@ __global__ void __launch_bounds__(kBlock) k_residual(uint32_t n, const double* _
 }
 
 // out = { Σ a_i b_i }
-__global__ void __launch_bounds__(kBlock) k_dot(uint32_t n, const double* __restrict__ a,
+static __global__ void __launch_bounds__(kBlock) k_dot(uint32_t n, const double* __restrict__ a,
                                                 const double* __restrict__ b, ReduceSlot slot) {
     double v[1] = {0.0};
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[0] += a[i] * b[i];
@@ -370,7 +370,7 @@ __global__ void __launch_bounds__(kBlock) k_dot(uint32_t n, const double* __rest
 }
 
 // FCG direction update (CG.cpp:69-74): c = (w.v)/(d.v); d = w - c d; out = { Σ d_i r_i }
-__global__ void __launch_bounds__(kBlock) k_fcg_direction(uint32_t n, const double* __restrict__ w,
+static __global__ void __launch_bounds__(kBlock) k_fcg_direction(uint32_t n, const double* __restrict__ w,
                                                           double* __restrict__ d, const double* __restrict__ r,
                                                           const double* __restrict__ sc_wv,
                                                           const double* __restrict__ sc_dv, ReduceSlot slot) {
@@ -385,7 +385,7 @@ __global__ void __launch_bounds__(kBlock) k_fcg_direction(uint32_t n, const doub
 }
 
 // FCG step (CG.cpp:77-79): a = (d.r)/(d.v); x += a d; r -= a v; out = { Σ r_i^2 }
-__global__ void __launch_bounds__(kBlock) k_fcg_step(uint32_t n, double* __restrict__ x, double* __restrict__ r,
+static __global__ void __launch_bounds__(kBlock) k_fcg_step(uint32_t n, double* __restrict__ x, double* __restrict__ r,
                                                      const double* __restrict__ d, const double* __restrict__ v,
                                                      const double* __restrict__ sc_dr,
                                                      const double* __restrict__ sc_dv, ReduceSlot slot) {
@@ -400,4 +400,46 @@ __global__ void __launch_bounds__(kBlock) k_fcg_step(uint32_t n, double* __restr
     grid_reduce<1>(acc, slot);
 }
 
+}  // namespace prism
+
+namespace prism {
+// ---------------------------------------------------------------------------
+// GMRES kernels (GMRES<double>::solve, GMRES.cpp:122-221)
+// ---------------------------------------------------------------------------
+// dst = src * alpha (BaseVector::scale by a reciprocal, GMRES.cpp:158,188)
+static __global__ void __launch_bounds__(kBlock) k_scale(uint32_t n, const double* __restrict__ src, double alpha,
+                                                         double* __restrict__ dst) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[i] = src[i] * alpha;
+}
+
+// Modified Gram-Schmidt link i of Arnoldi step j (GMRES.cpp:174-180):
+//   w -= h_prev * v_prev   (h_prev from device memory; skipped when v_prev is null)
+//   out = { Σ w_i * v_next_i }  (or Σ w_i^2 when v_next is null: the new norm)
+static __global__ void __launch_bounds__(kBlock) k_mgs(uint32_t n, double* __restrict__ w,
+                                                       const double* __restrict__ v_prev,
+                                                       const double* __restrict__ h_prev,
+                                                       const double* __restrict__ v_next, ReduceSlot slot) {
+    const double h = v_prev ? *h_prev : 0.0;
+    double acc[1] = {0.0};
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double wi = w[i];
+        if (v_prev) {
+            wi = wi + -1.0 * (h * v_prev[i]);
+            w[i] = wi;
+        }
+        acc[0] += v_next ? wi * v_next[i] : wi * wi;
+    }
+    grid_reduce<1>(acc, slot);
+}
+
+// x += B * ksi over ncols columns of a column-major n x ncols block, summed
+// column by column per element (DenseMatrix::MatVec, DenseMatrix.cpp:208-243).
+static __global__ void __launch_bounds__(kBlock) k_gemv_add(uint32_t n, const double* __restrict__ B, uint32_t ncols,
+                                                            const double* __restrict__ ksi, double* __restrict__ x) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double acc = 0.0;
+        for (uint32_t c = 0; c < ncols; ++c) acc += B[(size_t)c * n + i] * ksi[c];
+        x[i] = x[i] + 1.0 * acc;
+    }
+}
 }  // namespace prism

@@ -42,6 +42,7 @@ enum Scalar : int {
     SC_DV = 4, SC_DR = 5,    // written together by k_spmv<.,2>: Σ v·d, Σ d·r
     SC_TMP = 6, SC_TMP2 = 7,
     SC_DR2 = 8,
+    SC_H0 = 16,              // GMRES Hessenberg column h_0 .. h_{j+1}
     kNumScalars = 16
 };
 
@@ -132,7 +133,10 @@ struct Handle {
     DevBuf<int> status;            // device status word of the bounded waits
     DevBuf<double> r, w, d, v, y;  // Krylov workspace (n each)
     DevBuf<double> xb, bb;         // host-pointer API staging
-    double* pinned = nullptr;      // host mirror of scalars (pinned)
+    DevBuf<double> V, Z, ksi;      // GMRES bases (n x (m+1), column-major) and LS coefficients
+    double* pinned = nullptr;      // host mirror of scalars (pinned), kScalarCapacity entries
+    static constexpr uint32_t kMaxKrylov = 1024;  // restart length limit
+    static constexpr uint32_t kScalarCapacity = kNumScalars + kMaxKrylov + 2;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
     ~Handle();
@@ -149,5 +153,6 @@ int selftest_wait_timeout(int device, unsigned long long wait_ns, int* device_st
 void init_device_info(DeviceInfo& info, int device);
 
 void fcg_solve(Handle& h, const prism_solve_opts& o, const double* b, double* x, prism_solve_stats* st);
+void gmres_solve(Handle& h, const prism_solve_opts& o, const double* b, double* x, prism_solve_stats* st);
 
 }  // namespace prism

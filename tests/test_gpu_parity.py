@@ -145,3 +145,51 @@ def test_bounded_wait_times_out_and_context_survives():
     S.set_precond(P.PRECOND_IC, tol=1e-3)
     x, st = S.solve(np.ones(A.n), tol=1e-8)
     assert st.converged
+
+
+@pytest.mark.parametrize("name", ["lap2d_8", "lap3d_6", "conv2d_16", "lap2d_64"])
+def test_fgmres_against_reference(name, manifest, load_golden):
+    """FlexibleGMRES with setRestart(true, 20) against the reference's outputs."""
+    g = load_golden(name)
+    S = system(g)
+    for key, e in manifest[name]["precond"].items():
+        if e.get("setup_rc") != 0:
+            continue
+        prec = P.PRISM_FP32 if key.endswith("fp32") else P.PRISM_FP64
+        S.set_precond(KIND[e["kind"]], tol=e["tol"], lfill=e["lfill"], precision=prec)
+        tag = f"{key}.fgmres20"
+        x, st = S.solve(g["b"], solver=P.SOLVER_FGMRES, tol=1e-8, restart=20)
+        ref = e[tag]
+        assert abs(st.num_iter - ref["iters"]) <= 1, (tag, st.num_iter, ref["iters"])
+        assert bool(st.converged) == ref["conv"]
+        if st.num_iter == ref["iters"]:
+            assert rel_err(x, g[f"{tag}.x"]) < REL_SOL, tag
+
+
+@pytest.mark.parametrize("name", ["lap2d_8", "lap3d_6", "conv2d_16", "lap2d_64"])
+def test_gmres_unpreconditioned_against_reference(name, manifest, load_golden):
+    g = load_golden(name)
+    S = system(g)
+    S.set_precond(P.PRECOND_NONE)
+    x, st = S.solve(g["b"], solver=P.SOLVER_GMRES, tol=1e-8, restart=30)
+    ref = manifest[name]["none.gmres30"]
+    assert abs(st.num_iter - ref["iters"]) <= 1, (st.num_iter, ref["iters"])
+    if st.num_iter == ref["iters"]:
+        assert rel_err(x, g["none.gmres30.x"]) < REL_SOL
+
+
+def test_fgmres_convection_3d_against_oracle():
+    """Nonsymmetric 3D problem beyond the fixtures: ILUT(20, 1e-2) + FGMRES(30), GPU vs oracle."""
+    A = P.CSRMatrix.laplacian(24, 20, 16, 0.4, -0.25, 0.1)
+    F = P.HostFactor(A, P.PRECOND_ILUT, tol=1e-2, lfill=20, precision=P.PRISM_FP32)
+    S = P.DeviceSystem(A)
+    S.attach(F)
+    b = np.random.default_rng(11).standard_normal(A.n)
+    x, st = S.solve(b, solver=P.SOLVER_FGMRES, tol=1e-10, restart=30)
+    f0, f1 = F.arrays(0), F.arrays(1)
+    OP = orc.Precond(2, A.n, f0[:3], f1[:3], f1[3])
+    xo, ito, erro, convo = orc.gmres(A.rowptr, A.col, A.val, b, OP, tol=1e-10, restart=30)
+    assert abs(st.num_iter - ito) <= 1 and st.converged == convo
+    if st.num_iter == ito:
+        assert rel_err(x, xo) < REL_SOL
+    assert abs(st.final_error - erro) < 1e-12
