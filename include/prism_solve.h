@@ -172,6 +172,40 @@ int32_t prism_factor_info(prism_factor f, uint64_t* mnnz, uint32_t* lower_levels
 /* attaches a host factor (built for a matrix of the same size) to a handle */
 int32_t prism_set_precond_factor(prism_handle h, prism_factor f);
 
+/* ---- AMSED / MSLR (AMSEDPrecondition, include/Preconditioner/AMSEDPrecondition.h:87-540) ----
+ * HID ordering by recursive bisection (the METIS calls of MetisTools.h:105-267
+ * are replaced by a deterministic level-structure bisection), per-subdomain
+ * RCM (vendored genrcm), ILDLT blocks, ICT on the last level, low-rank
+ * correction from the classic generalized Lanczos process. */
+typedef struct prism_amsed_opts {
+    int32_t levels;           /* levelNum (m_nlev_setup) */
+    int32_t lanczos_steps;    /* lanczosSteps (AMSED_MSTEPS = 30) */
+    int32_t low_rank;         /* lowRankSize (AMSED_RANK = 16): cap of the MSLR (basic) rank */
+    double eig_bound;         /* eigCorrectBound (AMSED_EIGVAL_CORRECTION = 0.8) */
+    int32_t lowrank_type;     /* 0 AMSEDBasic (MSLR), 1 AMSEDEigenvalueDeflation */
+    int32_t lanczos_type;     /* 0 UseClassicLanczos (the restarted variant is not provided) */
+    int32_t reorder;          /* 0 MatrixReorderNo, 2 MatrixReorderRCM (AMD is not provided) */
+    double factor_tol;        /* AMSED_FACTOR_TOLRANCE = 1e-3 */
+    uint32_t minsep;          /* AMSED_MINSEP = 3 */
+    uint64_t seed;            /* seed of the Lanczos start vector (the reference draws std::random_device) */
+} prism_amsed_opts;
+void prism_amsed_default_opts(prism_amsed_opts* o);
+int32_t prism_set_precond_amsed(prism_handle h, const prism_amsed_opts* o, int32_t precision);
+int32_t prism_factor_create_amsed(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val,
+                                  const prism_amsed_opts* o, int32_t precision, prism_factor* out);
+/* structure export for parity checks (arrays may be NULL to query sizes) */
+int32_t prism_amsed_info(prism_factor f, uint32_t* nlev, uint32_t* lev_ptr, uint32_t* ncomps, uint32_t* ranks,
+                         uint64_t* mnnz);
+int32_t prism_amsed_perm(prism_factor f, uint32_t* pperm);
+int32_t prism_amsed_dom_ptr(prism_factor f, int32_t level, uint32_t* dom_ptr);
+/* block factor of (level, block): ILDLT unit L^T + D, or (last level, block 0) IC L^T */
+int32_t prism_amsed_block(prism_factor f, int32_t level, int32_t block, uint32_t* n, uint64_t* nnz,
+                          uint32_t* rowptr, uint32_t* col, double* val, double* diag);
+/* which = 0: E (level rows x C columns), 1: C block */
+int32_t prism_amsed_coupling(prism_factor f, int32_t level, int32_t which, uint32_t* nrows, uint64_t* nnz,
+                             uint32_t* rowptr, uint32_t* col, double* val);
+int32_t prism_amsed_lowrank(prism_factor f, int32_t level, uint32_t* rank, uint32_t* nrem, double* W, double* H);
+
 /* out = M^{-1} in (in == out allowed) */
 int32_t prism_apply_device(prism_handle h, const double* in_d, double* out_d);
 int32_t prism_apply(prism_handle h, const double* in, double* out);

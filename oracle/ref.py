@@ -67,6 +67,15 @@ def load(fast: bool = False) -> C.CDLL:
     lib.ref_gmres_solve.argtypes = [vp, vp, C.c_int, C.c_uint, C.c_double, _f64p, _f64p,
                                     C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_int)]
     lib.ref_omp_max_threads.restype = C.c_int
+    lib.ref_set_seed.argtypes = [C.c_uint]
+    lib.ref_amsed_create.restype = vp
+    lib.ref_amsed_create.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int]
+    lib.ref_amsed_info.argtypes = [vp, C.POINTER(C.c_uint), C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_uint)]
+    lib.ref_amsed_perm.argtypes = [vp, C.c_void_p]
+    lib.ref_amsed_dom_ptr.argtypes = [vp, C.c_int, C.c_void_p]
+    lib.ref_amsed_block.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_uint), C.POINTER(C.c_uint), C.c_void_p,
+                                    C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.ref_amsed_lowrank.argtypes = [vp, C.c_int, C.POINTER(C.c_uint), C.POINTER(C.c_uint), C.c_void_p, C.c_void_p]
     _LIBS[key] = lib
     return lib
 
@@ -170,3 +179,67 @@ def gmres_solve(A: RefCSR, P: RefPrecond | None, b, x0=None, tol=1e-8, restart=5
     A.lib.ref_gmres_solve(A.h, P.h if P else None, int(flexible), restart, tol,
                           np.ascontiguousarray(b, np.float64), x, C.byref(it), C.byref(err), C.byref(conv))
     return x, it.value, err.value, bool(conv.value)
+
+
+KIND_AMSED = 5
+
+
+class RefAmsed(RefPrecond):
+    """AMSEDPrecondition<low, double>(A, levels, lanczosSteps, lowRankSize, eigCorrectBound,
+    localReorderType, lowRankType, lanczosType) through the shim (METIS stand-in, seeded
+    Lanczos start vector: base seed + call index, the product's convention)."""
+
+    def __init__(self, A: RefCSR, levels, lanczos_steps, low_rank, eig_bound=0.8, reorder=2, lowrank_type=1,
+                 lanczos_type=0, low_precision=False, seed=20241116):
+        self.A = A
+        self.lib = A.lib
+        self.kind = KIND_AMSED
+        self.seed = seed
+        self.h = self.lib.ref_amsed_create(A.h, levels, lanczos_steps, low_rank, eig_bound, reorder, lowrank_type,
+                                           lanczos_type, int(low_precision))
+
+    def setup(self) -> int:
+        self.lib.ref_set_seed(self.seed)
+        return self.lib.ref_precond_setup(self.h)
+
+    def info(self):
+        nlev, mnnz = C.c_uint(), C.c_uint()
+        self.lib.ref_amsed_info(self.h, C.byref(nlev), None, None, None, C.byref(mnnz))
+        L = nlev.value
+        lev_ptr = np.zeros(L + 1, np.uint32)
+        ncomps = np.zeros(L, np.uint32)
+        ranks = np.zeros(L, np.uint32)
+        self.lib.ref_amsed_info(self.h, C.byref(nlev), lev_ptr.ctypes.data, ncomps.ctypes.data, ranks.ctypes.data,
+                                C.byref(mnnz))
+        return {"nlev": L, "lev_ptr": lev_ptr, "ncomps": ncomps, "ranks": ranks, "mnnz": mnnz.value}
+
+    def perm(self):
+        n, _ = self.A.dims()
+        p = np.zeros(n, np.uint32)
+        self.lib.ref_amsed_perm(self.h, p.ctypes.data)
+        return p
+
+    def dom_ptr(self, level):
+        nc = int(self.info()["ncomps"][level])
+        d = np.zeros(nc + 1, np.uint32)
+        self.lib.ref_amsed_dom_ptr(self.h, level, d.ctypes.data)
+        return d
+
+    def block(self, level, block):
+        n, nnz = C.c_uint(), C.c_uint()
+        self.lib.ref_amsed_block(self.h, level, block, C.byref(n), C.byref(nnz), None, None, None, None)
+        rp = np.zeros(n.value + 1, np.uint32)
+        ci = np.zeros(nnz.value, np.uint32)
+        v = np.zeros(nnz.value, np.float64)
+        d = np.zeros(n.value, np.float64)
+        self.lib.ref_amsed_block(self.h, level, block, C.byref(n), C.byref(nnz), rp.ctypes.data, ci.ctypes.data,
+                                 v.ctypes.data, d.ctypes.data)
+        return rp, ci, v, d
+
+    def lowrank(self, level):
+        r, nrem = C.c_uint(), C.c_uint()
+        self.lib.ref_amsed_lowrank(self.h, level, C.byref(r), C.byref(nrem), None, None)
+        W = np.zeros(r.value * nrem.value)
+        H = np.zeros(r.value)
+        self.lib.ref_amsed_lowrank(self.h, level, C.byref(r), C.byref(nrem), W.ctypes.data, H.ctypes.data)
+        return W.reshape(r.value, nrem.value).T.copy(), H

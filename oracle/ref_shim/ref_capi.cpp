@@ -22,6 +22,10 @@
 #include "utils/MemoryTools/SharedPtrTools.h"
 #include "utils/TimerTools/CPUtimer.hpp"
 #include "Preconditioner/BasePreconditon.h"
+#include "utils/ExternalTools/MatrixReorderTools.h"
+#include "utils/ExternalTools/MetisTools.h"
+#include "utils/TestTools/WriteMtxTools.h"
+#include "utils/TestTools/checkTools.hpp"
 #define private public
 #define protected public
 #include "Preconditioner/IncompleteCholesky.h"
@@ -29,6 +33,7 @@
 #include "Preconditioner/IncompleteLU.h"
 #include "Solver/CG.h"
 #include "Solver/GMRES.h"
+#include "Preconditioner/AMSEDPrecondition.h"
 #undef private
 #undef protected
 
@@ -37,8 +42,10 @@ using namespace HOST;
 namespace {
 using CSRd = CSRMatrix<FLOAT64>;
 
+unsigned g_seed_base = 20241116u, g_seed_calls = 0u;
+
 struct RefPrecond {
-    int kind;        // 1 = IC, 2 = ILUT, 3 = ILDLT
+    int kind;        // 1 = IC, 2 = ILUT, 3 = ILDLT, 5 = AMSED
     int lowPrecision;  // 1 = factor values stored in FP32
     std::shared_ptr<BasePrecondition<FLOAT64>> p;
 };
@@ -156,6 +163,7 @@ void* ref_precond_create(void* hA, int kind, int lowPrecision, double tol, int l
 
 int ref_precond_setup(void* h) {
     auto* r = static_cast<RefPrecond*>(h);
+    if (r->kind == 5) g_seed_calls = 0;
     try {
         r->p->setup();
     } catch (...) {
@@ -237,3 +245,120 @@ int ref_gmres_solve(void* hA, void* hP, int gmresType, unsigned restart, double 
 int ref_omp_max_threads(void) { return omp_get_max_threads(); }
 
 }  // extern "C"
+
+// ---- AMSED -------------------------------------------------------------------
+extern "C" unsigned prism_ref_next_seed(void) { return g_seed_base + g_seed_calls++; }
+
+extern "C" void ref_set_seed(unsigned seed) {
+    g_seed_base = seed;
+    g_seed_calls = 0;
+}
+
+extern "C" void* ref_amsed_create(void* hA, int levels, int lanczos_steps, int low_rank, double eig_bound, int reorder,
+                       int lowrank_type, int lanczos_type, int low_precision) {
+    auto* A = static_cast<CSRd*>(hA);
+    std::shared_ptr<CSRd> sp(A, [](CSRd*) {});
+    auto* r = new RefPrecond{5, low_precision, nullptr};
+    auto ro = (MatrixReorderOption_t)reorder;
+    auto lt = (LowRankCorrectType_t)lowrank_type;
+    auto lz = (LanczosType_t)lanczos_type;
+    if (low_precision)
+        r->p = std::make_shared<AMSEDPrecondition<FLOAT32, FLOAT64>>(sp, levels, lanczos_steps, low_rank, eig_bound, ro, lt, lz);
+    else
+        r->p = std::make_shared<AMSEDPrecondition<FLOAT64, FLOAT64>>(sp, levels, lanczos_steps, low_rank, eig_bound, ro, lt, lz);
+    return r;
+}
+
+template <typename Low>
+static AMSEDPrecondition<Low, FLOAT64>* amsed(void* h) {
+    return static_cast<AMSEDPrecondition<Low, FLOAT64>*>(static_cast<RefPrecond*>(h)->p.get());
+}
+
+template <typename Low>
+static void amsed_info_t(void* h, unsigned* nlev, unsigned* lev_ptr, unsigned* ncomps, unsigned* ranks,
+                         unsigned* mnnz) {
+    auto* a = amsed<Low>(h);
+    *nlev = a->m_nlev_used;
+    if (mnnz) *mnnz = a->getPreconditionNonZeroCount();
+    for (UINT32 l = 0; l < a->m_nlev_used; ++l) {
+        if (ncomps) ncomps[l] = a->m_levs_all[l]->ncomps;
+        if (ranks) ranks[l] = a->m_levs_all[l]->rank;
+    }
+    if (lev_ptr)
+        for (UINT32 l = 0; l <= a->m_nlev_used; ++l) lev_ptr[l] = a->m_lev_ptr_v[l];
+}
+
+extern "C" void ref_amsed_info(void* h, unsigned* nlev, unsigned* lev_ptr, unsigned* ncomps, unsigned* ranks, unsigned* mnnz) {
+    if (static_cast<RefPrecond*>(h)->lowPrecision) amsed_info_t<FLOAT32>(h, nlev, lev_ptr, ncomps, ranks, mnnz);
+    else amsed_info_t<FLOAT64>(h, nlev, lev_ptr, ncomps, ranks, mnnz);
+}
+
+template <typename Low>
+static void amsed_perm_t(void* h, unsigned* perm) {
+    auto* a = amsed<Low>(h);
+    for (UINT32 i = 0; i < a->m_pperm.getLength(); ++i) perm[i] = a->m_pperm[i];
+}
+
+extern "C" void ref_amsed_perm(void* h, unsigned* perm) {
+    if (static_cast<RefPrecond*>(h)->lowPrecision) amsed_perm_t<FLOAT32>(h, perm);
+    else amsed_perm_t<FLOAT64>(h, perm);
+}
+
+template <typename Low>
+static void amsed_dom_t(void* h, int level, unsigned* dom) {
+    auto* a = amsed<Low>(h);
+    auto& d = *a->m_dom_ptr_v2[level];
+    for (UINT32 i = 0; i < d.getLength(); ++i) dom[i] = d[i];
+}
+
+extern "C" void ref_amsed_dom_ptr(void* h, int level, unsigned* dom) {
+    if (static_cast<RefPrecond*>(h)->lowPrecision) amsed_dom_t<FLOAT32>(h, level, dom);
+    else amsed_dom_t<FLOAT64>(h, level, dom);
+}
+
+// block factor: last level -> IncompleteCholesky L^T; other levels -> IncompleteLDLT L^T + D
+template <typename Low>
+static void amsed_block_t(void* h, int level, int block, unsigned* n, unsigned* nnz, unsigned* rowptr, unsigned* col,
+                          double* val, double* diag) {
+    auto* a = amsed<Low>(h);
+    auto& L = *a->m_levs_all[level];
+    const CSRMatrix<Low>* M;
+    const bool last = (UINT32)level == a->m_nlev_used - 1;
+    if (last) M = &*static_cast<IncompleteCholesky<Low, FLOAT64>*>(L.B_precond[block].get())->m_matTransL;
+    else M = &*static_cast<IncompleteLDLT<Low, FLOAT64>*>(L.B_precond[block].get())->m_matTransL;
+    *n = M->getRowNum();
+    *nnz = M->getRowOffsetPtr(0)[M->getRowNum()];
+    if (rowptr) {
+        for (UINT32 i = 0; i <= *n; ++i) rowptr[i] = M->getRowOffsetPtr(0)[i];
+        for (UINT32 k = 0; k < *nnz; ++k) { col[k] = M->getColIndicesPtr(0)[k]; val[k] = (double)M->getCSRValuesPtr(0)[k]; }
+        if (!last && diag) {
+            auto* p = static_cast<IncompleteLDLT<Low, FLOAT64>*>(L.B_precond[block].get());
+            for (UINT32 i = 0; i < *n; ++i) diag[i] = (*p->m_diagVals)[i];
+        }
+    }
+}
+
+extern "C" void ref_amsed_block(void* h, int level, int block, unsigned* n, unsigned* nnz, unsigned* rowptr, unsigned* col,
+                     double* val, double* diag) {
+    if (static_cast<RefPrecond*>(h)->lowPrecision) amsed_block_t<FLOAT32>(h, level, block, n, nnz, rowptr, col, val, diag);
+    else amsed_block_t<FLOAT64>(h, level, block, n, nnz, rowptr, col, val, diag);
+}
+
+template <typename Low>
+static void amsed_lowrank_t(void* h, int level, unsigned* rank, unsigned* nrem, double* W, double* H) {
+    auto* a = amsed<Low>(h);
+    auto& L = *a->m_levs_all[level];
+    *rank = L.rank;
+    *nrem = a->m_lev_ptr_v[a->m_nlev_used] - a->m_lev_ptr_v[level + 1];
+    if (W && L.rank) {
+        const double* w = L.W_mat.getMatValPtr();
+        for (size_t k = 0; k < (size_t)L.rank * *nrem; ++k) W[k] = w[k];
+        for (UINT32 i = 0; i < L.rank; ++i) H[i] = L.H_vec[i];
+    }
+}
+
+extern "C" void ref_amsed_lowrank(void* h, int level, unsigned* rank, unsigned* nrem, double* W, double* H) {
+    if (static_cast<RefPrecond*>(h)->lowPrecision) amsed_lowrank_t<FLOAT32>(h, level, rank, nrem, W, H);
+    else amsed_lowrank_t<FLOAT64>(h, level, rank, nrem, W, H);
+}
+

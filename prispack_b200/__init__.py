@@ -40,6 +40,19 @@ class SolveOpts(C.Structure):
     _fields_ = [("solver", C.c_int32), ("tol", C.c_double), ("max_iter", C.c_uint32), ("restart", C.c_uint32)]
 
 
+class AmsedOpts(C.Structure):
+    """prism_amsed_opts (include/prism_solve.h); defaults from prism_amsed_default_opts."""
+    _fields_ = [("levels", C.c_int32), ("lanczos_steps", C.c_int32), ("low_rank", C.c_int32),
+                ("eig_bound", C.c_double), ("lowrank_type", C.c_int32), ("lanczos_type", C.c_int32),
+                ("reorder", C.c_int32), ("factor_tol", C.c_double), ("minsep", C.c_uint32), ("seed", C.c_uint64)]
+
+
+# reference enum spellings (AMSEDPrecondition.h:53-72, MatrixReorderTools.h:14-18)
+AMSEDBasic, AMSEDEigenvalueDeflation = 0, 1
+UseClassicLanczos, UseRestartLanczos = 0, 1
+MatrixReorderNo, MatrixReorderAMD, MatrixReorderRCM = 0, 1, 2
+
+
 class SolveStats(C.Structure):
     _fields_ = [("num_iter", C.c_int32), ("converged", C.c_int32), ("final_error", C.c_double),
                 ("true_rel_residual", C.c_double), ("precond_applies", C.c_uint32),
@@ -85,6 +98,18 @@ _SIGS = {
     "prism_precond_sweep_device": (C.c_int32, [_vp, C.c_int32, _vp, _vp, C.c_int32]),
     "prism_precond_sweep_info": (C.c_int32, [_vp, C.c_int32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64),
                                              C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+    "prism_amsed_default_opts": (None, [C.POINTER(AmsedOpts)]),
+    "prism_set_precond_amsed": (C.c_int32, [_vp, C.POINTER(AmsedOpts), C.c_int32]),
+    "prism_factor_create_amsed": (C.c_int32, [C.c_uint32, _u32p, _u32p, _f64p, C.POINTER(AmsedOpts), C.c_int32,
+                                              C.POINTER(_vp)]),
+    "prism_amsed_info": (C.c_int32, [_vp, C.POINTER(C.c_uint32), _vp, _vp, _vp, C.POINTER(C.c_uint64)]),
+    "prism_amsed_perm": (C.c_int32, [_vp, _vp]),
+    "prism_amsed_dom_ptr": (C.c_int32, [_vp, C.c_int32, _vp]),
+    "prism_amsed_block": (C.c_int32, [_vp, C.c_int32, C.c_int32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64),
+                                      _vp, _vp, _vp, _vp]),
+    "prism_amsed_coupling": (C.c_int32, [_vp, C.c_int32, C.c_int32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64),
+                                         _vp, _vp, _vp]),
+    "prism_amsed_lowrank": (C.c_int32, [_vp, C.c_int32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), _vp, _vp]),
     "prism_apply_device": (C.c_int32, [_vp, _vp, _vp]),
     "prism_apply": (C.c_int32, [_vp, _f64p, _f64p]),
     "prism_solve_device": (C.c_int32, [_vp, C.POINTER(SolveOpts), _vp, _vp, C.POINTER(SolveStats)]),
@@ -213,6 +238,87 @@ class HostFactor:
         return {"mnnz": m.value, "lower_levels": lo.value, "upper_levels": up.value}
 
 
+def amsed_opts(**kw) -> AmsedOpts:
+    o = AmsedOpts()
+    load().prism_amsed_default_opts(C.byref(o))
+    for k, v in kw.items():
+        if not hasattr(o, k):
+            raise KeyError(k)
+        setattr(o, k, v)
+    return o
+
+
+class HostAmsed:
+    """AMSED / MSLR setup built on the host (prism_factor_create_amsed): the HID
+    permutation, level structure, block factors and low-rank terms; attachable
+    to a DeviceSystem of the same size and exportable for parity checks."""
+
+    def __init__(self, A: CSRMatrix, opts: AmsedOpts | None = None, precision: int = PRISM_FP64, **kw):
+        self.lib = load()
+        self.opts = opts if opts is not None else amsed_opts(**kw)
+        h = _vp()
+        _check(self.lib.prism_factor_create_amsed(A.n, A.rowptr, A.col, A.val, C.byref(self.opts), precision,
+                                                  C.byref(h)))
+        self.h = h
+        self.n = A.n
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.prism_factor_destroy(self.h)
+            self.h = None
+
+    def info(self) -> dict:
+        nlev, mnnz = C.c_uint32(), C.c_uint64()
+        _check(self.lib.prism_amsed_info(self.h, C.byref(nlev), None, None, None, C.byref(mnnz)))
+        L = nlev.value
+        lev_ptr = np.zeros(L + 1, np.uint32)
+        ncomps = np.zeros(L, np.uint32)
+        ranks = np.zeros(L, np.uint32)
+        _check(self.lib.prism_amsed_info(self.h, C.byref(nlev), lev_ptr.ctypes.data, ncomps.ctypes.data,
+                                         ranks.ctypes.data, C.byref(mnnz)))
+        return {"nlev": L, "lev_ptr": lev_ptr, "ncomps": ncomps, "ranks": ranks, "mnnz": mnnz.value}
+
+    def perm(self):
+        p = np.zeros(self.n, np.uint32)
+        _check(self.lib.prism_amsed_perm(self.h, p.ctypes.data))
+        return p
+
+    def dom_ptr(self, level: int):
+        nc = int(self.info()["ncomps"][level])
+        d = np.zeros(nc + 1, np.uint32)
+        _check(self.lib.prism_amsed_dom_ptr(self.h, level, d.ctypes.data))
+        return d
+
+    def block(self, level: int, block: int):
+        n, nnz = C.c_uint32(), C.c_uint64()
+        _check(self.lib.prism_amsed_block(self.h, level, block, C.byref(n), C.byref(nnz), None, None, None, None))
+        rp = np.zeros(n.value + 1, np.uint32)
+        ci = np.zeros(nnz.value, np.uint32)
+        v = np.zeros(nnz.value, np.float64)
+        d = np.zeros(n.value, np.float64)
+        _check(self.lib.prism_amsed_block(self.h, level, block, C.byref(n), C.byref(nnz), rp.ctypes.data,
+                                          ci.ctypes.data, v.ctypes.data, d.ctypes.data))
+        return rp, ci, v, d
+
+    def coupling(self, level: int, which: int = 0):
+        nr, nnz = C.c_uint32(), C.c_uint64()
+        _check(self.lib.prism_amsed_coupling(self.h, level, which, C.byref(nr), C.byref(nnz), None, None, None))
+        rp = np.zeros(nr.value + 1, np.uint32)
+        ci = np.zeros(nnz.value, np.uint32)
+        v = np.zeros(nnz.value, np.float64)
+        _check(self.lib.prism_amsed_coupling(self.h, level, which, C.byref(nr), C.byref(nnz), rp.ctypes.data,
+                                             ci.ctypes.data, v.ctypes.data))
+        return rp, ci, v
+
+    def lowrank(self, level: int):
+        r, nrem = C.c_uint32(), C.c_uint32()
+        _check(self.lib.prism_amsed_lowrank(self.h, level, C.byref(r), C.byref(nrem), None, None))
+        W = np.zeros(r.value * nrem.value, np.float64)
+        H = np.zeros(r.value, np.float64)
+        _check(self.lib.prism_amsed_lowrank(self.h, level, C.byref(r), C.byref(nrem), W.ctypes.data, H.ctypes.data))
+        return W.reshape(r.value, nrem.value).T.copy() if r.value else W.reshape(nrem.value, 0), H
+
+
 # =============================================================================
 # Device operator: one C-ABI handle (A on the GPU + preconditioner + workspace)
 # =============================================================================
@@ -269,7 +375,11 @@ class DeviceSystem:
         else:
             raise PrismError(9, f"preconditioner kind {kind} not available")
 
-    def attach(self, factor: "HostFactor"):
+    def set_amsed(self, opts: AmsedOpts | None = None, precision: int = PRISM_FP64, **kw):
+        o = opts if opts is not None else amsed_opts(**kw)
+        _check(self.lib.prism_set_precond_amsed(self.h, C.byref(o), precision))
+
+    def attach(self, factor):
         _check(self.lib.prism_set_precond_factor(self.h, factor.h))
 
     def precond_nnz(self) -> int:
@@ -467,3 +577,31 @@ class GMRES:
 
     def getConvergence(self):
         return bool(self.stats.converged)
+
+
+class AMSEDPrecondition:
+    """AMSEDPrecondition<Low, double>(A, levelNum, lanczosSteps, lowRankSize, eigCorrectBound,
+    localReorderType, lowRankType, lanczosType) (AMSEDPrecondition.cpp:60-79)."""
+
+    def __init__(self, system: DeviceSystem, levelNum, lanczosSteps, lowRankSize, eigCorrectBound=0.8,
+                 localReorderType=MatrixReorderRCM, lowRankType=AMSEDEigenvalueDeflation,
+                 lanczosType=UseClassicLanczos, precision=PRISM_FP64, seed=20241116):
+        self.system = system
+        self.opts = amsed_opts(levels=levelNum, lanczos_steps=lanczosSteps, low_rank=lowRankSize,
+                               eig_bound=eigCorrectBound, reorder=localReorderType, lowrank_type=lowRankType,
+                               lanczos_type=lanczosType, seed=seed)
+        self.precision = precision
+        self.host = None
+
+    def setup(self):
+        if self.host is None:
+            self.host = HostAmsed(self.system.A, self.opts, self.precision)
+            self.system.attach(self.host)
+
+    def MInvSolve(self, vec):
+        self.setup()
+        return self.system.apply(vec)
+
+    def getPreconditionNonZeroCount(self):
+        self.setup()
+        return self.host.info()["mnnz"]

@@ -1,0 +1,196 @@
+// AMSED / MSLR preconditioner apply on the device:
+// AMSEDPrecondition::MInvSolve (source/Preconditioner/AMSEDPrecondition.cpp:1976-2087)
+// and levelCInvRecursiveSolve (:1494-1587).
+//
+// Per level the diagonal blocks of all subdomains form one block-diagonal
+// factor, so a level's block solve is one lower and one upper sync-free sweep
+// over every subdomain at once (the reference runs them as OpenMP tasks,
+// :1690-1754).  E^T is stored explicitly so that x2 -= E^T x1 is a gather
+// (the reference scatters, CSRMatrix.h:453-486).  The low-rank term
+// W (H o (W^T x)) is a multi-dot plus a rank-r update.  The permutation of
+// the right-hand side (prepareRightHand / recoverRightHand) brackets the
+// recursion.  All scratch is allocated once, at construction.
+#include <algorithm>
+#include <cstring>
+
+#include "amsed_setup.hpp"
+#include "kernels.cuh"
+#include "solve.cuh"
+
+namespace prism {
+
+namespace {
+// CSR transpose for a rectangular nrows x ncols matrix (column order inside
+// each output row = increasing source row, i.e. the reference's scatter order)
+void transpose_rect(const CsrHost& M, uint32_t ncols, std::vector<uint32_t>& trp, std::vector<uint32_t>& tcol,
+                    std::vector<double>& tval) {
+    const uint64_t nnz = M.nnz();
+    trp.assign((size_t)ncols + 1, 0);
+    tcol.resize(nnz);
+    tval.resize(nnz);
+    for (uint64_t k = 0; k < nnz; ++k) trp[M.col[k] + 1]++;
+    for (uint32_t c = 0; c < ncols; ++c) trp[c + 1] += trp[c];
+    std::vector<uint32_t> fill(trp.begin(), trp.end() - 1);
+    for (uint32_t r = 0; r < M.n; ++r)
+        for (uint32_t k = M.rowptr[r]; k < M.rowptr[r + 1]; ++k) {
+            const uint32_t c = M.col[k];
+            tcol[fill[c]] = r;
+            tval[fill[c]] = M.val[k];
+            fill[c]++;
+        }
+}
+
+void upload_csr(DeviceCsr& d, uint32_t nrows, const std::vector<uint32_t>& rp, const std::vector<uint32_t>& ci,
+                const std::vector<double>& v, cudaStream_t st) {
+    d.n = nrows;
+    d.nnz = rp.empty() ? 0 : rp[nrows];
+    d.rowptr.upload(rp.data(), rp.size(), st);
+    d.col.upload(ci.data(), ci.size(), st);
+    d.val.upload(v.data(), v.size(), st);
+    if (d.col.size() == 0) d.col.alloc(1);
+    if (d.val.size() == 0) d.val.alloc(1);
+}
+}  // namespace
+
+AmsedPrecond::AmsedPrecond(Handle& h, std::shared_ptr<const HostAmsed> a) : h_(h), a_(std::move(a)) {
+    if (a_->fp32) build(*a_->s32);
+    else build(*a_->s64);
+}
+
+uint64_t AmsedPrecond::mnnz() const { return a_->fp32 ? a_->s32->mnnz : a_->s64->mnnz; }
+
+template <typename Low>
+void AmsedPrecond::build(const AmsedSetup<Low>& S) {
+    cudaStream_t st = h_.stream;
+    n_ = S.n;
+    nlev_ = S.nlev;
+    lev_ptr_ = S.lev_ptr;
+    pperm_.upload(S.pperm.data(), S.pperm.size(), st);
+    X_.alloc(n_);
+    sweep_tmp_.alloc(n_);
+    lv_.clear();
+    lv_.resize(nlev_);
+    uint32_t max_rank = 0;
+    for (uint32_t l = 0; l < nlev_; ++l) {
+        const AmsedLevel<Low>& L = S.levels[l];
+        Level& D = lv_[l];
+        D.nb = S.lev_ptr[l + 1] - S.lev_ptr[l];
+        D.nrem = S.n - S.lev_ptr[l + 1];
+        Sweep<Low> lo, up;
+        if (l + 1 == nlev_) {
+            // last level: IC of block 0 (the reference factors and applies only B_mat[0], :694-716, :1504-1508)
+            D.nfac = L.B[0].n;
+            ic_sweeps<Low>(L.Lt[0], lo, up);
+        } else {
+            // block-diagonal ILDLT of all subdomains of the level
+            CsrT<Low> Lt;
+            std::vector<double> Dg;
+            Lt.n = D.nb;
+            Lt.rowptr.assign((size_t)D.nb + 1, 0);
+            for (uint32_t b = 0; b < L.ncomps; ++b) {
+                const uint32_t off = L.dom_ptr[b] - L.dom_ptr[0];
+                const CsrT<Low>& f = L.Lt[b];
+                for (uint32_t i = 0; i < f.n; ++i) {
+                    for (uint32_t k = f.rowptr[i]; k < f.rowptr[i + 1]; ++k) {
+                        Lt.col.push_back(f.col[k] + off);
+                        Lt.val.push_back(f.val[k]);
+                    }
+                    Lt.rowptr[off + i + 1] = (uint32_t)Lt.col.size();
+                }
+                Dg.insert(Dg.end(), L.D[b].begin(), L.D[b].end());
+            }
+            D.nfac = D.nb;
+            ildlt_sweeps<Low>(Lt, Dg, lo, up);
+        }
+        tune_sweep<Low>(h_, D.lower, lo);
+        tune_sweep<Low>(h_, D.upper, up);
+        if (l + 1 < nlev_) {
+            upload_csr(D.E, L.E.n, L.E.rowptr, L.E.col, L.E.val, st);
+            std::vector<uint32_t> trp, tcol;
+            std::vector<double> tval;
+            transpose_rect(L.E, D.nrem, trp, tcol, tval);
+            upload_csr(D.Et, D.nrem, trp, tcol, tval, st);
+            D.rank = L.rank;
+            if (D.rank > (uint32_t)kMaxRank)
+                throw Error(PRISM_ERR_UNSUPPORTED, "low-rank correction above " + std::to_string(kMaxRank) + " columns");
+            if (D.rank) {
+                D.W.upload(L.W.data(), L.W.size(), st);
+                D.H.upload(L.H.data(), L.H.size(), st);
+                D.t.alloc(D.rank);
+            }
+            D.xc.alloc(std::max<uint32_t>(D.nrem, 1));
+            D.tmp.alloc(std::max<uint32_t>(D.nb, 1));
+            D.tmp2.alloc(std::max<uint32_t>(D.nb, 1));
+            max_rank = std::max(max_rank, D.rank);
+        }
+    }
+    partial_.alloc((size_t)std::max<uint32_t>(max_rank, 1) * (size_t)h_.info.sms * 4);
+    PRISM_CUDA(cudaStreamSynchronize(st));
+}
+
+// out = B_level^{-1} in over the level's rows (in == out allowed)
+void AmsedPrecond::block_solve(cudaStream_t st, int level, const double* in, double* out) {
+    Level& L = lv_[level];
+    if (L.nfac < L.nb && in != out)  // rows without a factor (last level beyond block 0) pass through
+        PRISM_CUDA(cudaMemcpyAsync(out + L.nfac, in + L.nfac, (L.nb - L.nfac) * sizeof(double),
+                                   cudaMemcpyDeviceToDevice, st));
+    launch_fill(st, h_, L.nfac, sweep_tmp_.get());
+    if (in != out) launch_fill(st, h_, L.nfac, out);
+    launch_sweep(h_, st, L.lower, in, sweep_tmp_.get());
+    if (in == out) launch_fill(st, h_, L.nfac, out);
+    launch_sweep(h_, st, L.upper, sweep_tmp_.get(), out);
+}
+
+// levelCInvRecursiveSolve(level, x): x is the C block of `level` (global rows lev_ptr[level+1]..n)
+void AmsedPrecond::c_solve(cudaStream_t st, int level, double* x) {
+    const int next = level + 1;
+    if (level == (int)nlev_ - 2) {
+        block_solve(st, next, x, x);
+        return;
+    }
+    Level& L = lv_[next];
+    const int vg = vec_grid(h_, std::max(L.nb, L.nrem));
+    // x1 = B^{-1} x1
+    block_solve(st, next, x, x);
+    // x2 -= E^T x1
+    launch_spmv(h_, st, L.nrem, L.Et.rowptr.get(), L.Et.col.get(), L.Et.val.get(), x, x + L.nb, 1);
+    // xc = x2 ; x2 = C^{-1} x2
+    PRISM_CUDA(cudaMemcpyAsync(L.xc.get(), x + L.nb, L.nrem * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    c_solve(st, next, x + L.nb);
+    // x2 += W (H o (W^T xc))
+    if (L.rank) {
+        const int g = vec_grid(h_, L.nrem);
+        k_lowrank_dots<<<g, kBlock, 0, st>>>(L.nrem, L.rank, L.W.get(), L.xc.get(), partial_.get());
+        PRISM_LAUNCHED();
+        k_lowrank_finish<<<1, 128, 0, st>>>((uint32_t)g, L.rank, partial_.get(), L.H.get(), L.t.get());
+        PRISM_LAUNCHED();
+        k_lowrank_add<<<g, kBlock, 0, st>>>(L.nrem, L.rank, L.W.get(), L.t.get(), x + L.nb);
+        PRISM_LAUNCHED();
+    }
+    // x1 -= B^{-1} (E x2)
+    launch_spmv(h_, st, L.nb, L.E.rowptr.get(), L.E.col.get(), L.E.val.get(), x + L.nb, L.tmp.get(), 0);
+    block_solve(st, next, L.tmp.get(), L.tmp2.get());
+    k_sub<<<vg, kBlock, 0, st>>>(L.nb, L.tmp2.get(), x);
+    PRISM_LAUNCHED();
+}
+
+void AmsedPrecond::apply(cudaStream_t st, const double* in, double* out) {
+    const int vg = vec_grid(h_, n_);
+    k_permute<<<vg, kBlock, 0, st>>>(n_, pperm_.get(), in, X_.get(), 0);
+    PRISM_LAUNCHED();
+    if (nlev_ == 1) block_solve(st, 0, X_.get(), X_.get());
+    else c_solve(st, -1, X_.get());
+    k_permute<<<vg, kBlock, 0, st>>>(n_, pperm_.get(), X_.get(), out, 1);
+    PRISM_LAUNCHED();
+}
+
+uint32_t AmsedPrecond::levels(int sweep) const {
+    uint32_t m = 0;
+    for (const Level& L : lv_) m = std::max(m, sweep == 0 ? L.lower.num_levels : L.upper.num_levels);
+    return m;
+}
+
+template void AmsedPrecond::build<double>(const AmsedSetup<double>&);
+template void AmsedPrecond::build<float>(const AmsedSetup<float>&);
+
+}  // namespace prism

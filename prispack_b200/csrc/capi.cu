@@ -48,8 +48,39 @@ struct DeviceGuard {
 struct prism_handle_s : Handle {};
 
 struct prism_factor_s {
-    std::shared_ptr<const prism::HostFactor> f;
+    std::shared_ptr<const prism::HostFactor> f;      // IC / ILUT / ILDLT
+    std::shared_ptr<const prism::HostAmsed> amsed;   // AMSED / MSLR
 };
+
+static prism::AmsedOptions to_options(const prism_amsed_opts* o) {
+    prism::AmsedOptions a;
+    a.levels = o->levels;
+    a.lanczos_steps = o->lanczos_steps;
+    a.low_rank = o->low_rank;
+    a.eig_bound = o->eig_bound;
+    a.lowrank_type = o->lowrank_type;
+    a.lanczos_type = o->lanczos_type;
+    a.reorder = o->reorder;
+    a.factor_tol = o->factor_tol;
+    a.minsep = o->minsep;
+    a.seed = o->seed;
+    return a;
+}
+
+static std::shared_ptr<prism::HostAmsed> build_amsed(const prism::CsrHost& A, const prism_amsed_opts* o,
+                                                     int32_t precision, int* rc, std::string* err) {
+    auto h = std::make_shared<prism::HostAmsed>();
+    h->fp32 = precision == PRISM_FP32;
+    h->opt = to_options(o);
+    if (h->fp32) {
+        h->s32 = std::make_shared<prism::AmsedSetup<float>>();
+        *rc = prism::amsed_setup<float>(A, h->opt, *h->s32, err);
+    } else {
+        h->s64 = std::make_shared<prism::AmsedSetup<double>>();
+        *rc = prism::amsed_setup<double>(A, h->opt, *h->s64, err);
+    }
+    return h;
+}
 
 static int32_t set_tri(prism_handle h, int kind, double tol, uint32_t lfill, int32_t precision) {
     if (!h) return fail(PRISM_ERR_ARG, "null handle");
@@ -229,11 +260,157 @@ int32_t prism_set_precond_ilut(prism_handle h, uint32_t lfill, double tol, int32
 
 int32_t prism_set_precond_factor(prism_handle h, prism_factor f) {
     if (!h || !f) return fail(PRISM_ERR_ARG, "null argument");
-    if (f->f->f0.n != h->A.n) return fail(PRISM_ERR_ARG, "factor dimension does not match the operator");
+    const uint32_t fn = f->f ? f->f->f0.n : (f->amsed->fp32 ? f->amsed->s32->n : f->amsed->s64->n);
+    if (fn != h->A.n) return fail(PRISM_ERR_ARG, "factor dimension does not match the operator");
     return guarded([&]() -> int {
         DeviceGuard g(h->info.device);
         h->P.reset();
-        h->P = std::make_unique<prism::TriangularPrecond>(*h, f->f);
+        if (f->f) h->P = std::make_unique<prism::TriangularPrecond>(*h, f->f);
+        else h->P = std::make_unique<prism::AmsedPrecond>(*h, f->amsed);
+        return PRISM_OK;
+    });
+}
+
+void prism_amsed_default_opts(prism_amsed_opts* o) {
+    if (!o) return;
+    prism::AmsedOptions a;
+    o->levels = a.levels;
+    o->lanczos_steps = a.lanczos_steps;
+    o->low_rank = a.low_rank;
+    o->eig_bound = a.eig_bound;
+    o->lowrank_type = a.lowrank_type;
+    o->lanczos_type = a.lanczos_type;
+    o->reorder = a.reorder;
+    o->factor_tol = a.factor_tol;
+    o->minsep = a.minsep;
+    o->seed = a.seed;
+}
+
+int32_t prism_set_precond_amsed(prism_handle h, const prism_amsed_opts* o, int32_t precision) {
+    if (!h || !o) return fail(PRISM_ERR_ARG, "null argument");
+    if (precision != PRISM_FP64 && precision != PRISM_FP32) return fail(PRISM_ERR_ARG, "bad precision");
+    return guarded([&]() -> int {
+        DeviceGuard g(h->info.device);
+        h->P.reset();
+        int rc = 0;
+        std::string err;
+        auto a = build_amsed(h->A_host, o, precision, &rc, &err);
+        if (rc) return fail(rc, err);
+        h->P = std::make_unique<prism::AmsedPrecond>(*h, a);
+        return PRISM_OK;
+    });
+}
+
+int32_t prism_factor_create_amsed(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val,
+                                  const prism_amsed_opts* o, int32_t precision, prism_factor* out) {
+    if (!out || !o) return fail(PRISM_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (n == 0 || !rowptr || !col || !val) return fail(PRISM_ERR_ARG, "empty or null CSR");
+    if (precision != PRISM_FP64 && precision != PRISM_FP32) return fail(PRISM_ERR_ARG, "bad precision");
+    std::string bad = prism::validate_csr(n, rowptr, col);
+    if (!bad.empty()) return fail(PRISM_ERR_BAD_MATRIX, bad);
+    return guarded([&]() -> int {
+        prism::CsrHost A;
+        A.n = n;
+        A.rowptr.assign(rowptr, rowptr + n + 1);
+        A.col.assign(col, col + rowptr[n]);
+        A.val.assign(val, val + rowptr[n]);
+        int rc = 0;
+        std::string err;
+        auto a = build_amsed(A, o, precision, &rc, &err);
+        if (rc) return fail(rc, err);
+        *out = new prism_factor_s{nullptr, std::move(a)};
+        return PRISM_OK;
+    });
+}
+
+// ---- AMSED structure export (parity checks) -------------------------------------
+}  // extern "C"
+
+template <typename F>
+static int32_t with_amsed(prism_factor f, F&& fn) {
+    if (!f || !f->amsed) return fail(PRISM_ERR_ARG, "not an AMSED factor");
+    return guarded([&]() -> int {
+        if (f->amsed->fp32) return fn(*f->amsed->s32);
+        return fn(*f->amsed->s64);
+    });
+}
+
+extern "C" {
+
+int32_t prism_amsed_info(prism_factor f, uint32_t* nlev, uint32_t* lev_ptr, uint32_t* ncomps, uint32_t* ranks,
+                         uint64_t* mnnz) {
+    return with_amsed(f, [&](const auto& S) -> int {
+        if (nlev) *nlev = S.nlev;
+        if (mnnz) *mnnz = S.mnnz;
+        for (uint32_t l = 0; l < S.nlev; ++l) {
+            if (ncomps) ncomps[l] = S.levels[l].ncomps;
+            if (ranks) ranks[l] = S.levels[l].rank;
+        }
+        if (lev_ptr) std::memcpy(lev_ptr, S.lev_ptr.data(), S.lev_ptr.size() * sizeof(uint32_t));
+        return PRISM_OK;
+    });
+}
+
+int32_t prism_amsed_perm(prism_factor f, uint32_t* pperm) {
+    if (!pperm) return fail(PRISM_ERR_ARG, "null output");
+    return with_amsed(f, [&](const auto& S) -> int {
+        std::memcpy(pperm, S.pperm.data(), S.pperm.size() * sizeof(uint32_t));
+        return PRISM_OK;
+    });
+}
+
+int32_t prism_amsed_dom_ptr(prism_factor f, int32_t level, uint32_t* dom_ptr) {
+    if (!dom_ptr) return fail(PRISM_ERR_ARG, "null output");
+    return with_amsed(f, [&](const auto& S) -> int {
+        if (level < 0 || (uint32_t)level >= S.nlev) return fail(PRISM_ERR_ARG, "level out of range");
+        const auto& d = S.levels[level].dom_ptr;
+        std::memcpy(dom_ptr, d.data(), d.size() * sizeof(uint32_t));
+        return PRISM_OK;
+    });
+}
+
+int32_t prism_amsed_block(prism_factor f, int32_t level, int32_t block, uint32_t* n, uint64_t* nnz,
+                          uint32_t* rowptr, uint32_t* col, double* val, double* diag) {
+    return with_amsed(f, [&](const auto& S) -> int {
+        if (level < 0 || (uint32_t)level >= S.nlev) return fail(PRISM_ERR_ARG, "level out of range");
+        const auto& L = S.levels[level];
+        if (block < 0 || (size_t)block >= L.Lt.size()) return fail(PRISM_ERR_ARG, "block out of range");
+        const auto& F = L.Lt[block];
+        if (n) *n = F.n;
+        if (nnz) *nnz = F.nnz();
+        if (rowptr) std::memcpy(rowptr, F.rowptr.data(), F.rowptr.size() * sizeof(uint32_t));
+        if (col) std::memcpy(col, F.col.data(), F.col.size() * sizeof(uint32_t));
+        if (val)
+            for (size_t k = 0; k < F.val.size(); ++k) val[k] = (double)F.val[k];
+        if (diag && block < (int32_t)L.D.size() && !L.D[block].empty())
+            std::memcpy(diag, L.D[block].data(), L.D[block].size() * sizeof(double));
+        return PRISM_OK;
+    });
+}
+
+int32_t prism_amsed_coupling(prism_factor f, int32_t level, int32_t which, uint32_t* nrows, uint64_t* nnz,
+                             uint32_t* rowptr, uint32_t* col, double* val) {
+    return with_amsed(f, [&](const auto& S) -> int {
+        if (level < 0 || (uint32_t)level + 1 >= S.nlev) return fail(PRISM_ERR_ARG, "level has no coupling block");
+        const prism::CsrHost& M = which == 0 ? S.levels[level].E : S.levels[level].C;
+        if (nrows) *nrows = M.n;
+        if (nnz) *nnz = M.nnz();
+        if (rowptr) std::memcpy(rowptr, M.rowptr.data(), M.rowptr.size() * sizeof(uint32_t));
+        if (col) std::memcpy(col, M.col.data(), M.col.size() * sizeof(uint32_t));
+        if (val) std::memcpy(val, M.val.data(), M.val.size() * sizeof(double));
+        return PRISM_OK;
+    });
+}
+
+int32_t prism_amsed_lowrank(prism_factor f, int32_t level, uint32_t* rank, uint32_t* nrem, double* W, double* H) {
+    return with_amsed(f, [&](const auto& S) -> int {
+        if (level < 0 || (uint32_t)level >= S.nlev) return fail(PRISM_ERR_ARG, "level out of range");
+        const auto& L = S.levels[level];
+        if (rank) *rank = L.rank;
+        if (nrem) *nrem = S.n - S.lev_ptr[level + 1];
+        if (W) std::memcpy(W, L.W.data(), L.W.size() * sizeof(double));
+        if (H) std::memcpy(H, L.H.data(), L.H.size() * sizeof(double));
         return PRISM_OK;
     });
 }
@@ -259,7 +436,7 @@ int32_t prism_factor_create(int32_t kind, uint32_t n, const uint32_t* rowptr, co
         std::string err;
         int rc = prism::build_triangular(kind, A, tol, lfill, precision == PRISM_FP32, *f, &err);
         if (rc) return fail(rc, err);
-        *out = new prism_factor_s{std::move(f)};
+        *out = new prism_factor_s{std::move(f), nullptr};
         return PRISM_OK;
     });
 }
@@ -271,7 +448,7 @@ int32_t prism_factor_destroy(prism_factor f) {
 
 int32_t prism_factor_get(prism_factor f, int32_t which, uint32_t* n, uint64_t* nnz, uint32_t* rowptr, uint32_t* col,
                          double* val, double* diag) {
-    if (!f) return fail(PRISM_ERR_ARG, "null factor");
+    if (!f || !f->f) return fail(PRISM_ERR_ARG, "null or non-triangular factor");
     int rc = prism::export_host_factor(*f->f, which, n, nnz, rowptr, col, val, diag);
     if (rc) return fail(rc, "which must be 0 (or 1 for ILUT)");
     return PRISM_OK;
@@ -279,6 +456,12 @@ int32_t prism_factor_get(prism_factor f, int32_t which, uint32_t* n, uint64_t* n
 
 int32_t prism_factor_info(prism_factor f, uint64_t* mnnz, uint32_t* lower_levels, uint32_t* upper_levels) {
     if (!f) return fail(PRISM_ERR_ARG, "null factor");
+    if (f->amsed) {
+        if (mnnz) *mnnz = f->amsed->fp32 ? f->amsed->s32->mnnz : f->amsed->s64->mnnz;
+        if (lower_levels) *lower_levels = 0;
+        if (upper_levels) *upper_levels = 0;
+        return PRISM_OK;
+    }
     const prism::HostFactor& F = *f->f;
     if (mnnz) *mnnz = F.mnnz;
     if (lower_levels) *lower_levels = F.fp32 ? F.lower32.num_levels : F.lower64.num_levels;

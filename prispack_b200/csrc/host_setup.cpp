@@ -478,6 +478,49 @@ void widen_csr(const CsrT<Low>& in, CsrT<double>& out) {
     out.val.assign(in.val.begin(), in.val.end());
 }
 
+}  // namespace
+
+template <typename Low>
+void ic_sweeps(const CsrT<Low>& Lt, Sweep<Low>& lo, Sweep<Low>& up) {
+    // IC: L^T rows hold the diagonal first.  Lower sweep = gather over L
+    // (transpose of the strictly upper part), upper sweep = gather over L^T.
+    const uint32_t n = Lt.n;
+    std::vector<uint32_t> urp(n + 1, 0), ucol;
+    std::vector<Low> uval;
+    std::vector<double> dg(n);
+    ucol.reserve(Lt.nnz());
+    uval.reserve(Lt.nnz());
+    for (uint32_t i = 0; i < n; ++i) {
+        dg[i] = (double)Lt.val[Lt.rowptr[i]];
+        for (uint32_t k = Lt.rowptr[i] + 1; k < Lt.rowptr[i + 1]; ++k) {
+            ucol.push_back(Lt.col[k]);
+            uval.push_back(Lt.val[k]);
+        }
+        urp[i + 1] = (uint32_t)ucol.size();
+    }
+    std::vector<uint32_t> lrp, lcol;
+    std::vector<Low> lval;
+    transpose_csr<Low>(n, urp, ucol, uval, lrp, lcol, lval);
+    build_sweep<Low>(n, lrp, lcol, lval, &dg, SWEEP_DIV, true, lo);
+    build_sweep<Low>(n, urp, ucol, uval, &dg, SWEEP_DIV, false, up);
+}
+
+template <typename Low>
+void ildlt_sweeps(const CsrT<Low>& Lt, const std::vector<double>& D, Sweep<Low>& lo, Sweep<Low>& up) {
+    // ILDLT: unit L^T without diagonal, D separate; D^{-1} folded into the upper sweep.
+    const uint32_t n = Lt.n;
+    std::vector<uint32_t> lrp, lcol;
+    std::vector<Low> lval;
+    transpose_csr<Low>(n, Lt.rowptr, Lt.col, Lt.val, lrp, lcol, lval);
+    build_sweep<Low>(n, lrp, lcol, lval, nullptr, SWEEP_NONE, true, lo);
+    build_sweep<Low>(n, Lt.rowptr, Lt.col, Lt.val, &D, SWEEP_PREDIV, false, up);
+}
+template void ic_sweeps<double>(const CsrT<double>&, Sweep<double>&, Sweep<double>&);
+template void ic_sweeps<float>(const CsrT<float>&, Sweep<float>&, Sweep<float>&);
+template void ildlt_sweeps<double>(const CsrT<double>&, const std::vector<double>&, Sweep<double>&, Sweep<double>&);
+template void ildlt_sweeps<float>(const CsrT<float>&, const std::vector<double>&, Sweep<float>&, Sweep<float>&);
+
+namespace {
 template <typename Low>
 int build_tri_t(int kind, const CsrHost& A, double tol, uint32_t lfill, HostFactor& F, Sweep<Low>& lo,
                 Sweep<Low>& up, std::string* err) {
@@ -488,24 +531,7 @@ int build_tri_t(int kind, const CsrHost& A, double tol, uint32_t lfill, HostFact
         CsrT<Low> Lt;
         int rc = ict_factor<Low>(A, tol, Lt, err);
         if (rc) return rc;
-        std::vector<uint32_t> urp(n + 1, 0), ucol;
-        std::vector<Low> uval;
-        std::vector<double> dg(n);
-        ucol.reserve(Lt.nnz());
-        uval.reserve(Lt.nnz());
-        for (uint32_t i = 0; i < n; ++i) {
-            dg[i] = (double)Lt.val[Lt.rowptr[i]];
-            for (uint32_t k = Lt.rowptr[i] + 1; k < Lt.rowptr[i + 1]; ++k) {
-                ucol.push_back(Lt.col[k]);
-                uval.push_back(Lt.val[k]);
-            }
-            urp[i + 1] = (uint32_t)ucol.size();
-        }
-        std::vector<uint32_t> lrp, lcol;
-        std::vector<Low> lval;
-        transpose_csr<Low>(n, urp, ucol, uval, lrp, lcol, lval);
-        build_sweep<Low>(n, lrp, lcol, lval, &dg, SWEEP_DIV, true, lo);
-        build_sweep<Low>(n, urp, ucol, uval, &dg, SWEEP_DIV, false, up);
+        ic_sweeps<Low>(Lt, lo, up);
         F.mnnz = Lt.nnz() * 2 + n;  // IncompleteCholesky.cpp:245
         widen_csr(Lt, F.f0);
         return 0;
@@ -516,11 +542,7 @@ int build_tri_t(int kind, const CsrHost& A, double tol, uint32_t lfill, HostFact
         std::vector<double> D;
         int rc = ildlt_factor<Low>(A, tol, Lt, D, err);
         if (rc) return rc;
-        std::vector<uint32_t> lrp, lcol;
-        std::vector<Low> lval;
-        transpose_csr<Low>(n, Lt.rowptr, Lt.col, Lt.val, lrp, lcol, lval);
-        build_sweep<Low>(n, lrp, lcol, lval, nullptr, SWEEP_NONE, true, lo);
-        build_sweep<Low>(n, Lt.rowptr, Lt.col, Lt.val, &D, SWEEP_PREDIV, false, up);
+        ildlt_sweeps<Low>(Lt, D, lo, up);
         F.mnnz = Lt.nnz() * 2 + n;  // IncompleteLDLT.cpp:185
         widen_csr(Lt, F.f0);
         F.diag = D;

@@ -133,6 +133,13 @@ struct HostFactor {
     Sweep<float> lower32, upper32;
 };
 
+// The two device sweeps of an IC factor (L^T with diagonal first) and of an
+// ILDLT factor (unit L^T without diagonal, pivots D).
+template <typename Low>
+void ic_sweeps(const CsrT<Low>& Lt, Sweep<Low>& lo, Sweep<Low>& up);
+template <typename Low>
+void ildlt_sweeps(const CsrT<Low>& Lt, const std::vector<double>& D, Sweep<Low>& lo, Sweep<Low>& up);
+
 int build_triangular(int kind, const CsrHost& A, double tol, uint32_t lfill, bool fp32, HostFactor& out,
                      std::string* err);
 

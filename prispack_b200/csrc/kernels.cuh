@@ -443,3 +443,91 @@ static __global__ void __launch_bounds__(kBlock) k_gemv_add(uint32_t n, const do
     }
 }
 }  // namespace prism
+
+namespace prism {
+// ---------------------------------------------------------------------------
+// AMSED apply kernels (AMSEDPrecondition::MInvSolve / levelCInvRecursiveSolve,
+// AMSEDPrecondition.cpp:1494-1587, 1976-2087)
+// ---------------------------------------------------------------------------
+// out[i] = in[perm[i]]  (prepareRightHand) / out[perm[i]] = in[i] (recoverRightHand)
+static __global__ void __launch_bounds__(kBlock) k_permute(uint32_t n, const uint32_t* __restrict__ perm,
+                                                           const double* __restrict__ in, double* __restrict__ out,
+                                                           int scatter) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (scatter) out[perm[i]] = in[i];
+        else out[i] = in[perm[i]];
+    }
+}
+
+// y[i] -= Σ_k M[i,k] x[k]   (x2 -= E^T x1 with E^T stored explicitly; one warp-group per row)
+template <int G>
+static __global__ void __launch_bounds__(kBlock) k_spmv_sub(uint32_t n, const uint32_t* __restrict__ rowptr,
+                                                            const uint32_t* __restrict__ col,
+                                                            const double* __restrict__ val,
+                                                            const double* __restrict__ x, double* __restrict__ y) {
+    const int lane = threadIdx.x & (G - 1);
+    const uint32_t groups = (gridDim.x * blockDim.x) / G;
+    const uint32_t gid = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+    const uint32_t sub = (threadIdx.x & 31) / G;
+    for (uint32_t row0 = gid - sub; row0 < n; row0 += groups) {
+        const uint32_t row = row0 + sub;
+        double s = 0.0;
+        if (row < n)
+            for (uint32_t k = __ldg(rowptr + row) + lane; k < __ldg(rowptr + row + 1); k += G)
+                s += __ldg(val + k) * __ldg(x + __ldg(col + k));
+        s = group_sum<G>(s);
+        if (lane == 0 && row < n) y[row] -= s;
+    }
+}
+
+// y -= x
+static __global__ void __launch_bounds__(kBlock) k_sub(uint32_t n, const double* __restrict__ x, double* __restrict__ y) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] -= x[i];
+}
+
+// Low-rank correction, first half: partial[b*r + c] = Σ_{j in block b} W[c*n + j] * x[j]
+// (W column-major n x r, r <= kMaxRank).  Each block strides over rows; the r
+// partial sums are reduced in a fixed order by k_lowrank_finish.
+constexpr int kMaxRank = 128;
+static __global__ void __launch_bounds__(kBlock) k_lowrank_dots(uint32_t n, uint32_t r, const double* __restrict__ W,
+                                                                const double* __restrict__ x,
+                                                                double* __restrict__ partial) {
+    __shared__ double acc[kMaxRank][kBlock / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (uint32_t c = 0; c < r; ++c) {
+        double s = 0.0;
+        const double* wc = W + (size_t)c * n;
+        for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+            s += wc[j] * x[j];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) acc[c][wid] = s;
+    }
+    __syncthreads();
+    for (uint32_t c = threadIdx.x; c < r; c += blockDim.x) {
+        double s = 0.0;
+        for (int w = 0; w < kBlock / 32; ++w) s += acc[c][w];
+        partial[(size_t)blockIdx.x * r + c] = s;
+    }
+}
+
+// t[c] = H[c] * Σ_b partial[b*r + c]  (one block, fixed order)
+static __global__ void k_lowrank_finish(uint32_t nblocks, uint32_t r, const double* __restrict__ partial,
+                                        const double* __restrict__ H, double* __restrict__ t) {
+    for (uint32_t c = threadIdx.x; c < r; c += blockDim.x) {
+        double s = 0.0;
+        for (uint32_t b = 0; b < nblocks; ++b) s += partial[(size_t)b * r + c];
+        t[c] = s * H[c];
+    }
+}
+
+// y[j] += Σ_c W[c*n + j] * t[c]   (DenseMatrix::MatVec then x2 += ..., column order per element)
+static __global__ void __launch_bounds__(kBlock) k_lowrank_add(uint32_t n, uint32_t r, const double* __restrict__ W,
+                                                               const double* __restrict__ t, double* __restrict__ y) {
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (uint32_t c = 0; c < r; ++c) s += W[(size_t)c * n + j] * t[c];
+        y[j] += s;
+    }
+}
+}  // namespace prism

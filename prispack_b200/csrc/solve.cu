@@ -17,6 +17,7 @@ std::atomic<uint64_t>& launch_counter() {
 namespace {
 constexpr unsigned long long kWaitNs = 1000000000ull;  // 1 s per dependency wait
 constexpr int kSpmvG = 8;                              // lanes per row in the CSR SpMV
+}  // namespace
 
 int vec_grid(const Handle& h, uint32_t n) {
     long want = ((long)n + kBlock - 1) / kBlock;
@@ -31,7 +32,7 @@ void launch_fill(cudaStream_t st, const Handle& h, uint32_t n, double* p) {
     PRISM_LAUNCHED();
 }
 
-void* slab_kernel(bool fp32, int op) {
+static void* slab_kernel(bool fp32, int op) {
     if (fp32) {
         switch (op) {
             case SWEEP_DIV: return (void*)k_sweep_slab<float, OP_DIV>;
@@ -48,7 +49,7 @@ void* slab_kernel(bool fp32, int op) {
     }
 }
 
-constexpr int kSlabThreads = 1024;
+static constexpr int kSlabThreads = 1024;
 
 void launch_sweep(const Handle& h, cudaStream_t st, const DevSweep& s, const double* in, double* out) {
     if (!s.n) return;
@@ -102,7 +103,18 @@ void launch_sweep(const Handle& h, cudaStream_t st, const DevSweep& s, const dou
     PRISM_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kBlock), args, 0, st));
     PRISM_LAUNCHED();
 }
-}  // namespace
+
+void launch_spmv(const Handle& h, cudaStream_t st, uint32_t nrows, const uint32_t* rowptr, const uint32_t* col,
+                 const double* val, const double* x, double* y, int sub) {
+    if (!nrows) return;
+    long want = ((long)nrows * kSpmvG + kBlock - 1) / kBlock;
+    long cap = (long)h.info.sms * 8;
+    int grid = (int)(want < cap ? want : cap);
+    ReduceSlot none{nullptr, nullptr, nullptr};
+    if (sub) k_spmv_sub<kSpmvG><<<grid, kBlock, 0, st>>>(nrows, rowptr, col, val, x, y);
+    else k_spmv<kSpmvG, 0><<<grid, kBlock, 0, st>>>(nrows, rowptr, col, val, x, y, nullptr, nullptr, none);
+    PRISM_LAUNCHED();
+}
 
 // ============================================================================
 // Bounded-wait self test: a two-row sweep whose first position depends on the
@@ -264,7 +276,6 @@ void DevSweep::upload(const Sweep<Low>& s0, const DeviceInfo& info, bool slab_la
     PRISM_CUDA(cudaStreamSynchronize(st));
 }
 
-namespace {
 // Sweep-kernel autotuner: uploads the sweep in the plain level order and in
 // the slab layout in turn, times a few launches of each on a random
 // right-hand side with CUDA events, and keeps the faster one.  Which kernel
@@ -307,7 +318,8 @@ void tune_sweep(Handle& h, DevSweep& d, const Sweep<Low>& s) {
     if (!best_slab) d.upload(s, h.info, false, h.stream);
     d.tuned_ms = best / 3.f;
 }
-}  // namespace
+template void tune_sweep<double>(Handle&, DevSweep&, const Sweep<double>&);
+template void tune_sweep<float>(Handle&, DevSweep&, const Sweep<float>&);
 
 TriangularPrecond::TriangularPrecond(Handle& h, std::shared_ptr<const HostFactor> f) : h_(h), f_(std::move(f)) {
     if (f_->fp32) {

@@ -10,6 +10,7 @@
 #include "../../include/prism_solve.h"
 #include "device_common.cuh"
 #include "host_setup.hpp"
+#include "amsed_setup.hpp"
 
 namespace prism {
 
@@ -122,6 +123,43 @@ class TriangularPrecond : public Precond {
 int export_host_factor(const HostFactor& f, int which, uint32_t* n, uint64_t* nnz, uint32_t* rowptr, uint32_t* col,
                        double* val, double* diag);
 
+// Host-built AMSED/MSLR setup, shared by any number of device handles.
+struct HostAmsed {
+    bool fp32 = false;
+    AmsedOptions opt;
+    std::shared_ptr<AmsedSetup<float>> s32;
+    std::shared_ptr<AmsedSetup<double>> s64;
+};
+
+// AMSED/MSLR apply on the device (amsed.cu).
+class AmsedPrecond : public Precond {
+  public:
+    AmsedPrecond(Handle& h, std::shared_ptr<const HostAmsed> a);
+    int kind() const override { return PRISM_PRECOND_AMSED; }
+    uint64_t mnnz() const override;
+    void apply(cudaStream_t st, const double* in, double* out) override;
+    uint32_t levels(int sweep) const override;
+
+  private:
+    struct Level {
+        uint32_t nb = 0, nfac = 0, nrem = 0, rank = 0;
+        DevSweep lower, upper;
+        DeviceCsr E, Et;
+        DevBuf<double> W, H, xc, tmp, tmp2, t;
+    };
+    template <typename Low>
+    void build(const AmsedSetup<Low>& S);
+    void block_solve(cudaStream_t st, int level, const double* in, double* out);
+    void c_solve(cudaStream_t st, int level, double* x);
+    Handle& h_;
+    std::shared_ptr<const HostAmsed> a_;
+    uint32_t n_ = 0, nlev_ = 0;
+    std::vector<uint32_t> lev_ptr_;
+    DevBuf<uint32_t> pperm_;
+    DevBuf<double> X_, sweep_tmp_, partial_;
+    std::vector<Level> lv_;
+};
+
 struct Handle {
     DeviceInfo info;
     cudaStream_t stream = nullptr;
@@ -145,6 +183,18 @@ struct Handle {
     void check_status();           // synchronises; throws on a raised device status
     void ensure_workspace();
 };
+
+// ---- launch helpers shared by the preconditioners --------------------------
+int vec_grid(const Handle& h, uint32_t n);
+// marks n doubles pending (the sweeps' readiness encoding)
+void launch_fill(cudaStream_t st, const Handle& h, uint32_t n, double* p);
+void launch_sweep(const Handle& h, cudaStream_t st, const DevSweep& s, const double* in, double* out);
+// y = M x (sub = 0) or y -= M x (sub = 1) for a CSR with nrows rows
+void launch_spmv(const Handle& h, cudaStream_t st, uint32_t nrows, const uint32_t* rowptr, const uint32_t* col,
+                 const double* val, const double* x, double* y, int sub);
+// uploads a sweep, choosing its kernel by timing both (see solve.cu)
+template <typename Low>
+void tune_sweep(Handle& h, DevSweep& d, const Sweep<Low>& s);
 
 // Runs the bounded-wait self test (see solve.cu); returns the device status the wait raised.
 int selftest_wait_timeout(int device, unsigned long long wait_ns, int* device_status);
