@@ -59,11 +59,101 @@ void orc_spmv(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const dou
     }
 }
 
+/* ---- AMSED ----------------------------------------------------------------- */
+static void ildlt_inplace(uint32_t n, const uint32_t* rp, const uint32_t* ci, const double* v, const double* D,
+                          double* vec) {
+    for (uint32_t i = 0; i < n; i++)
+        for (uint32_t k = rp[i]; k < rp[i + 1]; k++) vec[ci[k]] -= v[k] * vec[i];
+    for (uint32_t i = 0; i < n; i++) vec[i] /= D[i];
+    for (uint32_t i = n; i-- > 0;)
+        for (uint32_t k = rp[i]; k < rp[i + 1]; k++) vec[i] -= v[k] * vec[ci[k]];
+}
+
+static void ic_inplace(uint32_t n, const uint32_t* rp, const uint32_t* ci, const double* v, double* vec) {
+    for (uint32_t i = 0; i < n; i++) {
+        double t = vec[i] / v[rp[i]];
+        vec[i] = t;
+        for (uint32_t k = rp[i] + 1; k < rp[i + 1]; k++) vec[ci[k]] -= v[k] * t;
+    }
+    for (uint32_t i = n; i-- > 0;) {
+        double t = vec[i];
+        for (uint32_t k = rp[i] + 1; k < rp[i + 1]; k++) t -= v[k] * vec[ci[k]];
+        vec[i] = t / v[rp[i]];
+    }
+}
+
+/* levelBlockInvSolve (AMSEDPrecondition.cpp:1690-1754): x starts at the level's first row */
+static void amsed_block_solve(const orc_amsed* S, uint32_t level, double* x) {
+    const orc_amsed_level* L = &S->levels[level];
+    const int last = level == S->nlev - 1;
+    for (uint32_t b = 0; b < L->ncomps; b++) {
+        double* seg = x + (L->dom_ptr[b] - L->dom_ptr[0]);
+        uint32_t nb = L->dom_ptr[b + 1] - L->dom_ptr[b];
+        if (last) {
+            if (b == 0) ic_inplace(nb, L->blk_rp[0], L->blk_ci[0], L->blk_val[0], seg);
+        } else {
+            ildlt_inplace(nb, L->blk_rp[b], L->blk_ci[b], L->blk_val[b], L->blk_diag[b], seg);
+        }
+    }
+}
+
+/* levelCInvRecursiveSolve(level, x, .) (AMSEDPrecondition.cpp:1494-1587); x = C block of `level` */
+static void amsed_c_solve(const orc_amsed* S, int level, double* x) {
+    const int next = level + 1;
+    if (level == (int)S->nlev - 2) {
+        const orc_amsed_level* LL = &S->levels[S->nlev - 1];
+        ic_inplace(LL->dom_ptr[1] - LL->dom_ptr[0], LL->blk_rp[0], LL->blk_ci[0], LL->blk_val[0], x);
+        return;
+    }
+    const orc_amsed_level* L = &S->levels[next];
+    const uint32_t nb = S->lev_ptr[next + 1] - S->lev_ptr[next];
+    const uint32_t nrem = S->n - S->lev_ptr[next + 1];
+    amsed_block_solve(S, (uint32_t)next, x);
+    double* xc = calloc(nrem ? nrem : 1, sizeof(double));
+    for (uint32_t i = 0; i < nb; i++) /* transMatPVec: scatter in row order */
+        for (uint32_t k = L->e_rp[i]; k < L->e_rp[i + 1]; k++) xc[L->e_ci[k]] += L->e_val[k] * x[i];
+    for (uint32_t i = 0; i < nrem; i++) x[nb + i] -= xc[i];
+    memcpy(xc, x + nb, nrem * sizeof(double));
+    amsed_c_solve(S, next, x + nb);
+    if (L->rank > 0) {
+        double* t = calloc(L->rank, sizeof(double));
+        double* t2 = calloc(nrem ? nrem : 1, sizeof(double));
+        for (uint32_t i = 0; i < L->rank; i++) /* DenseMatrix::transposeVec */
+            for (uint32_t j = 0; j < nrem; j++) t[i] += L->W[(size_t)i * nrem + j] * xc[j];
+        for (uint32_t i = 0; i < L->rank; i++) t[i] *= L->H[i];
+        for (uint32_t i = 0; i < L->rank; i++) /* DenseMatrix::MatVec */
+            for (uint32_t j = 0; j < nrem; j++) t2[j] += L->W[(size_t)i * nrem + j] * t[i];
+        for (uint32_t j = 0; j < nrem; j++) x[nb + j] += t2[j];
+        free(t);
+        free(t2);
+    }
+    double* tmp = calloc(nb ? nb : 1, sizeof(double));
+    for (uint32_t i = 0; i < nb; i++) { /* MatPVecWithRawPtr */
+        double s = 0;
+        for (uint32_t k = L->e_rp[i]; k < L->e_rp[i + 1]; k++) s += x[nb + L->e_ci[k]] * L->e_val[k];
+        tmp[i] = s;
+    }
+    amsed_block_solve(S, (uint32_t)next, tmp);
+    for (uint32_t i = 0; i < nb; i++) x[i] -= tmp[i];
+    free(tmp);
+    free(xc);
+}
+
+void orc_amsed_apply(const orc_amsed* S, double* vec) {
+    double* p = malloc((size_t)S->n * sizeof(double));
+    for (uint32_t i = 0; i < S->n; i++) p[i] = vec[S->pperm[i]]; /* prepareRightHand */
+    amsed_c_solve(S, -1, p);
+    for (uint32_t i = 0; i < S->n; i++) vec[S->pperm[i]] = p[i]; /* recoverRightHand */
+    free(p);
+}
+
 /* TriangularPrecondition::MInvSolve (include/Preconditioner/BasePreconditon.h:307-315):
  * lower, (ILDLT: diagonal), upper -- in place. */
 void orc_precond_apply(const orc_precond* P, double* vec) {
     const uint32_t n = P->n;
-    if (P->kind == 1) {
+    if (P->kind == 5) {
+        orc_amsed_apply(P->amsed, vec);
+    } else if (P->kind == 1) {
         /* IncompleteCholesky::MSolveLowerUsePtr (IncompleteCholesky.cpp:249-271): column scatter */
         for (uint32_t i = 0; i < n; i++) {
             uint32_t k = P->rp0[i];

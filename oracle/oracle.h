@@ -13,9 +13,36 @@
 #define PRISM_ORACLE_H
 #include <stdint.h>
 
+/* One level of an AMSED/MSLR hierarchy (LevelStructure,
+ * include/Preconditioner/AMSEDPrecondition.h:75-85) in permuted numbering. */
+typedef struct orc_amsed_level {
+    uint32_t ncomps;
+    const uint32_t* dom_ptr;          /* ncomps + 1 global offsets */
+    const uint32_t* const* blk_rp;    /* per block: ILDLT unit L^T (last level: block 0 IC L^T) */
+    const uint32_t* const* blk_ci;
+    const double* const* blk_val;
+    const double* const* blk_diag;    /* per block: ILDLT pivots (unused on the last level) */
+    const uint32_t* e_rp;             /* E: this level's B rows x its C columns (non-last levels) */
+    const uint32_t* e_ci;
+    const double* e_val;
+    uint32_t rank;
+    const double* W;                  /* nrem x rank, column-major */
+    const double* H;
+} orc_amsed_level;
+
+typedef struct orc_amsed {
+    uint32_t n, nlev;
+    const uint32_t* pperm;            /* new -> original */
+    const uint32_t* lev_ptr;          /* nlev + 1 */
+    const orc_amsed_level* levels;
+} orc_amsed;
+
+/* AMSEDPrecondition::MInvSolve(vec) (AMSEDPrecondition.cpp:2063-2087), in place */
+void orc_amsed_apply(const orc_amsed* S, double* vec);
+
 /* preconditioner described by its stored factor arrays (values widened to double) */
 typedef struct orc_precond {
-    int kind;                 /* 0 none, 1 IC, 2 ILUT, 3 ILDLT */
+    int kind;                 /* 0 none, 1 IC, 2 ILUT, 3 ILDLT, 5 AMSED (amsed != NULL) */
     uint32_t n;
     const uint32_t* rp0;      /* IC/ILDLT: L^T rows; ILUT: L rows */
     const uint32_t* ci0;
@@ -24,6 +51,7 @@ typedef struct orc_precond {
     const uint32_t* ci1;
     const double* v1;
     const double* diag;       /* ILDLT: D; ILUT: Dinv */
+    const orc_amsed* amsed;
 } orc_precond;
 
 void orc_laplacian(int nx, int ny, int nz, double ax, double ay, double az, double shift,

@@ -17,11 +17,23 @@ _u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
 
 
+class _AmsedLevel(C.Structure):
+    _fields_ = [("ncomps", C.c_uint32), ("dom_ptr", C.c_void_p),
+                ("blk_rp", C.c_void_p), ("blk_ci", C.c_void_p), ("blk_val", C.c_void_p), ("blk_diag", C.c_void_p),
+                ("e_rp", C.c_void_p), ("e_ci", C.c_void_p), ("e_val", C.c_void_p),
+                ("rank", C.c_uint32), ("W", C.c_void_p), ("H", C.c_void_p)]
+
+
+class _Amsed(C.Structure):
+    _fields_ = [("n", C.c_uint32), ("nlev", C.c_uint32), ("pperm", C.c_void_p), ("lev_ptr", C.c_void_p),
+                ("levels", C.c_void_p)]
+
+
 class _Precond(C.Structure):
     _fields_ = [("kind", C.c_int), ("n", C.c_uint32),
                 ("rp0", C.c_void_p), ("ci0", C.c_void_p), ("v0", C.c_void_p),
                 ("rp1", C.c_void_p), ("ci1", C.c_void_p), ("v1", C.c_void_p),
-                ("diag", C.c_void_p)]
+                ("diag", C.c_void_p), ("amsed", C.c_void_p)]
 
 
 def build() -> str:
@@ -41,6 +53,7 @@ def lib() -> C.CDLL:
                                        C.c_double, _u32p, _u32p, _f64p]
         _LIB.orc_spmv.argtypes = [C.c_uint32, _u32p, _u32p, _f64p, _f64p, _f64p]
         _LIB.orc_precond_apply.argtypes = [C.POINTER(_Precond), _f64p]
+        _LIB.orc_amsed_apply.argtypes = [C.POINTER(_Amsed), _f64p]
         _LIB.orc_cg.argtypes = [C.c_uint32, _u32p, _u32p, _f64p, C.POINTER(_Precond), C.c_int, C.c_double,
                                 C.c_uint32, _f64p, _f64p, C.POINTER(C.c_int32), C.POINTER(C.c_double),
                                 C.POINTER(C.c_int32)]
@@ -112,3 +125,65 @@ def gmres(rp, ci, v, b, P=None, x0=None, tol=1e-8, restart=50, flexible=True):
     lib().orc_gmres(n, rp, ci, v, C.byref(P.s) if P else None, int(flexible), restart, tol,
                     np.ascontiguousarray(b, np.float64), x, C.byref(it), C.byref(err), C.byref(conv))
     return x, it.value, err.value, bool(conv.value)
+
+
+class Amsed:
+    """An AMSED/MSLR hierarchy for the oracle, from any exporter with the
+    HostAmsed interface (info/perm/dom_ptr/block/coupling/lowrank)."""
+
+    def __init__(self, src):
+        self.keep = []
+        inf = src.info()
+        nlev = inf["nlev"]
+        n = int(inf["lev_ptr"][-1])
+
+        def arr(a, dt):
+            a = np.ascontiguousarray(a, dt)
+            self.keep.append(a)
+            return a.ctypes.data
+
+        def ptrs(lst):
+            a = (C.c_void_p * max(len(lst), 1))(*lst)
+            self.keep.append(a)
+            return C.cast(a, C.c_void_p).value
+
+        levels = (_AmsedLevel * nlev)()
+        for l in range(nlev):
+            L = levels[l]
+            dom = src.dom_ptr(l)
+            L.ncomps = len(dom) - 1
+            L.dom_ptr = arr(dom, np.uint32)
+            nblk = 1 if l == nlev - 1 else L.ncomps
+            rps, cis, vals, diags = [], [], [], []
+            for b in range(nblk):
+                rp, ci, v, d = src.block(l, b)
+                rps.append(arr(rp, np.uint32)); cis.append(arr(ci, np.uint32))
+                vals.append(arr(v, np.float64)); diags.append(arr(d, np.float64))
+            L.blk_rp, L.blk_ci, L.blk_val, L.blk_diag = ptrs(rps), ptrs(cis), ptrs(vals), ptrs(diags)
+            if l < nlev - 1:
+                erp, eci, ev = src.coupling(l, 0)
+                L.e_rp, L.e_ci, L.e_val = arr(erp, np.uint32), arr(eci, np.uint32), arr(ev, np.float64)
+                W, H = src.lowrank(l)
+                L.rank = len(H)
+                if L.rank:
+                    L.W = arr(np.asfortranarray(W).ravel(order="F"), np.float64)
+                    L.H = arr(H, np.float64)
+        self.levels = levels
+        s = _Amsed()
+        s.n, s.nlev = n, nlev
+        s.pperm = arr(src.perm(), np.uint32)
+        s.lev_ptr = arr(inf["lev_ptr"], np.uint32)
+        s.levels = C.cast(levels, C.c_void_p).value
+        self.s = s
+        self.n = n
+
+    def apply(self, vec):
+        out = np.array(vec, np.float64, copy=True)
+        lib().orc_amsed_apply(C.byref(self.s), out)
+        return out
+
+    def precond(self) -> "Precond":
+        P = Precond(5, self.n)
+        P.s.amsed = C.cast(C.pointer(self.s), C.c_void_p).value
+        P.keep.append(self)
+        return P

@@ -75,6 +75,7 @@ def load(fast: bool = False) -> C.CDLL:
     lib.ref_amsed_dom_ptr.argtypes = [vp, C.c_int, C.c_void_p]
     lib.ref_amsed_block.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_uint), C.POINTER(C.c_uint), C.c_void_p,
                                     C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.ref_rcm.argtypes = [C.c_uint, _u32p, _u32p, _u32p]
     lib.ref_amsed_lowrank.argtypes = [vp, C.c_int, C.POINTER(C.c_uint), C.POINTER(C.c_uint), C.c_void_p, C.c_void_p]
     _LIBS[key] = lib
     return lib
@@ -243,3 +244,11 @@ class RefAmsed(RefPrecond):
         H = np.zeros(r.value)
         self.lib.ref_amsed_lowrank(self.h, level, C.byref(r), C.byref(nrem), W.ctypes.data, H.ctypes.data)
         return W.reshape(r.value, nrem.value).T.copy(), H
+
+
+def rcm(rowptr, col):
+    """rcmReorderCSR: perm[new] = old (vendored genrcm)."""
+    n = len(rowptr) - 1
+    p = np.zeros(n, np.uint32)
+    load().ref_rcm(n, np.ascontiguousarray(rowptr, np.uint32), np.ascontiguousarray(col, np.uint32), p)
+    return p

@@ -362,3 +362,13 @@ extern "C" void ref_amsed_lowrank(void* h, int level, unsigned* rank, unsigned* 
     else amsed_lowrank_t<FLOAT64>(h, level, rank, nrem, W, H);
 }
 
+
+// rcmReorderCSR (include/utils/ExternalTools/MatrixReorderTools.h:51-85) on a caller CSR
+extern "C" void ref_rcm(unsigned n, const unsigned* rowptr, const unsigned* col, unsigned* perm) {
+    CSRd A(n, n, rowptr[n], memoryBase);
+    for (UINT32 i = 0; i <= n; ++i) A.getRowOffsetPtr(0)[i] = rowptr[i];
+    for (UINT32 k = 0; k < rowptr[n]; ++k) { A.getColIndicesPtr(0)[k] = col[k]; A.getCSRValuesPtr(0)[k] = 1.0; }
+    DenseVector<UINT32> p(n);
+    rcmReorderCSR(A, p);
+    for (UINT32 i = 0; i < n; ++i) perm[i] = p[i];
+}

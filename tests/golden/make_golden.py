@@ -37,6 +37,13 @@ CASES = [
     ("lap2d_64", (64, 64, 1, 0.0, 0.0, 0.0, 0.0), True, False),
 ]
 SEED = 20241116
+AMSED_SEED = 20241116
+# (name, grid, levels, lanczos steps, low rank, lowrank type (0 MSLR, 1 deflation), FP32 factors)
+AMSED_CASES = [
+    ("amsed_12c_mslr", (12, 12, 12), 3, 30, 16, 0, False),
+    ("amsed_16c_defl32", (16, 16, 16), 3, 40, 20, 1, True),
+    ("amsed_40sq_l4", (40, 40, 1), 4, 30, 16, 0, False),
+]
 
 
 def digest(*arrays) -> str:
@@ -114,6 +121,37 @@ def main():
         meta["none.gmres30"] = {"iters": it, "err": err, "conv": conv}
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
         manifest[name] = meta
+    # ---- AMSED / MSLR (reference AMSEDPrecondition behind the METIS stand-in) ----
+    amsed = {}
+    for name, grid, levels, steps, rank, ltype, low in AMSED_CASES:
+        A = ref.RefCSR.laplacian(*grid)
+        rp, ci, v = A.arrays()
+        n = len(rp) - 1
+        R = ref.RefAmsed(A, levels, steps, rank, 0.8, 2, ltype, 0, low, seed=AMSED_SEED)
+        assert R.setup() == 0
+        inf = R.info()
+        entry = {"grid": grid, "levels": levels, "lanczos_steps": steps, "low_rank": rank, "lowrank_type": ltype,
+                 "fp32": low, "seed": AMSED_SEED, "nlev": inf["nlev"], "lev_ptr": inf["lev_ptr"].tolist(),
+                 "ncomps": inf["ncomps"].tolist(), "ranks": inf["ranks"].tolist(), "mnnz": inf["mnnz"],
+                 "perm_sha": digest(R.perm()), "blocks": {}}
+        for lv in range(inf["nlev"]):
+            entry["blocks"][str(lv)] = {"dom_ptr": R.dom_ptr(lv).tolist()}
+            nb = 1 if lv == inf["nlev"] - 1 else int(inf["ncomps"][lv])
+            entry["blocks"][str(lv)]["sha"] = [digest(*R.block(lv, b)[:3]) +
+                                               ("" if lv == inf["nlev"] - 1 else digest(R.block(lv, b)[3]))
+                                               for b in range(nb)]
+            if lv < inf["nlev"] - 1 and inf["ranks"][lv] > 0:
+                W, H = R.lowrank(lv)
+                entry["blocks"][str(lv)]["H"] = sorted(H.tolist())
+        probe = rhs(n, SEED + 1)
+        b = rhs(n, SEED)
+        out = {"probe": probe, "b": b, "apply": R.apply(probe)}
+        x, it, err, conv = ref.cg_solve(A, R, b, tol=1e-10, maxit=500, flexible=True)
+        out["cg.x"] = x
+        entry["cg"] = {"iters": it, "err": err, "conv": conv}
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+        amsed[name] = entry
+    manifest["_amsed"] = amsed
     manifest["_seed"] = SEED
     manifest["_generator"] = "tests/golden/make_golden.py via oracle/_ref/libprism_ref.so (reference sources, parity flags)"
     with open(os.path.join(HERE, "manifest.json"), "w") as f:

@@ -1,0 +1,91 @@
+"""GPU parity of the AMSED / MSLR apply and FCG/FGMRES + AMSED: the device
+kernels, called through the C ABI, against the oracle's restatement of
+levelCInvRecursiveSolve on the same host setup and against the reference's
+golden outputs.  Tolerances as in test_gpu_parity.py."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import prispack_b200 as P
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+CASES = ["amsed_12c_mslr", "amsed_16c_defl32", "amsed_40sq_l4"]
+
+
+def rel_err(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def build(e):
+    A = P.CSRMatrix.laplacian(*e["grid"])
+    H = P.HostAmsed(A, levels=e["levels"], lanczos_steps=e["lanczos_steps"], low_rank=e["low_rank"],
+                    lowrank_type=e["lowrank_type"], seed=e["seed"],
+                    precision=P.PRISM_FP32 if e["fp32"] else P.PRISM_FP64)
+    return A, H
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_amsed_apply_vs_oracle_and_reference(name, manifest, load_golden):
+    e = manifest["_amsed"][name]
+    g = load_golden(name)
+    A, H = build(e)
+    S = P.DeviceSystem(A)
+    S.attach(H)
+    out = S.apply(g["probe"])
+    assert rel_err(out, orc.Amsed(H).apply(g["probe"])) < 1e-12
+    assert rel_err(out, g["apply"]) < 1e-11
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_fcg_amsed_vs_reference(name, manifest, load_golden):
+    e = manifest["_amsed"][name]
+    g = load_golden(name)
+    A, H = build(e)
+    S = P.DeviceSystem(A)
+    S.attach(H)
+    x, st = S.solve(g["b"], tol=1e-10, max_iter=500)
+    assert abs(st.num_iter - e["cg"]["iters"]) <= 1 and st.converged
+    if st.num_iter == e["cg"]["iters"]:
+        assert rel_err(x, g["cg.x"]) < 1e-10
+    assert st.true_rel_residual < 1.5e-10
+
+
+@pytest.mark.parametrize("grid,prec,lt", [((28, 28, 28), P.PRISM_FP32, 0), ((24, 20, 16), P.PRISM_FP64, 1)])
+def test_fcg_amsed_3d_vs_oracle(grid, prec, lt):
+    A = P.CSRMatrix.laplacian(*grid)
+    H = P.HostAmsed(A, levels=3, lanczos_steps=40, low_rank=32, lowrank_type=lt, precision=prec)
+    S = P.DeviceSystem(A)
+    S.attach(H)
+    b = np.random.default_rng(7).standard_normal(A.n)
+    assert rel_err(S.apply(b), orc.Amsed(H).apply(b)) < 1e-12
+    x, st = S.solve(b, tol=1e-10, max_iter=500)
+    xo, ito, _, _ = orc.cg(A.rowptr, A.col, A.val, b, orc.Amsed(H).precond(), tol=1e-10, maxit=500)
+    assert abs(st.num_iter - ito) <= 1
+    if st.num_iter == ito:
+        assert rel_err(x, xo) < 1e-10
+
+
+def test_fgmres_amsed_vs_oracle():
+    A = P.CSRMatrix.laplacian(20, 20, 20)
+    H = P.HostAmsed(A, levels=4, lanczos_steps=30, low_rank=16, lowrank_type=0)
+    S = P.DeviceSystem(A)
+    S.attach(H)
+    b = np.random.default_rng(8).uniform(-1, 1, A.n)
+    x, st = S.solve(b, solver=P.SOLVER_FGMRES, tol=1e-10, restart=30)
+    xo, ito, erro, _ = orc.gmres(A.rowptr, A.col, A.val, b, orc.Amsed(H).precond(), tol=1e-10, restart=30)
+    assert abs(st.num_iter - ito) <= 1
+    if st.num_iter == ito:
+        assert rel_err(x, xo) < 1e-10
+
+
+def test_reference_named_wrapper():
+    A = P.CSRMatrix.laplacian(16, 16, 16)
+    S = P.DeviceSystem(A)
+    M = P.AMSEDPrecondition(S, 3, 30, 16, 0.8, P.MatrixReorderRCM, P.AMSEDBasic, P.UseClassicLanczos)
+    solver = P.CG(A.n, M, P.FlexibleCG, 1e-10, 500)
+    x = solver.solve(S, np.ones(A.n), np.zeros(A.n))
+    assert solver.getConvergence() and solver.getNumIter() > 1
+    assert M.getPreconditionNonZeroCount() > A.nnz
