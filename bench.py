@@ -1,14 +1,19 @@
 """Solve-phase benchmark: time-to-1e-10 relative residual on one B200 per rank.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl prism|reference]
+                    [--precond amsed|ic] [--grid G]
 
 Workload (default): 3D Poisson 7-point Laplacian 128^3 (n = 2,097,152,
 nnz = 14,581,760; generateLaplacianCSR), b ~ N(0,1) from a fixed seed, x0 = 0,
-flexible CG + threshold incomplete Cholesky ICT(1e-3), relative tolerance
-1e-10, max 1000 iterations.  The preconditioner is set up once on the host
+flexible CG + AMSED/MSLR (3 HID levels, local RCM, ILDLT(1e-3) blocks, ICT(1e-3)
+on the last level, low-rank correction of rank <= 32 per level from 64 classic
+generalized Lanczos steps, MSLR correction H = lambda/(1-lambda)), relative
+tolerance 1e-10, max 1000 iterations.  `--precond ic` runs FCG + ICT(1e-3) on
+the same system instead.  The preconditioner is set up once on the host
 (outside the timed region); one step is one complete device-resident solve.
 The headline is the mixed-precision solve (FP32 factor values, FP64 Krylov
-vectors and scalars); the same solve with FP64 factor values is timed beside it.
+vectors and scalars, the reference's <float,double> instantiation); the same
+solve with FP64 factor values is timed beside it.
 
 Multi-GPU: replicas only (one independent system per rank, no collective on the
 data path); the process group is used for the barrier and the max over ranks.
@@ -28,15 +33,23 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "time-to-1e-10 rel. residual (FCG + ICT(1e-3), mixed FP32-factor / FP64-Krylov)"
+METRIC = "time-to-1e-10 rel. residual, mixed FP32-factor / FP64-Krylov, 1 B200"
+AMSED = dict(levels=3, lanczos_steps=64, low_rank=32, eig_bound=0.8, lowrank_type=0, lanczos_type=0, reorder=2)
 SEED = 2024
 
 
-def workload(grid: int, tol: float) -> str:
+def workload(grid: int, tol: float, precond: str) -> str:
     n = grid ** 3
     nnz = 7 * n - 6 * grid * grid
-    return (f"3D Poisson 7-pt {grid}^3 (n={n}, nnz={nnz}), FCG + ICT(1e-3), tol {tol:g}, "
-            f"b~N(0,1) seed {SEED}")
+    pc = ("AMSED/MSLR (3 levels, RCM, rank<=32, 64 Lanczos steps)" if precond == "amsed" else "ICT(1e-3)")
+    return f"3D Poisson 7-pt {grid}^3 (n={n}, nnz={nnz}), FCG + {pc}, tol {tol:g}, b~N(0,1) seed {SEED}"
+
+
+def build_precond(PB, A, precond: str, precision: int):
+    """Host setup of the preconditioner (timed separately, outside the solve)."""
+    if precond == "amsed":
+        return PB.HostAmsed(A, precision=precision, **AMSED)
+    return PB.HostFactor(A, PB.PRECOND_IC, tol=1e-3, precision=precision)
 
 
 def parse():
@@ -46,6 +59,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="prism", choices=["prism", "reference"])
     p.add_argument("--grid", type=int, default=128)
+    p.add_argument("--precond", default="amsed", choices=["amsed", "ic"])
     p.add_argument("--tol", type=float, default=1e-10)
     p.add_argument("--no-fp64", action="store_true", help="skip the FP64-factor comparison solve")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -119,14 +133,19 @@ class CpuReference:
     Setup runs once in the constructor (so the solve's own setup() is a no-op,
     IncompleteCholesky.cpp:105) and is excluded from the timings."""
 
-    def __init__(self, grid: int, tol: float):
+    def __init__(self, grid: int, tol: float, precond: str = "amsed"):
         from oracle import ref
         self.tol = tol
         self.b = np.random.default_rng(SEED).standard_normal(grid ** 3)
         t0 = time.perf_counter()
         if ref.available(fast=True):
             self.A = ref.RefCSR.laplacian(grid, grid, grid, fast=True)
-            self.P = ref.RefPrecond(self.A, ref.KIND_IC, True, 1e-3)
+            if precond == "amsed":
+                a = AMSED
+                self.P = ref.RefAmsed(self.A, a["levels"], a["lanczos_steps"], a["low_rank"], a["eig_bound"],
+                                      a["reorder"], a["lowrank_type"], a["lanczos_type"], True)
+            else:
+                self.P = ref.RefPrecond(self.A, ref.KIND_IC, True, 1e-3)
             self.P.setup()
             self.cores, self.kind = 4, "reference"
             self._solve = lambda k: ref.cg_solve(self.A, self.P, self.b, tol=tol, maxit=k, flexible=True)[1]
@@ -134,9 +153,13 @@ class CpuReference:
             import prispack_b200 as PB
             from oracle import oracle as orc
             A = PB.CSRMatrix.laplacian(grid, grid, grid)
-            F = PB.HostFactor(A, PB.PRECOND_IC, tol=1e-3, precision=PB.PRISM_FP32)
-            rp, ci, v, _ = F.arrays(0)
-            OP = orc.Precond(1, A.n, (rp, ci, v))
+            F = build_precond(PB, A, precond, PB.PRISM_FP32)
+            if precond == "amsed":
+                self._keep = orc.Amsed(F)
+                OP = self._keep.precond()
+            else:
+                rp, ci, v, _ = F.arrays(0)
+                OP = orc.Precond(1, A.n, (rp, ci, v))
             self.cores, self.kind = 1, "port"
             self._solve = lambda k: orc.cg(A.rowptr, A.col, A.val, self.b, OP, tol=tol, maxit=k)[1]
         self.setup_s = time.perf_counter() - t0
@@ -186,7 +209,7 @@ def main():
     n = A.n
     b_host = np.random.default_rng(SEED).standard_normal(n)
     t0 = time.perf_counter()
-    F32 = PB.HostFactor(A, PB.PRECOND_IC, tol=1e-3, precision=PB.PRISM_FP32)
+    F32 = build_precond(PB, A, args.precond, PB.PRISM_FP32)
     setup32_s = time.perf_counter() - t0
     S = PB.DeviceSystem(A, device=local)
     stream = torch.cuda.current_stream()
@@ -247,13 +270,16 @@ def main():
         e2e.append(e0.elapsed_time(e1))
     e2e_ms = statistics.mean(e2e)
 
-    # ---- dominant kernel: one triangular sweep, timed alone with CUDA events
-    info = S.sweep_info(0)
-    vin = torch.randn(n, dtype=torch.float64, device="cuda")
-    vout = torch.empty_like(vin)
+    # ---- dominant kernel: the triangular sweeps, each timed alone with CUDA events.  For AMSED
+    # these are the lower/upper sweeps of the level-0 block-diagonal factor (every subdomain in
+    # one launch, the largest sweeps of the apply); for ICT the whole-matrix factor's sweeps.
     reps = 10
-    sweep_ms = []
+    sweep_ms, sweep_infos = [], []
     for sw in (0, 1):
+        info = S.sweep_info(sw)
+        sweep_infos.append(info)
+        vin = torch.randn(info["n"], dtype=torch.float64, device="cuda")
+        vout = torch.empty_like(vin)
         S.sweep_device(sw, vin, vout, 1)
         torch.cuda.synchronize()
         tot = 0.0
@@ -267,13 +293,13 @@ def main():
             torch.cuda.synchronize()
             tot += s0.elapsed_time(s1)
         sweep_ms.append(tot / reps)
-    # algorithmic bytes of one sweep launch: per stored entry a column index (4 B) and a
-    # value (4 B FP32); per row its offset (4 B), position->row map (4 B), diagonal (8 B),
-    # right-hand side read (8 B) and result write (8 B)
-    sweep_bytes = info["nnz"] * (4 + info["value_bytes"]) + n * 32 + 4
-    sweep_avg_ms = statistics.mean(sweep_ms)
-    achieved = sweep_bytes / (sweep_avg_ms * 1e-3) / 1e9
+    # algorithmic bytes of one sweep launch: per stored entry a column index (4 B) and a value
+    # (4 B FP32); per row its offset (4 B), position->row map (4 B), diagonal (8 B), right-hand
+    # side read (8 B) and result write (8 B)
+    sweep_bytes = [i["nnz"] * (4 + i["value_bytes"]) + i["n"] * 32 + 4 for i in sweep_infos]
+    achieved = statistics.mean(b_ / (t * 1e-3) / 1e9 for b_, t in zip(sweep_bytes, sweep_ms))
     peak, peak_src = measured_peak_gbs()
+    vin = torch.randn(n, dtype=torch.float64, device="cuda")
 
     # ---- SpMV alone (the other bandwidth kernel), for reference
     spmv_ms = []
@@ -292,7 +318,7 @@ def main():
     fp64 = None
     if not args.no_fp64:
         t0 = time.perf_counter()
-        F64 = PB.HostFactor(A, PB.PRECOND_IC, tol=1e-3, precision=PB.PRISM_FP64)
+        F64 = build_precond(PB, A, args.precond, PB.PRISM_FP64)
         setup64_s = time.perf_counter() - t0
         S.attach(F64)
         ms64, stats64, _ = timed_solves(max(1, args.steps // 2), 1)
@@ -309,7 +335,7 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            cpu = CpuReference(g, args.tol).sample(args.cpu_sample_s, iters)
+            cpu = CpuReference(g, args.tol, args.precond).sample(args.cpu_sample_s, iters)
             cpu.pop("iters", None)
         except Exception as e:  # reported, not fatal
             cpu = {"value": None, "unit": "ms", "cores": 0, "kind": "unavailable", "sample": str(e)[:200]}
@@ -328,9 +354,9 @@ def main():
             "vs_baseline": None,
             "dtype": "f64 (Krylov) / f32 (factor values)",
             "data": "synthetic",
-            "config": {"workload": workload(g, args.tol), "n": n, "nnz": A.nnz, "precond_nnz": F32.info()["mnnz"],
-                       "sweep_levels": [S.sweep_info(0)["levels"], S.sweep_info(1)["levels"]],
-                       "sweep_kernels": [S.sweep_info(0)["kernel"], S.sweep_info(1)["kernel"]],
+            "config": {"workload": workload(g, args.tol, args.precond), "n": n, "nnz": A.nnz, "precond_nnz": F32.info()["mnnz"],
+                       "amsed": ({k: (v.tolist() if hasattr(v, "tolist") else v) for k, v in F32.info().items()}
+                                 if args.precond == "amsed" else None),
                        "iterations": iters, "true_rel_residual": stats32[-1][1],
                        "converged": bool(stats32[-1][2]), "host_setup_s": round(setup32_s, 2),
                        "l2": "inputs larger than L2 (A 216 MB + factor > 600 MB per solve)",
@@ -338,11 +364,14 @@ def main():
                        "spmv_per_iter": 1},
             "e2e": {"value": round(e2e_ms, 4), "unit": "ms", "h2d_bytes_per_step": 2 * 8 * n,
                     "d2h_bytes_per_step": 8 * n},
-            "roofline": {"bound": "hbm", "kernel": "triangular sweep, FP32 values (lower+upper avg)",
+            "roofline": {"bound": "hbm",
+                         "kernel": ("level-0 block-diagonal sweeps" if args.precond == "amsed" else "ICT sweeps")
+                                   + ", FP32 values (lower/upper average)",
                          "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "peak_source": peak_src,
                          "bytes_per_launch": sweep_bytes, "launch_ms": [round(t, 4) for t in sweep_ms],
-                         "traffic": None},
+                         "rows": [i["n"] for i in sweep_infos], "wavefronts": [i["levels"] for i in sweep_infos],
+                         "kernels": [i["kernel"] for i in sweep_infos], "traffic": None},
             "spmv": {"ms": round(statistics.median(spmv_ms), 4), "bytes": spmv_bytes, "GB/s": round(spmv_gbs, 1),
                      "frac": round(spmv_gbs / peak, 4)},
             "fp64_factor": fp64,
@@ -361,7 +390,7 @@ def reference_arm(args, rank, world):
     if rank != 0:
         return
     from oracle import ref
-    R = CpuReference(args.grid, args.tol)
+    R = CpuReference(args.grid, args.tol, args.precond)
     full = R.sample(0.0, None)          # one full solve: learns the iteration count (untimed warm-up)
     full_iters = full["iters"]
     vals, desc = [], full
@@ -374,7 +403,7 @@ def reference_arm(args, rank, world):
     line = {"impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "ms", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(v, 3), "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64 (Krylov) / f32 (factor values)",
-            "data": "synthetic", "config": {"workload": workload(args.grid, args.tol)},
+            "data": "synthetic", "config": {"workload": workload(args.grid, args.tol, args.precond)},
             "cpu_baseline": {"value": round(v, 3), "unit": "ms", "cores": desc["cores"], "kind": desc["kind"],
                              "sample": desc["sample"]},
             "e2e": {"value": round(v, 3), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}

@@ -210,7 +210,10 @@ int32_t prism_amsed_lowrank(prism_factor f, int32_t level, uint32_t* rank, uint3
 int32_t prism_apply_device(prism_handle h, const double* in_d, double* out_d);
 int32_t prism_apply(prism_handle h, const double* in, double* out);
 
-/* One triangular sweep alone (sweep 0 = lower, 1 = upper), on device vectors,
+/* One triangular sweep alone (IC/ILUT/ILDLT: sweep 0 = lower, 1 = upper;
+ * AMSED: sweep 2*level + 0/1 = lower/upper sweep of that HID level's
+ * block-diagonal factor, whose rows are numbered from the level's first row),
+ * on device vectors,
  * for timing the sweep kernel by itself (the preconditioner apply is
  * prism_apply_device).  prepare = 1: mark out_d pending (the sweep's readiness
  * encoding) then sweep; 0: sweep only (the caller marked out_d already);

@@ -190,6 +190,28 @@ uint32_t AmsedPrecond::levels(int sweep) const {
     return m;
 }
 
+bool AmsedPrecond::run_sweep(cudaStream_t st, int sweep, const double* in, double* out, int prepare) {
+    if (sweep < 0 || sweep >= (int)(2 * nlev_)) return false;
+    const Level& L = lv_[sweep / 2];
+    const DevSweep& s = (sweep & 1) ? L.upper : L.lower;
+    if (prepare != 0) launch_fill(st, h_, s.n, out);
+    if (prepare != 2) launch_sweep(h_, st, s, in, out);
+    return true;
+}
+
+bool AmsedPrecond::sweep_info(int sweep, uint32_t* n, uint64_t* nnz, uint32_t* vbytes, uint32_t* levels,
+                              uint32_t* kernel) const {
+    if (sweep < 0 || sweep >= (int)(2 * nlev_)) return false;
+    const Level& L = lv_[sweep / 2];
+    const DevSweep& s = (sweep & 1) ? L.upper : L.lower;
+    if (n) *n = s.n;
+    if (nnz) *nnz = s.fp32 ? s.val32.size() : s.val64.size();
+    if (vbytes) *vbytes = s.fp32 ? 4 : 8;
+    if (levels) *levels = s.num_levels;
+    if (kernel) *kernel = s.num_ctas > 0 ? 2 : 1;
+    return true;
+}
+
 template void AmsedPrecond::build<double>(const AmsedSetup<double>&);
 template void AmsedPrecond::build<float>(const AmsedSetup<float>&);
 

@@ -529,14 +529,14 @@ int32_t prism_apply(prism_handle h, const double* in, double* out) {
 int32_t prism_precond_sweep_device(prism_handle h, int32_t sweep, const double* in_d, double* out_d,
                                    int32_t prepare) {
     if (!h || !in_d || !out_d) return fail(PRISM_ERR_ARG, "null argument");
-    if (sweep != 0 && sweep != 1) return fail(PRISM_ERR_ARG, "sweep must be 0 or 1");
+    if (sweep < 0) return fail(PRISM_ERR_ARG, "sweep must be >= 0");
     if (in_d == out_d) return fail(PRISM_ERR_ARG, "a sweep cannot run in place");
     if (!h->P) return fail(PRISM_ERR_NOT_READY, "no preconditioner set");
     return guarded([&]() -> int {
         DeviceGuard g(h->info.device);
         if (prepare < 0 || prepare > 2) return fail(PRISM_ERR_ARG, "prepare must be 0, 1 or 2");
         if (!h->P->run_sweep(h->stream, sweep, in_d, out_d, prepare))
-            return fail(PRISM_ERR_UNSUPPORTED, "preconditioner has no single sweeps");
+            return fail(PRISM_ERR_ARG, "no such sweep for this preconditioner");
         return PRISM_OK;
     });
 }

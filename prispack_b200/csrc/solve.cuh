@@ -139,6 +139,10 @@ class AmsedPrecond : public Precond {
     uint64_t mnnz() const override;
     void apply(cudaStream_t st, const double* in, double* out) override;
     uint32_t levels(int sweep) const override;
+    // sweeps are numbered 2*level + (0: lower, 1: upper) over the HID levels
+    bool run_sweep(cudaStream_t st, int sweep, const double* in, double* out, int prepare) override;
+    bool sweep_info(int sweep, uint32_t* n, uint64_t* nnz, uint32_t* vbytes, uint32_t* levels,
+                    uint32_t* kernel) const override;
 
   private:
     struct Level {
