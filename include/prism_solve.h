@@ -201,10 +201,25 @@ int32_t prism_amsed_dom_ptr(prism_factor f, int32_t level, uint32_t* dom_ptr);
 /* block factor of (level, block): ILDLT unit L^T + D, or (last level, block 0) IC L^T */
 int32_t prism_amsed_block(prism_factor f, int32_t level, int32_t block, uint32_t* n, uint64_t* nnz,
                           uint32_t* rowptr, uint32_t* col, double* val, double* diag);
-/* which = 0: E (level rows x C columns), 1: C block */
+/* which = 0: E (level rows x C columns), 1: C block (AMSED), 2: F (GMSLR) */
 int32_t prism_amsed_coupling(prism_factor f, int32_t level, int32_t which, uint32_t* nrows, uint64_t* nnz,
                              uint32_t* rowptr, uint32_t* col, double* val);
 int32_t prism_amsed_lowrank(prism_factor f, int32_t level, uint32_t* rank, uint32_t* nrem, double* W, double* H);
+
+/* ---- GMSLR (GMSLRPrecondition, include/Preconditioner/GMSLRPrecondition.h:45-411) ----
+ * Same HID ordering and level structure as AMSED; ILUT(lfill = 20, factor_tol)
+ * blocks on every level (factor_tol default 1e-2 = GMSLR_FACTOR_TOLRANCE) and
+ * the coupling x2 -= F x1 with F = A(C rows, B columns).  Options reuse
+ * prism_amsed_opts (levels, lanczos_steps, low_rank, reorder, factor_tol,
+ * minsep); the structure exports above apply, prism_amsed_coupling with
+ * which = 2 returns F, and ranks report min(lanczos_steps, low_rank). */
+void prism_gmslr_default_opts(prism_amsed_opts* o);
+int32_t prism_set_precond_gmslr(prism_handle h, const prism_amsed_opts* o, int32_t precision);
+int32_t prism_factor_create_gmslr(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val,
+                                  const prism_amsed_opts* o, int32_t precision, prism_factor* out);
+/* ILUT factor of (level, block): which = 0 L, 1 U; dinv receives the inverse pivots */
+int32_t prism_gmslr_block(prism_factor f, int32_t level, int32_t block, int32_t which, uint32_t* n,
+                          uint64_t* nnz, uint32_t* rowptr, uint32_t* col, double* val, double* dinv);
 
 /* out = M^{-1} in (in == out allowed) */
 int32_t prism_apply_device(prism_handle h, const double* in_d, double* out_d);

@@ -82,14 +82,30 @@ static void ic_inplace(uint32_t n, const uint32_t* rp, const uint32_t* ci, const
     }
 }
 
-/* levelBlockInvSolve (AMSEDPrecondition.cpp:1690-1754): x starts at the level's first row */
+/* IncompleteLU::MSolveLower/UpperUsePtr (IncompleteLU.cpp:268-297), in place */
+static void ilut_inplace(uint32_t n, const uint32_t* lrp, const uint32_t* lci, const double* lv, const uint32_t* urp,
+                         const uint32_t* uci, const double* uv, const double* dinv, double* vec) {
+    for (uint32_t i = 0; i < n; i++)
+        for (uint32_t k = lrp[i]; k < lrp[i + 1]; k++) vec[i] -= lv[k] * vec[lci[k]];
+    for (uint32_t i = n; i > 0; i--) {
+        for (uint32_t k = urp[i - 1]; k < urp[i]; k++) vec[i - 1] -= uv[k] * vec[uci[k]];
+        vec[i - 1] *= dinv[i - 1];
+    }
+}
+
+/* levelBlockInvSolve (AMSEDPrecondition.cpp:1690-1754, GMSLRDPrecondition.cpp:1170-1229):
+ * x starts at the level's first row */
 static void amsed_block_solve(const orc_amsed* S, uint32_t level, double* x) {
     const orc_amsed_level* L = &S->levels[level];
     const int last = level == S->nlev - 1;
     for (uint32_t b = 0; b < L->ncomps; b++) {
         double* seg = x + (L->dom_ptr[b] - L->dom_ptr[0]);
         uint32_t nb = L->dom_ptr[b + 1] - L->dom_ptr[b];
-        if (last) {
+        if (S->gmslr) {
+            if (!last || b == 0)
+                ilut_inplace(nb, L->blk_rp[b], L->blk_ci[b], L->blk_val[b], L->blk_rp1[b], L->blk_ci1[b],
+                             L->blk_val1[b], L->blk_diag[b], seg);
+        } else if (last) {
             if (b == 0) ic_inplace(nb, L->blk_rp[0], L->blk_ci[0], L->blk_val[0], seg);
         } else {
             ildlt_inplace(nb, L->blk_rp[b], L->blk_ci[b], L->blk_val[b], L->blk_diag[b], seg);
@@ -102,7 +118,11 @@ static void amsed_c_solve(const orc_amsed* S, int level, double* x) {
     const int next = level + 1;
     if (level == (int)S->nlev - 2) {
         const orc_amsed_level* LL = &S->levels[S->nlev - 1];
-        ic_inplace(LL->dom_ptr[1] - LL->dom_ptr[0], LL->blk_rp[0], LL->blk_ci[0], LL->blk_val[0], x);
+        if (S->gmslr)
+            ilut_inplace(LL->dom_ptr[1] - LL->dom_ptr[0], LL->blk_rp[0], LL->blk_ci[0], LL->blk_val[0], LL->blk_rp1[0],
+                         LL->blk_ci1[0], LL->blk_val1[0], LL->blk_diag[0], x);
+        else
+            ic_inplace(LL->dom_ptr[1] - LL->dom_ptr[0], LL->blk_rp[0], LL->blk_ci[0], LL->blk_val[0], x);
         return;
     }
     const orc_amsed_level* L = &S->levels[next];
@@ -110,8 +130,16 @@ static void amsed_c_solve(const orc_amsed* S, int level, double* x) {
     const uint32_t nrem = S->n - S->lev_ptr[next + 1];
     amsed_block_solve(S, (uint32_t)next, x);
     double* xc = calloc(nrem ? nrem : 1, sizeof(double));
-    for (uint32_t i = 0; i < nb; i++) /* transMatPVec: scatter in row order */
-        for (uint32_t k = L->e_rp[i]; k < L->e_rp[i + 1]; k++) xc[L->e_ci[k]] += L->e_val[k] * x[i];
+    if (S->gmslr) { /* x_copy = F x1 (GMSLRDPrecondition.cpp:1080) */
+        for (uint32_t i = 0; i < nrem; i++) {
+            double s = 0;
+            for (uint32_t k = L->f_rp[i]; k < L->f_rp[i + 1]; k++) s += x[L->f_ci[k]] * L->f_val[k];
+            xc[i] = s;
+        }
+    } else { /* transMatPVec: scatter in row order */
+        for (uint32_t i = 0; i < nb; i++)
+            for (uint32_t k = L->e_rp[i]; k < L->e_rp[i + 1]; k++) xc[L->e_ci[k]] += L->e_val[k] * x[i];
+    }
     for (uint32_t i = 0; i < nrem; i++) x[nb + i] -= xc[i];
     memcpy(xc, x + nb, nrem * sizeof(double));
     amsed_c_solve(S, next, x + nb);

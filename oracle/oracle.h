@@ -28,10 +28,18 @@ typedef struct orc_amsed_level {
     uint32_t rank;
     const double* W;                  /* nrem x rank, column-major */
     const double* H;
+    /* GMSLR: ILUT blocks (blk_* = L) and F = A(C rows, B cols) */
+    const uint32_t* const* blk_rp1;   /* per block: U */
+    const uint32_t* const* blk_ci1;
+    const double* const* blk_val1;
+    const uint32_t* f_rp;
+    const uint32_t* f_ci;
+    const double* f_val;
 } orc_amsed_level;
 
 typedef struct orc_amsed {
     uint32_t n, nlev;
+    int gmslr;                        /* 0: AMSED, 1: GMSLR */
     const uint32_t* pperm;            /* new -> original */
     const uint32_t* lev_ptr;          /* nlev + 1 */
     const orc_amsed_level* levels;

@@ -21,12 +21,14 @@ class _AmsedLevel(C.Structure):
     _fields_ = [("ncomps", C.c_uint32), ("dom_ptr", C.c_void_p),
                 ("blk_rp", C.c_void_p), ("blk_ci", C.c_void_p), ("blk_val", C.c_void_p), ("blk_diag", C.c_void_p),
                 ("e_rp", C.c_void_p), ("e_ci", C.c_void_p), ("e_val", C.c_void_p),
-                ("rank", C.c_uint32), ("W", C.c_void_p), ("H", C.c_void_p)]
+                ("rank", C.c_uint32), ("W", C.c_void_p), ("H", C.c_void_p),
+                ("blk_rp1", C.c_void_p), ("blk_ci1", C.c_void_p), ("blk_val1", C.c_void_p),
+                ("f_rp", C.c_void_p), ("f_ci", C.c_void_p), ("f_val", C.c_void_p)]
 
 
 class _Amsed(C.Structure):
-    _fields_ = [("n", C.c_uint32), ("nlev", C.c_uint32), ("pperm", C.c_void_p), ("lev_ptr", C.c_void_p),
-                ("levels", C.c_void_p)]
+    _fields_ = [("n", C.c_uint32), ("nlev", C.c_uint32), ("gmslr", C.c_int), ("pperm", C.c_void_p),
+                ("lev_ptr", C.c_void_p), ("levels", C.c_void_p)]
 
 
 class _Precond(C.Structure):
@@ -128,10 +130,12 @@ def gmres(rp, ci, v, b, P=None, x0=None, tol=1e-8, restart=50, flexible=True):
 
 
 class Amsed:
-    """An AMSED/MSLR hierarchy for the oracle, from any exporter with the
-    HostAmsed interface (info/perm/dom_ptr/block/coupling/lowrank)."""
+    """An AMSED/MSLR (or GMSLR) hierarchy for the oracle, from any exporter
+    with the HostAmsed interface (info/perm/dom_ptr/block/coupling/lowrank;
+    GMSLR: gmslr_block)."""
 
     def __init__(self, src):
+        gmslr = bool(getattr(src, "is_gmslr", False))
         self.keep = []
         inf = src.info()
         nlev = inf["nlev"]
@@ -154,15 +158,26 @@ class Amsed:
             L.ncomps = len(dom) - 1
             L.dom_ptr = arr(dom, np.uint32)
             nblk = 1 if l == nlev - 1 else L.ncomps
-            rps, cis, vals, diags = [], [], [], []
+            rps, cis, vals, diags, rps1, cis1, vals1 = [], [], [], [], [], [], []
             for b in range(nblk):
-                rp, ci, v, d = src.block(l, b)
+                if gmslr:
+                    rp, ci, v, d = src.gmslr_block(l, b, 0)
+                    rp1, ci1, v1, _ = src.gmslr_block(l, b, 1)
+                    rps1.append(arr(rp1, np.uint32)); cis1.append(arr(ci1, np.uint32)); vals1.append(arr(v1, np.float64))
+                else:
+                    rp, ci, v, d = src.block(l, b)
                 rps.append(arr(rp, np.uint32)); cis.append(arr(ci, np.uint32))
                 vals.append(arr(v, np.float64)); diags.append(arr(d, np.float64))
             L.blk_rp, L.blk_ci, L.blk_val, L.blk_diag = ptrs(rps), ptrs(cis), ptrs(vals), ptrs(diags)
+            if gmslr:
+                L.blk_rp1, L.blk_ci1, L.blk_val1 = ptrs(rps1), ptrs(cis1), ptrs(vals1)
             if l < nlev - 1:
                 erp, eci, ev = src.coupling(l, 0)
                 L.e_rp, L.e_ci, L.e_val = arr(erp, np.uint32), arr(eci, np.uint32), arr(ev, np.float64)
+                if gmslr:
+                    frp, fci, fv = src.coupling(l, 2)
+                    L.f_rp, L.f_ci, L.f_val = arr(frp, np.uint32), arr(fci, np.uint32), arr(fv, np.float64)
+                    continue
                 W, H = src.lowrank(l)
                 L.rank = len(H)
                 if L.rank:
@@ -171,6 +186,7 @@ class Amsed:
         self.levels = levels
         s = _Amsed()
         s.n, s.nlev = n, nlev
+        s.gmslr = int(gmslr)
         s.pperm = arr(src.perm(), np.uint32)
         s.lev_ptr = arr(inf["lev_ptr"], np.uint32)
         s.levels = C.cast(levels, C.c_void_p).value

@@ -76,6 +76,13 @@ def load(fast: bool = False) -> C.CDLL:
     lib.ref_amsed_block.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_uint), C.POINTER(C.c_uint), C.c_void_p,
                                     C.c_void_p, C.c_void_p, C.c_void_p]
     lib.ref_rcm.argtypes = [C.c_uint, _u32p, _u32p, _u32p]
+    lib.ref_gmslr_create.restype = vp
+    lib.ref_gmslr_create.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
+    lib.ref_gmslr_info.argtypes = [vp, C.POINTER(C.c_uint), C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.POINTER(C.c_uint), C.POINTER(C.c_double)]
+    lib.ref_gmslr_perm.argtypes = [vp, C.c_void_p]
+    lib.ref_gmslr_block.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint), C.POINTER(C.c_uint),
+                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.ref_amsed_lowrank.argtypes = [vp, C.c_int, C.POINTER(C.c_uint), C.POINTER(C.c_uint), C.c_void_p, C.c_void_p]
     _LIBS[key] = lib
     return lib
@@ -252,3 +259,45 @@ def rcm(rowptr, col):
     p = np.zeros(n, np.uint32)
     load().ref_rcm(n, np.ascontiguousarray(rowptr, np.uint32), np.ascontiguousarray(col, np.uint32), p)
     return p
+
+
+KIND_GMSLR = 4
+
+
+class RefGmslr(RefPrecond):
+    """GMSLRPrecondition<low, double>(A, levelNum, lanczosSteps, lowRankSize, localReorderType)."""
+
+    def __init__(self, A: RefCSR, levels, lanczos_steps=20, low_rank=12, reorder=2, low_precision=False):
+        self.A = A
+        self.lib = A.lib
+        self.kind = KIND_GMSLR
+        self.h = self.lib.ref_gmslr_create(A.h, levels, lanczos_steps, low_rank, reorder, int(low_precision))
+
+    def info(self):
+        nlev, mnnz, wmax = C.c_uint(), C.c_uint(), C.c_double()
+        self.lib.ref_gmslr_info(self.h, C.byref(nlev), None, None, None, C.byref(mnnz), C.byref(wmax))
+        L = nlev.value
+        lev_ptr = np.zeros(L + 1, np.uint32)
+        ncomps = np.zeros(L, np.uint32)
+        ranks = np.zeros(L, np.uint32)
+        self.lib.ref_gmslr_info(self.h, C.byref(nlev), lev_ptr.ctypes.data, ncomps.ctypes.data, ranks.ctypes.data,
+                                C.byref(mnnz), C.byref(wmax))
+        return {"nlev": L, "lev_ptr": lev_ptr, "ncomps": ncomps, "ranks": ranks, "mnnz": mnnz.value,
+                "w_max_abs": wmax.value}
+
+    def perm(self):
+        n, _ = self.A.dims()
+        p = np.zeros(n, np.uint32)
+        self.lib.ref_gmslr_perm(self.h, p.ctypes.data)
+        return p
+
+    def block(self, level, block, which):
+        n, nnz = C.c_uint(), C.c_uint()
+        self.lib.ref_gmslr_block(self.h, level, block, which, C.byref(n), C.byref(nnz), None, None, None, None)
+        rp = np.zeros(n.value + 1, np.uint32)
+        ci = np.zeros(nnz.value, np.uint32)
+        v = np.zeros(nnz.value)
+        d = np.zeros(n.value)
+        self.lib.ref_gmslr_block(self.h, level, block, which, C.byref(n), C.byref(nnz), rp.ctypes.data,
+                                 ci.ctypes.data, v.ctypes.data, d.ctypes.data)
+        return rp, ci, v, d

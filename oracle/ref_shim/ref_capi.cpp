@@ -34,6 +34,7 @@
 #include "Solver/CG.h"
 #include "Solver/GMRES.h"
 #include "Preconditioner/AMSEDPrecondition.h"
+#include "Preconditioner/GMSLRPrecondition.h"
 #undef private
 #undef protected
 
@@ -371,4 +372,83 @@ extern "C" void ref_rcm(unsigned n, const unsigned* rowptr, const unsigned* col,
     DenseVector<UINT32> p(n);
     rcmReorderCSR(A, p);
     for (UINT32 i = 0; i < n; ++i) perm[i] = p[i];
+}
+
+// ---- GMSLR -------------------------------------------------------------------
+extern "C" void* ref_gmslr_create(void* hA, int levels, int lanczos_steps, int low_rank, int reorder,
+                                  int low_precision) {
+    auto* A = static_cast<CSRd*>(hA);
+    std::shared_ptr<CSRd> sp(A, [](CSRd*) {});
+    auto* r = new RefPrecond{4, low_precision, nullptr};
+    auto ro = (MatrixReorderOption_t)reorder;
+    if (low_precision)
+        r->p = std::make_shared<GMSLRPrecondition<FLOAT32, FLOAT64>>(sp, levels, lanczos_steps, low_rank, ro);
+    else
+        r->p = std::make_shared<GMSLRPrecondition<FLOAT64, FLOAT64>>(sp, levels, lanczos_steps, low_rank, ro);
+    return r;
+}
+
+template <typename Low>
+static GMSLRPrecondition<Low, FLOAT64>* gmslr(void* h) {
+    return static_cast<GMSLRPrecondition<Low, FLOAT64>*>(static_cast<RefPrecond*>(h)->p.get());
+}
+
+template <typename Low>
+static void gmslr_info_t(void* h, unsigned* nlev, unsigned* lev_ptr, unsigned* ncomps, unsigned* ranks, unsigned* mnnz,
+                         double* wmax) {
+    auto* a = gmslr<Low>(h);
+    *nlev = a->m_nlev_used;
+    if (mnnz) *mnnz = a->getPreconditionNonZeroCount();
+    double m = 0.0;
+    for (UINT32 l = 0; l < a->m_nlev_used; ++l) {
+        auto& L = *a->m_levs_all[l];
+        if (ncomps) ncomps[l] = L.ncomps;
+        if (ranks) ranks[l] = L.rank;
+        if (l + 1 < a->m_nlev_used && L.rank)
+            for (size_t k = 0; k < (size_t)L.rank * L.W_mat.getRowNum(); ++k)
+                m = std::max(m, std::fabs(L.W_mat.getMatValPtr()[k]));
+    }
+    if (wmax) *wmax = m;
+    if (lev_ptr)
+        for (UINT32 l = 0; l <= a->m_nlev_used; ++l) lev_ptr[l] = a->m_lev_ptr_v[l];
+}
+
+extern "C" void ref_gmslr_info(void* h, unsigned* nlev, unsigned* lev_ptr, unsigned* ncomps, unsigned* ranks,
+                               unsigned* mnnz, double* wmax) {
+    if (static_cast<RefPrecond*>(h)->lowPrecision) gmslr_info_t<FLOAT32>(h, nlev, lev_ptr, ncomps, ranks, mnnz, wmax);
+    else gmslr_info_t<FLOAT64>(h, nlev, lev_ptr, ncomps, ranks, mnnz, wmax);
+}
+
+template <typename Low>
+static void gmslr_perm_t(void* h, unsigned* perm) {
+    auto* a = gmslr<Low>(h);
+    for (UINT32 i = 0; i < a->m_pperm.getLength(); ++i) perm[i] = a->m_pperm[i];
+}
+
+extern "C" void ref_gmslr_perm(void* h, unsigned* perm) {
+    if (static_cast<RefPrecond*>(h)->lowPrecision) gmslr_perm_t<FLOAT32>(h, perm);
+    else gmslr_perm_t<FLOAT64>(h, perm);
+}
+
+// ILUT block factor (which 0: L, 1: U; diag: Dinv)
+template <typename Low>
+static void gmslr_block_t(void* h, int level, int block, int which, unsigned* n, unsigned* nnz, unsigned* rowptr,
+                          unsigned* col, double* val, double* diag) {
+    auto* a = gmslr<Low>(h);
+    auto& L = *a->m_levs_all[level];
+    auto* lu = static_cast<IncompleteLU<Low, FLOAT64>*>(L.B_precond[block].get());
+    const CSRMatrix<Low>* M = which == 0 ? &*lu->m_L : &*lu->m_U;
+    *n = M->getRowNum();
+    *nnz = M->getRowOffsetPtr(0)[M->getRowNum()];
+    if (rowptr) {
+        for (UINT32 i = 0; i <= *n; ++i) rowptr[i] = M->getRowOffsetPtr(0)[i];
+        for (UINT32 k = 0; k < *nnz; ++k) { col[k] = M->getColIndicesPtr(0)[k]; val[k] = (double)M->getCSRValuesPtr(0)[k]; }
+        if (diag) for (UINT32 i = 0; i < *n; ++i) diag[i] = (double)(*lu->m_diagVals)[i];
+    }
+}
+
+extern "C" void ref_gmslr_block(void* h, int level, int block, int which, unsigned* n, unsigned* nnz,
+                                unsigned* rowptr, unsigned* col, double* val, double* diag) {
+    if (static_cast<RefPrecond*>(h)->lowPrecision) gmslr_block_t<FLOAT32>(h, level, block, which, n, nnz, rowptr, col, val, diag);
+    else gmslr_block_t<FLOAT64>(h, level, block, which, n, nnz, rowptr, col, val, diag);
 }

@@ -110,6 +110,12 @@ _SIGS = {
     "prism_amsed_coupling": (C.c_int32, [_vp, C.c_int32, C.c_int32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64),
                                          _vp, _vp, _vp]),
     "prism_amsed_lowrank": (C.c_int32, [_vp, C.c_int32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), _vp, _vp]),
+    "prism_gmslr_default_opts": (None, [C.POINTER(AmsedOpts)]),
+    "prism_set_precond_gmslr": (C.c_int32, [_vp, C.POINTER(AmsedOpts), C.c_int32]),
+    "prism_factor_create_gmslr": (C.c_int32, [C.c_uint32, _u32p, _u32p, _f64p, C.POINTER(AmsedOpts), C.c_int32,
+                                              C.POINTER(_vp)]),
+    "prism_gmslr_block": (C.c_int32, [_vp, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_uint32),
+                                      C.POINTER(C.c_uint64), _vp, _vp, _vp, _vp]),
     "prism_apply_device": (C.c_int32, [_vp, _vp, _vp]),
     "prism_apply": (C.c_int32, [_vp, _f64p, _f64p]),
     "prism_solve_device": (C.c_int32, [_vp, C.POINTER(SolveOpts), _vp, _vp, C.POINTER(SolveStats)]),
@@ -317,6 +323,43 @@ class HostAmsed:
         H = np.zeros(r.value, np.float64)
         _check(self.lib.prism_amsed_lowrank(self.h, level, C.byref(r), C.byref(nrem), W.ctypes.data, H.ctypes.data))
         return W.reshape(r.value, nrem.value).T.copy() if r.value else W.reshape(nrem.value, 0), H
+
+
+def gmslr_opts(**kw) -> AmsedOpts:
+    o = AmsedOpts()
+    load().prism_gmslr_default_opts(C.byref(o))
+    for k, v in kw.items():
+        if not hasattr(o, k):
+            raise KeyError(k)
+        setattr(o, k, v)
+    return o
+
+
+class HostGmslr(HostAmsed):
+    """GMSLR setup built on the host (prism_factor_create_gmslr)."""
+
+    is_gmslr = True
+
+    def __init__(self, A: CSRMatrix, opts: AmsedOpts | None = None, precision: int = PRISM_FP64, **kw):
+        self.lib = load()
+        self.opts = opts if opts is not None else gmslr_opts(**kw)
+        h = _vp()
+        _check(self.lib.prism_factor_create_gmslr(A.n, A.rowptr, A.col, A.val, C.byref(self.opts), precision,
+                                                  C.byref(h)))
+        self.h = h
+        self.n = A.n
+
+    def gmslr_block(self, level: int, block: int, which: int):
+        n, nnz = C.c_uint32(), C.c_uint64()
+        _check(self.lib.prism_gmslr_block(self.h, level, block, which, C.byref(n), C.byref(nnz), None, None, None,
+                                          None))
+        rp = np.zeros(n.value + 1, np.uint32)
+        ci = np.zeros(nnz.value, np.uint32)
+        v = np.zeros(nnz.value, np.float64)
+        d = np.zeros(n.value, np.float64)
+        _check(self.lib.prism_gmslr_block(self.h, level, block, which, C.byref(n), C.byref(nnz), rp.ctypes.data,
+                                          ci.ctypes.data, v.ctypes.data, d.ctypes.data))
+        return rp, ci, v, d
 
 
 # =============================================================================
@@ -596,6 +639,32 @@ class AMSEDPrecondition:
     def setup(self):
         if self.host is None:
             self.host = HostAmsed(self.system.A, self.opts, self.precision)
+            self.system.attach(self.host)
+
+    def MInvSolve(self, vec):
+        self.setup()
+        return self.system.apply(vec)
+
+    def getPreconditionNonZeroCount(self):
+        self.setup()
+        return self.host.info()["mnnz"]
+
+
+class GMSLRPrecondition:
+    """GMSLRPrecondition<Low, double>(A, levelNum, lanczosSteps, lowRankSize, localReorderType)
+    (GMSLRDPrecondition.cpp:41-55)."""
+
+    def __init__(self, system: DeviceSystem, levelNum, lanczosSteps=20, lowRankSize=12,
+                 localReorderType=MatrixReorderRCM, precision=PRISM_FP64):
+        self.system = system
+        self.opts = gmslr_opts(levels=levelNum, lanczos_steps=lanczosSteps, low_rank=lowRankSize,
+                               reorder=localReorderType)
+        self.precision = precision
+        self.host = None
+
+    def setup(self):
+        if self.host is None:
+            self.host = HostGmslr(self.system.A, self.opts, self.precision)
             self.system.attach(self.host)
 
     def MInvSolve(self, vec):

@@ -53,6 +53,7 @@ void upload_csr(DeviceCsr& d, uint32_t nrows, const std::vector<uint32_t>& rp, c
 }  // namespace
 
 AmsedPrecond::AmsedPrecond(Handle& h, std::shared_ptr<const HostAmsed> a) : h_(h), a_(std::move(a)) {
+    gmslr_ = a_->opt.family == 4;
     if (a_->fp32) build(*a_->s32);
     else build(*a_->s64);
 }
@@ -77,7 +78,35 @@ void AmsedPrecond::build(const AmsedSetup<Low>& S) {
         D.nb = S.lev_ptr[l + 1] - S.lev_ptr[l];
         D.nrem = S.n - S.lev_ptr[l + 1];
         Sweep<Low> lo, up;
-        if (l + 1 == nlev_) {
+        if (gmslr_) {
+            // ILUT blocks on every level (the last level: block 0 only, GMSLRDPrecondition.cpp:664-688)
+            const uint32_t nblk = l + 1 == nlev_ ? 1 : L.ncomps;
+            D.nfac = l + 1 == nlev_ ? L.B[0].n : D.nb;
+            CsrT<Low> Lc, Uc;
+            std::vector<Low> Dc;
+            Lc.n = Uc.n = D.nfac;
+            Lc.rowptr.assign((size_t)D.nfac + 1, 0);
+            Uc.rowptr.assign((size_t)D.nfac + 1, 0);
+            for (uint32_t b = 0; b < nblk; ++b) {
+                const uint32_t off = L.dom_ptr[b] - L.dom_ptr[0];
+                const CsrT<Low>& fl = L.Lt[b];
+                const CsrT<Low>& fu = L.U[b];
+                for (uint32_t i = 0; i < fl.n; ++i) {
+                    for (uint32_t k = fl.rowptr[i]; k < fl.rowptr[i + 1]; ++k) {
+                        Lc.col.push_back(fl.col[k] + off);
+                        Lc.val.push_back(fl.val[k]);
+                    }
+                    Lc.rowptr[off + i + 1] = (uint32_t)Lc.col.size();
+                    for (uint32_t k = fu.rowptr[i]; k < fu.rowptr[i + 1]; ++k) {
+                        Uc.col.push_back(fu.col[k] + off);
+                        Uc.val.push_back(fu.val[k]);
+                    }
+                    Uc.rowptr[off + i + 1] = (uint32_t)Uc.col.size();
+                }
+                Dc.insert(Dc.end(), L.Dinv[b].begin(), L.Dinv[b].end());
+            }
+            ilut_sweeps<Low>(Lc, Uc, Dc, lo, up);
+        } else if (l + 1 == nlev_) {
             // last level: IC of block 0 (the reference factors and applies only B_mat[0], :694-716, :1504-1508)
             D.nfac = L.B[0].n;
             ic_sweeps<Low>(L.Lt[0], lo, up);
@@ -106,10 +135,16 @@ void AmsedPrecond::build(const AmsedSetup<Low>& S) {
         tune_sweep<Low>(h_, D.upper, up);
         if (l + 1 < nlev_) {
             upload_csr(D.E, L.E.n, L.E.rowptr, L.E.col, L.E.val, st);
-            std::vector<uint32_t> trp, tcol;
-            std::vector<double> tval;
-            transpose_rect(L.E, D.nrem, trp, tcol, tval);
-            upload_csr(D.Et, D.nrem, trp, tcol, tval, st);
+            if (gmslr_) {
+                // x2 -= F x1 with F = A(C rows, B cols) (GMSLRDPrecondition.cpp:1080)
+                upload_csr(D.Et, D.nrem, L.F.rowptr, L.F.col, L.F.val, st);
+            } else {
+                // x2 -= E^T x1 (AMSEDPrecondition.cpp:1535-1540), E^T explicit
+                std::vector<uint32_t> trp, tcol;
+                std::vector<double> tval;
+                transpose_rect(L.E, D.nrem, trp, tcol, tval);
+                upload_csr(D.Et, D.nrem, trp, tcol, tval, st);
+            }
             D.rank = L.rank;
             if (D.rank > (uint32_t)kMaxRank)
                 throw Error(PRISM_ERR_UNSUPPORTED, "low-rank correction above " + std::to_string(kMaxRank) + " columns");

@@ -616,6 +616,7 @@ void classic_lanczos(AmsedSetup<Low>& S, int level, const AmsedOptions& opt, uns
     }
     const uint32_t r = (uint32_t)chosen.size();
     L.rank = r;
+    L.rank_reported = r;
     L.W.assign((size_t)nr * r, 0.0);
     for (uint32_t i = 0; i < r; ++i) {
         double* wc = L.W.data() + (size_t)i * nr;
@@ -633,7 +634,12 @@ void classic_lanczos(AmsedSetup<Low>& S, int level, const AmsedOptions& opt, uns
 
 template <typename Low>
 int amsed_setup(const CsrHost& A, const AmsedOptions& opt, AmsedSetup<Low>& S, std::string* err) {
-    if (opt.lanczos_type != 0) {
+    if (opt.family != 4 && opt.family != 5) {
+        if (err) *err = "family must be 5 (AMSED) or 4 (GMSLR)";
+        return SETUP_BAD_INPUT;
+    }
+    const bool gmslr = opt.family == 4;
+    if (!gmslr && opt.lanczos_type != 0) {
         if (err) *err = "only the classic generalized Lanczos (UseClassicLanczos) is provided";
         return SETUP_BAD_INPUT;
     }
@@ -704,8 +710,43 @@ int amsed_setup(const CsrHost& A, const AmsedOptions& opt, AmsedSetup<Low>& S, s
         if (level + 1 < tlvl) {
             const uint32_t n_start = S.lev_ptr[level], n_end = S.lev_ptr[level + 1];
             L.E = range_matrix(Apq, n_start, n_end, n_end, n);
-            L.C = range_matrix(Apq, n_end, n, n_end, n);
+            if (gmslr) L.F = range_matrix(Apq, n_end, n, n_start, n_end);
+            else L.C = range_matrix(Apq, n_end, n, n_end, n);
         }
+    }
+    if (gmslr) {
+        // GMSLR setupMSLR (GMSLRDPrecondition.cpp:649-733): ILUT(GMSLR_LFILL = 20, tol) on the last
+        // level's block 0 and on every block of the other levels.  Its low-rank step
+        // (reorthogonalSecondArnoldi + computeArnoldiEigenValuesAndEigenVectors, :849-1036)
+        // calls LAPACKE_dhseqr with COMPZ = 'V' on a zero-initialised Z, which returns Q*Z = 0:
+        // W is identically zero and the correction W H W^T vanishes.  The Arnoldi process is
+        // therefore not run; the rank the reference reports (min(lanczosSteps, lowRankSize))
+        // and its non-zero accounting (rank * n_remain + rank) are kept.
+        const uint32_t lfill = 20;
+        for (int level = (int)tlvl - 1; level >= 0; --level) {
+            AmsedLevel<Low>& L = S.levels[level];
+            const uint32_t nblk = level == (int)tlvl - 1 ? 1 : L.ncomps;
+            L.Lt.resize(nblk);
+            L.U.resize(nblk);
+            L.Dinv.resize(nblk);
+            for (uint32_t b = 0; b < nblk; ++b) {
+                int rc = ilut_factor<Low>(L.B[b], lfill, opt.factor_tol, L.Lt[b], L.U[b], L.Dinv[b], err);
+                if (rc) return rc;
+                const uint64_t m = L.Lt[b].nnz() + L.U[b].nnz() + L.B[b].n;
+                S.mnnz += m;
+                S.incomp_nnz += m;
+            }
+            if (level + 1 < (int)tlvl) {
+                const uint32_t k = (uint32_t)std::min(opt.lanczos_steps, opt.low_rank);
+                const uint32_t nr = n - S.lev_ptr[level + 1];
+                L.rank = 0;
+                L.rank_reported = k;
+                const uint64_t lr = (uint64_t)k * nr + k;
+                S.mnnz += lr;
+                S.lowrank_nnz += lr;
+            }
+        }
+        return SETUP_OK;
     }
     // ---- MSLR (setupMSLR, :652-743): IC on the last level, then per level ILDLT + Lanczos ----
     {

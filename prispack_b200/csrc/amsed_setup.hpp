@@ -13,6 +13,8 @@
 namespace prism {
 
 struct AmsedOptions {
+    int32_t family = 5;              // 5: AMSED (ILDLT blocks, ICT last level, Lanczos correction)
+                                     // 4: GMSLR (ILUT(20, tol) blocks and last level, F = A(C, B) coupling)
     int32_t levels = 3;              // m_nlev_setup
     int32_t lanczos_steps = 30;      // m_lanczosSteps (AMSED_MSTEPS)
     int32_t low_rank = 16;           // m_lowRankSize (AMSED_RANK); caps the MSLR (basic) rank
@@ -31,11 +33,16 @@ struct AmsedLevel {
     uint32_t ncomps = 0;
     std::vector<uint32_t> dom_ptr;          // global (permuted) row offsets of the domains, ncomps + 1
     std::vector<CsrHost> B;                 // diagonal blocks, local numbering
-    std::vector<CsrT<Low>> Lt;              // per block: ILDLT unit L^T (last level: IC L^T incl. diagonal)
+    std::vector<CsrT<Low>> Lt;              // per block: ILDLT unit L^T (last level: IC L^T incl. diagonal);
+                                            // GMSLR: ILUT L
     std::vector<std::vector<double>> D;     // per block: ILDLT pivots (empty on the last level)
+    std::vector<CsrT<Low>> U;               // GMSLR: per block ILUT U
+    std::vector<std::vector<Low>> Dinv;     // GMSLR: per block ILUT inverse pivots
     CsrHost E;                              // coupling rows of this level's B x columns of its C block
+    CsrHost F;                              // GMSLR: C rows x B columns (GMSLRDPrecondition.cpp:239)
     CsrHost C;                              // the level's C block (for the Lanczos process)
-    uint32_t rank = 0;
+    uint32_t rank = 0;                      // columns of W used by the apply
+    uint32_t rank_reported = 0;             // rank the reference reports (GMSLR: W is identically zero)
     std::vector<double> H;                  // rank
     std::vector<double> W;                  // n_remain x rank, column-major
 };

@@ -68,10 +68,11 @@ static prism::AmsedOptions to_options(const prism_amsed_opts* o) {
 }
 
 static std::shared_ptr<prism::HostAmsed> build_amsed(const prism::CsrHost& A, const prism_amsed_opts* o,
-                                                     int32_t precision, int* rc, std::string* err) {
+                                                     int32_t precision, int* rc, std::string* err, int family = 5) {
     auto h = std::make_shared<prism::HostAmsed>();
     h->fp32 = precision == PRISM_FP32;
     h->opt = to_options(o);
+    h->opt.family = family;
     if (h->fp32) {
         h->s32 = std::make_shared<prism::AmsedSetup<float>>();
         *rc = prism::amsed_setup<float>(A, h->opt, *h->s32, err);
@@ -301,6 +302,53 @@ int32_t prism_set_precond_amsed(prism_handle h, const prism_amsed_opts* o, int32
     });
 }
 
+void prism_gmslr_default_opts(prism_amsed_opts* o) {
+    if (!o) return;
+    prism_amsed_default_opts(o);
+    o->lanczos_steps = 20;  // GMSLR_MSTEPS
+    o->low_rank = 12;       // GMSLR_RANK
+    o->factor_tol = 1e-2;   // GMSLR_FACTOR_TOLRANCE (ILUT lfill is GMSLR_LFILL = 20)
+    o->lowrank_type = 0;
+}
+
+int32_t prism_set_precond_gmslr(prism_handle h, const prism_amsed_opts* o, int32_t precision) {
+    if (!h || !o) return fail(PRISM_ERR_ARG, "null argument");
+    if (precision != PRISM_FP64 && precision != PRISM_FP32) return fail(PRISM_ERR_ARG, "bad precision");
+    return guarded([&]() -> int {
+        DeviceGuard g(h->info.device);
+        h->P.reset();
+        int rc = 0;
+        std::string err;
+        auto a = build_amsed(h->A_host, o, precision, &rc, &err, 4);
+        if (rc) return fail(rc, err);
+        h->P = std::make_unique<prism::AmsedPrecond>(*h, a);
+        return PRISM_OK;
+    });
+}
+
+int32_t prism_factor_create_gmslr(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val,
+                                  const prism_amsed_opts* o, int32_t precision, prism_factor* out) {
+    if (!out || !o) return fail(PRISM_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (n == 0 || !rowptr || !col || !val) return fail(PRISM_ERR_ARG, "empty or null CSR");
+    if (precision != PRISM_FP64 && precision != PRISM_FP32) return fail(PRISM_ERR_ARG, "bad precision");
+    std::string bad = prism::validate_csr(n, rowptr, col);
+    if (!bad.empty()) return fail(PRISM_ERR_BAD_MATRIX, bad);
+    return guarded([&]() -> int {
+        prism::CsrHost A;
+        A.n = n;
+        A.rowptr.assign(rowptr, rowptr + n + 1);
+        A.col.assign(col, col + rowptr[n]);
+        A.val.assign(val, val + rowptr[n]);
+        int rc = 0;
+        std::string err;
+        auto a = build_amsed(A, o, precision, &rc, &err, 4);
+        if (rc) return fail(rc, err);
+        *out = new prism_factor_s{nullptr, std::move(a)};
+        return PRISM_OK;
+    });
+}
+
 int32_t prism_factor_create_amsed(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val,
                                   const prism_amsed_opts* o, int32_t precision, prism_factor* out) {
     if (!out || !o) return fail(PRISM_ERR_ARG, "null argument");
@@ -345,7 +393,7 @@ int32_t prism_amsed_info(prism_factor f, uint32_t* nlev, uint32_t* lev_ptr, uint
         if (mnnz) *mnnz = S.mnnz;
         for (uint32_t l = 0; l < S.nlev; ++l) {
             if (ncomps) ncomps[l] = S.levels[l].ncomps;
-            if (ranks) ranks[l] = S.levels[l].rank;
+            if (ranks) ranks[l] = S.levels[l].rank_reported;
         }
         if (lev_ptr) std::memcpy(lev_ptr, S.lev_ptr.data(), S.lev_ptr.size() * sizeof(uint32_t));
         return PRISM_OK;
@@ -393,12 +441,32 @@ int32_t prism_amsed_coupling(prism_factor f, int32_t level, int32_t which, uint3
                              uint32_t* rowptr, uint32_t* col, double* val) {
     return with_amsed(f, [&](const auto& S) -> int {
         if (level < 0 || (uint32_t)level + 1 >= S.nlev) return fail(PRISM_ERR_ARG, "level has no coupling block");
-        const prism::CsrHost& M = which == 0 ? S.levels[level].E : S.levels[level].C;
+        const prism::CsrHost& M = which == 0 ? S.levels[level].E : (which == 1 ? S.levels[level].C : S.levels[level].F);
         if (nrows) *nrows = M.n;
         if (nnz) *nnz = M.nnz();
         if (rowptr) std::memcpy(rowptr, M.rowptr.data(), M.rowptr.size() * sizeof(uint32_t));
         if (col) std::memcpy(col, M.col.data(), M.col.size() * sizeof(uint32_t));
         if (val) std::memcpy(val, M.val.data(), M.val.size() * sizeof(double));
+        return PRISM_OK;
+    });
+}
+
+int32_t prism_gmslr_block(prism_factor f, int32_t level, int32_t block, int32_t which, uint32_t* n, uint64_t* nnz,
+                          uint32_t* rowptr, uint32_t* col, double* val, double* dinv) {
+    return with_amsed(f, [&](const auto& S) -> int {
+        if (level < 0 || (uint32_t)level >= S.nlev) return fail(PRISM_ERR_ARG, "level out of range");
+        const auto& L = S.levels[level];
+        if (L.U.empty()) return fail(PRISM_ERR_ARG, "not a GMSLR factor");
+        if (block < 0 || (size_t)block >= L.U.size()) return fail(PRISM_ERR_ARG, "block out of range");
+        const auto& F = which == 0 ? L.Lt[block] : L.U[block];
+        if (n) *n = F.n;
+        if (nnz) *nnz = F.nnz();
+        if (rowptr) std::memcpy(rowptr, F.rowptr.data(), F.rowptr.size() * sizeof(uint32_t));
+        if (col) std::memcpy(col, F.col.data(), F.col.size() * sizeof(uint32_t));
+        if (val)
+            for (size_t k = 0; k < F.val.size(); ++k) val[k] = (double)F.val[k];
+        if (dinv)
+            for (size_t k = 0; k < L.Dinv[block].size(); ++k) dinv[k] = (double)L.Dinv[block][k];
         return PRISM_OK;
     });
 }

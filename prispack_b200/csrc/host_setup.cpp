@@ -515,6 +515,16 @@ void ildlt_sweeps(const CsrT<Low>& Lt, const std::vector<double>& D, Sweep<Low>&
     build_sweep<Low>(n, lrp, lcol, lval, nullptr, SWEEP_NONE, true, lo);
     build_sweep<Low>(n, Lt.rowptr, Lt.col, Lt.val, &D, SWEEP_PREDIV, false, up);
 }
+template <typename Low>
+void ilut_sweeps(const CsrT<Low>& L, const CsrT<Low>& U, const std::vector<Low>& Dinv, Sweep<Low>& lo, Sweep<Low>& up) {
+    std::vector<double> dd(Dinv.begin(), Dinv.end());
+    build_sweep<Low>(L.n, L.rowptr, L.col, L.val, nullptr, SWEEP_NONE, true, lo);
+    build_sweep<Low>(U.n, U.rowptr, U.col, U.val, &dd, SWEEP_MUL, false, up);
+}
+template void ilut_sweeps<double>(const CsrT<double>&, const CsrT<double>&, const std::vector<double>&,
+                                  Sweep<double>&, Sweep<double>&);
+template void ilut_sweeps<float>(const CsrT<float>&, const CsrT<float>&, const std::vector<float>&, Sweep<float>&,
+                                 Sweep<float>&);
 template void ic_sweeps<double>(const CsrT<double>&, Sweep<double>&, Sweep<double>&);
 template void ic_sweeps<float>(const CsrT<float>&, Sweep<float>&, Sweep<float>&);
 template void ildlt_sweeps<double>(const CsrT<double>&, const std::vector<double>&, Sweep<double>&, Sweep<double>&);
@@ -554,8 +564,7 @@ int build_tri_t(int kind, const CsrHost& A, double tol, uint32_t lfill, HostFact
         int rc = ilut_factor<Low>(A, lfill, tol, L, U, Dinv, err);
         if (rc) return rc;
         std::vector<double> dd(Dinv.begin(), Dinv.end());
-        build_sweep<Low>(n, L.rowptr, L.col, L.val, nullptr, SWEEP_NONE, true, lo);
-        build_sweep<Low>(n, U.rowptr, U.col, U.val, &dd, SWEEP_MUL, false, up);
+        ilut_sweeps<Low>(L, U, Dinv, lo, up);
         F.mnnz = L.nnz() + U.nnz() + n;  // IncompleteLU.cpp:264
         widen_csr(L, F.f0);
         widen_csr(U, F.f1);

@@ -135,7 +135,7 @@ struct HostAmsed {
 class AmsedPrecond : public Precond {
   public:
     AmsedPrecond(Handle& h, std::shared_ptr<const HostAmsed> a);
-    int kind() const override { return PRISM_PRECOND_AMSED; }
+    int kind() const override { return gmslr_ ? PRISM_PRECOND_GMSLR : PRISM_PRECOND_AMSED; }
     uint64_t mnnz() const override;
     void apply(cudaStream_t st, const double* in, double* out) override;
     uint32_t levels(int sweep) const override;
@@ -148,7 +148,7 @@ class AmsedPrecond : public Precond {
     struct Level {
         uint32_t nb = 0, nfac = 0, nrem = 0, rank = 0;
         DevSweep lower, upper;
-        DeviceCsr E, Et;
+        DeviceCsr E, Et;   // Et: the downward coupling, E^T (AMSED) or F (GMSLR)
         DevBuf<double> W, H, xc, tmp, tmp2, t;
     };
     template <typename Low>
@@ -157,6 +157,7 @@ class AmsedPrecond : public Precond {
     void c_solve(cudaStream_t st, int level, double* x);
     Handle& h_;
     std::shared_ptr<const HostAmsed> a_;
+    bool gmslr_ = false;
     uint32_t n_ = 0, nlev_ = 0;
     std::vector<uint32_t> lev_ptr_;
     DevBuf<uint32_t> pperm_;

@@ -12,8 +12,14 @@ parity build) on seeded model problems and stores their outputs:
 * CG (FlexibleCG, NormalCG) and GMRES (FlexibleGMRES with restart) results:
   iteration count, reported error, convergence flag and solution.
 
+* AMSED / MSLR and GMSLR hierarchies (permutation, level pointers, block
+  factor digests, low-rank spectra), their MInvSolve on a seeded vector and a
+  preconditioned FCG / FGMRES solve.
+
 Usage (needs the reference sources, i.e. only where oracle/_ref was built):
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle ref && python tests/golden/make_golden.py [basic] [amsed] [gmslr]
+(no argument regenerates every section; a named section updates only its own
+files and manifest entries).
 """
 from __future__ import annotations
 
@@ -44,6 +50,12 @@ AMSED_CASES = [
     ("amsed_16c_defl32", (16, 16, 16), 3, 40, 20, 1, True),
     ("amsed_40sq_l4", (40, 40, 1), 4, 30, 16, 0, False),
 ]
+# (name, grid with convection, levels, lanczos steps, low rank, FP32 factors)
+GMSLR_CASES = [
+    ("gmslr_16c_conv", (16, 16, 16, 0.3, 0.1, 0.0, 0.0), 3, 20, 12, False),
+    ("gmslr_40sq_conv32", (40, 40, 1, 0.2, -0.3, 0.0, 0.0), 4, 20, 12, True),
+    ("gmslr_12c_lap", (12, 12, 12, 0.0, 0.0, 0.0, 0.0), 2, 20, 12, False),
+]
 
 
 def digest(*arrays) -> str:
@@ -57,10 +69,28 @@ def rhs(n: int, seed: int) -> np.ndarray:
     return np.random.default_rng(seed).uniform(-1.0, 1.0, n)
 
 
-def main():
+def main(sections):
     if not ref.available():
         raise SystemExit("oracle/_ref/libprism_ref.so not built: run `make -C oracle ref` where the reference exists")
+    path = os.path.join(HERE, "manifest.json")
     manifest = {}
+    if os.path.exists(path) and set(sections) != {"basic", "amsed", "gmslr"}:
+        with open(path) as f:
+            manifest = json.load(f)
+    if "basic" in sections:
+        basic(manifest)
+    if "amsed" in sections:
+        amsed_section(manifest)
+    if "gmslr" in sections:
+        gmslr_section(manifest)
+    manifest["_seed"] = SEED
+    manifest["_generator"] = "tests/golden/make_golden.py via oracle/_ref/libprism_ref.so (reference sources, parity flags)"
+    with open(path, "w") as f:
+        json.dump(manifest, f, indent=1, sort_keys=True)
+    print("wrote", ", ".join(sections))
+
+
+def basic(manifest):
     for name, grid, sym, full in CASES:
         A = ref.RefCSR.laplacian(*grid)
         rp, ci, v = A.arrays()
@@ -121,7 +151,10 @@ def main():
         meta["none.gmres30"] = {"iters": it, "err": err, "conv": conv}
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
         manifest[name] = meta
-    # ---- AMSED / MSLR (reference AMSEDPrecondition behind the METIS stand-in) ----
+
+
+def amsed_section(manifest):
+    """AMSED / MSLR (reference AMSEDPrecondition behind the METIS stand-in)."""
     amsed = {}
     for name, grid, levels, steps, rank, ltype, low in AMSED_CASES:
         A = ref.RefCSR.laplacian(*grid)
@@ -152,12 +185,36 @@ def main():
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
         amsed[name] = entry
     manifest["_amsed"] = amsed
-    manifest["_seed"] = SEED
-    manifest["_generator"] = "tests/golden/make_golden.py via oracle/_ref/libprism_ref.so (reference sources, parity flags)"
-    with open(os.path.join(HERE, "manifest.json"), "w") as f:
-        json.dump(manifest, f, indent=1, sort_keys=True)
-    print("wrote", len(CASES), "cases")
+
+
+def gmslr_section(manifest):
+    """GMSLR (reference GMSLRPrecondition behind the METIS stand-in): ILUT blocks,
+    F coupling; its low-rank W is identically zero (dhseqr with COMPZ='V' on a
+    zero Z), which the entry records as w_max_abs."""
+    gm = {}
+    for name, grid, levels, steps, rank, low in GMSLR_CASES:
+        A = ref.RefCSR.laplacian(*grid)
+        n = A.dims()[0]
+        R = ref.RefGmslr(A, levels, steps, rank, 2, low)
+        assert R.setup() == 0
+        inf = R.info()
+        entry = {"grid": grid, "levels": levels, "lanczos_steps": steps, "low_rank": rank, "fp32": low,
+                 "nlev": inf["nlev"], "lev_ptr": inf["lev_ptr"].tolist(), "ncomps": inf["ncomps"].tolist(),
+                 "ranks": inf["ranks"].tolist(), "mnnz": inf["mnnz"], "w_max_abs": inf["w_max_abs"],
+                 "perm_sha": digest(R.perm()), "blocks": {}}
+        for lv in range(inf["nlev"]):
+            nb = 1 if lv == inf["nlev"] - 1 else int(inf["ncomps"][lv])
+            entry["blocks"][str(lv)] = [[digest(*R.block(lv, b, w)) for w in (0, 1)] for b in range(nb)]
+        probe = rhs(n, SEED + 1)
+        b = rhs(n, SEED)
+        out = {"probe": probe, "b": b, "apply": R.apply(probe)}
+        x, it, err, conv = ref.gmres_solve(A, R, b, tol=1e-10, restart=30, flexible=True)
+        out["fgmres30.x"] = x
+        entry["fgmres30"] = {"iters": it, "err": err, "conv": conv}
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+        gm[name] = entry
+    manifest["_gmslr"] = gm
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:] or ["basic", "amsed", "gmslr"])

@@ -89,3 +89,65 @@ def test_reference_named_wrapper():
     x = solver.solve(S, np.ones(A.n), np.zeros(A.n))
     assert solver.getConvergence() and solver.getNumIter() > 1
     assert M.getPreconditionNonZeroCount() > A.nnz
+
+
+# ---------------------------------------------------------------- GMSLR
+GMSLR_CASES = ["gmslr_16c_conv", "gmslr_40sq_conv32", "gmslr_12c_lap"]
+
+
+def build_gmslr(e):
+    A = P.CSRMatrix.laplacian(*e["grid"])
+    G = P.HostGmslr(A, levels=e["levels"], lanczos_steps=e["lanczos_steps"], low_rank=e["low_rank"],
+                    precision=P.PRISM_FP32 if e["fp32"] else P.PRISM_FP64)
+    return A, G
+
+
+@pytest.mark.parametrize("name", GMSLR_CASES)
+def test_gmslr_apply_vs_oracle_and_reference(name, manifest, load_golden):
+    e = manifest["_gmslr"][name]
+    g = load_golden(name)
+    A, G = build_gmslr(e)
+    S = P.DeviceSystem(A)
+    S.attach(G)
+    out = S.apply(g["probe"])
+    assert rel_err(out, orc.Amsed(G).apply(g["probe"])) < 1e-12
+    assert rel_err(out, g["apply"]) < 1e-12
+
+
+@pytest.mark.parametrize("name", GMSLR_CASES)
+def test_fgmres_gmslr_vs_reference(name, manifest, load_golden):
+    e = manifest["_gmslr"][name]
+    g = load_golden(name)
+    A, G = build_gmslr(e)
+    S = P.DeviceSystem(A)
+    S.attach(G)
+    x, st = S.solve(g["b"], solver=P.SOLVER_FGMRES, tol=1e-10, restart=30)
+    assert abs(st.num_iter - e["fgmres30"]["iters"]) <= 1 and st.converged
+    if st.num_iter == e["fgmres30"]["iters"]:
+        assert rel_err(x, g["fgmres30.x"]) < 1e-9
+    assert st.true_rel_residual < 1.5e-10
+
+
+def test_fgmres_gmslr_convection_3d_vs_oracle():
+    A = P.CSRMatrix.laplacian(32, 32, 32, 0.4, 0.2, 0.1)
+    G = P.HostGmslr(A, levels=4, precision=P.PRISM_FP32)
+    S = P.DeviceSystem(A)
+    S.attach(G)
+    b = np.random.default_rng(9).uniform(-1, 1, A.n)
+    assert rel_err(S.apply(b), orc.Amsed(G).apply(b)) < 1e-12
+    x, st = S.solve(b, solver=P.SOLVER_FGMRES, tol=1e-10, restart=50)
+    xo, ito, _, _ = orc.gmres(A.rowptr, A.col, A.val, b, orc.Amsed(G).precond(), tol=1e-10, restart=50)
+    assert abs(st.num_iter - ito) <= 1 and st.converged
+    if st.num_iter == ito:
+        assert rel_err(x, xo) < 1e-9
+
+
+def test_gmslr_reference_named_wrapper():
+    A = P.CSRMatrix.laplacian(16, 16, 16, 0.3, 0.0, 0.0)
+    S = P.DeviceSystem(A)
+    M = P.GMSLRPrecondition(S, 3, 20, 12, P.MatrixReorderRCM)
+    solver = P.GMRES(A.n, M, 1e-10, P.FlexibleGMRES)
+    solver.setRestart(True, 30)
+    x = solver.solve(S, np.ones(A.n), np.zeros(A.n))
+    assert solver.getConvergence() and solver.getNumIter() > 1
+    assert M.getPreconditionNonZeroCount() > A.nnz
