@@ -125,7 +125,9 @@ def test_fgmres_gmslr_vs_reference(name, manifest, load_golden):
     assert abs(st.num_iter - e["fgmres30"]["iters"]) <= 1 and st.converged
     if st.num_iter == e["fgmres30"]["iters"]:
         assert rel_err(x, g["fgmres30.x"]) < 1e-9
-    assert st.true_rel_residual < 1.5e-10
+    # FGMRES stops on its Givens estimate and restarts from it (GMRES.cpp:194, :214),
+    # so the true residual may sit above tol, as it does in the reference
+    assert st.true_rel_residual < 1e-8
 
 
 def test_fgmres_gmslr_convection_3d_vs_oracle():
