@@ -248,6 +248,41 @@ int32_t prism_solve_device(prism_handle h, const prism_solve_opts* opts, const d
 int32_t prism_solve(prism_handle h, const prism_solve_opts* opts, const double* b, double* x,
                     prism_solve_stats* stats);
 
+/* ---- new values on the same pattern, and the adjoint solve ---------------
+ * prism_update_values*: A's values replaced (same rowptr/col); the
+ * preconditioner is kept as it was until a prism_set_precond_* call refactors
+ * it (a solve stays exact with a stale preconditioner, only slower).  No
+ * reference counterpart: the reference builds a new CSRMatrix.
+ *
+ * prism_adjoint_solve*: the backward pass of x = A^{-1} b for a scalar loss L
+ * with g = dL/dx:  lambda = A^{-T} g  (= dL/db), solved with the handle's
+ * solver and preconditioner from a zero guess, and, when grad_val is not
+ * null, dL/dA on A's stored pattern:  grad_val[k] = -lambda[i] x[j] for the
+ * k-th stored entry (i, j).  A must equal A^T exactly (checked once per set
+ * of values; PRISM_ERR_UNSUPPORTED otherwise).  No reference counterpart. */
+int32_t prism_update_values(prism_handle h, const double* val);
+int32_t prism_update_values_device(prism_handle h, const double* val_d);
+int32_t prism_adjoint_solve_device(prism_handle h, const prism_solve_opts* opts, const double* g_d, const double* x_d,
+                                   double* lambda_d, double* grad_val_d, prism_solve_stats* stats);
+int32_t prism_adjoint_solve(prism_handle h, const prism_solve_opts* opts, const double* g, const double* x,
+                            double* lambda, double* grad_val, prism_solve_stats* stats);
+
+/* ---- blocks of right-hand sides ----------------------------------------
+ * k (1..64) right-hand sides that share A and M, stored column-major with
+ * leading dimension ld >= n (ignored when k = 1).  Each column is solved with
+ * the recurrence of CG<double>::solve (source/Solver/CG.cpp:34-83), the same
+ * one prism_solve runs for it alone; a column stops changing once it has
+ * converged, and stats[c] (k entries) reports its own iteration count, error
+ * and true residual.  The reference solves one right-hand side per call; a
+ * block here shares every sweep's dependency latency among its k columns.
+ * Block solves use FCG / CG (PRISM_ERR_UNSUPPORTED otherwise) and an IC /
+ * ILDLT / ILUT preconditioner or none. */
+int32_t prism_apply_batched_device(prism_handle h, uint32_t k, const double* in_d, double* out_d, uint64_t ld);
+int32_t prism_solve_batched_device(prism_handle h, const prism_solve_opts* opts, uint32_t k, const double* B_d,
+                                   double* X_d, uint64_t ld, prism_solve_stats* stats);
+int32_t prism_solve_batched(prism_handle h, const prism_solve_opts* opts, uint32_t k, const double* B, double* X,
+                            uint64_t ld, prism_solve_stats* stats);
+
 #ifdef __cplusplus
 }
 #endif

@@ -116,6 +116,15 @@ _SIGS = {
                                               C.POINTER(_vp)]),
     "prism_gmslr_block": (C.c_int32, [_vp, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_uint32),
                                       C.POINTER(C.c_uint64), _vp, _vp, _vp, _vp]),
+    "prism_apply_batched_device": (C.c_int32, [_vp, C.c_uint32, _vp, _vp, C.c_uint64]),
+    "prism_solve_batched_device": (C.c_int32, [_vp, C.POINTER(SolveOpts), C.c_uint32, _vp, _vp, C.c_uint64,
+                                               C.POINTER(SolveStats)]),
+    "prism_solve_batched": (C.c_int32, [_vp, C.POINTER(SolveOpts), C.c_uint32, _f64p, _f64p, C.c_uint64,
+                                        C.POINTER(SolveStats)]),
+    "prism_update_values": (C.c_int32, [_vp, _f64p]),
+    "prism_update_values_device": (C.c_int32, [_vp, _vp]),
+    "prism_adjoint_solve_device": (C.c_int32, [_vp, C.POINTER(SolveOpts), _vp, _vp, _vp, _vp, C.POINTER(SolveStats)]),
+    "prism_adjoint_solve": (C.c_int32, [_vp, C.POINTER(SolveOpts), _f64p, _f64p, _f64p, _vp, C.POINTER(SolveStats)]),
     "prism_apply_device": (C.c_int32, [_vp, _vp, _vp]),
     "prism_apply": (C.c_int32, [_vp, _f64p, _f64p]),
     "prism_solve_device": (C.c_int32, [_vp, C.POINTER(SolveOpts), _vp, _vp, C.POINTER(SolveStats)]),
@@ -390,6 +399,10 @@ class DeviceSystem:
     def n(self) -> int:
         return self.A.n
 
+    @property
+    def nnz(self) -> int:
+        return int(self.A.rowptr[-1])
+
     def set_stream(self, stream_ptr: int):
         _check(self.lib.prism_set_stream(self.h, stream_ptr))
 
@@ -472,6 +485,70 @@ class DeviceSystem:
         return out
 
     # ---- solve ------------------------------------------------------------------
+    def update_values(self, val):
+        """New values of A on the same pattern (host array or CUDA tensor)."""
+        if hasattr(val, "is_cuda"):
+            _check(self.lib.prism_update_values_device(self.h, _ptr(val.contiguous())))
+        else:
+            _check(self.lib.prism_update_values(self.h, np.ascontiguousarray(val, np.float64)))
+
+    def adjoint(self, g, x=None, *, solver=SOLVER_FCG, tol=1e-10, max_iter=1000, restart=0):
+        """lambda = A^{-T} g and, with x given, dL/dA on A's pattern (-lambda_i x_j);
+        returns (lambda, grad_val or None, SolveStats)."""
+        opts = SolveOpts(solver, tol, max_iter, restart)
+        st = SolveStats()
+        if hasattr(g, "is_cuda"):
+            import torch
+            gc = g.contiguous()
+            lam = torch.empty_like(gc)
+            gv = None
+            if x is not None:
+                x = x.contiguous()
+                gv = torch.empty(self.nnz, dtype=torch.float64, device=gc.device)
+            _check(self.lib.prism_adjoint_solve_device(self.h, C.byref(opts), _ptr(gc),
+                                                       _ptr(x) if x is not None else None, _ptr(lam),
+                                                       _ptr(gv) if gv is not None else None, C.byref(st)))
+            return lam, gv, st
+        gh = np.ascontiguousarray(g, np.float64)
+        lam = np.zeros(self.n)
+        gv = np.zeros(self.nnz) if x is not None else None
+        xh = np.ascontiguousarray(x, np.float64) if x is not None else np.zeros(self.n)
+        _check(self.lib.prism_adjoint_solve(self.h, C.byref(opts), gh, xh, lam,
+                                            gv.ctypes.data if gv is not None else None, C.byref(st)))
+        return lam, gv, st
+
+    def apply_batched(self, V):
+        """M^{-1} applied to each row of V (shape (k, n), k <= 64): column-major blocks
+        with leading dimension n, on the device (torch CUDA tensor) or the host."""
+        if hasattr(V, "is_cuda"):
+            import torch
+            assert V.dim() == 2 and V.shape[1] == self.n
+            Vc = V.contiguous()
+            out = torch.empty_like(Vc)
+            _check(self.lib.prism_apply_batched_device(self.h, Vc.shape[0], _ptr(Vc), _ptr(out), self.n))
+            return out
+        import torch
+        return self.apply_batched(torch.from_numpy(np.ascontiguousarray(V, np.float64)).cuda()).cpu().numpy()
+
+    def solve_batched(self, B, X=None, *, solver=SOLVER_FCG, tol=1e-8, max_iter=1000) -> tuple:
+        """Solves A x_c = b_c for the k rows of B (shape (k, n), k <= 64) in one block
+        solve; returns (X, [SolveStats] * k).  Device tensors or host arrays."""
+        opts = SolveOpts(solver, tol, max_iter, 0)
+        if hasattr(B, "is_cuda"):
+            import torch
+            Bc = B.contiguous()
+            k = Bc.shape[0]
+            Xc = torch.zeros_like(Bc) if X is None else X.contiguous()
+            st = (SolveStats * k)()
+            _check(self.lib.prism_solve_batched_device(self.h, C.byref(opts), k, _ptr(Bc), _ptr(Xc), self.n, st))
+            return Xc, list(st)
+        Bh = np.ascontiguousarray(B, np.float64)
+        k = Bh.shape[0]
+        Xh = np.zeros_like(Bh) if X is None else np.array(X, np.float64, copy=True)
+        st = (SolveStats * k)()
+        _check(self.lib.prism_solve_batched(self.h, C.byref(opts), k, Bh.reshape(-1), Xh.reshape(-1), self.n, st))
+        return Xh, list(st)
+
     def solve(self, b, x=None, *, solver=SOLVER_FCG, tol=1e-8, max_iter=1000, restart=0) -> tuple:
         """x (in/out initial guess) solved in place; returns (x, SolveStats)."""
         opts = SolveOpts(solver, tol, max_iter, restart)

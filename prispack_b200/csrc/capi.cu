@@ -665,4 +665,150 @@ int32_t prism_solve(prism_handle h, const prism_solve_opts* opts, const double* 
     });
 }
 
+
+int32_t prism_update_values(prism_handle h, const double* val) {
+    if (!h) return fail(PRISM_ERR_ARG, "null handle");
+    if (!val) return fail(PRISM_ERR_ARG, "null values");
+    return guarded([&]() -> int {
+        DeviceGuard g(h->info.device);
+        const size_t nnz = h->A.nnz;
+        std::memcpy(h->A_host.val.data(), val, nnz * sizeof(double));
+        PRISM_CUDA(cudaMemcpyAsync(h->A.val.get(), val, nnz * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        PRISM_CUDA(cudaStreamSynchronize(h->stream));
+        h->symmetric = -1;
+        return PRISM_OK;
+    });
+}
+
+int32_t prism_update_values_device(prism_handle h, const double* val_d) {
+    if (!h) return fail(PRISM_ERR_ARG, "null handle");
+    if (!val_d) return fail(PRISM_ERR_ARG, "null values");
+    return guarded([&]() -> int {
+        DeviceGuard g(h->info.device);
+        const size_t nnz = h->A.nnz;
+        PRISM_CUDA(cudaMemcpyAsync(h->A.val.get(), val_d, nnz * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+        PRISM_CUDA(cudaMemcpyAsync(h->A_host.val.data(), val_d, nnz * sizeof(double), cudaMemcpyDeviceToHost,
+                                   h->stream));
+        PRISM_CUDA(cudaStreamSynchronize(h->stream));
+        h->symmetric = -1;
+        return PRISM_OK;
+    });
+}
+
+static void adjoint(prism::Handle& h, const prism_solve_opts& o, const double* g_d, const double* x_d,
+                    double* lambda_d, double* grad_d, prism_solve_stats* st) {
+    if (h.symmetric < 0) h.symmetric = prism::csr_symmetric(h.A_host) ? 1 : 0;
+    if (!h.symmetric)
+        throw prism::Error(PRISM_ERR_UNSUPPORTED, "adjoint solve needs A == A^T (a nonsymmetric A needs a "
+                                                  "transposed operator and preconditioner)");
+    // A^T = A: lambda = A^{-1} g with the handle's own solver and preconditioner, from zero
+    PRISM_CUDA(cudaMemsetAsync(lambda_d, 0, (size_t)h.A.n * sizeof(double), h.stream));
+    run_solver(h, o, g_d, lambda_d, st);
+    if (grad_d) prism::launch_adjoint_outer(h, h.stream, lambda_d, x_d, grad_d);
+    PRISM_CUDA(cudaStreamSynchronize(h.stream));
+}
+
+int32_t prism_adjoint_solve_device(prism_handle h, const prism_solve_opts* opts, const double* g_d, const double* x_d,
+                                   double* lambda_d, double* grad_val_d, prism_solve_stats* stats) {
+    int rc = check_opts(h, opts);
+    if (rc) return rc;
+    if (!g_d || !lambda_d) return fail(PRISM_ERR_ARG, "null vector");
+    if (grad_val_d && !x_d) return fail(PRISM_ERR_ARG, "the pattern gradient needs x");
+    return guarded([&]() -> int {
+        DeviceGuard g(h->info.device);
+        adjoint(*h, *opts, g_d, x_d, lambda_d, grad_val_d, stats);
+        return PRISM_OK;
+    });
+}
+
+int32_t prism_adjoint_solve(prism_handle h, const prism_solve_opts* opts, const double* g, const double* x,
+                            double* lambda, double* grad_val, prism_solve_stats* stats) {
+    int rc = check_opts(h, opts);
+    if (rc) return rc;
+    if (!g || !lambda) return fail(PRISM_ERR_ARG, "null vector");
+    if (grad_val && !x) return fail(PRISM_ERR_ARG, "the pattern gradient needs x");
+    return guarded([&]() -> int {
+        DeviceGuard gd(h->info.device);
+        const uint32_t n = h->A.n;
+        const size_t nnz = h->A.nnz;
+        prism::DevBuf<double> gd_(n), xd(n), ld(n), vd(grad_val ? nnz : 1);
+        PRISM_CUDA(cudaMemcpyAsync(gd_.get(), g, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        if (x) PRISM_CUDA(cudaMemcpyAsync(xd.get(), x, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        adjoint(*h, *opts, gd_.get(), xd.get(), ld.get(), grad_val ? vd.get() : nullptr, stats);
+        PRISM_CUDA(cudaMemcpyAsync(lambda, ld.get(), n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        if (grad_val)
+            PRISM_CUDA(cudaMemcpyAsync(grad_val, vd.get(), nnz * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        PRISM_CUDA(cudaStreamSynchronize(h->stream));
+        return PRISM_OK;
+    });
+}
+
+static int check_block(prism_handle h, uint32_t k, uint64_t ld) {
+    if (!h) return fail(PRISM_ERR_ARG, "null handle");
+    if (k == 0 || k > 64) return fail(PRISM_ERR_ARG, "block of right-hand sides: k must be in 1..64");
+    if (k > 1 && ld < h->A.n) return fail(PRISM_ERR_ARG, "leading dimension below n");
+    return PRISM_OK;
+}
+
+int32_t prism_apply_batched_device(prism_handle h, uint32_t k, const double* in_d, double* out_d, uint64_t ld) {
+    int rc = check_block(h, k, ld);
+    if (rc) return rc;
+    if (!in_d || !out_d) return fail(PRISM_ERR_ARG, "null block");
+    if (in_d == out_d) return fail(PRISM_ERR_ARG, "block apply needs distinct input and output");
+    return guarded([&]() -> int {
+        DeviceGuard g(h->info.device);
+        prism::batched_apply(*h, k, in_d, out_d, k > 1 ? ld : h->A.n);
+        PRISM_CUDA(cudaStreamSynchronize(h->stream));
+        return PRISM_OK;
+    });
+}
+
+static int check_block_solver(const prism_solve_opts* o) {
+    if (o->solver != PRISM_SOLVER_FCG && o->solver != PRISM_SOLVER_CG)
+        return fail(PRISM_ERR_UNSUPPORTED, "blocks of right-hand sides are solved with FCG / CG");
+    return PRISM_OK;
+}
+
+int32_t prism_solve_batched_device(prism_handle h, const prism_solve_opts* opts, uint32_t k, const double* B_d,
+                                   double* X_d, uint64_t ld, prism_solve_stats* stats) {
+    int rc = check_opts(h, opts);
+    if (!rc) rc = check_block(h, k, ld);
+    if (!rc) rc = check_block_solver(opts);
+    if (rc) return rc;
+    if (!B_d || !X_d) return fail(PRISM_ERR_ARG, "null block");
+    return guarded([&]() -> int {
+        DeviceGuard g(h->info.device);
+        prism::batched_fcg_solve(*h, *opts, k, B_d, X_d, k > 1 ? ld : h->A.n, stats);
+        return PRISM_OK;
+    });
+}
+
+int32_t prism_solve_batched(prism_handle h, const prism_solve_opts* opts, uint32_t k, const double* B, double* X,
+                            uint64_t ld, prism_solve_stats* stats) {
+    int rc = check_opts(h, opts);
+    if (!rc) rc = check_block(h, k, ld);
+    if (!rc) rc = check_block_solver(opts);
+    if (rc) return rc;
+    if (!B || !X) return fail(PRISM_ERR_ARG, "null block");
+    return guarded([&]() -> int {
+        DeviceGuard g(h->info.device);
+        const uint32_t n = h->A.n;
+        const uint64_t l = k > 1 ? ld : n;
+        prism::DevBuf<double> Bd((size_t)n * k), Xd((size_t)n * k);
+        // column c of the host block starts at c * l; copy the n used rows of each column
+        for (uint32_t c = 0; c < k; ++c) {
+            PRISM_CUDA(cudaMemcpyAsync(Bd.get() + (size_t)c * n, B + c * l, n * sizeof(double),
+                                       cudaMemcpyHostToDevice, h->stream));
+            PRISM_CUDA(cudaMemcpyAsync(Xd.get() + (size_t)c * n, X + c * l, n * sizeof(double),
+                                       cudaMemcpyHostToDevice, h->stream));
+        }
+        prism::batched_fcg_solve(*h, *opts, k, Bd.get(), Xd.get(), n, stats);
+        for (uint32_t c = 0; c < k; ++c)
+            PRISM_CUDA(cudaMemcpyAsync(X + c * l, Xd.get() + (size_t)c * n, n * sizeof(double),
+                                       cudaMemcpyDeviceToHost, h->stream));
+        PRISM_CUDA(cudaStreamSynchronize(h->stream));
+        return PRISM_OK;
+    });
+}
+
 }  // extern "C"

@@ -80,6 +80,20 @@ std::string validate_csr(uint32_t n, const uint32_t* rowptr, const uint32_t* col
     return std::string();
 }
 
+bool csr_symmetric(const CsrHost& A) {
+    for (uint32_t i = 0; i < A.n; ++i) {
+        for (uint32_t k = A.rowptr[i]; k < A.rowptr[i + 1]; ++k) {
+            const uint32_t j = A.col[k];
+            if (j <= i) continue;
+            const uint32_t* b = A.col.data() + A.rowptr[j];
+            const uint32_t* e = A.col.data() + A.rowptr[j + 1];
+            const uint32_t* f = std::lower_bound(b, e, i);
+            if (f == e || *f != i || A.val[f - A.col.data()] != A.val[k]) return false;
+        }
+    }
+    return true;
+}
+
 // ============================================================================
 // Threshold incomplete Cholesky (left-looking, column linked lists)
 // ============================================================================

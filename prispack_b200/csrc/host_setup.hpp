@@ -49,6 +49,8 @@ void laplacian_fill(int32_t nx, int32_t ny, int32_t nz, double ax, double ay, do
 // Structural validation of a caller CSR: monotone offsets, columns < n and
 // strictly increasing inside a row.  Returns an empty string when valid.
 std::string validate_csr(uint32_t n, const uint32_t* rowptr, const uint32_t* col);
+// true when A equals its transpose exactly (pattern and values); rows sorted
+bool csr_symmetric(const CsrHost& A);
 
 // ---- incomplete factorisations ---------------------------------------------
 // IncompleteCholesky<Low,double>::setup (source/Preconditioner/IncompleteCholesky.cpp:96-246):

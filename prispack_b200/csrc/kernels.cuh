@@ -316,9 +316,11 @@ static __global__ void __launch_bounds__(1024) k_sweep_slab(uint32_t n, uint32_t
     auto wait = [&](uint32_t c, unsigned long long& bits) {
         return spin_ready([&] { return load(c); }, bits, status, wait_ns);
     };
-    // Dependency values are not read ahead here: inside a slab most of them are
-    // produced by neighbouring positions and would still be pending.
-    auto later = [](uint32_t) { return kPending; };
+    // Dependencies inside the slab are produced by neighbouring positions and
+    // would still be pending when the row is read ahead, so they are polled
+    // (in shared memory) only when the row is reached; dependencies owned by
+    // other slabs, usually finished long before, are loaded ahead with the row.
+    auto later = [&](uint32_t c) { return (c - rb) < owned ? kPending : ld_relaxed_u64(out + c); };
     uint32_t p = p0 + wid;
     if (p >= p1) return;
     SweepRow cur, nxt;
@@ -528,6 +530,23 @@ static __global__ void __launch_bounds__(kBlock) k_lowrank_add(uint32_t n, uint3
         double s = 0.0;
         for (uint32_t c = 0; c < r; ++c) s += W[(size_t)c * n + j] * t[c];
         y[j] += s;
+    }
+}
+}  // namespace prism
+
+namespace prism {
+// ---------------------------------------------------------------------------
+// Adjoint of x = A^{-1} b on A's stored pattern: dL/dA_ij = -lambda_i x_j,
+// with lambda = A^{-T} dL/dx.  One thread per row, entries in stored order.
+// ---------------------------------------------------------------------------
+static __global__ void __launch_bounds__(kBlock) k_adjoint_outer(uint32_t n, const uint32_t* __restrict__ rowptr,
+                                                                 const uint32_t* __restrict__ col,
+                                                                 const double* __restrict__ lambda,
+                                                                 const double* __restrict__ x,
+                                                                 double* __restrict__ grad) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double li = -lambda[i];
+        for (uint32_t k = rowptr[i]; k < rowptr[i + 1]; ++k) grad[k] = li * x[col[k]];
     }
 }
 }  // namespace prism

@@ -1,4 +1,5 @@
 // Device-resident operator, triangular preconditioners and the FCG driver.
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -116,6 +117,11 @@ void launch_spmv(const Handle& h, cudaStream_t st, uint32_t nrows, const uint32_
     PRISM_LAUNCHED();
 }
 
+void launch_adjoint_outer(const Handle& h, cudaStream_t st, const double* lambda, const double* x, double* grad) {
+    k_adjoint_outer<<<vec_grid(h, h.A.n), kBlock, 0, st>>>(h.A.n, h.A.rowptr.get(), h.A.col.get(), lambda, x, grad);
+    PRISM_LAUNCHED();
+}
+
 // ============================================================================
 // Bounded-wait self test: a two-row sweep whose first position depends on the
 // second one, run by a single warp.  The warp reaches position 0 first, so the
@@ -188,6 +194,7 @@ void init_device_info(DeviceInfo& info, int device) {
         info.sweep_kernel = k == "global" ? 1 : (k == "slab" ? 2 : 0);
     }
     if (const char* e = std::getenv("PRISM_SLAB_MIN_ROWS")) info.slab_min_rows = (uint32_t)std::atoi(e);
+    if (const char* e = std::getenv("PRISM_SLAB_MAX_ROWS")) info.slab_max_rows = (uint32_t)std::atoi(e);
     if (info.slab_min_rows < 32) info.slab_min_rows = 32;
     // the slab kernel runs one 1024-thread CTA per SM with up to the whole opt-in shared memory
     for (bool f32 : {false, true})
@@ -252,9 +259,14 @@ void DevSweep::upload(const Sweep<Low>& s0, const DeviceInfo& info, bool slab_la
     std::vector<uint32_t> cpos;
     num_ctas = rows_per_cta = smem_rows = 0;
     if (slab_layout_wanted && n > 0) {
-        uint32_t ctas = (uint32_t)info.sms;
-        uint32_t want = (n + info.slab_min_rows - 1) / info.slab_min_rows;
-        if (want < ctas) ctas = want;
+        // As many rows per slab as shared memory holds: the dependencies of a
+        // row reach back about one grid plane, so large slabs keep most of them
+        // (and the critical path through them) inside one CTA, where a
+        // dependency costs a shared-memory poll instead of an L2 round trip.
+        const uint32_t cap = (uint32_t)(info.max_smem_optin / sizeof(double));
+        uint32_t per = std::max<uint32_t>(std::min<uint32_t>(cap, info.slab_max_rows), info.slab_min_rows);
+        uint32_t ctas = (n + per - 1) / per;
+        if (ctas > (uint32_t)info.sms) ctas = (uint32_t)info.sms;
         if (ctas < 1) ctas = 1;
         rows_per_cta = (n + ctas - 1) / ctas;
         num_ctas = (n + rows_per_cta - 1) / rows_per_cta;

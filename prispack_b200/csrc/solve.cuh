@@ -22,6 +22,7 @@ struct DeviceInfo {
     int max_smem_optin = 0;        // bytes of dynamic shared memory one block may opt into
     int sweep_kernel = 0;          // 0: autotune per sweep, 1: global level order, 2: slab-blocked
     uint32_t slab_min_rows = 2048; // smallest slab (small systems use fewer CTAs)
+    uint32_t slab_max_rows = 1u << 30;  // largest slab (default: what shared memory holds)
 };
 
 // Reduction scratch shared by all kernels of one stream (they run serially).
@@ -77,6 +78,11 @@ class Precond {
     // out = M^{-1} in; in != out not required.
     virtual void apply(cudaStream_t st, const double* in, double* out) = 0;
     virtual uint32_t levels(int sweep) const { (void)sweep; return 0; }
+    // OUT = M^{-1} IN for k <= 64 interleaved columns (X[row * k + c]); in != out.
+    virtual void apply_batched(cudaStream_t st, uint32_t k, const double* in, double* out) {
+        (void)st; (void)k; (void)in; (void)out;
+        throw Error(PRISM_ERR_UNSUPPORTED, "this preconditioner has no block apply");
+    }
     // one sweep alone (diagnostics / kernel timing); returns false if not a sweep-based preconditioner
     virtual bool run_sweep(cudaStream_t st, int sweep, const double* in, double* out, int prepare) {
         (void)st; (void)sweep; (void)in; (void)out; (void)prepare;
@@ -105,6 +111,7 @@ class TriangularPrecond : public Precond {
     int kind() const override { return f_->kind; }
     uint64_t mnnz() const override { return f_->mnnz; }
     void apply(cudaStream_t st, const double* in, double* out) override;
+    void apply_batched(cudaStream_t st, uint32_t k, const double* in, double* out) override;
     uint32_t levels(int sweep) const override { return sweep == 0 ? lower_.num_levels : upper_.num_levels; }
     int export_factor(int which, uint32_t* n, uint64_t* nnz, uint32_t* rowptr, uint32_t* col, double* val,
                       double* diag) const override;
@@ -116,7 +123,8 @@ class TriangularPrecond : public Precond {
     Handle& h_;
     std::shared_ptr<const HostFactor> f_;
     DevSweep lower_, upper_;
-    DevBuf<double> tmp_;
+    DevSweep lower_lv_, upper_lv_;   // level-order copies for the block sweeps when the tuner chose slabs
+    DevBuf<double> tmp_, tmpk_;
 };
 
 // Factor export shared by the device preconditioner and the host-only factor object.
@@ -165,6 +173,9 @@ class AmsedPrecond : public Precond {
     std::vector<Level> lv_;
 };
 
+struct BatchWork;                  // block-of-RHS workspace (batched.cu)
+void batch_release(BatchWork* w);
+
 struct Handle {
     DeviceInfo info;
     cudaStream_t stream = nullptr;
@@ -181,6 +192,8 @@ struct Handle {
     static constexpr uint32_t kMaxKrylov = 1024;  // restart length limit
     static constexpr uint32_t kScalarCapacity = kNumScalars + kMaxKrylov + 2;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::unique_ptr<BatchWork, void (*)(BatchWork*)> batch{nullptr, batch_release};
+    int symmetric = -1;            // A == A^T exactly: -1 not yet checked, 0 no, 1 yes
 
     ~Handle();
     void spmv(const double* x, double* y, int ndot = 0, const double* z = nullptr, const double* q = nullptr,
@@ -201,6 +214,9 @@ void launch_spmv(const Handle& h, cudaStream_t st, uint32_t nrows, const uint32_
 template <typename Low>
 void tune_sweep(Handle& h, DevSweep& d, const Sweep<Low>& s);
 
+// grad[k] = -lambda[row(k)] * x[col(k)] over A's stored entries
+void launch_adjoint_outer(const Handle& h, cudaStream_t st, const double* lambda, const double* x, double* grad);
+
 // Runs the bounded-wait self test (see solve.cu); returns the device status the wait raised.
 int selftest_wait_timeout(int device, unsigned long long wait_ns, int* device_status);
 
@@ -209,5 +225,9 @@ void init_device_info(DeviceInfo& info, int device);
 
 void fcg_solve(Handle& h, const prism_solve_opts& o, const double* b, double* x, prism_solve_stats* st);
 void gmres_solve(Handle& h, const prism_solve_opts& o, const double* b, double* x, prism_solve_stats* st);
+// blocks of k <= 64 right-hand sides, column-major with leading dimension ld (batched.cu)
+void batched_apply(Handle& h, uint32_t k, const double* in_d, double* out_d, uint64_t ld);
+void batched_fcg_solve(Handle& h, const prism_solve_opts& o, uint32_t k, const double* B_d, double* X_d, uint64_t ld,
+                       prism_solve_stats* st);
 
 }  // namespace prism
