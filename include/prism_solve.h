@@ -113,6 +113,28 @@ uint64_t prism_kernel_launch_count(void);
  * counterpart (the reference has no device-side waits). */
 int32_t prism_selftest_wait_timeout(int32_t device, uint64_t wait_ns, int32_t* device_status);
 
+/* True residual norms of k right-hand sides without any allocation.  No
+ * counterpart in the reference (its solvers only report the recursive
+ * residual, source/Solver/CG.cpp:58).  For callers that cannot let a library
+ * call cudaMalloc/cudaFree: a framework whose pool allocator owns the device
+ * memory, a process at the edge of device memory, or a loop on a
+ * latency-sensitive stream that a cudaMalloc/cudaFree synchronization would
+ * stall.  Computes, for c < k,
+ *   norms_d[2c]   = || b_c - A x_c ||_2,   norms_d[2c+1] = || b_c ||_2,
+ * with A given as device CSR arrays (rowptr_d[n+1], col_d[nnz], val_d[nnz])
+ * and x, b as k column-major columns of leading dimension ld (ignored for
+ * k = 1).  All pointers are caller-owned device memory on `device`; the
+ * kernel is queued on `stream` (a cudaStream_t, NULL = legacy default) and the
+ * call returns without synchronizing.  Scratch is a fixed 151,808-byte
+ * __device__ array per device, so 1 <= k <= 16; larger k is rejected with
+ * PRISM_ERR_ARG.  Calls that may overlap on the same device (unordered
+ * streams, other threads) race on that scratch: order them.  The first call
+ * on a device sets up the scratch address; make it before any stream capture
+ * begins.  On success nothing is allocated. */
+int32_t prism_residual_norms_noalloc(int32_t device, uint32_t n, const uint32_t* rowptr_d, const uint32_t* col_d,
+                                     const double* val_d, const double* x_d, const double* b_d, uint32_t k,
+                                     uint64_t ld, double* norms_d, void* stream);
+
 /* ---- model problems (host) --------------------------------------------- */
 /* sizes of generateLaplacianCSR(nx,ny,nz,...): n = nx*ny*nz, nnz exact */
 int32_t prism_laplacian_dims(int32_t nx, int32_t ny, int32_t nz, uint32_t* n, uint32_t* nnz);

@@ -116,6 +116,8 @@ _SIGS = {
                                               C.POINTER(_vp)]),
     "prism_gmslr_block": (C.c_int32, [_vp, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_uint32),
                                       C.POINTER(C.c_uint64), _vp, _vp, _vp, _vp]),
+    "prism_residual_norms_noalloc": (C.c_int32, [C.c_int32, C.c_uint32, _vp, _vp, _vp, _vp, _vp, C.c_uint32,
+                                                 C.c_uint64, _vp, _vp]),
     "prism_apply_batched_device": (C.c_int32, [_vp, C.c_uint32, _vp, _vp, C.c_uint64]),
     "prism_solve_batched_device": (C.c_int32, [_vp, C.POINTER(SolveOpts), C.c_uint32, _vp, _vp, C.c_uint64,
                                                C.POINTER(SolveStats)]),

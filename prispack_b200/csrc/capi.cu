@@ -45,6 +45,14 @@ struct DeviceGuard {
 };
 }  // namespace
 
+namespace prism {
+int record_error(int status, const char* msg) {
+    if (status == PRISM_OK) g_last_error.clear();
+    else g_last_error = msg;
+    return status;
+}
+}  // namespace prism
+
 struct prism_handle_s : Handle {};
 
 struct prism_factor_s {
