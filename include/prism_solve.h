@@ -113,6 +113,20 @@ uint64_t prism_kernel_launch_count(void);
  * counterpart (the reference has no device-side waits). */
 int32_t prism_selftest_wait_timeout(int32_t device, uint64_t wait_ns, int32_t* device_status);
 
+/* Host self test of the streamed round layout of the triangular sweep kernel:
+ * builds the sweep of the gather-form CSR (row r lists its dependencies and
+ * coefficients; lower != 0: dependencies precede the row, else follow it),
+ * with diag (may be null for op 2), op = 0: (in - s)/d, 1: (in - s)*d,
+ * 2: in - s, 3: in/d - s, factor values in `precision`, cuts it into
+ * num_ctas slabs of rows_per_cta rows (rows_per_cta = 0: the slab boundaries
+ * the device layout chooses), and replays the kernel's decoding of every
+ * record on the host into out.  PRISM_ERR_ARG with the reason when the
+ * layout is inconsistent.  No reference counterpart (the reference solves
+ * sequentially, IncompleteLDLT.cpp:188-233). */
+int32_t prism_selftest_stream_layout(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val,
+                                     const double* diag, int32_t op, int32_t lower, int32_t precision,
+                                     uint32_t num_ctas, uint32_t rows_per_cta, const double* in, double* out);
+
 /* True residual norms of k right-hand sides without any allocation.  No
  * counterpart in the reference (its solvers only report the recursive
  * residual, source/Solver/CG.cpp:58).  For callers that cannot let a library

@@ -70,6 +70,8 @@ _SIGS = {
     "prism_version": (C.c_int32, []),
     "prism_kernel_launch_count": (C.c_uint64, []),
     "prism_selftest_wait_timeout": (C.c_int32, [C.c_int32, C.c_uint64, C.POINTER(C.c_int32)]),
+    "prism_selftest_stream_layout": (C.c_int32, [C.c_uint32, _u32p, _u32p, _f64p, _vp, C.c_int32, C.c_int32,
+                                                 C.c_int32, C.c_uint32, C.c_uint32, _f64p, _f64p]),
     "prism_laplacian_dims": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     "prism_laplacian_fill": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
                                          C.c_double, _u32p, _u32p, _f64p]),
@@ -167,6 +169,23 @@ def selftest_wait_timeout(device: int = 0, wait_ns: int = 50_000_000) -> int:
     st = C.c_int32(-1)
     _check(load().prism_selftest_wait_timeout(device, wait_ns, C.byref(st)))
     return st.value
+
+
+def selftest_stream_layout(rowptr, col, val, in_, *, diag=None, op: int = 2, lower: bool = True,
+                           precision: int = 0, num_ctas: int = 4, rows_per_cta: int | None = None):
+    """Host replay of the streamed round layout of the sweep kernel (no GPU): returns the
+    sweep's solution as the kernel would compute it, or raises PrismError naming the flaw.
+    rows_per_cta = 0 lets the layout choose the slab boundaries."""
+    rp = np.ascontiguousarray(rowptr, np.uint32)
+    n = len(rp) - 1
+    rpc = rows_per_cta if rows_per_cta is not None else -(-n // num_ctas)
+    out = np.zeros(n)
+    d = np.ascontiguousarray(diag, np.float64) if diag is not None else None
+    _check(load().prism_selftest_stream_layout(n, rp, np.ascontiguousarray(col, np.uint32),
+                                               np.ascontiguousarray(val, np.float64),
+                                               d.ctypes.data if d is not None else None, op, int(lower), precision,
+                                               num_ctas, rpc, np.ascontiguousarray(in_, np.float64), out))
+    return out
 
 
 def _ptr(t) -> int:
@@ -472,7 +491,7 @@ class DeviceSystem:
         _check(self.lib.prism_precond_sweep_info(self.h, sweep, C.byref(n), C.byref(nnz), C.byref(vb), C.byref(lv),
                                                  C.byref(kk)))
         return {"n": n.value, "nnz": nnz.value, "value_bytes": vb.value, "levels": lv.value,
-                "kernel": {1: "level-order", 2: "slab"}.get(kk.value, "?")}
+                "kernel": {1: "level-order", 2: "slab", 3: "stream"}.get(kk.value, "?")}
 
     def apply(self, vec):
         """out = M^{-1} vec (MInvSolve(vecIN, vecOUT))."""

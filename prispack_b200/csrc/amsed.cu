@@ -169,10 +169,10 @@ void AmsedPrecond::block_solve(cudaStream_t st, int level, const double* in, dou
     if (L.nfac < L.nb && in != out)  // rows without a factor (last level beyond block 0) pass through
         PRISM_CUDA(cudaMemcpyAsync(out + L.nfac, in + L.nfac, (L.nb - L.nfac) * sizeof(double),
                                    cudaMemcpyDeviceToDevice, st));
-    launch_fill(st, h_, L.nfac, sweep_tmp_.get());
-    if (in != out) launch_fill(st, h_, L.nfac, out);
+    if (!L.lower.self_filling()) launch_fill(st, h_, L.nfac, sweep_tmp_.get());
+    if (in != out && !L.upper.self_filling()) launch_fill(st, h_, L.nfac, out);
     launch_sweep(h_, st, L.lower, in, sweep_tmp_.get());
-    if (in == out) launch_fill(st, h_, L.nfac, out);
+    if (in == out && !L.upper.self_filling()) launch_fill(st, h_, L.nfac, out);
     launch_sweep(h_, st, L.upper, sweep_tmp_.get(), out);
 }
 
@@ -229,8 +229,8 @@ bool AmsedPrecond::run_sweep(cudaStream_t st, int sweep, const double* in, doubl
     if (sweep < 0 || sweep >= (int)(2 * nlev_)) return false;
     const Level& L = lv_[sweep / 2];
     const DevSweep& s = (sweep & 1) ? L.upper : L.lower;
-    if (prepare != 0) launch_fill(st, h_, s.n, out);
-    if (prepare != 2) launch_sweep(h_, st, s, in, out);
+    if (prepare != 0) launch_sweep_prepare(h_, st, s, in, out);
+    if (prepare != 2) launch_sweep_kernel(h_, st, s, in, out);
     return true;
 }
 
@@ -240,10 +240,10 @@ bool AmsedPrecond::sweep_info(int sweep, uint32_t* n, uint64_t* nnz, uint32_t* v
     const Level& L = lv_[sweep / 2];
     const DevSweep& s = (sweep & 1) ? L.upper : L.lower;
     if (n) *n = s.n;
-    if (nnz) *nnz = s.fp32 ? s.val32.size() : s.val64.size();
+    if (nnz) *nnz = s.entries();
     if (vbytes) *vbytes = s.fp32 ? 4 : 8;
     if (levels) *levels = s.num_levels;
-    if (kernel) *kernel = s.num_ctas > 0 ? 2 : 1;
+    if (kernel) *kernel = s.layout == LAYOUT_STREAM ? 3 : (s.layout == LAYOUT_SLAB ? 2 : 1);
     return true;
 }
 

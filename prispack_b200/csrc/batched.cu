@@ -444,7 +444,7 @@ void launch_bt_fill(cudaStream_t st, const Handle& h, uint64_t count, double* p)
 
 void launch_bt_sweep(const Handle& h, cudaStream_t st, const DevSweep& s, uint32_t k, const double* in, double* out) {
     if (!s.n) return;
-    if (s.num_ctas > 0) throw Error(PRISM_ERR_ARG, "block sweep needs the level-order layout");
+    if (s.layout != LAYOUT_LEVEL) throw Error(PRISM_ERR_ARG, "block sweep needs the level-order layout");
     void* fn = s.fp32 ? bt_sweep_kernel<float>(s.op) : bt_sweep_kernel<double>(s.op);
     int occ = 0;
     PRISM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kBlock, 0));
@@ -490,10 +490,10 @@ void launch_bt_unpack(cudaStream_t st, const Handle& h, uint32_t n, uint32_t k, 
 void TriangularPrecond::apply_batched(cudaStream_t st, uint32_t k, const double* in, double* out) {
     const uint32_t n = h_.A.n;
     auto level_order = [&](const DevSweep& tuned, DevSweep& mine, bool lower) -> const DevSweep& {
-        if (tuned.num_ctas == 0) return tuned;
+        if (tuned.layout == LAYOUT_LEVEL) return tuned;
         if (mine.n != tuned.n) {
-            if (f_->fp32) mine.upload(lower ? f_->lower32 : f_->upper32, h_.info, false, h_.stream);
-            else mine.upload(lower ? f_->lower64 : f_->upper64, h_.info, false, h_.stream);
+            if (f_->fp32) mine.upload(lower ? f_->lower32 : f_->upper32, h_.info, LAYOUT_LEVEL, h_.stream);
+            else mine.upload(lower ? f_->lower64 : f_->upper64, h_.info, LAYOUT_LEVEL, h_.stream);
         }
         return mine;
     };

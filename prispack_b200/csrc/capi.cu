@@ -106,6 +106,35 @@ static int32_t set_tri(prism_handle h, int kind, double tol, uint32_t lfill, int
     });
 }
 
+template <typename Low>
+static int stream_selftest(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val,
+                           const double* diag, int op, bool lower, uint32_t num_ctas, uint32_t rows_per_cta,
+                           const double* in, double* out) {
+    const uint64_t nnz = rowptr[n];
+    std::vector<uint32_t> rp(rowptr, rowptr + n + 1), ci(col, col + nnz);
+    std::vector<Low> v(nnz);
+    for (uint64_t k = 0; k < nnz; ++k) v[k] = (Low)val[k];
+    std::vector<double> d;
+    if (diag) d.assign(diag, diag + n);
+    prism::Sweep<Low> s;
+    prism::build_sweep<Low>(n, rp, ci, v, diag ? &d : nullptr, op, lower, s);
+    // rows_per_cta = 0: the slab boundaries the device layout would choose
+    std::vector<uint32_t> start;
+    if (rows_per_cta == 0) {
+        start = prism::slab_ranges<Low>(s, num_ctas);
+    } else {
+        if ((uint64_t)num_ctas * rows_per_cta < n) return fail(PRISM_ERR_UNSUPPORTED, "slabs do not cover the rows");
+        for (uint32_t b = 0; b <= num_ctas; ++b)
+            start.push_back((uint32_t)std::min<uint64_t>((uint64_t)b * rows_per_cta, n));
+    }
+    prism::StreamLayout L;
+    std::string why;
+    if (!prism::stream_layout<Low>(s, start, prism::kNoSlot, L, &why)) return fail(PRISM_ERR_UNSUPPORTED, why);
+    why = prism::stream_layout_replay<Low>(s, L, in, out);
+    if (!why.empty()) return fail(PRISM_ERR_ARG, "stream layout: " + why);
+    return PRISM_OK;
+}
+
 extern "C" {
 
 const char* prism_last_error(void) { return g_last_error.c_str(); }
@@ -123,6 +152,22 @@ int32_t prism_selftest_wait_timeout(int32_t device, uint64_t wait_ns, int32_t* d
         prism::selftest_wait_timeout(device, wait_ns, &s);
         *device_status = s;
         return PRISM_OK;
+    });
+}
+
+int32_t prism_selftest_stream_layout(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val,
+                                     const double* diag, int32_t op, int32_t lower, int32_t precision,
+                                     uint32_t num_ctas, uint32_t rows_per_cta, const double* in, double* out) {
+    if (!rowptr || !col || !val || !in || !out) return fail(PRISM_ERR_ARG, "null array");
+    if (op < 0 || op > 3 || (op != 2 && !diag)) return fail(PRISM_ERR_ARG, "bad op / missing diagonal");
+    return guarded([&]() -> int {
+        for (uint32_t r = 0; r < n; ++r)
+            for (uint32_t k = rowptr[r]; k < rowptr[r + 1]; ++k)
+                if (col[k] >= n || (lower ? col[k] >= r : col[k] <= r))
+                    return fail(PRISM_ERR_ARG, "dependency on the wrong side of the diagonal");
+        if (precision == PRISM_FP32)
+            return stream_selftest<float>(n, rowptr, col, val, diag, op, lower != 0, num_ctas, rows_per_cta, in, out);
+        return stream_selftest<double>(n, rowptr, col, val, diag, op, lower != 0, num_ctas, rows_per_cta, in, out);
     });
 }
 

@@ -440,20 +440,20 @@ void build_sweep(uint32_t n, const std::vector<uint32_t>& rowptr, const std::vec
 }
 
 template <typename Low>
-void slab_layout(const Sweep<Low>& s, uint32_t num_ctas, uint32_t rows_per_cta, std::vector<uint32_t>& cta_pos,
-                 Sweep<Low>& out) {
+void slab_layout_ranges(const Sweep<Low>& s, const std::vector<uint32_t>& start, std::vector<uint32_t>& cta_pos,
+                        Sweep<Low>& out) {
     const uint32_t n = s.n;
+    const uint32_t num_ctas = (uint32_t)start.size() - 1;
+    std::vector<uint32_t> owner(n);
+    for (uint32_t b = 0; b < num_ctas; ++b)
+        for (uint32_t r = start[b]; r < start[b + 1]; ++r) owner[r] = b;
     cta_pos.assign((size_t)num_ctas + 1, 0);
-    for (uint32_t r = 0; r < n; ++r) cta_pos[std::min<uint32_t>(r / rows_per_cta, num_ctas - 1) + 1]++;
+    for (uint32_t r = 0; r < n; ++r) cta_pos[owner[r] + 1]++;
     for (uint32_t b = 0; b < num_ctas; ++b) cta_pos[b + 1] += cta_pos[b];
     // the global (level, row) order, bucketed by owning CTA, stays (level, row) ordered per CTA
     std::vector<uint32_t> fill(cta_pos.begin(), cta_pos.end() - 1);
     std::vector<uint32_t> newpos_of_old(n);
-    for (uint32_t p = 0; p < n; ++p) {
-        const uint32_t r = s.order[p];
-        const uint32_t b = std::min<uint32_t>(r / rows_per_cta, num_ctas - 1);
-        newpos_of_old[p] = fill[b]++;
-    }
+    for (uint32_t p = 0; p < n; ++p) newpos_of_old[p] = fill[owner[s.order[p]]]++;
     out.n = n;
     out.op = s.op;
     out.lower = s.lower;
@@ -478,6 +478,76 @@ void slab_layout(const Sweep<Low>& s, uint32_t num_ctas, uint32_t rows_per_cta, 
         std::copy(s.col.begin() + s.rowptr[p], s.col.begin() + s.rowptr[p + 1], out.col.begin() + out.rowptr[q]);
         std::copy(s.val.begin() + s.rowptr[p], s.val.begin() + s.rowptr[p + 1], out.val.begin() + out.rowptr[q]);
     }
+}
+
+template <typename Low>
+void slab_layout(const Sweep<Low>& s, uint32_t num_ctas, uint32_t rows_per_cta, std::vector<uint32_t>& cta_pos,
+                 Sweep<Low>& out) {
+    std::vector<uint32_t> start((size_t)num_ctas + 1);
+    for (uint32_t b = 0; b <= num_ctas; ++b) start[b] = (uint32_t)std::min<uint64_t>((uint64_t)b * rows_per_cta, s.n);
+    start[num_ctas] = s.n;
+    slab_layout_ranges<Low>(s, start, cta_pos, out);
+}
+
+template <typename Low>
+std::vector<uint32_t> slab_ranges(const Sweep<Low>& s, uint32_t num_ctas) {
+    const uint32_t n = s.n;
+    // cut points: row boundaries that no dependency crosses (independent blocks of a
+    // block-diagonal factor, e.g. the subdomains of an AMSED level)
+    std::vector<uint32_t> reach(n);  // per row: farthest dependency (lowest for a lower sweep)
+    for (uint32_t p = 0; p < n; ++p) {
+        const uint32_t r = s.order[p];
+        uint32_t m = r;
+        for (uint32_t k = s.rowptr[p]; k < s.rowptr[p + 1]; ++k)
+            m = s.lower ? std::min(m, s.col[k]) : std::max(m, s.col[k]);
+        reach[r] = m;
+    }
+    std::vector<uint32_t> cuts{0};
+    if (s.lower) {
+        std::vector<uint32_t> suf((size_t)n + 1, n);
+        for (uint32_t r = n; r-- > 0;) suf[r] = std::min(suf[r + 1], reach[r]);
+        for (uint32_t b = 1; b < n; ++b)
+            if (suf[b] >= b) cuts.push_back(b);
+    } else {
+        uint32_t pre = 0;
+        for (uint32_t b = 1; b < n; ++b) {
+            pre = std::max(pre, reach[b - 1]);
+            if (pre < b) cuts.push_back(b);
+        }
+    }
+    cuts.push_back(n);
+    // segments of at least half a slab; smaller pieces join their neighbour
+    const uint64_t target = ((uint64_t)n + num_ctas - 1) / num_ctas;
+    std::vector<uint32_t> seg{0};
+    for (size_t i = 1; i + 1 < cuts.size(); ++i)
+        if (cuts[i] - seg.back() >= target / 2 && n - cuts[i] >= target / 2) seg.push_back(cuts[i]);
+    seg.push_back(n);
+    // CTAs per segment in proportion to its rows (at least one each), then even splits
+    const uint32_t nseg = (uint32_t)seg.size() - 1;
+    std::vector<uint32_t> k(nseg, 1);
+    uint32_t used = nseg;
+    while (used < num_ctas) {
+        uint32_t best = 0;
+        double worst = -1.0;
+        for (uint32_t i = 0; i < nseg; ++i) {
+            const double per = (double)(seg[i + 1] - seg[i]) / k[i];
+            if (per > worst) {
+                worst = per;
+                best = i;
+            }
+        }
+        ++k[best];
+        ++used;
+    }
+    std::vector<uint32_t> start{0};
+    for (uint32_t i = 0; i < nseg; ++i) {
+        const uint64_t len = seg[i + 1] - seg[i];
+        for (uint32_t j = 1; j <= k[i]; ++j) start.push_back(seg[i] + (uint32_t)(len * j / k[i]));
+    }
+    std::vector<uint32_t> out{0};  // empty slabs dropped
+    for (size_t i = 1; i < start.size(); ++i)
+        if (start[i] > out.back()) out.push_back(start[i]);
+    return out;
 }
 
 // ============================================================================
@@ -599,6 +669,303 @@ int build_triangular(int kind, const CsrHost& A, double tol, uint32_t lfill, boo
     return build_tri_t<double>(kind, A, tol, lfill, out, out.lower64, out.upper64, err);
 }
 
+template <typename Low>
+bool stream_layout(const Sweep<Low>& s, const std::vector<uint32_t>& start, uint32_t max_slots, StreamLayout& out,
+                   std::string* why) {
+    auto fail = [&](const std::string& m) {
+        if (why) *why = m;
+        return false;
+    };
+    const uint32_t n = s.n;
+    if (n == 0 || start.size() < 2) return fail("empty sweep");
+    const uint32_t num_ctas = (uint32_t)start.size() - 1;
+    if (start[0] != 0 || start[num_ctas] != n) return fail("slabs do not cover the rows");
+    for (uint32_t b = 0; b < num_ctas; ++b) {
+        if (start[b + 1] <= start[b]) return fail("a slab without rows");
+        if (start[b + 1] - start[b] > 0xFFFFu) return fail("slab larger than 65535 rows");
+    }
+    if (max_slots > kNoSlot) max_slots = kNoSlot;
+    Sweep<Low> sl;
+    std::vector<uint32_t> cpos;
+    slab_layout_ranges<Low>(s, start, cpos, sl);
+    const uint32_t vb = (uint32_t)sizeof(Low);
+    const bool recip = s.op == SWEEP_DIV || s.op == SWEEP_PREDIV;
+    out = StreamLayout();
+    out.num_ctas = num_ctas;
+    out.slab_start = start;
+    out.cta_pos = cpos;
+    out.cta_round.assign((size_t)num_ctas + 1, 0);
+    out.in_slot.assign(n, 0);
+
+    struct Round {
+        uint32_t p0, p1, L;
+        std::vector<uint32_t> xrow, xslot, xwait;
+    };
+    constexpr uint32_t kNone = 0xFFFFFFFFu;
+    std::vector<uint32_t> round_of(n, kNone);   // by row: round of the slab being laid out
+    std::vector<uint32_t> seen(n, kNone);       // by row: slab that last read it ...
+    std::vector<int64_t> last_use(n, -1);       // ... and the last round of that slab reading it
+    std::vector<uint32_t> slot_of(n, kNoSlot);  // by row: its value slot in the slab being laid out
+    std::vector<uint32_t> slot_in(n, kNone);    // by row: slab that slot_of refers to
+    for (uint32_t b = 0; b < num_ctas; ++b) {
+        const uint32_t rb = start[b], re = start[b + 1];
+        const uint32_t P0 = cpos[b], P1 = cpos[b + 1];
+        std::vector<Round> R;
+        // 1. rounds: consecutive positions, at most kRoundRows, no dependency inside a round.
+        // A dependency has a lower level, hence an earlier position, so its round is known.
+        for (uint32_t p = P0; p < P1;) {
+            Round rd;
+            rd.p0 = p;
+            const uint32_t id = (uint32_t)R.size();
+            while (p < P1 && p - rd.p0 < kRoundRows) {
+                bool clash = false;
+                for (uint32_t k = sl.rowptr[p]; k < sl.rowptr[p + 1] && !clash; ++k) {
+                    const uint32_t d = sl.col[k];
+                    clash = d >= rb && d < re && round_of[d] == id;
+                }
+                if (clash) break;
+                round_of[sl.order[p]] = id;
+                ++p;
+            }
+            rd.p1 = p;
+            rd.L = 0;
+            for (uint32_t q = rd.p0; q < rd.p1; ++q) rd.L = std::max(rd.L, sl.rowptr[q + 1] - sl.rowptr[q]);
+            if (rd.L > 0xFFFFu) return fail("a row with more than 65535 entries");
+            R.push_back(std::move(rd));
+        }
+        if (R.size() >= 0xFFFFu) return fail("more than 65534 rounds in a slab");
+        // 2. last reading round of every value the slab reads (its own rows and halo rows)
+        for (uint32_t r = 0; r < R.size(); ++r)
+            for (uint32_t p = R[r].p0; p < R[r].p1; ++p)
+                for (uint32_t k = sl.rowptr[p]; k < sl.rowptr[p + 1]; ++k) {
+                    const uint32_t d = sl.col[k];
+                    if (seen[d] != b) {
+                        seen[d] = b;
+                        last_use[d] = -1;
+                    }
+                    last_use[d] = std::max<int64_t>(last_use[d], r);
+                }
+        // 3. slots: a value occupies its slot from the round that writes it (its own round for a
+        // slab row, its first reading round for a halo row) through its last reading round.  A
+        // slot released after round r takes a row result of round r + 1 or later; a halo value
+        // only from round r + 2 on, because the kernel copies round r + 2's halo in while round
+        // r + 1 computes, when only rounds up to r are known to be done.  Oldest first.
+        std::vector<uint32_t> free_q;
+        size_t free_head = 0;
+        std::vector<int64_t> slot_last{INT64_MAX};  // last reading round of the slot's value; slot 0 holds 0.0
+        std::vector<std::vector<uint32_t>> release(R.size());
+        auto take = [&](int64_t last, uint32_t& slot, uint32_t& wait, int64_t free_by) -> bool {
+            if (free_head < free_q.size() && slot_last[free_q[free_head]] <= free_by) {
+                slot = free_q[free_head++];
+            } else {
+                if (slot_last.size() >= max_slots) return false;
+                slot = (uint32_t)slot_last.size();
+                slot_last.push_back(-1);
+            }
+            wait = (uint32_t)(slot_last[slot] + 1);  // rounds to finish before the slot is overwritten
+            slot_last[slot] = last;
+            release[(size_t)last].push_back(slot);
+            return true;
+        };
+        for (uint32_t r = 0; r < R.size(); ++r) {
+            if (r > 0)
+                for (uint32_t q : release[r - 1]) free_q.push_back(q);
+            // halo rows first read in round r: copied in by a prefetcher
+            for (uint32_t p = R[r].p0; p < R[r].p1; ++p)
+                for (uint32_t k = sl.rowptr[p]; k < sl.rowptr[p + 1]; ++k) {
+                    const uint32_t d = sl.col[k];
+                    if ((d >= rb && d < re) || slot_in[d] == b) continue;
+                    uint32_t slot, wait;
+                    if (!take(last_use[d], slot, wait, (int64_t)r - 2))
+                        return fail("more value slots than shared memory holds");
+                    if (wait > (r > 0 ? r - 1 : 0)) return fail("a prefetch would wait on its own or a later round");
+                    slot_of[d] = slot;
+                    slot_in[d] = b;
+                    R[r].xrow.push_back(d);
+                    R[r].xslot.push_back(slot);
+                    R[r].xwait.push_back(wait);
+                }
+            // rows of round r read later in the slab: their results go to a slot
+            for (uint32_t p = R[r].p0; p < R[r].p1; ++p) {
+                const uint32_t row = sl.order[p];
+                if (seen[row] == b && last_use[row] > (int64_t)r) {
+                    uint32_t slot, wait;
+                    if (!take(last_use[row], slot, wait, (int64_t)r - 1))
+                        return fail("more value slots than shared memory holds");
+                    if (wait > r) return fail("a slot reused inside its round");
+                    slot_of[row] = slot;
+                    slot_in[row] = b;
+                }
+            }
+        }
+        out.slots = std::max<uint32_t>(out.slots, (uint32_t)slot_last.size());
+        out.cta_round[b + 1] = out.cta_round[b] + (uint32_t)R.size();
+        out.max_rounds_per_cta = std::max<uint32_t>(out.max_rounds_per_cta, (uint32_t)R.size());
+        // 4. records of this slab's rounds
+        for (uint32_t r = 0; r < R.size(); ++r) {
+            const Round& rd = R[r];
+            const uint32_t nr = rd.p1 - rd.p0, X = (uint32_t)rd.xrow.size();
+            const RoundRec rec = round_rec(nr, rd.L, X, vb);
+            const uint64_t off = out.blob.size();
+            if ((off + rec.bytes) / 8 > 0xFFFFFFFFull) return fail("blob beyond 32 GB");
+            out.blob.resize(off + rec.bytes, 0);
+            uint8_t* base = out.blob.data() + off;
+            double* diag = reinterpret_cast<double*>(base + rec.diag);
+            uint16_t* lrow = reinterpret_cast<uint16_t*>(base + rec.lrow);
+            uint16_t* oslot = reinterpret_cast<uint16_t*>(base + rec.oslot);
+            uint16_t* col = reinterpret_cast<uint16_t*>(base + rec.col);
+            Low* val = reinterpret_cast<Low*>(base + rec.val);
+            uint32_t* xrow = reinterpret_cast<uint32_t*>(base + rec.xrow);
+            uint16_t* xslot = reinterpret_cast<uint16_t*>(base + rec.xslot);
+            uint16_t* xwait = reinterpret_cast<uint16_t*>(base + rec.xwait);
+            for (uint32_t p = rd.p0; p < rd.p1; ++p) {
+                const uint32_t j = p - rd.p0, row = sl.order[p];
+                diag[j] = recip ? 1.0 / sl.diag[p] : sl.diag[p];  // divisions become products
+                lrow[j] = (uint16_t)(row - rb);
+                oslot[j] = (uint16_t)(slot_in[row] == b && seen[row] == b && last_use[row] > (int64_t)r
+                                          ? slot_of[row] : kNoSlot);
+                out.in_slot[row] = (uint32_t)((off + rec.in) / 8 + j);
+                for (uint32_t k = sl.rowptr[p]; k < sl.rowptr[p + 1]; ++k) {
+                    const uint32_t d = sl.col[k], e = (k - sl.rowptr[p]) * rec.m + j;
+                    if (slot_in[d] != b || slot_of[d] == 0) return fail("a dependency without a value slot");
+                    col[e] = (uint16_t)slot_of[d];
+                    val[e] = sl.val[k];
+                }
+            }
+            for (uint32_t x = 0; x < X; ++x) {
+                xrow[x] = rd.xrow[x];
+                xslot[x] = (uint16_t)rd.xslot[x];
+                xwait[x] = (uint16_t)rd.xwait[x];
+            }
+            out.meta.push_back((uint32_t)(off / 16));
+            out.meta.push_back(rec.bytes);
+            out.meta.push_back(nr | (rd.L << 16));
+            out.meta.push_back(X);
+            out.max_round_bytes = std::max(out.max_round_bytes, rec.bytes);
+        }
+    }
+    out.num_rounds = out.cta_round[num_ctas];
+    return true;
+}
+
+template <typename Low>
+std::string stream_layout_replay(const Sweep<Low>& s, const StreamLayout& L, const double* in, double* out) {
+    const uint32_t n = s.n;
+    const uint32_t vb = (uint32_t)sizeof(Low);
+    const bool recip = s.op == SWEEP_DIV || s.op == SWEEP_PREDIV;
+    std::vector<uint8_t> blob = L.blob;
+    if (L.in_slot.size() != n) return "in_slot size";
+    for (uint32_t r = 0; r < n; ++r) {
+        if ((uint64_t)L.in_slot[r] * 8 + 8 > blob.size()) return "in_slot beyond the blob";
+        std::memcpy(blob.data() + (uint64_t)L.in_slot[r] * 8, in + r, 8);
+    }
+    std::vector<uint32_t> pos_of(n);
+    for (uint32_t p = 0; p < n; ++p) pos_of[s.order[p]] = p;
+    std::vector<uint8_t> done(n, 0);
+    struct Cta {
+        uint32_t next = 0;
+        std::vector<double> xs;
+        std::vector<int64_t> owner;  // row whose value the slot holds (-1: none)
+    };
+    std::vector<Cta> ctas(L.num_ctas);
+    for (Cta& c : ctas) {
+        c.xs.assign(L.slots, 0.0);
+        c.owner.assign(L.slots, -1);
+    }
+    uint32_t finished = 0;
+    const uint32_t total = L.cta_round[L.num_ctas];
+    while (finished < total) {
+        bool progress = false;
+        for (uint32_t b = 0; b < L.num_ctas; ++b) {
+            Cta& c = ctas[b];
+            const uint32_t rb = L.slab_start[b];
+            if (rb >= n) return "a slab beyond the rows";
+            const uint32_t owned = L.slab_start[b + 1] - rb;
+            const uint32_t R = L.cta_round[b + 1] - L.cta_round[b];
+            while (c.next < R) {
+                const uint32_t r = c.next, gr = L.cta_round[b] + r;
+                const uint64_t off = (uint64_t)L.meta[(size_t)gr * 4] * 16;
+                const uint32_t bytes = L.meta[(size_t)gr * 4 + 1], nr = L.meta[(size_t)gr * 4 + 2] & 0xFFFFu,
+                               Lr = L.meta[(size_t)gr * 4 + 2] >> 16, X = L.meta[(size_t)gr * 4 + 3];
+                const RoundRec rec = round_rec(nr, Lr, X, vb);
+                if (off % 16 || rec.bytes != bytes || off + bytes > blob.size() || bytes > L.max_round_bytes)
+                    return "round record outside the blob";
+                if (nr == 0 || nr > kRoundRows) return "round size";
+                const uint8_t* base = blob.data() + off;
+                const uint32_t* xrow = reinterpret_cast<const uint32_t*>(base + rec.xrow);
+                const uint16_t* xslot = reinterpret_cast<const uint16_t*>(base + rec.xslot);
+                const uint16_t* xwait = reinterpret_cast<const uint16_t*>(base + rec.xwait);
+                bool ready = true;
+                for (uint32_t x = 0; x < X && ready; ++x) {
+                    if (xrow[x] >= n) return "halo row out of range";
+                    if (xrow[x] >= rb && xrow[x] < rb + owned) return "halo row inside the slab";
+                    ready = done[xrow[x]] != 0;
+                }
+                if (!ready) break;  // an upstream slab first
+                for (uint32_t x = 0; x < X; ++x) {
+                    if (xslot[x] >= L.slots || xslot[x] == 0) return "halo slot out of range";
+                    // the kernel copies round r's halo in while round r - 1 computes
+                    if (xwait[x] > (r > 0 ? r - 1 : 0)) return "a prefetch waits on its own or a later round";
+                    c.xs[xslot[x]] = out[xrow[x]];
+                    c.owner[xslot[x]] = xrow[x];
+                }
+                const double* vin = reinterpret_cast<const double*>(base + rec.in);
+                const double* diag = reinterpret_cast<const double*>(base + rec.diag);
+                const uint16_t* lrow = reinterpret_cast<const uint16_t*>(base + rec.lrow);
+                const uint16_t* oslot = reinterpret_cast<const uint16_t*>(base + rec.oslot);
+                const uint16_t* col = reinterpret_cast<const uint16_t*>(base + rec.col);
+                const Low* val = reinterpret_cast<const Low*>(base + rec.val);
+                // the rows of a round run at once: all of them read before any writes
+                std::vector<double> res(nr);
+                for (uint32_t j = 0; j < nr; ++j) {
+                    if (lrow[j] >= owned) return "row outside its slab";
+                    const uint32_t row = rb + lrow[j];
+                    if (done[row]) return "row visited twice";
+                    const uint32_t p = pos_of[row];
+                    const uint32_t len = s.rowptr[p + 1] - s.rowptr[p];
+                    if (len > Lr) return "row longer than its round's entry table";
+                    if (diag[j] != (recip ? 1.0 / s.diag[p] : s.diag[p])) return "diagonal";
+                    double acc = 0.0;
+                    for (uint32_t t = 0; t < Lr; ++t) {
+                        const uint32_t e = t * rec.m + j;
+                        if (col[e] >= L.slots) return "dependency slot out of range";
+                        if (t >= len) {  // padding: slot 0 (0.0) times 0
+                            if (col[e] != 0 || val[e] != (Low)0) return "padding entry";
+                            continue;
+                        }
+                        const uint32_t k = s.rowptr[p] + t;
+                        if (col[e] == 0) return "a dependency in the zero slot";
+                        if (c.owner[col[e]] != (int64_t)s.col[k]) return "a slot does not hold the dependency";
+                        if (!done[s.col[k]]) return "a dependency read before it was finished";
+                        if (val[e] != s.val[k]) return "coefficient";
+                        acc += (double)val[e] * c.xs[col[e]];
+                    }
+                    if (s.op == SWEEP_DIV || s.op == SWEEP_MUL) res[j] = (vin[j] - acc) * diag[j];
+                    else if (s.op == SWEEP_NONE) res[j] = vin[j] - acc;
+                    else res[j] = vin[j] * diag[j] - acc;
+                }
+                for (uint32_t j = 0; j < nr; ++j) {
+                    const uint32_t row = rb + lrow[j];
+                    out[row] = res[j];
+                    done[row] = 1;
+                    if (oslot[j] != kNoSlot) {
+                        if (oslot[j] >= L.slots || oslot[j] == 0) return "result slot out of range";
+                        c.xs[oslot[j]] = res[j];
+                        c.owner[oslot[j]] = row;
+                    }
+                }
+                ++c.next;
+                ++finished;
+                progress = true;
+            }
+        }
+        if (!progress) return "rounds wait on each other";
+    }
+    for (uint32_t r = 0; r < n; ++r)
+        if (!done[r]) return "row never visited";
+    return std::string();
+}
+
 // ---- explicit instantiations ------------------------------------------------
 template int ict_factor<double>(const CsrHost&, double, CsrT<double>&, std::string*);
 template int ict_factor<float>(const CsrHost&, double, CsrT<float>&, std::string*);
@@ -617,6 +984,15 @@ template void transpose_csr<float>(uint32_t, const std::vector<uint32_t>&, const
 template void slab_layout<double>(const Sweep<double>&, uint32_t, uint32_t, std::vector<uint32_t>&,
                                   Sweep<double>&);
 template void slab_layout<float>(const Sweep<float>&, uint32_t, uint32_t, std::vector<uint32_t>&, Sweep<float>&);
+template std::vector<uint32_t> slab_ranges<double>(const Sweep<double>&, uint32_t);
+template std::vector<uint32_t> slab_ranges<float>(const Sweep<float>&, uint32_t);
+template bool stream_layout<double>(const Sweep<double>&, const std::vector<uint32_t>&, uint32_t, StreamLayout&,
+                                    std::string*);
+template bool stream_layout<float>(const Sweep<float>&, const std::vector<uint32_t>&, uint32_t, StreamLayout&,
+                                   std::string*);
+template std::string stream_layout_replay<double>(const Sweep<double>&, const StreamLayout&, const double*,
+                                                  double*);
+template std::string stream_layout_replay<float>(const Sweep<float>&, const StreamLayout&, const double*, double*);
 template void build_sweep<double>(uint32_t, const std::vector<uint32_t>&, const std::vector<uint32_t>&,
                                   const std::vector<double>&, const std::vector<double>*, int, bool, Sweep<double>&);
 template void build_sweep<float>(uint32_t, const std::vector<uint32_t>&, const std::vector<uint32_t>&,

@@ -105,6 +105,89 @@ template <typename Low>
 void slab_layout(const Sweep<Low>& s, uint32_t num_ctas, uint32_t rows_per_cta, std::vector<uint32_t>& cta_pos,
                  Sweep<Low>& out);
 
+// Streamed round layout of a sweep (k_sweep_stream).
+//
+// The rows are cut into slabs of contiguous rows, one per CTA; each slab's
+// positions, in (level, row) order, are cut greedily into rounds of at most
+// kRoundRows consecutive positions none of which depends on another row of
+// the same round, so a CTA can compute a round's rows all at once, one thread
+// per row.  Every value a round reads lives in a shared-memory value slot:
+// a row of the slab gets a slot when it has readers in the slab (its result
+// is written there), a row of another slab (a "halo" row) gets one for the
+// rounds that read it (a prefetcher copies it there from global memory).
+// Slots are reused once their value's last reader has run; for halo values
+// the prefetcher first waits until that round is done (xwait).  Slot 0 holds
+// 0.0 and pads short rows.  Each round is one 16-byte aligned record, with
+// m = nr rounded up to a multiple of 8 and L = the round's longest row:
+//
+//   f64 in[m]        right-hand side of each row (written per call)
+//   f64 diag[m]      (1 / diag for the dividing operations)
+//   u16 lrow[m]      row - first row of the slab
+//   u16 oslot[m]     value slot of the row's result (0xFFFF: no reader in the slab)
+//   u16 col[L][m]    entry k of row j at k*m + j: value slot of the dependency (0: padding)
+//   Low val[L][m]    its coefficient (0: padding)
+//   u32 xrow[X]      halo rows whose values this round copies in ...
+//   u16 xslot[X]     ... into these slots ...
+//   u16 xwait[X]     ... once this many rounds of the slab are done
+//
+// (the halo sections padded to 16 bytes).  meta[r] = {offset / 16, bytes,
+// nr | L << 16, X}; the rounds of CTA b are [cta_round[b], cta_round[b+1]);
+// in_slot[row] indexes the row's `in` entry in the blob (in doubles).
+#ifdef __CUDACC__
+#define PRISM_HD __host__ __device__
+#else
+#define PRISM_HD
+#endif
+constexpr uint32_t kRoundRows = 64;
+constexpr uint32_t kNoSlot = 0xFFFFu;
+struct RoundRec {
+    uint32_t m, in, diag, lrow, oslot, col, val, xrow, xslot, xwait, bytes;
+};
+PRISM_HD inline uint32_t pad16(uint32_t b) { return (b + 15u) & ~15u; }
+PRISM_HD inline RoundRec round_rec(uint32_t nr, uint32_t L, uint32_t X, uint32_t vb) {
+    RoundRec r;
+    r.m = (nr + 7u) & ~7u;
+    r.in = 0;
+    r.diag = 8u * r.m;
+    r.lrow = 16u * r.m;
+    r.oslot = 18u * r.m;
+    r.col = 20u * r.m;
+    r.val = r.col + 2u * L * r.m;
+    r.xrow = r.val + vb * L * r.m;
+    r.xslot = r.xrow + pad16(4u * X);
+    r.xwait = r.xslot + pad16(2u * X);
+    r.bytes = r.xwait + pad16(2u * X);
+    return r;
+}
+struct StreamLayout {
+    uint32_t num_ctas = 0, num_rounds = 0, max_round_bytes = 0, max_rounds_per_cta = 0;
+    uint32_t slots = 0;                // value slots of the CTA that needs most
+    std::vector<uint32_t> slab_start, cta_pos, cta_round, meta, in_slot;
+    std::vector<uint8_t> blob;
+};
+// Slab boundaries for num_ctas CTAs (num_ctas + 1 entries, empty slabs
+// dropped): rows are first split where no dependency crosses (independent
+// diagonal blocks, such as the subdomains of an AMSED level, never share a
+// slab), CTAs are given to those segments in proportion to their rows, and
+// each segment is split evenly.
+template <typename Low>
+std::vector<uint32_t> slab_ranges(const Sweep<Low>& s, uint32_t num_ctas);
+// Builds the records for slabs [start[b], start[b+1]).  For the dividing
+// operations (SWEEP_DIV, SWEEP_PREDIV) the record holds 1 / diag and the
+// kernel multiplies.  Returns false (and why) when the sweep does not fit the
+// record format or needs more than max_slots value slots in one slab.
+template <typename Low>
+bool stream_layout(const Sweep<Low>& s, const std::vector<uint32_t>& start, uint32_t max_slots, StreamLayout& out,
+                   std::string* why);
+// Replays k_sweep_stream on the host: stages `in` as the prep kernel does,
+// runs each slab's rounds in order (a round only once the halo rows it copies
+// in are finished), checks every offset, that each slot read holds the value
+// of the dependency it stands for, that no slot is overwritten before its last
+// reader ran and that no prefetch waits on its own or a later round, and
+// solves the sweep.  Returns an empty string, or what is wrong with the layout.
+template <typename Low>
+std::string stream_layout_replay(const Sweep<Low>& s, const StreamLayout& L, const double* in, double* out);
+
 // Builds a sweep from a gather-form CSR (row r lists its dependencies and
 // coefficients, in the order the reference accumulates them) plus optional
 // per-row diagonal.  Computes the exact integer level schedule:

@@ -7,6 +7,7 @@
 #include "../../include/prism_solve.h"
 #include "kernels.cuh"
 #include "solve.cuh"
+#include "stream_sweep.cuh"
 
 namespace prism {
 
@@ -52,8 +53,57 @@ static void* slab_kernel(bool fp32, int op) {
 
 static constexpr int kSlabThreads = 1024;
 
-void launch_sweep(const Handle& h, cudaStream_t st, const DevSweep& s, const double* in, double* out) {
+static void* stream_kernel(bool fp32, int op) {
+    if (fp32) {
+        switch (op) {
+            case SWEEP_DIV: return (void*)k_sweep_stream<float, OP_DIV>;
+            case SWEEP_MUL: return (void*)k_sweep_stream<float, OP_MUL>;
+            case SWEEP_NONE: return (void*)k_sweep_stream<float, OP_NONE>;
+            default: return (void*)k_sweep_stream<float, OP_PREDIV>;
+        }
+    }
+    switch (op) {
+        case SWEEP_DIV: return (void*)k_sweep_stream<double, OP_DIV>;
+        case SWEEP_MUL: return (void*)k_sweep_stream<double, OP_MUL>;
+        case SWEEP_NONE: return (void*)k_sweep_stream<double, OP_NONE>;
+        default: return (void*)k_sweep_stream<double, OP_PREDIV>;
+    }
+}
+
+void launch_sweep_prepare(const Handle& h, cudaStream_t st, const DevSweep& s, const double* in, double* out) {
     if (!s.n) return;
+    if (s.layout != LAYOUT_STREAM) {
+        launch_fill(st, h, s.n, out);
+        return;
+    }
+    k_stream_prep<<<vec_grid(h, s.n), kBlock, 0, st>>>(s.n, s.str_in_slot.get(), in,
+                                                       reinterpret_cast<double*>(s.str_blob.get()),
+                                                       reinterpret_cast<unsigned long long*>(out));
+    PRISM_LAUNCHED();
+}
+
+void launch_sweep_kernel(const Handle& h, cudaStream_t st, const DevSweep& s, const double* in, double* out) {
+    if (!s.n) return;
+    if (s.layout == LAYOUT_STREAM) {
+        (void)in;
+        StreamArgs a;
+        a.blob = s.str_blob.get();
+        a.meta = reinterpret_cast<const uint4*>(s.str_meta.get());
+        a.cta_round = s.str_cta_round.get();
+        a.slab_start = s.str_slab_start.get();
+        a.n = s.n;
+        a.ring_bytes = s.str_ring;
+        a.meta_slots = s.str_meta_slots;
+        a.slots = s.str_slots;
+        a.out = out;
+        a.status = h.status.get();
+        a.wait_ns = kWaitNs;
+        void* args[] = {&a};
+        PRISM_CUDA(cudaLaunchCooperativeKernel(stream_kernel(s.fp32, s.op), dim3(s.str_ctas), dim3(kStrThreads), args,
+                                               s.str_smem, st));
+        PRISM_LAUNCHED();
+        return;
+    }
     if (s.num_ctas > 0) {
         void* fn = slab_kernel(s.fp32, s.op);
         uint32_t n = s.n, rpc = s.rows_per_cta, smem_rows = s.smem_rows;
@@ -103,6 +153,11 @@ void launch_sweep(const Handle& h, cudaStream_t st, const DevSweep& s, const dou
     // progress argument of k_sweep relies on.
     PRISM_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kBlock), args, 0, st));
     PRISM_LAUNCHED();
+}
+
+void launch_sweep(const Handle& h, cudaStream_t st, const DevSweep& s, const double* in, double* out) {
+    if (s.layout == LAYOUT_STREAM) launch_sweep_prepare(h, st, s, in, out);
+    launch_sweep_kernel(h, st, s, in, out);
 }
 
 void launch_spmv(const Handle& h, cudaStream_t st, uint32_t nrows, const uint32_t* rowptr, const uint32_t* col,
@@ -191,16 +246,21 @@ void init_device_info(DeviceInfo& info, int device) {
     PRISM_CUDA(cudaDeviceGetAttribute(&info.max_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
     if (const char* e = std::getenv("PRISM_SWEEP_KERNEL")) {
         const std::string k(e);
-        info.sweep_kernel = k == "global" ? 1 : (k == "slab" ? 2 : 0);
+        info.sweep_kernel = k == "global" ? 1 : (k == "slab" ? 2 : (k == "stream" ? 3 : 0));
     }
     if (const char* e = std::getenv("PRISM_SLAB_MIN_ROWS")) info.slab_min_rows = (uint32_t)std::atoi(e);
     if (const char* e = std::getenv("PRISM_SLAB_MAX_ROWS")) info.slab_max_rows = (uint32_t)std::atoi(e);
     if (info.slab_min_rows < 32) info.slab_min_rows = 32;
     // the slab kernel runs one 1024-thread CTA per SM with up to the whole opt-in shared memory
+    if (const char* e = std::getenv("PRISM_STREAM_MIN_ROWS")) info.stream_min_rows = (uint32_t)std::atoi(e);
+    if (info.stream_min_rows < 32) info.stream_min_rows = 32;
     for (bool f32 : {false, true})
-        for (int op = 0; op < 4; ++op)
+        for (int op = 0; op < 4; ++op) {
             PRISM_CUDA(cudaFuncSetAttribute(slab_kernel(f32, op), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             info.max_smem_optin));
+            PRISM_CUDA(cudaFuncSetAttribute(stream_kernel(f32, op), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            info.max_smem_optin));
+        }
 }
 
 Handle::~Handle() {
@@ -248,8 +308,61 @@ void Handle::check_status() {
 // ============================================================================
 // Sweeps and triangular preconditioners
 // ============================================================================
+void DevSweep::release() {
+    order.release(); rowptr.release(); col.release(); cta_pos.release();
+    val64.release(); diag.release(); val32.release();
+    str_blob.release(); str_meta.release(); str_cta_round.release(); str_slab_start.release(); str_in_slot.release();
+    num_ctas = rows_per_cta = smem_rows = 0;
+    str_ctas = str_ring = str_meta_slots = str_slots = str_rounds = str_smem = 0;
+    str_nnz = 0;
+}
+
 template <typename Low>
-void DevSweep::upload(const Sweep<Low>& s0, const DeviceInfo& info, bool slab_layout_wanted, cudaStream_t st) {
+bool DevSweep::upload(const Sweep<Low>& s0, const DeviceInfo& info, int lay, cudaStream_t st) {
+    if (lay == LAYOUT_STREAM) {
+        // One persistent CTA per SM (fewer for small sweeps); shared memory holds the
+        // round table, the value slots and, in what is left, the ring the round
+        // records stream through.
+        const uint32_t nn = s0.n;
+        if (nn == 0) return false;
+        uint32_t ctas = std::min<uint32_t>((uint32_t)info.sms, (nn + info.stream_min_rows - 1) / info.stream_min_rows);
+        if (ctas < 1) ctas = 1;
+        const std::vector<uint32_t> start = slab_ranges<Low>(s0, ctas);
+        ctas = (uint32_t)start.size() - 1;
+        const uint64_t smem = (uint64_t)info.max_smem_optin;
+        StreamLayout L;
+        const uint32_t slot_cap = (uint32_t)std::min<uint64_t>(kNoSlot, (smem - kStrFixedSmem) / 8 / 2);
+        if (!stream_layout<Low>(s0, start, slot_cap, L, nullptr)) return false;
+        const uint64_t fixed = (uint64_t)kStrFixedSmem + (uint64_t)L.max_rounds_per_cta * 16 +
+                               (((uint64_t)L.slots * 8 + 127) & ~127ull);
+        // Round r + 1 must land while round r still occupies the ring (the row threads wait
+        // for it before finishing round r); wherever round r sits, a ring of three records
+        // has room for one more next to it.
+        if (fixed + 3ull * L.max_round_bytes > smem) return false;
+        const uint32_t ring = (uint32_t)((smem - fixed) & ~15ull);
+        release();
+        n = s0.n;
+        num_levels = s0.num_levels;
+        op = s0.op;
+        fp32 = std::is_same<Low, float>::value;
+        layout = LAYOUT_STREAM;
+        str_ctas = ctas;
+        str_ring = ring;
+        str_meta_slots = L.max_rounds_per_cta;
+        str_slots = L.slots;
+        str_rounds = L.num_rounds;
+        str_smem = (uint32_t)(fixed + ring);
+        str_nnz = s0.val.size();
+        str_blob.upload(L.blob.data(), L.blob.size(), st);
+        str_meta.upload(L.meta.data(), L.meta.size(), st);
+        str_cta_round.upload(L.cta_round.data(), L.cta_round.size(), st);
+        str_slab_start.upload(L.slab_start.data(), L.slab_start.size(), st);
+        str_in_slot.upload(L.in_slot.data(), L.in_slot.size(), st);
+        PRISM_CUDA(cudaStreamSynchronize(st));
+        return true;
+    }
+    release();
+    layout = lay;
     n = s0.n;
     num_levels = s0.num_levels;
     op = s0.op;
@@ -257,8 +370,7 @@ void DevSweep::upload(const Sweep<Low>& s0, const DeviceInfo& info, bool slab_la
     const Sweep<Low>* s = &s0;
     Sweep<Low> slab;
     std::vector<uint32_t> cpos;
-    num_ctas = rows_per_cta = smem_rows = 0;
-    if (slab_layout_wanted && n > 0) {
+    if (lay == LAYOUT_SLAB && n > 0) {
         // As many rows per slab as shared memory holds: the dependencies of a
         // row reach back about one grid plane, so large slabs keep most of them
         // (and the critical path through them) inside one CTA, where a
@@ -274,6 +386,8 @@ void DevSweep::upload(const Sweep<Low>& s0, const DeviceInfo& info, bool slab_la
         slab_layout<Low>(s0, num_ctas, rows_per_cta, cpos, slab);
         s = &slab;
         cta_pos.upload(cpos.data(), cpos.size(), st);
+    } else {
+        layout = LAYOUT_LEVEL;
     }
     order.upload(s->order.data(), s->order.size(), st);
     rowptr.upload(s->rowptr.data(), s->rowptr.size(), st);
@@ -286,18 +400,25 @@ void DevSweep::upload(const Sweep<Low>& s0, const DeviceInfo& info, bool slab_la
     if (fp32 && val32.size() == 0) val32.alloc(1);
     if (!fp32 && val64.size() == 0) val64.alloc(1);
     PRISM_CUDA(cudaStreamSynchronize(st));
+    return true;
 }
 
-// Sweep-kernel autotuner: uploads the sweep in the plain level order and in
-// the slab layout in turn, times a few launches of each on a random
-// right-hand side with CUDA events, and keeps the faster one.  Which kernel
-// wins depends on how many rows a wavefront holds and how far dependencies
-// reach (the slab kernel pays off when most of them stay inside a slab).
+// Sweep-kernel autotuner: uploads the sweep in each device layout in turn
+// (level order for k_sweep, slabs for k_sweep_slab, streamed rounds for
+// k_sweep_stream), times a few launches of each, output marking included, on
+// a fixed right-hand side with CUDA events, and keeps the fastest.  Which
+// kernel wins depends on how many rows a wavefront holds and how far
+// dependencies reach.
 template <typename Low>
 void tune_sweep(Handle& h, DevSweep& d, const Sweep<Low>& s) {
     const int mode = h.info.sweep_kernel;
-    if (mode != 0 || s.n == 0) {
-        d.upload(s, h.info, mode == 2, h.stream);
+    if (s.n == 0) {
+        d.upload(s, h.info, LAYOUT_LEVEL, h.stream);
+        return;
+    }
+    if (mode != 0) {
+        const int want = mode == 2 ? LAYOUT_SLAB : (mode == 3 ? LAYOUT_STREAM : LAYOUT_LEVEL);
+        if (!d.upload(s, h.info, want, h.stream)) d.upload(s, h.info, LAYOUT_LEVEL, h.stream);
         return;
     }
     DevBuf<double> in(s.n), out(s.n);
@@ -308,14 +429,14 @@ void tune_sweep(Handle& h, DevSweep& d, const Sweep<Low>& s) {
     PRISM_CUDA(cudaEventCreate(&e0));
     PRISM_CUDA(cudaEventCreate(&e1));
     float best = 0.f;
-    bool best_slab = false;
-    for (bool slab : {false, true}) {
-        d.upload(s, h.info, slab, h.stream);
+    int best_layout = -1;
+    for (int lay : {LAYOUT_LEVEL, LAYOUT_SLAB, LAYOUT_STREAM}) {
+        if (!d.upload(s, h.info, lay, h.stream)) continue;
         float tot = 0.f;
         for (int it = 0; it < 4; ++it) {
-            launch_fill(h.stream, h, s.n, out.get());
             PRISM_CUDA(cudaEventRecord(e0, h.stream));
-            launch_sweep(h, h.stream, d, in.get(), out.get());
+            launch_sweep_prepare(h, h.stream, d, in.get(), out.get());
+            launch_sweep_kernel(h, h.stream, d, in.get(), out.get());
             PRISM_CUDA(cudaEventRecord(e1, h.stream));
             PRISM_CUDA(cudaEventSynchronize(e1));
             float ms = 0.f;
@@ -323,11 +444,14 @@ void tune_sweep(Handle& h, DevSweep& d, const Sweep<Low>& s) {
             if (it > 0) tot += ms;  // first launch is a warm-up
         }
         h.check_status();
-        if (!slab || tot < best) { best = tot; best_slab = slab; }
+        if (best_layout < 0 || tot < best) {
+            best = tot;
+            best_layout = lay;
+        }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    if (!best_slab) d.upload(s, h.info, false, h.stream);
+    if (d.layout != best_layout) d.upload(s, h.info, best_layout, h.stream);
     d.tuned_ms = best / 3.f;
 }
 template void tune_sweep<double>(Handle&, DevSweep&, const Sweep<double>&);
@@ -346,26 +470,26 @@ TriangularPrecond::TriangularPrecond(Handle& h, std::shared_ptr<const HostFactor
 void TriangularPrecond::apply(cudaStream_t st, const double* in, double* out) {
     const uint32_t n = h_.A.n;
     if (tmp_.size() < n) tmp_.alloc(n);
-    launch_fill(st, h_, n, tmp_.get());
-    if (in != out) launch_fill(st, h_, n, out);
+    if (!lower_.self_filling()) launch_fill(st, h_, n, tmp_.get());
+    if (in != out && !upper_.self_filling()) launch_fill(st, h_, n, out);
     launch_sweep(h_, st, lower_, in, tmp_.get());
-    if (in == out) launch_fill(st, h_, n, out);
+    if (in == out && !upper_.self_filling()) launch_fill(st, h_, n, out);
     launch_sweep(h_, st, upper_, tmp_.get(), out);
 }
 
 bool TriangularPrecond::run_sweep(cudaStream_t st, int sweep, const double* in, double* out, int prepare) {
     const DevSweep& s = sweep == 0 ? lower_ : upper_;
-    if (prepare != 0) launch_fill(st, h_, s.n, out);
-    if (prepare != 2) launch_sweep(h_, st, s, in, out);
+    if (prepare != 0) launch_sweep_prepare(h_, st, s, in, out);
+    if (prepare != 2) launch_sweep_kernel(h_, st, s, in, out);
     return true;
 }
 
 bool TriangularPrecond::sweep_info(int sweep, uint32_t* n, uint64_t* nnz, uint32_t* vbytes, uint32_t* levels,
                                    uint32_t* kernel) const {
     const DevSweep& s = sweep == 0 ? lower_ : upper_;
-    if (kernel) *kernel = s.num_ctas > 0 ? 2 : 1;
+    if (kernel) *kernel = s.layout == LAYOUT_STREAM ? 3 : (s.layout == LAYOUT_SLAB ? 2 : 1);
     if (n) *n = s.n;
-    if (nnz) *nnz = s.fp32 ? s.val32.size() : s.val64.size();
+    if (nnz) *nnz = s.entries();
     if (vbytes) *vbytes = s.fp32 ? 4 : 8;
     if (levels) *levels = s.num_levels;
     return true;

@@ -20,9 +20,10 @@ struct DeviceInfo {
     int sms = 148;
     int sweep_blocks_per_sm = 1;   // co-resident k_sweep blocks (cooperative launch bound)
     int max_smem_optin = 0;        // bytes of dynamic shared memory one block may opt into
-    int sweep_kernel = 0;          // 0: autotune per sweep, 1: global level order, 2: slab-blocked
+    int sweep_kernel = 0;          // 0: autotune per sweep, 1: global level order, 2: slab-blocked, 3: streamed rounds
     uint32_t slab_min_rows = 2048; // smallest slab (small systems use fewer CTAs)
     uint32_t slab_max_rows = 1u << 30;  // largest slab (default: what shared memory holds)
+    uint32_t stream_min_rows = 1024;    // smallest streamed slab (small systems use fewer CTAs)
 };
 
 // Reduction scratch shared by all kernels of one stream (they run serially).
@@ -55,18 +56,33 @@ struct DeviceCsr {
     DevBuf<double> val;
 };
 
+// Device layouts of a triangular sweep.
+enum SweepLayout : int { LAYOUT_LEVEL = 0, LAYOUT_SLAB = 1, LAYOUT_STREAM = 2 };
+
 // One triangular sweep resident on the device (see build_sweep for the layout).
 struct DevSweep {
     uint32_t n = 0, num_levels = 0;
     int op = SWEEP_NONE;
     bool fp32 = false;
-    // slab layout (k_sweep_slab) when num_ctas > 0, plain level order (k_sweep) otherwise
+    int layout = LAYOUT_LEVEL;
+    // LAYOUT_SLAB (k_sweep_slab): num_ctas > 0
     uint32_t num_ctas = 0, rows_per_cta = 0, smem_rows = 0;
     DevBuf<uint32_t> order, rowptr, col, cta_pos;
     DevBuf<double> val64, diag;
     DevBuf<float> val32;
+    // LAYOUT_STREAM (k_sweep_stream): round records, see StreamLayout
+    uint32_t str_ctas = 0, str_ring = 0, str_meta_slots = 0, str_slots = 0, str_rounds = 0, str_smem = 0;
+    uint64_t str_nnz = 0;
+    DevBuf<unsigned char> str_blob;
+    DevBuf<uint32_t> str_meta, str_cta_round, str_slab_start, str_in_slot;
+    // Uploads the sweep in the given layout; false (nothing uploaded) when the
+    // layout does not fit the sweep (stream layout only).
     template <typename Low>
-    void upload(const Sweep<Low>& s, const DeviceInfo& info, bool slab, cudaStream_t st);
+    bool upload(const Sweep<Low>& s, const DeviceInfo& info, int layout, cudaStream_t st);
+    // the stream layout marks its own output pending; the others need launch_fill first
+    bool self_filling() const { return layout == LAYOUT_STREAM; }
+    uint64_t entries() const { return layout == LAYOUT_STREAM ? str_nnz : (fp32 ? val32.size() : val64.size()); }
+    void release();
     float tuned_ms = 0.f;          // time of the chosen kernel at setup (0: not tuned)
 };
 
@@ -206,7 +222,13 @@ struct Handle {
 int vec_grid(const Handle& h, uint32_t n);
 // marks n doubles pending (the sweeps' readiness encoding)
 void launch_fill(cudaStream_t st, const Handle& h, uint32_t n, double* p);
+// One sweep: out = T^{-1} in.  Layouts other than LAYOUT_STREAM need `out`
+// marked pending (launch_fill) first; the stream layout does that itself.
 void launch_sweep(const Handle& h, cudaStream_t st, const DevSweep& s, const double* in, double* out);
+// The two halves of a sweep: marking `out` pending (and, for the stream
+// layout, staging `in` into the round records), then the sweep kernel.
+void launch_sweep_prepare(const Handle& h, cudaStream_t st, const DevSweep& s, const double* in, double* out);
+void launch_sweep_kernel(const Handle& h, cudaStream_t st, const DevSweep& s, const double* in, double* out);
 // y = M x (sub = 0) or y -= M x (sub = 1) for a CSR with nrows rows
 void launch_spmv(const Handle& h, cudaStream_t st, uint32_t nrows, const uint32_t* rowptr, const uint32_t* col,
                  const double* val, const double* x, double* y, int sub);
