@@ -17,19 +17,20 @@
 // ones) are copied into their slots by prefetcher warps as soon as they are
 // finished, while the slab is still working on earlier rounds.
 //
-// Roles (1024 threads):
+// Roles (384 threads; the polling warps sleep between polls so that the row
+// threads, which carry the dependency chain, keep the issue slots):
 //   warps 0..1    row threads: thread j computes row j of each round, then each
 //                 warp arrives on the round's mbarrier and waits for it.
-//   warps 2..29   prefetchers: warp 2+k handles rounds k, k+28, ...: it waits
+//   warps 2..9    prefetchers: warp 2+k handles rounds k, k+8, ...: it waits
 //                 until the round's record has landed, polls each new halo row
 //                 in global memory until it is finished, waits until the slot's
 //                 previous value has had its last reader (xwait), writes the
 //                 slot and arrives on the barrier that ends the round before,
 //                 whose phase therefore also means "the next round's halo is in".
-//   warp 30       publisher: copies each finished round's results (left by the
+//   warp 10       publisher: copies each finished round's results (left by the
 //                 row threads in the round's record) to global memory, so the
 //                 row threads touch shared memory only.
-//   warp 31       producer: issues the bulk copies of the records into the
+//   warp 11       producer: issues the bulk copies of the records into the
 //                 ring in order, publishes how many have landed, and recycles
 //                 the ring space of published rounds.
 //
@@ -52,15 +53,15 @@
 
 namespace prism {
 
-constexpr int kStrThreads = 1024;
 constexpr int kStrRowWarps = (int)kRoundRows / 32;     // row threads: one per row of a round
-constexpr int kStrPrefetchWarps = 28;                  // warps kStrRowWarps .. 29
-constexpr int kStrPublisher = 30;
-constexpr int kStrProducer = 31;
+constexpr int kStrPrefetchWarps = 8;                   // warps kStrRowWarps .. kStrPublisher - 1
+constexpr int kStrPublisher = kStrRowWarps + kStrPrefetchWarps;
+constexpr int kStrProducer = kStrPublisher + 1;
+constexpr int kStrThreads = 32 * (kStrProducer + 1);
 constexpr uint32_t kStrMaxRounds = 64;                 // rounds in flight (ring table slots)
 // copy barriers, round barriers, start barrier (+pad), ring offsets, words
 constexpr uint32_t kStrFixedSmem = 64 * 8 + 64 * 8 + 16 + 64 * 4 + 32;
-static_assert(kStrRowWarps + kStrPrefetchWarps == kStrPublisher, "warp roles");
+static_assert(kStrThreads <= 1024, "warp roles");
 
 struct StreamArgs {
     const unsigned char* blob;
@@ -172,7 +173,7 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
     volatile uint32_t* vwords = words;
     // bounded-wait helper: true (and the CTA told to leave) after wait_ns without success
     auto give_up = [&](unsigned& spins, unsigned long long t0) {
-        if ((++spins & 63u) != 0u) return false;
+        if ((++spins & 15u) != 0u) return false;
         if (vwords[2] != 0 || ld_relaxed_s32(status) != 0 || globaltimer_ns() - t0 > wait_ns) {
             atomicCAS(status, 0, 6);
             vwords[2] = 1;
@@ -233,7 +234,7 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
                 t_event = globaltimer_ns();
                 spins = 0;
             } else {
-                __nanosleep(32);
+                __nanosleep(spins < 16 ? 64 : 256);  // polling warps leave issue slots to the row threads
                 if (give_up(spins, t_event)) {
                     failed = true;
                     break;
@@ -257,7 +258,7 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
             unsigned spins = 0;
             bool ok = true;
             while (ld_acquire_shared_u32(words + 1) <= r) {
-                __nanosleep(32);
+                __nanosleep(spins < 16 ? 64 : 256);  // polling warps leave issue slots to the row threads
                 if (give_up(spins, t0)) {
                     ok = false;
                     break;
@@ -279,7 +280,7 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
 
     if (warp >= kStrRowWarps) {
         // ------------------------------------------------------------------ prefetchers
-        // Warp k copies in the halo of rounds k, k + 28, ... and then arrives on the barrier
+        // Warp k copies in the halo of rounds k, k + 8, ... and then arrives on the barrier
         // that ends the round before (start_bar for round 0).  That barrier's previous phase
         // (64 rounds earlier) is over: the record of round q is in the ring only once round
         // q - 64 has been published.  Round R is a stand-in that only arrives.
@@ -289,7 +290,7 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
             unsigned spins = 0;
             if (q == R) {
                 while (R >= kStrMaxRounds && ld_acquire_shared_u32(words + 1) + kStrMaxRounds < R + 1) {
-                    __nanosleep(32);
+                    __nanosleep(spins < 16 ? 64 : 256);  // polling warps leave issue slots to the row threads
                     if (give_up(spins, t0)) {
                         ok = false;
                         break;
@@ -299,7 +300,7 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
                 break;
             }
             while (ld_acquire_shared_u32(words) <= q) {
-                __nanosleep(32);
+                __nanosleep(spins < 16 ? 64 : 256);  // polling warps leave issue slots to the row threads
                 if (give_up(spins, t0)) {
                     ok = false;
                     break;
@@ -334,7 +335,7 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
                         t0 = globaltimer_ns();
                         spins = 0;
                         while (ld_acquire_shared_u32(words + 1) < need) {
-                            __nanosleep(32);
+                            __nanosleep(spins < 16 ? 64 : 256);  // polling warps leave issue slots to the row threads
                             if (give_up(spins, t0)) {
                                 ok = false;
                                 break;
@@ -400,13 +401,25 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
         if (j < cur.nr) {
             const uint16_t* col = reinterpret_cast<const uint16_t*>(ring + cur.col) + j;
             const Low* val = reinterpret_cast<const Low*>(ring + cur.val) + j;
+            const uint32_t m = cur.m;
             double s0 = 0.0, s1 = 0.0;
-            uint32_t k = 0;
-            for (; k + 2 <= cur.L; k += 2) {
-                s0 += (double)val[k * cur.m] * xs[col[k * cur.m]];
-                s1 += (double)val[(k + 1) * cur.m] * xs[col[(k + 1) * cur.m]];
+            // four entries at a time: their slot indices and coefficients first, then the
+            // four value reads together, so shared-memory latency is paid once per four
+            for (uint32_t k = 0; k < cur.L; k += 4) {
+                uint32_t c[4];
+                double v[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const bool in = k + u < cur.L;
+                    c[u] = in ? col[(k + u) * m] : 0u;
+                    v[u] = in ? (double)val[(k + u) * m] : 0.0;
+                }
+                double x[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) x[u] = xs[c[u]];
+                s0 += v[0] * x[0] + v[2] * x[2];
+                s1 += v[1] * x[1] + v[3] * x[3];
             }
-            if (k < cur.L) s0 += (double)val[k * cur.m] * xs[col[k * cur.m]];
             const double s = s0 + s1;
             double res;
             if (OP == OP_DIV || OP == OP_MUL) res = (cur.vin - s) * cur.dg;  // dg = 1/diag for OP_DIV
