@@ -27,12 +27,10 @@
 //                 previous value has had its last reader (xwait), writes the
 //                 slot and arrives on the barrier that ends the round before,
 //                 whose phase therefore also means "the next round's halo is in".
-//   warp 10       publisher: copies each finished round's results (left by the
-//                 row threads in the round's record) to global memory, so the
-//                 row threads touch shared memory only.
+//   warp 10       idle.
 //   warp 11       producer: issues the bulk copies of the records into the
 //                 ring in order, publishes how many have landed, and recycles
-//                 the ring space of published rounds.
+//                 the ring space of finished rounds.
 //
 // Finished values are published in global memory with the kPending encoding
 // of k_sweep (the 8-byte word itself says whether it is finished); a prep
@@ -48,6 +46,8 @@
 // the producer waits (again bounded) for its copies in flight, and every
 // warp returns.
 #pragma once
+
+#include <type_traits>
 
 #include "kernels.cuh"
 
@@ -141,7 +141,7 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
     uint64_t* round_bar = tma_bar + 64;                                      // [64] end of round r (r % 64)
     uint64_t* start_bar = round_bar + 64;                                    // round 0's halo in place
     uint32_t* ring_off = reinterpret_cast<uint32_t*>(sm + 64 * 8 * 2 + 16);  // [64]
-    uint32_t* words = ring_off + 64;  // landed, rounds done, abort, published
+    uint32_t* words = ring_off + 64;  // landed, rounds done, abort
     uint4* meta_s = reinterpret_cast<uint4*>(sm + kStrFixedSmem);            // [meta_slots]
     double* xs = reinterpret_cast<double*>(meta_s + a.meta_slots);           // [slots]; xs[0] = 0
     unsigned char* ring = reinterpret_cast<unsigned char*>(xs) + ((a.slots * 8u + 127u) & ~127u);
@@ -157,7 +157,7 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
         words[0] = 0;  // records landed
         words[1] = 0;  // rounds done
         words[2] = 0;  // abort
-        words[3] = 0;  // rounds published
+
         for (uint32_t i = 0; i < kStrMaxRounds; ++i) {
             mbar_init(tma_bar + i, 1);
             mbar_init(round_bar + i, kStrRowWarps + 1);  // the row warps + the next round's prefetcher
@@ -191,7 +191,7 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
         bool failed = false;
         while (landed < R) {
             bool event = false;
-            const uint32_t done = ld_acquire_shared_u32(words + 3);
+            const uint32_t done = ld_acquire_shared_u32(words + 1);  // rounds done: their records are free
             while (freed < landed && freed < done) {
                 ++freed;
                 event = true;
@@ -251,39 +251,14 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
         return;
     }
 
-    if (warp == kStrPublisher) {
-        // ------------------------------------------------------------------ publisher
-        for (uint32_t r = 0; r < R; ++r) {
-            const unsigned long long t0 = globaltimer_ns();
-            unsigned spins = 0;
-            bool ok = true;
-            while (ld_acquire_shared_u32(words + 1) <= r) {
-                __nanosleep(spins < 16 ? 64 : 256);  // polling warps leave issue slots to the row threads
-                if (give_up(spins, t0)) {
-                    ok = false;
-                    break;
-                }
-            }
-            if (!__all_sync(0xFFFFFFFFu, ok)) return;
-            const uint4 m = meta_s[r];
-            const uint32_t nr = m.z & 0xFFFFu;
-            const RoundRec rec = round_rec(nr, m.z >> 16, m.w, vb);
-            const unsigned char* base = ring + ring_off[r % kStrMaxRounds];
-            const unsigned long long* res = reinterpret_cast<const unsigned long long*>(base + rec.in);
-            const uint16_t* lrow = reinterpret_cast<const uint16_t*>(base + rec.lrow);
-            for (uint32_t j = (uint32_t)lane; j < nr; j += 32) st_relaxed_u64(a.out + rb + lrow[j], res[j]);
-            __syncwarp();
-            if (lane == 0) st_release_shared_u32(words + 3, r + 1);
-        }
-        return;
-    }
+    if (warp == kStrPublisher) return;  // results go to global memory from the row threads
 
     if (warp >= kStrRowWarps) {
         // ------------------------------------------------------------------ prefetchers
         // Warp k copies in the halo of rounds k, k + 8, ... and then arrives on the barrier
         // that ends the round before (start_bar for round 0).  That barrier's previous phase
         // (64 rounds earlier) is over: the record of round q is in the ring only once round
-        // q - 64 has been published.  Round R is a stand-in that only arrives.
+        // q - 64 is done.  Round R is a stand-in that only arrives.
         for (uint32_t q = (uint32_t)(warp - kStrRowWarps); q <= R; q += kStrPrefetchWarps) {
             bool ok = true;
             unsigned long long t0 = globaltimer_ns();
@@ -360,15 +335,20 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
     // ---------------------------------------------------------------------- row threads
     // Thread j computes row j of each round: its entries sit at j, j + m, j + 2m, ...
     // of the round's entry table (m = rows rounded up to 8), padded with slot 0 (0.0)
-    // to the round's longest row, so the loop has the same length for every thread.
-    // Round r+1's record fields are read into registers before the barrier that ends
-    // round r; after it only the value-slot reads, the sum and the result remain.
+    // to the round's longest row.  Before waiting for the barrier that ends round r,
+    // each thread reads round r+1's record -- up to 32 entries, right-hand side,
+    // diagonal, slots -- into registers; after it only the value-slot reads (all
+    // independent, issued back to back), the sums and the result remain on the chain.
     const uint32_t j = threadIdx.x;
+    constexpr int kRegEntries = 32;
     struct Row {
-        uint32_t nr, L, m, col, val;  // rows, entries per row, stride, section offsets (ring-relative)
-        uint32_t os, base;
+        uint32_t nr, L, m, rest;        // rows, entries per row, stride, ring offset of entries past 32
+        uint32_t os, lr, base;
         double vin, dg;
+        uint32_t c[kRegEntries];
+        Low v[kRegEntries];
     };
+    Row cur;
     auto load_row = [&](uint32_t r, Row& w) {
         const uint4 m = meta_s[r];
         w.nr = m.z & 0xFFFFu;
@@ -376,14 +356,39 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
         const RoundRec rec = round_rec(w.nr, w.L, m.w, vb);
         w.base = ring_off[r % kStrMaxRounds];
         w.m = rec.m;
-        w.col = w.base + rec.col;
-        w.val = w.base + rec.val;
-        if (j < w.nr) {
-            const unsigned char* base = ring + w.base;
-            w.vin = reinterpret_cast<const double*>(base + rec.in)[j];
-            w.dg = reinterpret_cast<const double*>(base + rec.diag)[j];
-            w.os = reinterpret_cast<const uint16_t*>(base + rec.oslot)[j];
-        }
+        w.rest = w.base + rec.col;
+        if (j >= w.nr) return;
+        const unsigned char* base = ring + w.base;
+        const uint16_t* col = reinterpret_cast<const uint16_t*>(base + rec.col) + j;
+        const Low* val = reinterpret_cast<const Low*>(base + rec.val) + j;
+        w.vin = reinterpret_cast<const double*>(base + rec.in)[j];
+        w.dg = reinterpret_cast<const double*>(base + rec.diag)[j];
+        w.os = reinterpret_cast<const uint16_t*>(base + rec.oslot)[j];
+        w.lr = reinterpret_cast<const uint16_t*>(base + rec.lrow)[j];
+        // only as many register entries as the round's longest row needs (8, 16 or 32)
+        auto fill = [&](auto nconst) {
+            constexpr int N = decltype(nconst)::value;
+#pragma unroll
+            for (int u = 0; u < N; ++u) {
+                const bool in = (uint32_t)u < w.L;
+                w.c[u] = in ? col[u * rec.m] : 0u;
+                w.v[u] = in ? val[u * rec.m] : (Low)0;
+            }
+        };
+        if (w.L <= 8) fill(std::integral_constant<int, 8>{});
+        else if (w.L <= 16) fill(std::integral_constant<int, 16>{});
+        else fill(std::integral_constant<int, 32>{});
+    };
+    // sum of the first N register entries (N a multiple of 4): value reads first, then four chains
+    auto dot_regs = [&](const Row& w, auto nconst) {
+        constexpr int N = decltype(nconst)::value;
+        double x[N];
+#pragma unroll
+        for (int u = 0; u < N; ++u) x[u] = xs[w.c[u]];
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int u = 0; u < N; ++u) acc[u & 3] += (double)w.v[u] * x[u];
+        return (acc[0] + acc[1]) + (acc[2] + acc[3]);
     };
     auto wait_phase = [&](uint64_t* bar, uint32_t parity) {
         if (mbar_try_parity(bar, parity)) return true;
@@ -394,33 +399,19 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
         return true;
     };
     if (!wait_phase(start_bar, 0)) return;
-    Row cur, nxt;
     load_row(0, cur);
     uint32_t landed_seen = 1;
     for (uint32_t r = 0; r < R; ++r) {
         if (j < cur.nr) {
-            const uint16_t* col = reinterpret_cast<const uint16_t*>(ring + cur.col) + j;
-            const Low* val = reinterpret_cast<const Low*>(ring + cur.val) + j;
-            const uint32_t m = cur.m;
-            double s0 = 0.0, s1 = 0.0;
-            // four entries at a time: their slot indices and coefficients first, then the
-            // four value reads together, so shared-memory latency is paid once per four
-            for (uint32_t k = 0; k < cur.L; k += 4) {
-                uint32_t c[4];
-                double v[4];
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const bool in = k + u < cur.L;
-                    c[u] = in ? col[(k + u) * m] : 0u;
-                    v[u] = in ? (double)val[(k + u) * m] : 0.0;
-                }
-                double x[4];
-#pragma unroll
-                for (int u = 0; u < 4; ++u) x[u] = xs[c[u]];
-                s0 += v[0] * x[0] + v[2] * x[2];
-                s1 += v[1] * x[1] + v[3] * x[3];
+            double s;
+            if (cur.L <= 8) s = dot_regs(cur, std::integral_constant<int, 8>{});
+            else if (cur.L <= 16) s = dot_regs(cur, std::integral_constant<int, 16>{});
+            else s = dot_regs(cur, std::integral_constant<int, 32>{});
+            if (cur.L > (uint32_t)kRegEntries) {  // rows longer than 32 entries
+                const uint16_t* col = reinterpret_cast<const uint16_t*>(ring + cur.rest) + j;
+                const Low* val = reinterpret_cast<const Low*>(ring + cur.rest + 2u * cur.L * cur.m) + j;
+                for (uint32_t k = kRegEntries; k < cur.L; ++k) s += (double)val[k * cur.m] * xs[col[k * cur.m]];
             }
-            const double s = s0 + s1;
             double res;
             if (OP == OP_DIV || OP == OP_MUL) res = (cur.vin - s) * cur.dg;  // dg = 1/diag for OP_DIV
             else if (OP == OP_NONE) res = cur.vin - s;
@@ -428,30 +419,30 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
             unsigned long long rbits = (unsigned long long)__double_as_longlong(res);
             if (res != res) rbits = kCanonicalNaN;
             if (cur.os != kNoSlot) xs[cur.os] = __longlong_as_double((long long)rbits);
-            // the result replaces the row's right-hand side; the publisher copies it out
-            reinterpret_cast<unsigned long long*>(ring + cur.base)[j] = rbits;
+            st_relaxed_u64(a.out + rb + cur.lr, rbits);
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(round_bar + r % kStrMaxRounds);
         const bool more = r + 1 < R;
-        bool have_next = false;
         if (more) {
             if (landed_seen <= r + 1) {
-                uint32_t l = 0;
-                if (lane == 0) l = ld_acquire_shared_u32(words);
-                landed_seen = __shfl_sync(0xFFFFFFFFu, l, 0);
+                // the next record normally landed long ago; otherwise wait for it here
+                const unsigned long long t0 = globaltimer_ns();
+                unsigned spins = 0;
+                bool ok = true;
+                do {
+                    uint32_t l = 0;
+                    if (lane == 0) l = ld_acquire_shared_u32(words);
+                    landed_seen = __shfl_sync(0xFFFFFFFFu, l, 0);
+                    if (landed_seen > r + 1) break;
+                    ok = !give_up(spins, t0);
+                } while (__all_sync(0xFFFFFFFFu, ok));
+                if (!__all_sync(0xFFFFFFFFu, ok)) return;
             }
-            if (landed_seen > r + 1) {
-                load_row(r + 1, nxt);
-                have_next = true;
-            }
+            load_row(r + 1, cur);
         }
         if (!wait_phase(round_bar + r % kStrMaxRounds, (r / kStrMaxRounds) & 1u)) return;
         if (threadIdx.x == 0) st_release_shared_u32(words + 1, r + 1);
-        if (more) {
-            if (have_next) cur = nxt;
-            else load_row(r + 1, cur);
-        }
     }
 }
 
