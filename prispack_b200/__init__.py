@@ -439,6 +439,11 @@ class DeviceSystem:
         _check(self.lib.prism_spmv(self.h, x, y))
         return y
 
+    def spmv_into(self, x, y):
+        """y = A x on CUDA tensors (y preallocated; no allocation in the call)."""
+        _check(self.lib.prism_spmv_device(self.h, _ptr(x), _ptr(y)))
+        return y
+
     # ---- preconditioner -------------------------------------------------------
     def set_precond(self, kind: int, *, tol: float = 1e-3, lfill: int = 20, precision: int = PRISM_FP64):
         if kind == PRECOND_NONE:

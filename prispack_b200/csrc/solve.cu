@@ -18,7 +18,8 @@ std::atomic<uint64_t>& launch_counter() {
 
 namespace {
 constexpr unsigned long long kWaitNs = 1000000000ull;  // 1 s per dependency wait
-constexpr int kSpmvG = 8;                              // lanes per row in the CSR SpMV
+constexpr int kSpmvSubG = 8;                           // lanes per row in k_spmv_sub
+constexpr int kSpmvG = 1, kSpmvU = 2;                  // k_spmv: lanes per row, rows per group and pass
 }  // namespace
 
 int vec_grid(const Handle& h, uint32_t n) {
@@ -163,12 +164,17 @@ void launch_sweep(const Handle& h, cudaStream_t st, const DevSweep& s, const dou
 void launch_spmv(const Handle& h, cudaStream_t st, uint32_t nrows, const uint32_t* rowptr, const uint32_t* col,
                  const double* val, const double* x, double* y, int sub) {
     if (!nrows) return;
-    long want = ((long)nrows * kSpmvG + kBlock - 1) / kBlock;
     long cap = (long)h.info.sms * 8;
-    int grid = (int)(want < cap ? want : cap);
     ReduceSlot none{nullptr, nullptr, nullptr};
-    if (sub) k_spmv_sub<kSpmvG><<<grid, kBlock, 0, st>>>(nrows, rowptr, col, val, x, y);
-    else k_spmv<kSpmvG, 0><<<grid, kBlock, 0, st>>>(nrows, rowptr, col, val, x, y, nullptr, nullptr, none);
+    if (sub) {
+        long want = ((long)nrows * kSpmvSubG + kBlock - 1) / kBlock;
+        k_spmv_sub<kSpmvSubG><<<(int)(want < cap ? want : cap), kBlock, 0, st>>>(nrows, rowptr, col, val, x, y);
+    } else {
+        const long rows_per_block = (long)(kBlock / 32) * (32 / kSpmvG) * kSpmvU;
+        long want = ((long)nrows + rows_per_block - 1) / rows_per_block;
+        k_spmv<kSpmvG, kSpmvU, 0><<<(int)(want < cap ? want : cap), kBlock, 0, st>>>(nrows, rowptr, col, val, x, y,
+                                                                                   nullptr, nullptr, none);
+    }
     PRISM_LAUNCHED();
 }
 
@@ -281,17 +287,18 @@ void Handle::ensure_workspace() {
 void Handle::spmv(const double* x, double* yout, int ndot, const double* z, const double* q, int scalar) {
     const uint32_t n = A.n;
     if (!n) return;
-    long want = ((long)n * kSpmvG + kBlock - 1) / kBlock;
+    const long rows_per_block = (long)(kBlock / 32) * (32 / kSpmvG) * kSpmvU;
+    long want = ((long)n + rows_per_block - 1) / rows_per_block;
     long cap = (long)info.sms * 8;
     int grid = (int)(want < cap ? want : cap);
     if (grid > Reducer::kMaxGrid) grid = Reducer::kMaxGrid;
     ReduceSlot slot = red.slot(scalar);
-    if (ndot == 0)
-        k_spmv<kSpmvG, 0><<<grid, kBlock, 0, stream>>>(n, A.rowptr.get(), A.col.get(), A.val.get(), x, yout, z, q, slot);
-    else if (ndot == 1)
-        k_spmv<kSpmvG, 1><<<grid, kBlock, 0, stream>>>(n, A.rowptr.get(), A.col.get(), A.val.get(), x, yout, z, q, slot);
-    else
-        k_spmv<kSpmvG, 2><<<grid, kBlock, 0, stream>>>(n, A.rowptr.get(), A.col.get(), A.val.get(), x, yout, z, q, slot);
+    const uint32_t* rp = A.rowptr.get();
+    const uint32_t* ci = A.col.get();
+    const double* va = A.val.get();
+    if (ndot == 0) k_spmv<kSpmvG, kSpmvU, 0><<<grid, kBlock, 0, stream>>>(n, rp, ci, va, x, yout, z, q, slot);
+    else if (ndot == 1) k_spmv<kSpmvG, kSpmvU, 1><<<grid, kBlock, 0, stream>>>(n, rp, ci, va, x, yout, z, q, slot);
+    else k_spmv<kSpmvG, kSpmvU, 2><<<grid, kBlock, 0, stream>>>(n, rp, ci, va, x, yout, z, q, slot);
     PRISM_LAUNCHED();
 }
 

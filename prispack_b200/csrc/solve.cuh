@@ -42,7 +42,7 @@ enum Scalar : int {
     SC_BB = 0, SC_RES = 1,   // written together by k_residual: Σ b², Σ (b - y)²
     SC_RR = 2,
     SC_WV = 3,
-    SC_DV = 4, SC_DR = 5,    // written together by k_spmv<.,2>: Σ v·d, Σ d·r
+    SC_DV = 4, SC_DR = 5,    // written together by k_spmv<.,.,2>: Σ v·d, Σ d·r
     SC_TMP = 6, SC_TMP2 = 7,
     SC_DR2 = 8,
     SC_H0 = 16,              // GMRES Hessenberg column h_0 .. h_{j+1}
