@@ -68,6 +68,9 @@ def parse():
     p.add_argument("--no-fp64", action="store_true", help="skip the FP64-factor comparison solve")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-sample-s", type=float, default=15.0, help="target seconds of reference CPU work")
+    p.add_argument("--config", type=int, default=2, choices=[2, 3, 5],
+                   help="2: the headline (3D Poisson, FCG + AMSED); 3: 3D convection-diffusion 100^3, "
+                        "FGMRES(50) + GMSLR; 5: differentiable 64^3 variable-coefficient diffusion")
     return p.parse_args()
 
 
@@ -189,11 +192,182 @@ class CpuReference:
 
 
 # ---------------------------------------------------------------------------
+# secondary workloads (one GPU; rank 0 only under torchrun)
+# ---------------------------------------------------------------------------
+CONVDIFF = dict(grid=100, pe=50.0, levels=4, low_rank=24, restart=50)
+
+
+def _device_ms(S, stream, fn, steps, warm):
+    import torch
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    out = [fn() for _ in range(steps)]
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    return ev0.elapsed_time(ev1) / steps, out
+
+
+def bench_convdiff(args, local):
+    """3D convection-diffusion 100^3 (central diffusion + first-order upwind
+    convection, v = (1, 0.5, 0.25) * Pe, Pe = 50), FGMRES(50) + GMSLR (4 levels,
+    rank 24, ILUT(20, 1e-2) blocks), FP32 factor values / FP64 Arnoldi, tol 1e-10;
+    the same solve with FP64 factors beside it, and the reference's own FGMRES +
+    GMSLR on the host cores."""
+    import torch
+    import prispack_b200 as PB
+    c = CONVDIFF
+    g, pe = c["grid"], c["pe"]
+    torch.cuda.set_device(local)
+    A = PB.CSRMatrix.convection_diffusion(g, g, g, pe, 0.5 * pe, 0.25 * pe)
+    b_host = np.random.default_rng(SEED).standard_normal(A.n)
+    stream = torch.cuda.current_stream()
+    res = {}
+    for name, prec in (("fp32", PB.PRISM_FP32), ("fp64", PB.PRISM_FP64)):
+        t0 = time.perf_counter()
+        G = PB.HostGmslr(A, levels=c["levels"], low_rank=c["low_rank"], precision=prec)
+        setup_s = time.perf_counter() - t0
+        S = PB.DeviceSystem(A, device=local)
+        S.set_stream(stream.cuda_stream)
+        S.attach(G)
+        b = torch.tensor(b_host, device="cuda")
+        x = torch.zeros(A.n, dtype=torch.float64, device="cuda")
+
+        def one():
+            x.zero_()
+            return S.solve(b, x, solver=PB.SOLVER_FGMRES, tol=args.tol, max_iter=1000, restart=c["restart"])[1]
+
+        ms, sts = _device_ms(S, stream, one, args.steps, args.warmup)
+        st = sts[-1]
+        res[name] = {"ms": ms, "iters": st.num_iter, "true_rel_residual": st.true_rel_residual,
+                     "converged": bool(st.converged), "host_setup_s": round(setup_s, 2), "info": G.info()}
+        if name == "fp32":
+            pin_b = torch.from_numpy(b_host).pin_memory()
+            pin_x = torch.zeros(A.n, dtype=torch.float64).pin_memory()
+            bnp, xnp = pin_b.numpy(), pin_x.numpy()
+
+            def host_one():
+                xnp[:] = 0.0
+                return S.solve(bnp, xnp, solver=PB.SOLVER_FGMRES, tol=args.tol, max_iter=1000,
+                               restart=c["restart"])[1]
+
+            res["e2e_ms"], _ = _device_ms(S, stream, host_one, max(1, args.steps), 1)
+        del S, G
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import ref
+        if ref.available(fast=True):
+            RA = ref.RefCSR.from_arrays(A.rowptr, A.col, A.val, fast=True)
+            RG = ref.RefGmslr(RA, c["levels"], 20, c["low_rank"], low_precision=True)
+            RG.setup()
+            t = time.perf_counter()
+            _, it, err, conv = ref.gmres_solve(RA, RG, b_host, tol=args.tol, restart=c["restart"], flexible=True)
+            cpu = {"value": round((time.perf_counter() - t) * 1e3, 1), "unit": "ms", "cores": 4, "kind": "reference",
+                   "sample": f"one full reference FGMRES({c['restart']}) + GMSLR solve: {it} iterations, "
+                             f"error {err:.2e}, converged {conv}; host setup excluded"}
+    r32, r64 = res["fp32"], res["fp64"]
+    info = r32["info"]
+    line = {"metric": "time-to-1e-10 rel. residual, FGMRES(50) + GMSLR, mixed FP32-factor / FP64-Arnoldi, 1 B200",
+            "value": round(r32["ms"], 3), "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(r32["ms"], 3), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 (Krylov) / f32 (factor values)", "data": "synthetic",
+            "config": {"workload": f"3D convection-diffusion {g}^3 (n={A.n}, nnz={A.nnz}), central diffusion + "
+                                   f"first-order upwind convection, v=(1,0.5,0.25)*{pe:g}, FGMRES({c['restart']}) + "
+                                   f"GMSLR ({c['levels']} levels, rank {c['low_rank']}), tol {args.tol:g}, "
+                                   f"b~N(0,1) seed {SEED}",
+                       "iterations": r32["iters"], "true_rel_residual": r32["true_rel_residual"],
+                       "converged": r32["converged"], "host_setup_s": r32["host_setup_s"],
+                       "gmslr": {"nlev": info["nlev"], "lev_ptr": info["lev_ptr"].tolist(),
+                                 "ncomps": info["ncomps"].tolist(), "ranks": info["ranks"].tolist(),
+                                 "mnnz": info["mnnz"]}},
+            "e2e": {"value": round(res["e2e_ms"], 3), "unit": "ms", "h2d_bytes_per_step": 16 * A.n,
+                    "d2h_bytes_per_step": 8 * A.n},
+            "fp64_factor": {"ms": round(r64["ms"], 3), "iters": r64["iters"],
+                            "true_rel_residual": r64["true_rel_residual"], "mixed_speedup": r64["ms"] / r32["ms"]},
+            "cpu_baseline": cpu}
+    print(json.dumps(line))
+
+
+def bench_adjoint(args, local):
+    """Differentiable solve: 3D variable-coefficient diffusion 64^3, kappa =
+    exp(g), g a Gaussian random field (sigma 1, correlation length 8 cells);
+    loss ||x - x*||^2; forward FCG + IC solve and hand-written adjoint (one
+    solve with the same preconditioner + the sampled outer product), timed
+    together; gradient wrt kappa checked against central differences
+    (h = 1e-6) on 64 random cells."""
+    import torch
+    import prispack_b200 as PB
+    from prispack_b200.autograd import DiffusionPattern, SolveSpec, gaussian_random_field, solve
+    torch.cuda.set_device(local)
+    D = DiffusionPattern(64, 64, 64)
+    kappa = np.exp(gaussian_random_field(D.shape, 1.0, 8.0, seed=SEED))
+    rng = np.random.default_rng(SEED + 1)
+    b_host, xs_host = rng.standard_normal(D.n), rng.standard_normal(D.n)
+    S = PB.DeviceSystem(D.matrix(kappa), device=local)
+    stream = torch.cuda.current_stream()
+    S.set_stream(stream.cuda_stream)
+    S.set_precond(PB.PRECOND_IC, tol=1e-3)  # factored once: every step runs with the same kappa
+    spec = SolveSpec(tol=1e-13, max_iter=5000, refactor=False)
+    b = torch.tensor(b_host, device="cuda")
+    xs = torch.tensor(xs_host, device="cuda")
+
+    def step():
+        kap = torch.tensor(kappa, device="cuda", requires_grad=True)
+        x = solve(S, D.values(kap), b, spec)
+        loss = ((x - xs) ** 2).sum()
+        loss.backward()
+        return kap.grad
+
+    ms, grads = _device_ms(S, stream, step, args.steps, args.warmup)
+    grad = grads[-1].cpu().numpy()
+    # central differences without cancellation: L+ - L- = d . (2 x- + d - 2 x*), d = x+ - x-
+    cells = rng.choice(D.n, 64, replace=False)
+    rows = np.repeat(np.arange(D.n), np.diff(D.A0.rowptr.astype(np.int64)))
+    h = 1e-6
+    fd = []
+    for m in cells:
+        kp, km = kappa.copy(), kappa.copy()
+        kp[m] += h
+        km[m] -= h
+        vp = D.values(torch.from_numpy(kp)).numpy()
+        vm = D.values(torch.from_numpy(km)).numpy()
+        S.update_values(vm)  # the factor of the unperturbed kappa stays: the solves stay exact
+        xm, _ = S.solve(b_host, tol=1e-13, max_iter=5000)
+        r = np.zeros(D.n)
+        np.add.at(r, rows, (vp - vm) * xm[D.A0.col])
+        S.update_values(vp)
+        d, _ = S.solve(-r, tol=1e-13, max_iter=5000)
+        fd.append(float(d @ (2 * xm + d - 2 * xs_host)) / (2 * h))
+    fd = np.array(fd)
+    err = np.abs(fd - grad[cells]) / np.maximum(np.abs(grad[cells]), 1e-12 * np.abs(grad).max())
+    line = {"metric": "forward + adjoint solve time, variable-coefficient diffusion, 1 B200", "value": round(ms, 3),
+            "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "3D variable-coefficient diffusion 64^3 (n=262144), kappa=exp(g), g Gaussian "
+                                   "random field (sigma 1, correlation length 8 cells), loss ||x - x*||^2, FCG + IC "
+                                   "(factored once), tol 1e-13; grad wrt kappa and b by the adjoint",
+                       "fd_check": {"cells": 64, "h": h, "max_rel_err": float(err.max()),
+                                    "median_rel_err": float(np.median(err))}}}
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.config != 2:
+        if rank != 0 or args.impl == "reference":
+            if args.impl == "reference" and rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "secondary configs carry their reference "
+                                  "timing in the prism line's cpu_baseline"}))
+            return
+        return bench_convdiff(args, local) if args.config == 3 else bench_adjoint(args, local)
 
     if args.impl == "reference":
         return reference_arm(args, rank, world)

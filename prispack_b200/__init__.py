@@ -229,6 +229,52 @@ class CSRMatrix:
         _check(lib.prism_laplacian_fill(nx, ny, nz, alphax, alphay, alphaz, shift, rp, ci, v))
         return cls(rp, ci, v)
 
+    @classmethod
+    def convection_diffusion(cls, nx, ny, nz, vx, vy, vz) -> "CSRMatrix":
+        """Steady convection-diffusion -Laplace(u) + v . grad(u) on the unit cube,
+        nx x ny x nz interior points (h = 1 / (n + 1) per axis, homogeneous
+        Dirichlet boundaries), 7-point central differences for diffusion and
+        first-order upwind differences for convection, scaled by h^2 per axis:
+        along an axis with grid spacing h and velocity v, the upstream neighbour
+        gets -(1 + h|v|), the downstream one -1, the diagonal 2 + h|v|.  A
+        nonsymmetric M-matrix with the pattern (and the row ordering, x fastest)
+        of generateLaplacianCSR(nx, ny, nz); the reference's generator offers
+        central convection only (source/MatrixClass/ModelProblem.cpp:85-93)."""
+        dims = (nx, ny, nz)
+        vel = (float(vx), float(vy), float(vz))
+        n = nx * ny * nz
+        idx = np.arange(n, dtype=np.int64)
+        coords = (idx % nx, (idx // nx) % ny, idx // (nx * ny))
+        strides = (1, nx, nx * ny)
+        rows, cols, vals = [idx], [idx], [np.zeros(n)]
+        for d in range(3):
+            if dims[d] == 1:
+                continue
+            h = 1.0 / (dims[d] + 1)
+            c = abs(vel[d]) * h
+            rows.append(idx)
+            cols.append(idx)
+            vals.append(np.full(n, 2.0 + c))
+            for sgn in (-1, 1):
+                ok = coords[d] + sgn >= 0 if sgn < 0 else coords[d] + sgn < dims[d]
+                upstream = (sgn < 0) == (vel[d] > 0)   # neighbour the flow comes from
+                w = -(1.0 + c) if upstream and vel[d] != 0.0 else -1.0
+                rows.append(idx[ok])
+                cols.append(idx[ok] + sgn * strides[d])
+                vals.append(np.full(int(ok.sum()), w))
+        r = np.concatenate(rows)
+        cc = np.concatenate(cols)
+        v = np.concatenate(vals)
+        key = r * n + cc
+        order = np.argsort(key, kind="stable")
+        key, v = key[order], v[order]
+        uk, start = np.unique(key, return_index=True)
+        vsum = np.add.reduceat(v, start)
+        rr, ccol = uk // n, uk % n
+        rowptr = np.zeros(n + 1, np.int64)
+        np.add.at(rowptr, rr + 1, 1)
+        return cls(np.cumsum(rowptr).astype(np.uint32), ccol.astype(np.uint32), vsum)
+
     def to_scipy(self):
         import scipy.sparse as sp
         return sp.csr_matrix((self.val, self.col, self.rowptr), shape=(self.n, self.n))
