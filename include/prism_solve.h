@@ -319,6 +319,23 @@ int32_t prism_solve_batched_device(prism_handle h, const prism_solve_opts* opts,
 int32_t prism_solve_batched(prism_handle h, const prism_solve_opts* opts, uint32_t k, const double* B, double* X,
                             uint64_t ld, prism_solve_stats* stats);
 
+/* ---- batches of independent systems -------------------------------------
+ * The handle's matrix holds nseg independent systems on its diagonal: rows
+ * [seg_ptr[s], seg_ptr[s+1]) couple only among themselves (PRISM_ERR_ARG
+ * otherwise; seg_ptr is a host array of nseg + 1 offsets from 0 to n).  Any
+ * IC / ILDLT / ILUT preconditioner set on the handle is then block diagonal
+ * too, and one SpMV and one pair of sweeps serve all systems.  Each system is
+ * solved with the recurrence of CG<double>::solve (source/Solver/CG.cpp:34-83)
+ * on its own scalars and stops changing once it has converged; stats[s]
+ * (nseg entries) reports its own iterations, error and true residual.  A
+ * system whose right-hand side is zero is left at x = 0, converged.  FCG / CG
+ * only.  The reference solves one system per call. */
+int32_t prism_solve_segments_device(prism_handle h, const prism_solve_opts* opts, uint32_t nseg,
+                                    const uint32_t* seg_ptr, const double* b_d, double* x_d,
+                                    prism_solve_stats* stats);
+int32_t prism_solve_segments(prism_handle h, const prism_solve_opts* opts, uint32_t nseg, const uint32_t* seg_ptr,
+                             const double* b, double* x, prism_solve_stats* stats);
+
 #ifdef __cplusplus
 }
 #endif

@@ -125,6 +125,10 @@ _SIGS = {
                                                C.POINTER(SolveStats)]),
     "prism_solve_batched": (C.c_int32, [_vp, C.POINTER(SolveOpts), C.c_uint32, _f64p, _f64p, C.c_uint64,
                                         C.POINTER(SolveStats)]),
+    "prism_solve_segments_device": (C.c_int32, [_vp, C.POINTER(SolveOpts), C.c_uint32, _u32p, _vp, _vp,
+                                                C.POINTER(SolveStats)]),
+    "prism_solve_segments": (C.c_int32, [_vp, C.POINTER(SolveOpts), C.c_uint32, _u32p, _f64p, _f64p,
+                                         C.POINTER(SolveStats)]),
     "prism_update_values": (C.c_int32, [_vp, _f64p]),
     "prism_update_values_device": (C.c_int32, [_vp, _vp]),
     "prism_adjoint_solve_device": (C.c_int32, [_vp, C.POINTER(SolveOpts), _vp, _vp, _vp, _vp, C.POINTER(SolveStats)]),
@@ -274,6 +278,18 @@ class CSRMatrix:
         rowptr = np.zeros(n + 1, np.int64)
         np.add.at(rowptr, rr + 1, 1)
         return cls(np.cumsum(rowptr).astype(np.uint32), ccol.astype(np.uint32), vsum)
+
+    @classmethod
+    def block_diagonal(cls, blocks) -> tuple:
+        """One CSR holding the given systems on its diagonal; returns (matrix, seg_ptr)."""
+        rps, cols, vals, seg = [np.zeros(1, np.int64)], [], [], [0]
+        for B in blocks:
+            rps.append(B.rowptr[1:].astype(np.int64) + rps[-1][-1])
+            cols.append(B.col.astype(np.int64) + seg[-1])
+            vals.append(B.val)
+            seg.append(seg[-1] + B.n)
+        return (cls(np.concatenate(rps).astype(np.uint32), np.concatenate(cols).astype(np.uint32),
+                    np.concatenate(vals)), np.array(seg, np.uint32))
 
     def to_scipy(self):
         import scipy.sparse as sp
@@ -620,6 +636,24 @@ class DeviceSystem:
         st = (SolveStats * k)()
         _check(self.lib.prism_solve_batched(self.h, C.byref(opts), k, Bh.reshape(-1), Xh.reshape(-1), self.n, st))
         return Xh, list(st)
+
+    def solve_segments(self, seg_ptr, b, x=None, *, solver=SOLVER_FCG, tol=1e-8, max_iter=1000) -> tuple:
+        """Solves the independent systems on the diagonal blocks [seg_ptr[s], seg_ptr[s+1])
+        of A at once; returns (x, [SolveStats] per system).  Device tensors or host arrays."""
+        sp = np.ascontiguousarray(seg_ptr, np.uint32)
+        nseg = len(sp) - 1
+        opts = SolveOpts(solver, tol, max_iter, 0)
+        st = (SolveStats * nseg)()
+        if hasattr(b, "is_cuda"):
+            import torch
+            bc = b.contiguous()
+            xc = torch.zeros_like(bc) if x is None else x
+            _check(self.lib.prism_solve_segments_device(self.h, C.byref(opts), nseg, sp, _ptr(bc), _ptr(xc), st))
+            return xc, list(st)
+        bh = np.ascontiguousarray(b, np.float64)
+        xh = np.zeros(self.n) if x is None else np.array(x, np.float64, copy=True)
+        _check(self.lib.prism_solve_segments(self.h, C.byref(opts), nseg, sp, bh, xh, st))
+        return xh, list(st)
 
     def solve(self, b, x=None, *, solver=SOLVER_FCG, tol=1e-8, max_iter=1000, restart=0) -> tuple:
         """x (in/out initial guess) solved in place; returns (x, SolveStats)."""

@@ -864,4 +864,37 @@ int32_t prism_solve_batched(prism_handle h, const prism_solve_opts* opts, uint32
     });
 }
 
+int32_t prism_solve_segments_device(prism_handle h, const prism_solve_opts* opts, uint32_t nseg,
+                                    const uint32_t* seg_ptr, const double* b_d, double* x_d,
+                                    prism_solve_stats* stats) {
+    int rc = check_opts(h, opts);
+    if (!rc) rc = check_block_solver(opts);
+    if (rc) return rc;
+    if (!seg_ptr || !b_d || !x_d) return fail(PRISM_ERR_ARG, "null argument");
+    return guarded([&]() -> int {
+        DeviceGuard g(h->info.device);
+        prism::segmented_fcg_solve(*h, *opts, nseg, seg_ptr, b_d, x_d, stats);
+        return PRISM_OK;
+    });
+}
+
+int32_t prism_solve_segments(prism_handle h, const prism_solve_opts* opts, uint32_t nseg, const uint32_t* seg_ptr,
+                             const double* b, double* x, prism_solve_stats* stats) {
+    int rc = check_opts(h, opts);
+    if (!rc) rc = check_block_solver(opts);
+    if (rc) return rc;
+    if (!seg_ptr || !b || !x) return fail(PRISM_ERR_ARG, "null argument");
+    return guarded([&]() -> int {
+        DeviceGuard g(h->info.device);
+        const uint32_t n = h->A.n;
+        prism::DevBuf<double> bd(n), xd(n);
+        PRISM_CUDA(cudaMemcpyAsync(bd.get(), b, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        PRISM_CUDA(cudaMemcpyAsync(xd.get(), x, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        prism::segmented_fcg_solve(*h, *opts, nseg, seg_ptr, bd.get(), xd.get(), stats);
+        PRISM_CUDA(cudaMemcpyAsync(x, xd.get(), n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        PRISM_CUDA(cudaStreamSynchronize(h->stream));
+        return PRISM_OK;
+    });
+}
+
 }  // extern "C"

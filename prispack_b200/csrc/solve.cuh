@@ -191,6 +191,8 @@ class AmsedPrecond : public Precond {
 
 struct BatchWork;                  // block-of-RHS workspace (batched.cu)
 void batch_release(BatchWork* w);
+struct SegWork;                    // batch-of-systems workspace (segments.cu)
+void seg_release(SegWork* w);
 
 struct Handle {
     DeviceInfo info;
@@ -209,6 +211,7 @@ struct Handle {
     static constexpr uint32_t kScalarCapacity = kNumScalars + kMaxKrylov + 2;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::unique_ptr<BatchWork, void (*)(BatchWork*)> batch{nullptr, batch_release};
+    std::unique_ptr<SegWork, void (*)(SegWork*)> seg{nullptr, seg_release};
     int symmetric = -1;            // A == A^T exactly: -1 not yet checked, 0 no, 1 yes
 
     ~Handle();
@@ -251,5 +254,8 @@ void gmres_solve(Handle& h, const prism_solve_opts& o, const double* b, double* 
 void batched_apply(Handle& h, uint32_t k, const double* in_d, double* out_d, uint64_t ld);
 void batched_fcg_solve(Handle& h, const prism_solve_opts& o, uint32_t k, const double* B_d, double* X_d, uint64_t ld,
                        prism_solve_stats* st);
+// independent systems on the diagonal blocks [seg_ptr[s], seg_ptr[s+1]) of the handle's matrix (segments.cu)
+void segmented_fcg_solve(Handle& h, const prism_solve_opts& o, uint32_t nseg, const uint32_t* seg_ptr,
+                         const double* b, double* x, prism_solve_stats* st);
 
 }  // namespace prism
