@@ -68,9 +68,10 @@ def parse():
     p.add_argument("--no-fp64", action="store_true", help="skip the FP64-factor comparison solve")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-sample-s", type=float, default=15.0, help="target seconds of reference CPU work")
-    p.add_argument("--config", type=int, default=2, choices=[2, 3, 5],
+    p.add_argument("--config", type=int, default=2, choices=[2, 3, 4, 5],
                    help="2: the headline (3D Poisson, FCG + AMSED); 3: 3D convection-diffusion 100^3, "
-                        "FGMRES(50) + GMSLR; 5: differentiable 64^3 variable-coefficient diffusion")
+                        "FGMRES(50) + GMSLR; 4: batched solves (64 RHS on 2D 512^2 + 256 uneven 2D systems); "
+                        "5: differentiable 64^3 variable-coefficient diffusion")
     return p.parse_args()
 
 
@@ -354,6 +355,126 @@ def bench_adjoint(args, local):
     print(json.dumps(line))
 
 
+def bench_batched(args, local):
+    """Batched solves, FCG + ICT(1e-3) with FP32 factor values, tol 1e-10:
+    (a) 2D Poisson 512^2 with a block of 64 random-normal right-hand sides,
+    one block solve (prism_solve_batched) against 64 solves one after another;
+    (b) 256 independent 2D Poisson systems on grids with sides drawn uniformly
+    from 32..256, assembled on the diagonal of one CSR and solved together
+    (prism_solve_segments) against solving a sample of them one by one.  The
+    reference solves one right-hand side and one system per call: its CPU time
+    is estimated from a sample of single solves."""
+    import torch
+    import prispack_b200 as PB
+    torch.cuda.set_device(local)
+    stream = torch.cuda.current_stream()
+    rng = np.random.default_rng(SEED)
+    tol = args.tol
+    # ---- (a) block of 64 right-hand sides
+    A = PB.CSRMatrix.laplacian(512, 512, 1)
+    k = 64
+    S = PB.DeviceSystem(A, device=local)
+    S.set_stream(stream.cuda_stream)
+    S.set_precond(PB.PRECOND_IC, tol=1e-3, precision=PB.PRISM_FP32)
+    B = torch.tensor(rng.standard_normal((k, A.n)), device="cuda")
+
+    def block():
+        return S.solve_batched(B, tol=tol, max_iter=1000)[1]
+
+    block_ms, bst = _device_ms(S, stream, block, max(1, args.steps // 2), 1)
+    bst = bst[-1]
+    x0 = torch.zeros(A.n, dtype=torch.float64, device="cuda")
+
+    def single():
+        x0.zero_()
+        return S.solve(B[0], x0, tol=tol, max_iter=1000)[1]
+
+    single_ms, sst = _device_ms(S, stream, single, max(1, args.steps), 1)
+    # ---- (b) 256 uneven systems
+    sides = rng.integers(32, 257, size=256)
+    blocks = [PB.CSRMatrix.laplacian(int(q), int(q), 1) for q in sides]
+    Ab, seg = PB.CSRMatrix.block_diagonal(blocks)
+    t0 = time.perf_counter()
+    Sb = PB.DeviceSystem(Ab, device=local)
+    Sb.set_stream(stream.cuda_stream)
+    Sb.set_precond(PB.PRECOND_IC, tol=1e-3, precision=PB.PRISM_FP32)
+    setup_s = time.perf_counter() - t0
+    bb = torch.tensor(rng.standard_normal(Ab.n), device="cuda")
+    xb = torch.zeros_like(bb)
+
+    def segs():
+        xb.zero_()
+        return Sb.solve_segments(seg, bb, xb, tol=tol, max_iter=1000)[1]
+
+    seg_ms, segst = _device_ms(Sb, stream, segs, max(1, args.steps // 2), 1)
+    segst = segst[-1]
+    # one-by-one on a sample of the systems (device solves, handles set up outside the timing)
+    sample = rng.choice(256, 24, replace=False)
+    one_ms, one_rows = 0.0, 0
+    for q in sample:
+        Sq = PB.DeviceSystem(blocks[q], device=local)
+        Sq.set_stream(stream.cuda_stream)
+        Sq.set_precond(PB.PRECOND_IC, tol=1e-3, precision=PB.PRISM_FP32)
+        bq = bb[seg[q]:seg[q + 1]].clone()
+        xq = torch.zeros_like(bq)
+
+        def one():
+            xq.zero_()
+            return Sq.solve(bq, xq, tol=tol, max_iter=1000)[1]
+
+        ms, _ = _device_ms(Sq, stream, one, 2, 1)
+        one_ms += ms
+        one_rows += blocks[q].n
+        del Sq
+    one_by_one_est = one_ms * Ab.n / one_rows
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import ref
+        if ref.available(fast=True):
+            RA = ref.RefCSR.laplacian(512, 512, 1, fast=True)
+            RP = ref.RefPrecond(RA, ref.KIND_IC, True, 1e-3)
+            RP.setup()
+            t = time.perf_counter()
+            it = ref.cg_solve(RA, RP, B[0].cpu().numpy(), tol=tol, maxit=1000, flexible=True)[1]
+            per_rhs = time.perf_counter() - t
+            cpu_rows, cpu_s = 0, 0.0
+            for q in sample[:8]:
+                Bq = blocks[q]
+                Rq = ref.RefCSR.from_arrays(Bq.rowptr, Bq.col, Bq.val, fast=True)
+                Pq = ref.RefPrecond(Rq, ref.KIND_IC, True, 1e-3)
+                Pq.setup()
+                t = time.perf_counter()
+                ref.cg_solve(Rq, Pq, bb[seg[q]:seg[q + 1]].cpu().numpy(), tol=tol, maxit=1000, flexible=True)
+                cpu_s += time.perf_counter() - t
+                cpu_rows += Bq.n
+            est = (per_rhs * k + cpu_s * Ab.n / cpu_rows) * 1e3
+            cpu = {"value": round(est, 1), "unit": "ms", "cores": 4, "kind": "reference",
+                   "sample": f"one reference FCG + ICT solve of the 512^2 system ({it} iterations, "
+                             f"{per_rhs:.2f} s) times 64, plus 8 of the uneven systems scaled by rows to all 256; "
+                             "setup excluded"}
+    total = block_ms + seg_ms
+    its = [q.num_iter for q in segst]
+    line = {"metric": "batched time-to-1e-10: 64 RHS on 2D Poisson 512^2 + 256 uneven 2D Poisson systems, 1 B200",
+            "value": round(total, 3), "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(total, 3), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 (Krylov) / f32 (factor values)", "data": "synthetic",
+            "config": {"workload": "FCG + ICT(1e-3), FP32 factor values, tol 1e-10; (a) 2D Poisson 512^2 "
+                                   "(n=262144) with 64 N(0,1) right-hand sides; (b) 256 2D Poisson systems, sides "
+                                   f"U{{32..256}} seed {SEED} (total n={Ab.n}, nnz={Ab.nnz})",
+                       "block_of_64": {"ms": round(block_ms, 3), "iters": [q.num_iter for q in bst][:4] + ["..."],
+                                       "all_converged": all(q.converged for q in bst),
+                                       "one_rhs_alone_ms": round(single_ms, 3),
+                                       "speedup_vs_64_single": round(64 * single_ms / block_ms, 2)},
+                       "uneven_256": {"ms": round(seg_ms, 3), "iters_min_max": [min(its), max(its)],
+                                      "all_converged": all(q.converged for q in segst),
+                                      "max_true_rel_residual": max(q.true_rel_residual for q in segst),
+                                      "one_by_one_est_ms": round(one_by_one_est, 1),
+                                      "speedup_vs_one_by_one": round(one_by_one_est / seg_ms, 2),
+                                      "host_setup_s": round(setup_s, 1)}},
+            "cpu_baseline": cpu}
+    print(json.dumps(line))
+
+
 # ---------------------------------------------------------------------------
 def main():
     args = parse()
@@ -367,7 +488,7 @@ def main():
                 print(json.dumps({"impl": "reference", "unavailable": "secondary configs carry their reference "
                                   "timing in the prism line's cpu_baseline"}))
             return
-        return bench_convdiff(args, local) if args.config == 3 else bench_adjoint(args, local)
+        return {3: bench_convdiff, 4: bench_batched, 5: bench_adjoint}[args.config](args, local)
 
     if args.impl == "reference":
         return reference_arm(args, rank, world)
