@@ -39,7 +39,9 @@ METRIC = "time-to-1e-10 rel. residual, mixed FP32-factor / FP64-Krylov, 1 B200"
 # wavefronts of the RCM order at the same iteration count.
 AMSED = dict(levels=3, lanczos_steps=64, low_rank=32, eig_bound=0.8, lowrank_type=0, lanczos_type=0, reorder=0)
 SEED = 2024
-TRAFFIC_RATIO = 181.2 / 183.6   # measured DRAM / algorithmic bytes of the level-0 sweep (ncu, 96^3)
+# measured DRAM / algorithmic bytes of the level-0 lower sweep at 96^3, per sweep kernel (one ncu capture each;
+# profiles/k_sweep_level0_lower_96cube.md, profiles/k_sweep_stream_level0_lower_96cube.md)
+TRAFFIC_RATIO = {"level-order": 181.2 / 183.6, "stream": 186.4 / 183.6}
 
 
 def workload(grid: int, tol: float, precond: str) -> str:
@@ -68,6 +70,9 @@ def parse():
     p.add_argument("--no-fp64", action="store_true", help="skip the FP64-factor comparison solve")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-sample-s", type=float, default=15.0, help="target seconds of reference CPU work")
+    p.add_argument("--only-sweep", default=None, choices=["global", "stream"],
+                   help="profiling aid: set up the workload with this sweep layout forced, run the level-0 "
+                        "lower sweep of the preconditioner four times and the SpMV twice, and exit (no JSON line)")
     p.add_argument("--config", type=int, default=2, choices=[2, 3, 4, 5],
                    help="2: the headline (3D Poisson, FCG + AMSED); 3: 3D convection-diffusion 100^3, "
                         "FGMRES(50) + GMSLR; 4: batched solves (64 RHS on 2D 512^2 + 256 uneven 2D systems); "
@@ -496,6 +501,26 @@ def main():
     import torch
     import prispack_b200 as PB
 
+    if args.only_sweep:
+        os.environ["PRISM_SWEEP_KERNEL"] = args.only_sweep
+        torch.cuda.set_device(local)
+        A = PB.CSRMatrix.laplacian(args.grid, args.grid, args.grid)
+        S = PB.DeviceSystem(A, device=local)
+        S.set_stream(torch.cuda.current_stream().cuda_stream)
+        S.attach(build_precond(PB, A, args.precond, PB.PRISM_FP32))
+        info = S.sweep_info(0)
+        vin = torch.tensor(np.random.default_rng(SEED).standard_normal(info["n"]), device="cuda")
+        vout = torch.empty_like(vin)
+        for _ in range(4):
+            S.sweep_device(0, vin, vout, 1)
+        x = torch.tensor(np.random.default_rng(SEED).standard_normal(A.n), device="cuda")
+        y = torch.empty_like(x)
+        for _ in range(2):
+            S.spmv_into(x, y)
+        torch.cuda.synchronize()
+        print(f"sweep 0: {info}", file=sys.stderr)
+        return
+
     torch.cuda.set_device(local)
     dist = None
     if world > 1:
@@ -673,12 +698,12 @@ def main():
                          "bytes_per_launch": sweep_bytes, "launch_ms": [round(t, 4) for t in sweep_ms],
                          "rows": [i["n"] for i in sweep_infos], "wavefronts": [i["levels"] for i in sweep_infos],
                          "kernels": [i["kernel"] for i in sweep_infos],
-                         # DRAM bytes per launch: the ratio dram__bytes_read+write / algorithmic bytes
-                         # of one ncu --set full capture of this sweep kernel on the 96^3 case (0.987),
-                         # scaled to this launch's algorithmic bytes
-                         "traffic": round(TRAFFIC_RATIO * statistics.mean(sweep_bytes)),
-                         "traffic_source": "ncu capture at 96^3 (181.2 MB DRAM / 183.6 MB algorithmic), "
-                                           "scaled by rows"},
+                         # DRAM bytes per launch: the ratio DRAM / algorithmic bytes of one ncu capture
+                         # of each sweep kernel on the 96^3 case, applied to this launch's algorithmic bytes
+                         "traffic": round(statistics.mean(TRAFFIC_RATIO.get(i["kernel"], 1.0) * b_
+                                                          for i, b_ in zip(sweep_infos, sweep_bytes))),
+                         "traffic_source": "ncu captures at 96^3 (level-order 181.2 MB, streamed 186.4 MB DRAM "
+                                           "per 183.6 MB algorithmic), scaled by rows"},
             "spmv": {"ms": round(statistics.median(spmv_ms), 4), "bytes": spmv_bytes, "GB/s": round(spmv_gbs, 1),
                      "frac": round(spmv_gbs / peak, 4)},
             "fp64_factor": fp64,
