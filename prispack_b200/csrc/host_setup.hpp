@@ -138,7 +138,7 @@ void slab_layout(const Sweep<Low>& s, uint32_t num_ctas, uint32_t rows_per_cta, 
 #else
 #define PRISM_HD
 #endif
-constexpr uint32_t kRoundRows = 64;
+constexpr uint32_t kRoundRows = 128;
 constexpr uint32_t kNoSlot = 0xFFFFu;
 struct RoundRec {
     uint32_t m, in, diag, lrow, oslot, col, val, xrow, xslot, xwait, bytes;

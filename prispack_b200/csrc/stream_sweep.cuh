@@ -6,7 +6,7 @@
 // Why.  A sweep is a chain of dependency wavefronts (about 2,000 for the
 // level-0 ILDLT factor of 3D Poisson 128^3).  When every dependency crosses
 // the L2 (k_sweep), each wavefront costs about two L2 round trips.  Here a
-// slab computes its rows in rounds of up to 64 mutually independent rows,
+// slab computes its rows in rounds of up to 128 mutually independent rows,
 // one thread per row, reading every dependency from a shared-memory value
 // slot, with an mbarrier between rounds, so the chain inside a slab costs a
 // few shared-memory reads and a barrier phase per round.  The L2 is kept off
@@ -17,18 +17,19 @@
 // ones) are copied into their slots by prefetcher warps as soon as they are
 // finished, while the slab is still working on earlier rounds.
 //
-// Roles (384 threads; the polling warps sleep between polls so that the row
+// Roles (352 threads; the polling warps sleep between polls so that the row
 // threads, which carry the dependency chain, keep the issue slots):
-//   warps 0..1    row threads: thread j computes row j of each round, then each
-//                 warp arrives on the round's mbarrier and waits for it.
-//   warps 2..9    prefetchers: warp 2+k handles rounds k, k+8, ...: it waits
+//   warps 0..3    row threads: thread j computes row j of each round, then each
+//                 warp arrives on the round's mbarrier and waits for it.  A
+//                 wavefront of a slab rarely holds more than 128 rows, so a
+//                 slab's chain of rounds is about as long as its chain of levels.
+//   warps 4..9    prefetchers: warp 4+k handles rounds k, k+6, ...: it waits
 //                 until the round's record has landed, polls each new halo row
 //                 in global memory until it is finished, waits until the slot's
 //                 previous value has had its last reader (xwait), writes the
 //                 slot and arrives on the barrier that ends the round before,
 //                 whose phase therefore also means "the next round's halo is in".
-//   warp 10       idle.
-//   warp 11       producer: issues the bulk copies of the records into the
+//   warp 10       producer: issues the bulk copies of the records into the
 //                 ring in order, publishes how many have landed, and recycles
 //                 the ring space of finished rounds.
 //
@@ -54,9 +55,8 @@
 namespace prism {
 
 constexpr int kStrRowWarps = (int)kRoundRows / 32;     // row threads: one per row of a round
-constexpr int kStrPrefetchWarps = 8;                   // warps kStrRowWarps .. kStrPublisher - 1
-constexpr int kStrPublisher = kStrRowWarps + kStrPrefetchWarps;
-constexpr int kStrProducer = kStrPublisher + 1;
+constexpr int kStrPrefetchWarps = 6;                   // warps kStrRowWarps .. kStrProducer - 1
+constexpr int kStrProducer = kStrRowWarps + kStrPrefetchWarps;
 constexpr int kStrThreads = 32 * (kStrProducer + 1);
 constexpr uint32_t kStrMaxRounds = 64;                 // rounds in flight (ring table slots)
 // copy barriers, round barriers, start barrier (+pad), ring offsets, words
@@ -251,11 +251,9 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
         return;
     }
 
-    if (warp == kStrPublisher) return;  // results go to global memory from the row threads
-
     if (warp >= kStrRowWarps) {
         // ------------------------------------------------------------------ prefetchers
-        // Warp k copies in the halo of rounds k, k + 8, ... and then arrives on the barrier
+        // Warp k copies in the halo of rounds k, k + 6, ... and then arrives on the barrier
         // that ends the round before (start_bar for round 0).  That barrier's previous phase
         // (64 rounds earlier) is over: the record of round q is in the ring only once round
         // q - 64 is done.  Round R is a stand-in that only arrives.
@@ -365,7 +363,7 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
         w.dg = reinterpret_cast<const double*>(base + rec.diag)[j];
         w.os = reinterpret_cast<const uint16_t*>(base + rec.oslot)[j];
         w.lr = reinterpret_cast<const uint16_t*>(base + rec.lrow)[j];
-        // only as many register entries as the round's longest row needs (8, 16 or 32)
+        // only as many register entries as the round's longest row needs (8, 16, 24, 28 or 32)
         auto fill = [&](auto nconst) {
             constexpr int N = decltype(nconst)::value;
 #pragma unroll
@@ -377,6 +375,8 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
         };
         if (w.L <= 8) fill(std::integral_constant<int, 8>{});
         else if (w.L <= 16) fill(std::integral_constant<int, 16>{});
+        else if (w.L <= 24) fill(std::integral_constant<int, 24>{});
+        else if (w.L <= 28) fill(std::integral_constant<int, 28>{});
         else fill(std::integral_constant<int, 32>{});
     };
     // sum of the first N register entries (N a multiple of 4): value reads first, then four chains
@@ -406,6 +406,8 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
             double s;
             if (cur.L <= 8) s = dot_regs(cur, std::integral_constant<int, 8>{});
             else if (cur.L <= 16) s = dot_regs(cur, std::integral_constant<int, 16>{});
+            else if (cur.L <= 24) s = dot_regs(cur, std::integral_constant<int, 24>{});
+            else if (cur.L <= 28) s = dot_regs(cur, std::integral_constant<int, 28>{});
             else s = dot_regs(cur, std::integral_constant<int, 32>{});
             if (cur.L > (uint32_t)kRegEntries) {  // rows longer than 32 entries
                 const uint16_t* col = reinterpret_cast<const uint16_t*>(ring + cur.rest) + j;
