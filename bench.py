@@ -294,7 +294,7 @@ def bench_convdiff(args, local):
             "fp64_factor": {"ms": round(r64["ms"], 3), "iters": r64["iters"],
                             "true_rel_residual": r64["true_rel_residual"], "mixed_speedup": r64["ms"] / r32["ms"]},
             "cpu_baseline": cpu}
-    print(json.dumps(line))
+    emit(line)
 
 
 def bench_adjoint(args, local):
@@ -357,7 +357,7 @@ def bench_adjoint(args, local):
                                    "(factored once), tol 1e-13; grad wrt kappa and b by the adjoint",
                        "fd_check": {"cells": 64, "h": h, "max_rel_err": float(err.max()),
                                     "median_rel_err": float(np.median(err))}}}
-    print(json.dumps(line))
+    emit(line)
 
 
 def bench_batched(args, local):
@@ -477,12 +477,31 @@ def bench_batched(args, local):
                                       "speedup_vs_one_by_one": round(one_by_one_est / seg_ms, 2),
                                       "host_setup_s": round(setup_s, 1)}},
             "cpu_baseline": cpu}
-    print(json.dumps(line))
+    emit(line)
 
 
 # ---------------------------------------------------------------------------
+_JSON_OUT = None
+
+
+def quiet_stdout():
+    """The reference library prints its setup progress to stdout; route fd 1 to
+    stderr for the whole run so that stdout carries the JSON line alone."""
+    global _JSON_OUT
+    sys.stdout.flush()
+    _JSON_OUT = os.fdopen(os.dup(1), "w")
+    os.dup2(2, 1)
+
+
+def emit(obj):
+    out = _JSON_OUT if _JSON_OUT is not None else sys.stdout
+    out.write(json.dumps(obj) + "\n")
+    out.flush()
+
+
 def main():
     args = parse()
+    quiet_stdout()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -490,8 +509,8 @@ def main():
     if args.config != 2:
         if rank != 0 or args.impl == "reference":
             if args.impl == "reference" and rank == 0:
-                print(json.dumps({"impl": "reference", "unavailable": "secondary configs carry their reference "
-                                  "timing in the prism line's cpu_baseline"}))
+                emit({"impl": "reference", "unavailable": "secondary configs carry their reference "
+                      "timing in the prism line's cpu_baseline"})
             return
         return {3: bench_convdiff, 4: bench_batched, 5: bench_adjoint}[args.config](args, local)
 
@@ -711,7 +730,7 @@ def main():
             "gpu_launches": int(launches / max(args.steps, 1)) * args.steps,
             "clocks": clk,
         }
-        print(json.dumps(line))
+        emit(line)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -741,7 +760,7 @@ def reference_arm(args, rank, world):
             "e2e": {"value": round(v, 3), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     if not ref.available(fast=True):
         line["note"] = "reference build absent on this host: the oracle port was timed"
-    print(json.dumps(line))
+    emit(line)
 
 
 if __name__ == "__main__":
