@@ -61,7 +61,14 @@ typedef enum prism_status {
 
 typedef enum prism_precision {
     PRISM_FP64 = 0,               /* factor values stored in double (<double,double> instantiation) */
-    PRISM_FP32 = 1                /* factor values stored in float  (<float,double> instantiation) */
+    PRISM_FP32 = 1,               /* factor values stored in float  (<float,double> instantiation) */
+    PRISM_FP32_APPLY = 2          /* float factor values and single-precision arithmetic inside the
+                                     triangular sweeps of the streamed kernel (right-hand side and
+                                     1/diag rounded to float, products and sums in float, results
+                                     widened to double); everything outside the sweeps, and sweeps
+                                     the streamed layout does not fit or block solves run, stays in
+                                     double.  No reference counterpart: the reference's float
+                                     instantiation computes in double. */
 } prism_precision;
 
 typedef enum prism_precond_kind {

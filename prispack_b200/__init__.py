@@ -19,6 +19,8 @@ LIB_PATH = os.path.join(_HERE, "_lib", "libprism_solve.so")
 
 # ---- enums (include/prism_solve.h) ------------------------------------------------
 PRISM_FP64, PRISM_FP32 = 0, 1
+# float factor values and single-precision arithmetic inside the streamed triangular sweeps
+PRISM_FP32_APPLY = 2
 PRECOND_NONE, PRECOND_IC, PRECOND_ILUT, PRECOND_ILDLT, PRECOND_GMSLR, PRECOND_AMSED = range(6)
 SOLVER_FCG, SOLVER_CG, SOLVER_FGMRES, SOLVER_GMRES = range(4)
 # reference spellings (include/Solver/CG.h:14-18, include/Solver/GMRES.h:15-18)

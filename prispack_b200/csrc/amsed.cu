@@ -131,8 +131,8 @@ void AmsedPrecond::build(const AmsedSetup<Low>& S) {
             D.nfac = D.nb;
             ildlt_sweeps<Low>(Lt, Dg, lo, up);
         }
-        tune_sweep<Low>(h_, D.lower, lo);
-        tune_sweep<Low>(h_, D.upper, up);
+        tune_sweep<Low>(h_, D.lower, lo, a_->apply32);
+        tune_sweep<Low>(h_, D.upper, up, a_->apply32);
         if (l + 1 < nlev_) {
             upload_csr(D.E, L.E.n, L.E.rowptr, L.E.col, L.E.val, st);
             if (gmslr_) {

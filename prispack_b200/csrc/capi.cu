@@ -75,10 +75,13 @@ static prism::AmsedOptions to_options(const prism_amsed_opts* o) {
     return a;
 }
 
+static bool valid_precision(int32_t p) { return p == PRISM_FP64 || p == PRISM_FP32 || p == PRISM_FP32_APPLY; }
+
 static std::shared_ptr<prism::HostAmsed> build_amsed(const prism::CsrHost& A, const prism_amsed_opts* o,
                                                      int32_t precision, int* rc, std::string* err, int family = 5) {
     auto h = std::make_shared<prism::HostAmsed>();
-    h->fp32 = precision == PRISM_FP32;
+    h->fp32 = precision != PRISM_FP64;
+    h->apply32 = precision == PRISM_FP32_APPLY;
     h->opt = to_options(o);
     h->opt.family = family;
     if (h->fp32) {
@@ -93,14 +96,15 @@ static std::shared_ptr<prism::HostAmsed> build_amsed(const prism::CsrHost& A, co
 
 static int32_t set_tri(prism_handle h, int kind, double tol, uint32_t lfill, int32_t precision) {
     if (!h) return fail(PRISM_ERR_ARG, "null handle");
-    if (precision != PRISM_FP64 && precision != PRISM_FP32) return fail(PRISM_ERR_ARG, "precision must be PRISM_FP64 or PRISM_FP32");
+    if (!valid_precision(precision)) return fail(PRISM_ERR_ARG, "precision must be PRISM_FP64, PRISM_FP32 or PRISM_FP32_APPLY");
     return guarded([&]() -> int {
         DeviceGuard g(h->info.device);
         h->P.reset();
         auto f = std::make_shared<prism::HostFactor>();
         std::string err;
-        int rc = prism::build_triangular(kind, h->A_host, tol, lfill, precision == PRISM_FP32, *f, &err);
+        int rc = prism::build_triangular(kind, h->A_host, tol, lfill, precision != PRISM_FP64, *f, &err);
         if (rc) return fail(rc, err);
+        f->apply32 = precision == PRISM_FP32_APPLY;
         h->P = std::make_unique<prism::TriangularPrecond>(*h, std::move(f));
         return PRISM_OK;
     });
@@ -165,7 +169,7 @@ int32_t prism_selftest_stream_layout(uint32_t n, const uint32_t* rowptr, const u
             for (uint32_t k = rowptr[r]; k < rowptr[r + 1]; ++k)
                 if (col[k] >= n || (lower ? col[k] >= r : col[k] <= r))
                     return fail(PRISM_ERR_ARG, "dependency on the wrong side of the diagonal");
-        if (precision == PRISM_FP32)
+        if (precision != PRISM_FP64)
             return stream_selftest<float>(n, rowptr, col, val, diag, op, lower != 0, num_ctas, rows_per_cta, in, out);
         return stream_selftest<double>(n, rowptr, col, val, diag, op, lower != 0, num_ctas, rows_per_cta, in, out);
     });
@@ -342,7 +346,7 @@ void prism_amsed_default_opts(prism_amsed_opts* o) {
 
 int32_t prism_set_precond_amsed(prism_handle h, const prism_amsed_opts* o, int32_t precision) {
     if (!h || !o) return fail(PRISM_ERR_ARG, "null argument");
-    if (precision != PRISM_FP64 && precision != PRISM_FP32) return fail(PRISM_ERR_ARG, "bad precision");
+    if (!valid_precision(precision)) return fail(PRISM_ERR_ARG, "bad precision");
     return guarded([&]() -> int {
         DeviceGuard g(h->info.device);
         h->P.reset();
@@ -366,7 +370,7 @@ void prism_gmslr_default_opts(prism_amsed_opts* o) {
 
 int32_t prism_set_precond_gmslr(prism_handle h, const prism_amsed_opts* o, int32_t precision) {
     if (!h || !o) return fail(PRISM_ERR_ARG, "null argument");
-    if (precision != PRISM_FP64 && precision != PRISM_FP32) return fail(PRISM_ERR_ARG, "bad precision");
+    if (!valid_precision(precision)) return fail(PRISM_ERR_ARG, "bad precision");
     return guarded([&]() -> int {
         DeviceGuard g(h->info.device);
         h->P.reset();
@@ -384,7 +388,7 @@ int32_t prism_factor_create_gmslr(uint32_t n, const uint32_t* rowptr, const uint
     if (!out || !o) return fail(PRISM_ERR_ARG, "null argument");
     *out = nullptr;
     if (n == 0 || !rowptr || !col || !val) return fail(PRISM_ERR_ARG, "empty or null CSR");
-    if (precision != PRISM_FP64 && precision != PRISM_FP32) return fail(PRISM_ERR_ARG, "bad precision");
+    if (!valid_precision(precision)) return fail(PRISM_ERR_ARG, "bad precision");
     std::string bad = prism::validate_csr(n, rowptr, col);
     if (!bad.empty()) return fail(PRISM_ERR_BAD_MATRIX, bad);
     return guarded([&]() -> int {
@@ -407,7 +411,7 @@ int32_t prism_factor_create_amsed(uint32_t n, const uint32_t* rowptr, const uint
     if (!out || !o) return fail(PRISM_ERR_ARG, "null argument");
     *out = nullptr;
     if (n == 0 || !rowptr || !col || !val) return fail(PRISM_ERR_ARG, "empty or null CSR");
-    if (precision != PRISM_FP64 && precision != PRISM_FP32) return fail(PRISM_ERR_ARG, "bad precision");
+    if (!valid_precision(precision)) return fail(PRISM_ERR_ARG, "bad precision");
     std::string bad = prism::validate_csr(n, rowptr, col);
     if (!bad.empty()) return fail(PRISM_ERR_BAD_MATRIX, bad);
     return guarded([&]() -> int {
@@ -544,7 +548,7 @@ int32_t prism_factor_create(int32_t kind, uint32_t n, const uint32_t* rowptr, co
     if (n == 0 || !rowptr || !col || !val) return fail(PRISM_ERR_ARG, "empty or null CSR");
     if (kind != PRISM_PRECOND_IC && kind != PRISM_PRECOND_ILUT && kind != PRISM_PRECOND_ILDLT)
         return fail(PRISM_ERR_UNSUPPORTED, "kind must be IC, ILUT or ILDLT");
-    if (precision != PRISM_FP64 && precision != PRISM_FP32) return fail(PRISM_ERR_ARG, "bad precision");
+    if (!valid_precision(precision)) return fail(PRISM_ERR_ARG, "bad precision");
     std::string bad = prism::validate_csr(n, rowptr, col);
     if (!bad.empty()) return fail(PRISM_ERR_BAD_MATRIX, bad);
     return guarded([&]() -> int {
@@ -555,7 +559,8 @@ int32_t prism_factor_create(int32_t kind, uint32_t n, const uint32_t* rowptr, co
         A.val.assign(val, val + rowptr[n]);
         auto f = std::make_shared<prism::HostFactor>();
         std::string err;
-        int rc = prism::build_triangular(kind, A, tol, lfill, precision == PRISM_FP32, *f, &err);
+        int rc = prism::build_triangular(kind, A, tol, lfill, precision != PRISM_FP64, *f, &err);
+        if (!rc) f->apply32 = precision == PRISM_FP32_APPLY;
         if (rc) return fail(rc, err);
         *out = new prism_factor_s{std::move(f), nullptr};
         return PRISM_OK;

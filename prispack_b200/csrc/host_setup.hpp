@@ -211,6 +211,7 @@ void transpose_csr(uint32_t n, const std::vector<uint32_t>& rowptr, const std::v
 struct HostFactor {
     int kind = 0;
     bool fp32 = false;
+    bool apply32 = false;  // single-precision arithmetic in the streamed sweeps
     uint64_t mnnz = 0;             // getPreconditionNonZeroCount()
     CsrT<double> f0, f1;           // IC/ILDLT: L^T; ILUT: L, U
     std::vector<double> diag;      // ILDLT: D; ILUT: Dinv

@@ -54,20 +54,29 @@ static void* slab_kernel(bool fp32, int op) {
 
 static constexpr int kSlabThreads = 1024;
 
-static void* stream_kernel(bool fp32, int op) {
+// acc32: single-precision arithmetic (float factor values only)
+static void* stream_kernel(bool fp32, int op, bool acc32) {
+    if (acc32) {
+        switch (op) {
+            case SWEEP_DIV: return (void*)k_sweep_stream<float, OP_DIV, float>;
+            case SWEEP_MUL: return (void*)k_sweep_stream<float, OP_MUL, float>;
+            case SWEEP_NONE: return (void*)k_sweep_stream<float, OP_NONE, float>;
+            default: return (void*)k_sweep_stream<float, OP_PREDIV, float>;
+        }
+    }
     if (fp32) {
         switch (op) {
-            case SWEEP_DIV: return (void*)k_sweep_stream<float, OP_DIV>;
-            case SWEEP_MUL: return (void*)k_sweep_stream<float, OP_MUL>;
-            case SWEEP_NONE: return (void*)k_sweep_stream<float, OP_NONE>;
-            default: return (void*)k_sweep_stream<float, OP_PREDIV>;
+            case SWEEP_DIV: return (void*)k_sweep_stream<float, OP_DIV, double>;
+            case SWEEP_MUL: return (void*)k_sweep_stream<float, OP_MUL, double>;
+            case SWEEP_NONE: return (void*)k_sweep_stream<float, OP_NONE, double>;
+            default: return (void*)k_sweep_stream<float, OP_PREDIV, double>;
         }
     }
     switch (op) {
-        case SWEEP_DIV: return (void*)k_sweep_stream<double, OP_DIV>;
-        case SWEEP_MUL: return (void*)k_sweep_stream<double, OP_MUL>;
-        case SWEEP_NONE: return (void*)k_sweep_stream<double, OP_NONE>;
-        default: return (void*)k_sweep_stream<double, OP_PREDIV>;
+        case SWEEP_DIV: return (void*)k_sweep_stream<double, OP_DIV, double>;
+        case SWEEP_MUL: return (void*)k_sweep_stream<double, OP_MUL, double>;
+        case SWEEP_NONE: return (void*)k_sweep_stream<double, OP_NONE, double>;
+        default: return (void*)k_sweep_stream<double, OP_PREDIV, double>;
     }
 }
 
@@ -100,7 +109,7 @@ void launch_sweep_kernel(const Handle& h, cudaStream_t st, const DevSweep& s, co
         a.status = h.status.get();
         a.wait_ns = kWaitNs;
         void* args[] = {&a};
-        PRISM_CUDA(cudaLaunchCooperativeKernel(stream_kernel(s.fp32, s.op), dim3(s.str_ctas), dim3(kStrThreads), args,
+        PRISM_CUDA(cudaLaunchCooperativeKernel(stream_kernel(s.fp32, s.op, s.acc32), dim3(s.str_ctas), dim3(kStrThreads), args,
                                                s.str_smem, st));
         PRISM_LAUNCHED();
         return;
@@ -264,8 +273,11 @@ void init_device_info(DeviceInfo& info, int device) {
         for (int op = 0; op < 4; ++op) {
             PRISM_CUDA(cudaFuncSetAttribute(slab_kernel(f32, op), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             info.max_smem_optin));
-            PRISM_CUDA(cudaFuncSetAttribute(stream_kernel(f32, op), cudaFuncAttributeMaxDynamicSharedMemorySize,
+            PRISM_CUDA(cudaFuncSetAttribute(stream_kernel(f32, op, false), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             info.max_smem_optin));
+            if (f32)
+                PRISM_CUDA(cudaFuncSetAttribute(stream_kernel(true, op, true),
+                                                cudaFuncAttributeMaxDynamicSharedMemorySize, info.max_smem_optin));
         }
 }
 
@@ -338,10 +350,12 @@ bool DevSweep::upload(const Sweep<Low>& s0, const DeviceInfo& info, int lay, cud
         ctas = (uint32_t)start.size() - 1;
         const uint64_t smem = (uint64_t)info.max_smem_optin;
         StreamLayout L;
-        const uint32_t slot_cap = (uint32_t)std::min<uint64_t>(kNoSlot, (smem - kStrFixedSmem) / 8 / 2);
+        const bool a32 = acc32 && std::is_same<Low, float>::value;
+        const uint64_t slot_bytes = a32 ? 4 : 8;  // one value slot
+        const uint32_t slot_cap = (uint32_t)std::min<uint64_t>(kNoSlot, (smem - kStrFixedSmem) / slot_bytes / 2);
         if (!stream_layout<Low>(s0, start, slot_cap, L, nullptr)) return false;
         const uint64_t fixed = (uint64_t)kStrFixedSmem + (uint64_t)L.max_rounds_per_cta * 16 +
-                               (((uint64_t)L.slots * 8 + 127) & ~127ull);
+                               (((uint64_t)L.slots * slot_bytes + 127) & ~127ull);
         // Round r + 1 must land while round r still occupies the ring (the row threads wait
         // for it before finishing round r); wherever round r sits, a ring of three records
         // has room for one more next to it.
@@ -352,6 +366,7 @@ bool DevSweep::upload(const Sweep<Low>& s0, const DeviceInfo& info, int lay, cud
         num_levels = s0.num_levels;
         op = s0.op;
         fp32 = std::is_same<Low, float>::value;
+        acc32 = a32;
         layout = LAYOUT_STREAM;
         str_ctas = ctas;
         str_ring = ring;
@@ -417,10 +432,17 @@ bool DevSweep::upload(const Sweep<Low>& s0, const DeviceInfo& info, int lay, cud
 // kernel wins depends on how many rows a wavefront holds and how far
 // dependencies reach.
 template <typename Low>
-void tune_sweep(Handle& h, DevSweep& d, const Sweep<Low>& s) {
+void tune_sweep(Handle& h, DevSweep& d, const Sweep<Low>& s, bool acc32) {
     const int mode = h.info.sweep_kernel;
+    d.acc32 = acc32 && std::is_same<Low, float>::value;
     if (s.n == 0) {
         d.upload(s, h.info, LAYOUT_LEVEL, h.stream);
+        return;
+    }
+    // single-precision arithmetic: only the streamed kernel has it (the other layouts, where
+    // the streamed one does not fit, compute in double)
+    if (d.acc32) {
+        if (!d.upload(s, h.info, LAYOUT_STREAM, h.stream)) d.upload(s, h.info, LAYOUT_LEVEL, h.stream);
         return;
     }
     if (mode != 0) {
@@ -461,13 +483,13 @@ void tune_sweep(Handle& h, DevSweep& d, const Sweep<Low>& s) {
     if (d.layout != best_layout) d.upload(s, h.info, best_layout, h.stream);
     d.tuned_ms = best / 3.f;
 }
-template void tune_sweep<double>(Handle&, DevSweep&, const Sweep<double>&);
-template void tune_sweep<float>(Handle&, DevSweep&, const Sweep<float>&);
+template void tune_sweep<double>(Handle&, DevSweep&, const Sweep<double>&, bool);
+template void tune_sweep<float>(Handle&, DevSweep&, const Sweep<float>&, bool);
 
 TriangularPrecond::TriangularPrecond(Handle& h, std::shared_ptr<const HostFactor> f) : h_(h), f_(std::move(f)) {
     if (f_->fp32) {
-        tune_sweep(h_, lower_, f_->lower32);
-        tune_sweep(h_, upper_, f_->upper32);
+        tune_sweep(h_, lower_, f_->lower32, f_->apply32);
+        tune_sweep(h_, upper_, f_->upper32, f_->apply32);
     } else {
         tune_sweep(h_, lower_, f_->lower64);
         tune_sweep(h_, upper_, f_->upper64);

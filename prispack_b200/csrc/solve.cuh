@@ -64,6 +64,7 @@ struct DevSweep {
     uint32_t n = 0, num_levels = 0;
     int op = SWEEP_NONE;
     bool fp32 = false;
+    bool acc32 = false;            // streamed layout: single-precision arithmetic (float values only)
     int layout = LAYOUT_LEVEL;
     // LAYOUT_SLAB (k_sweep_slab): num_ctas > 0
     uint32_t num_ctas = 0, rows_per_cta = 0, smem_rows = 0;
@@ -150,6 +151,7 @@ int export_host_factor(const HostFactor& f, int which, uint32_t* n, uint64_t* nn
 // Host-built AMSED/MSLR setup, shared by any number of device handles.
 struct HostAmsed {
     bool fp32 = false;
+    bool apply32 = false;  // single-precision arithmetic in the streamed sweeps
     AmsedOptions opt;
     std::shared_ptr<AmsedSetup<float>> s32;
     std::shared_ptr<AmsedSetup<double>> s64;
@@ -235,9 +237,10 @@ void launch_sweep_kernel(const Handle& h, cudaStream_t st, const DevSweep& s, co
 // y = M x (sub = 0) or y -= M x (sub = 1) for a CSR with nrows rows
 void launch_spmv(const Handle& h, cudaStream_t st, uint32_t nrows, const uint32_t* rowptr, const uint32_t* col,
                  const double* val, const double* x, double* y, int sub);
-// uploads a sweep, choosing its kernel by timing both (see solve.cu)
+// uploads a sweep, choosing its kernel by timing the layouts (see solve.cu);
+// acc32 (float values only): single-precision arithmetic, streamed layout only
 template <typename Low>
-void tune_sweep(Handle& h, DevSweep& d, const Sweep<Low>& s);
+void tune_sweep(Handle& h, DevSweep& d, const Sweep<Low>& s, bool acc32 = false);
 
 // grad[k] = -lambda[row(k)] * x[col(k)] over A's stored entries
 void launch_adjoint_outer(const Handle& h, cudaStream_t st, const double* lambda, const double* x, double* grad);

@@ -134,7 +134,9 @@ static __global__ void __launch_bounds__(kBlock) k_stream_prep(uint32_t n, const
     }
 }
 
-template <typename Low, int OP>
+// Acc: the arithmetic type of the sweep (double; float for the single-precision apply,
+// whose value slots, products and sums are float and whose results are widened to double).
+template <typename Low, int OP, typename Acc>
 static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const StreamArgs a) {
     extern __shared__ __align__(128) unsigned char sm[];
     uint64_t* tma_bar = reinterpret_cast<uint64_t*>(sm);                     // [64] record copies
@@ -143,8 +145,8 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
     uint32_t* ring_off = reinterpret_cast<uint32_t*>(sm + 64 * 8 * 2 + 16);  // [64]
     uint32_t* words = ring_off + 64;  // landed, rounds done, abort
     uint4* meta_s = reinterpret_cast<uint4*>(sm + kStrFixedSmem);            // [meta_slots]
-    double* xs = reinterpret_cast<double*>(meta_s + a.meta_slots);           // [slots]; xs[0] = 0
-    unsigned char* ring = reinterpret_cast<unsigned char*>(xs) + ((a.slots * 8u + 127u) & ~127u);
+    Acc* xs = reinterpret_cast<Acc*>(meta_s + a.meta_slots);                 // [slots]; xs[0] = 0
+    unsigned char* ring = reinterpret_cast<unsigned char*>(xs) + ((a.slots * (uint32_t)sizeof(Acc) + 127u) & ~127u);
     const uint32_t b = blockIdx.x;
     const uint32_t rb = a.slab_start[b];
     const uint32_t r0 = a.cta_round[b];
@@ -153,7 +155,7 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
 
     for (uint32_t i = threadIdx.x; i < R; i += blockDim.x) meta_s[i] = __ldg(a.meta + r0 + i);
     if (threadIdx.x == 0) {
-        xs[0] = 0.0;
+        xs[0] = (Acc)0;
         words[0] = 0;  // records landed
         words[1] = 0;  // rounds done
         words[2] = 0;  // abort
@@ -315,7 +317,7 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
                             }
                         }
                     }
-                    if (ok) xs[xslot[idx[u]]] = __longlong_as_double((long long)v[u]);
+                    if (ok) xs[xslot[idx[u]]] = (Acc)__longlong_as_double((long long)v[u]);
                 }
             }
             if (!__all_sync(0xFFFFFFFFu, ok)) {
@@ -342,7 +344,7 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
     struct Row {
         uint32_t nr, L, m, rest;        // rows, entries per row, stride, ring offset of entries past 32
         uint32_t os, lr, base;
-        double vin, dg;
+        Acc vin, dg;
         uint32_t c[kRegEntries];
         Low v[kRegEntries];
     };
@@ -359,8 +361,8 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
         const unsigned char* base = ring + w.base;
         const uint16_t* col = reinterpret_cast<const uint16_t*>(base + rec.col) + j;
         const Low* val = reinterpret_cast<const Low*>(base + rec.val) + j;
-        w.vin = reinterpret_cast<const double*>(base + rec.in)[j];
-        w.dg = reinterpret_cast<const double*>(base + rec.diag)[j];
+        w.vin = (Acc)reinterpret_cast<const double*>(base + rec.in)[j];
+        w.dg = (Acc)reinterpret_cast<const double*>(base + rec.diag)[j];
         w.os = reinterpret_cast<const uint16_t*>(base + rec.oslot)[j];
         w.lr = reinterpret_cast<const uint16_t*>(base + rec.lrow)[j];
         // only as many register entries as the round's longest row needs (8, 16, 24, 28 or 32)
@@ -382,12 +384,12 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
     // sum of the first N register entries (N a multiple of 4): value reads first, then four chains
     auto dot_regs = [&](const Row& w, auto nconst) {
         constexpr int N = decltype(nconst)::value;
-        double x[N];
+        Acc x[N];
 #pragma unroll
         for (int u = 0; u < N; ++u) x[u] = xs[w.c[u]];
-        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        Acc acc[4] = {(Acc)0, (Acc)0, (Acc)0, (Acc)0};
 #pragma unroll
-        for (int u = 0; u < N; ++u) acc[u & 3] += (double)w.v[u] * x[u];
+        for (int u = 0; u < N; ++u) acc[u & 3] += (Acc)w.v[u] * x[u];
         return (acc[0] + acc[1]) + (acc[2] + acc[3]);
     };
     auto wait_phase = [&](uint64_t* bar, uint32_t parity) {
@@ -403,7 +405,7 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
     uint32_t landed_seen = 1;
     for (uint32_t r = 0; r < R; ++r) {
         if (j < cur.nr) {
-            double s;
+            Acc s;
             if (cur.L <= 8) s = dot_regs(cur, std::integral_constant<int, 8>{});
             else if (cur.L <= 16) s = dot_regs(cur, std::integral_constant<int, 16>{});
             else if (cur.L <= 24) s = dot_regs(cur, std::integral_constant<int, 24>{});
@@ -412,15 +414,19 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
             if (cur.L > (uint32_t)kRegEntries) {  // rows longer than 32 entries
                 const uint16_t* col = reinterpret_cast<const uint16_t*>(ring + cur.rest) + j;
                 const Low* val = reinterpret_cast<const Low*>(ring + cur.rest + 2u * cur.L * cur.m) + j;
-                for (uint32_t k = kRegEntries; k < cur.L; ++k) s += (double)val[k * cur.m] * xs[col[k * cur.m]];
+                for (uint32_t k = kRegEntries; k < cur.L; ++k) s += (Acc)val[k * cur.m] * xs[col[k * cur.m]];
             }
-            double res;
+            Acc res;
             if (OP == OP_DIV || OP == OP_MUL) res = (cur.vin - s) * cur.dg;  // dg = 1/diag for OP_DIV
             else if (OP == OP_NONE) res = cur.vin - s;
             else res = cur.vin * cur.dg - s;                                  // dg = 1/diag
-            unsigned long long rbits = (unsigned long long)__double_as_longlong(res);
-            if (res != res) rbits = kCanonicalNaN;
-            if (cur.os != kNoSlot) xs[cur.os] = __longlong_as_double((long long)rbits);
+            const double rd = (double)res;
+            unsigned long long rbits = (unsigned long long)__double_as_longlong(rd);
+            if (rd != rd) rbits = kCanonicalNaN;
+            if (cur.os != kNoSlot) {
+                if constexpr (sizeof(Acc) == 8) xs[cur.os] = __longlong_as_double((long long)rbits);
+                else xs[cur.os] = res;
+            }
             st_relaxed_u64(a.out + rb + cur.lr, rbits);
         }
         __syncwarp();
