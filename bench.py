@@ -43,7 +43,10 @@ AMSED = dict(levels=3, lanczos_steps=64, low_rank=32, eig_bound=0.8, lowrank_typ
 SEED = 2024
 # measured DRAM / algorithmic bytes of the level-0 lower sweep at 96^3, per sweep kernel (one ncu capture each;
 # profiles/k_sweep_level0_lower_96cube.md, profiles/k_sweep_stream_level0_lower_96cube.md)
-TRAFFIC_RATIO = {"level-order": 181.2 / 183.6, "stream": 186.4 / 183.6}
+# DRAM / algorithmic bytes of one ncu capture of each sweep kernel on the 96^3 level-0 lower
+# sweep (profiles/): level order 181.2 MB, streamed with single-precision arithmetic 188.0 MB,
+# of 183.6 MB algorithmic
+TRAFFIC_RATIO = {"level-order": 181.2 / 183.6, "stream": 188.0 / 183.6}
 
 
 def workload(grid: int, tol: float, precond: str) -> str:
@@ -528,7 +531,8 @@ def main():
         A = PB.CSRMatrix.laplacian(args.grid, args.grid, args.grid)
         S = PB.DeviceSystem(A, device=local)
         S.set_stream(torch.cuda.current_stream().cuda_stream)
-        S.attach(build_precond(PB, A, args.precond, PB.PRISM_FP32))
+        prec = PB.PRISM_FP32_APPLY if args.only_sweep == "stream" else PB.PRISM_FP32
+        S.attach(build_precond(PB, A, args.precond, prec))
         info = S.sweep_info(0)
         vin = torch.tensor(np.random.default_rng(SEED).standard_normal(info["n"]), device="cuda")
         vout = torch.empty_like(vin)
@@ -733,8 +737,8 @@ def main():
                          # of each sweep kernel on the 96^3 case, applied to this launch's algorithmic bytes
                          "traffic": round(statistics.mean(TRAFFIC_RATIO.get(i["kernel"], 1.0) * b_
                                                           for i, b_ in zip(sweep_infos, sweep_bytes))),
-                         "traffic_source": "ncu captures at 96^3 (level-order 181.2 MB, streamed 186.4 MB DRAM "
-                                           "per 183.6 MB algorithmic), scaled by rows"},
+                         "traffic_source": "ncu captures at 96^3 (level-order 181.2 MB, streamed single-precision "
+                                           "188.0 MB DRAM per 183.6 MB algorithmic), scaled by rows"},
             "spmv": {"ms": round(statistics.median(spmv_ms), 4), "bytes": spmv_bytes, "GB/s": round(spmv_gbs, 1),
                      "frac": round(spmv_gbs / peak, 4)},
             "fp64_factor": fp64,
