@@ -687,10 +687,7 @@ def main():
         S.attach(F32)
 
     # ---- max over ranks
-    vals = torch.tensor([ms32, e2e_ms], dtype=torch.float64, device="cuda")
-    if dist is not None:
-        dist.all_reduce(vals, op=dist.ReduceOp.MAX)
-    ms32, e2e_ms = float(vals[0]), float(vals[1])
+    ms32, e2e_ms = max_over_ranks([ms32, e2e_ms], dist, "cuda")
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -751,6 +748,17 @@ def main():
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def max_over_ranks(values, dist=None, device="cpu"):
+    """Replicas run concurrently, so a job's time is its slowest rank's: the
+    element-wise max of `values` over the process group (identity without one).
+    Every rank takes this step, in the same order."""
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.cpu()]
 
 
 def reference_arm(args, rank, world):
