@@ -813,8 +813,7 @@ bool stream_layout(const Sweep<Low>& s, const std::vector<uint32_t>& start, uint
             double* diag = reinterpret_cast<double*>(base + rec.diag);
             uint16_t* lrow = reinterpret_cast<uint16_t*>(base + rec.lrow);
             uint16_t* oslot = reinterpret_cast<uint16_t*>(base + rec.oslot);
-            uint16_t* col = reinterpret_cast<uint16_t*>(base + rec.col);
-            Low* val = reinterpret_cast<Low*>(base + rec.val);
+            uint8_t* ent = base + rec.ent;
             uint32_t* xrow = reinterpret_cast<uint32_t*>(base + rec.xrow);
             uint16_t* xslot = reinterpret_cast<uint16_t*>(base + rec.xslot);
             uint16_t* xwait = reinterpret_cast<uint16_t*>(base + rec.xwait);
@@ -828,8 +827,11 @@ bool stream_layout(const Sweep<Low>& s, const std::vector<uint32_t>& start, uint
                 for (uint32_t k = sl.rowptr[p]; k < sl.rowptr[p + 1]; ++k) {
                     const uint32_t d = sl.col[k], e = (k - sl.rowptr[p]) * rec.m + j;
                     if (slot_in[d] != b || slot_of[d] == 0) return fail("a dependency without a value slot");
-                    col[e] = (uint16_t)slot_of[d];
-                    val[e] = sl.val[k];
+                    // {slot word, value}: the slot in the low half of a word as wide as the value
+                    uint8_t* at = ent + (size_t)e * rec.eb;
+                    const uint64_t slot = slot_of[d];
+                    std::memcpy(at, &slot, 4);  // little-endian: the low bytes of the slot word
+                    std::memcpy(at + vb, &sl.val[k], vb);
                 }
             }
             for (uint32_t x = 0; x < X; ++x) {
@@ -913,8 +915,17 @@ std::string stream_layout_replay(const Sweep<Low>& s, const StreamLayout& L, con
                 const double* diag = reinterpret_cast<const double*>(base + rec.diag);
                 const uint16_t* lrow = reinterpret_cast<const uint16_t*>(base + rec.lrow);
                 const uint16_t* oslot = reinterpret_cast<const uint16_t*>(base + rec.oslot);
-                const uint16_t* col = reinterpret_cast<const uint16_t*>(base + rec.col);
-                const Low* val = reinterpret_cast<const Low*>(base + rec.val);
+                const uint8_t* ent = base + rec.ent;
+                auto ent_slot = [&](uint32_t e) {
+                    uint64_t w = 0;
+                    std::memcpy(&w, ent + (size_t)e * rec.eb, vb);
+                    return w;
+                };
+                auto ent_val = [&](uint32_t e) {
+                    Low v;
+                    std::memcpy(&v, ent + (size_t)e * rec.eb + vb, vb);
+                    return v;
+                };
                 // the rows of a round run at once: all of them read before any writes
                 std::vector<double> res(nr);
                 for (uint32_t j = 0; j < nr; ++j) {
@@ -928,17 +939,19 @@ std::string stream_layout_replay(const Sweep<Low>& s, const StreamLayout& L, con
                     double acc = 0.0;
                     for (uint32_t t = 0; t < Lr; ++t) {
                         const uint32_t e = t * rec.m + j;
-                        if (col[e] >= L.slots) return "dependency slot out of range";
+                        const uint64_t cs = ent_slot(e);
+                        const Low cv = ent_val(e);
+                        if (cs >= L.slots) return "dependency slot out of range";
                         if (t >= len) {  // padding: slot 0 (0.0) times 0
-                            if (col[e] != 0 || val[e] != (Low)0) return "padding entry";
+                            if (cs != 0 || cv != (Low)0) return "padding entry";
                             continue;
                         }
                         const uint32_t k = s.rowptr[p] + t;
-                        if (col[e] == 0) return "a dependency in the zero slot";
-                        if (c.owner[col[e]] != (int64_t)s.col[k]) return "a slot does not hold the dependency";
+                        if (cs == 0) return "a dependency in the zero slot";
+                        if (c.owner[cs] != (int64_t)s.col[k]) return "a slot does not hold the dependency";
                         if (!done[s.col[k]]) return "a dependency read before it was finished";
-                        if (val[e] != s.val[k]) return "coefficient";
-                        acc += (double)val[e] * c.xs[col[e]];
+                        if (cv != s.val[k]) return "coefficient";
+                        acc += (double)cv * c.xs[cs];
                     }
                     if (s.op == SWEEP_DIV || s.op == SWEEP_MUL) res[j] = (vin[j] - acc) * diag[j];
                     else if (s.op == SWEEP_NONE) res[j] = vin[j] - acc;

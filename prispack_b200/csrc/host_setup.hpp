@@ -124,8 +124,9 @@ void slab_layout(const Sweep<Low>& s, uint32_t num_ctas, uint32_t rows_per_cta, 
 //   f64 diag[m]      (1 / diag for the dividing operations)
 //   u16 lrow[m]      row - first row of the slab
 //   u16 oslot[m]     value slot of the row's result (0xFFFF: no reader in the slab)
-//   u16 col[L][m]    entry k of row j at k*m + j: value slot of the dependency (0: padding)
-//   Low val[L][m]    its coefficient (0: padding)
+//   ent[L][m]        entry k of row j at k*m + j, one load each: the value slot of the
+//                    dependency (0: padding) and its coefficient (0: padding), as
+//                    {u32 slot, f32 value} (8 bytes) or {u64 slot, f64 value} (16 bytes)
 //   u32 xrow[X]      halo rows whose values this round copies in ...
 //   u16 xslot[X]     ... into these slots ...
 //   u16 xwait[X]     ... once this many rounds of the slab are done
@@ -141,7 +142,7 @@ void slab_layout(const Sweep<Low>& s, uint32_t num_ctas, uint32_t rows_per_cta, 
 constexpr uint32_t kRoundRows = 128;
 constexpr uint32_t kNoSlot = 0xFFFFu;
 struct RoundRec {
-    uint32_t m, in, diag, lrow, oslot, col, val, xrow, xslot, xwait, bytes;
+    uint32_t m, in, diag, lrow, oslot, ent, eb, xrow, xslot, xwait, bytes;
 };
 PRISM_HD inline uint32_t pad16(uint32_t b) { return (b + 15u) & ~15u; }
 PRISM_HD inline RoundRec round_rec(uint32_t nr, uint32_t L, uint32_t X, uint32_t vb) {
@@ -151,9 +152,9 @@ PRISM_HD inline RoundRec round_rec(uint32_t nr, uint32_t L, uint32_t X, uint32_t
     r.diag = 8u * r.m;
     r.lrow = 16u * r.m;
     r.oslot = 18u * r.m;
-    r.col = 20u * r.m;
-    r.val = r.col + 2u * L * r.m;
-    r.xrow = r.val + vb * L * r.m;
+    r.ent = 20u * r.m;
+    r.eb = 2u * vb;  // slot word + value, each vb bytes
+    r.xrow = r.ent + r.eb * L * r.m;
     r.xslot = r.xrow + pad16(4u * X);
     r.xwait = r.xslot + pad16(2u * X);
     r.bytes = r.xwait + pad16(2u * X);

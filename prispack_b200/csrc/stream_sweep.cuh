@@ -333,7 +333,8 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
     }
 
     // ---------------------------------------------------------------------- row threads
-    // Thread j computes row j of each round: its entries sit at j, j + m, j + 2m, ...
+    // Thread j computes row j of each round: its entries ({slot, coefficient}, one load
+    // each) sit at j, j + m, j + 2m, ...
     // of the round's entry table (m = rows rounded up to 8), padded with slot 0 (0.0)
     // to the round's longest row.  Before waiting for the barrier that ends round r,
     // each thread reads round r+1's record -- up to 32 entries, right-hand side,
@@ -349,6 +350,18 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
         Low v[kRegEntries];
     };
     Row cur;
+    // record entry k of this thread: {slot, coefficient}; one 8-byte load for float values,
+    // the slot word's low half and the double for double values
+    auto ent_get = [](const unsigned char* ent, uint32_t k, uint32_t& c, Low& v) {
+        if constexpr (sizeof(Low) == 4) {
+            const unsigned long long e = reinterpret_cast<const unsigned long long*>(ent)[k];
+            c = (uint32_t)e;
+            v = __uint_as_float((uint32_t)(e >> 32));
+        } else {
+            c = reinterpret_cast<const uint32_t*>(ent)[4 * k];
+            v = reinterpret_cast<const double*>(ent)[2 * k + 1];
+        }
+    };
     auto load_row = [&](uint32_t r, Row& w) {
         const uint4 m = meta_s[r];
         w.nr = m.z & 0xFFFFu;
@@ -356,11 +369,10 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
         const RoundRec rec = round_rec(w.nr, w.L, m.w, vb);
         w.base = ring_off[r % kStrMaxRounds];
         w.m = rec.m;
-        w.rest = w.base + rec.col;
+        w.rest = w.base + rec.ent;
         if (j >= w.nr) return;
         const unsigned char* base = ring + w.base;
-        const uint16_t* col = reinterpret_cast<const uint16_t*>(base + rec.col) + j;
-        const Low* val = reinterpret_cast<const Low*>(base + rec.val) + j;
+        const unsigned char* ent = base + rec.ent + (size_t)j * rec.eb;
         w.vin = (Acc)reinterpret_cast<const double*>(base + rec.in)[j];
         w.dg = (Acc)reinterpret_cast<const double*>(base + rec.diag)[j];
         w.os = reinterpret_cast<const uint16_t*>(base + rec.oslot)[j];
@@ -370,9 +382,9 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
             constexpr int N = decltype(nconst)::value;
 #pragma unroll
             for (int u = 0; u < N; ++u) {
-                const bool in = (uint32_t)u < w.L;
-                w.c[u] = in ? col[u * rec.m] : 0u;
-                w.v[u] = in ? val[u * rec.m] : (Low)0;
+                w.c[u] = 0u;
+                w.v[u] = (Low)0;
+                if ((uint32_t)u < w.L) ent_get(ent, u * rec.m, w.c[u], w.v[u]);
             }
         };
         if (w.L <= 8) fill(std::integral_constant<int, 8>{});
@@ -412,9 +424,13 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
             else if (cur.L <= 28) s = dot_regs(cur, std::integral_constant<int, 28>{});
             else s = dot_regs(cur, std::integral_constant<int, 32>{});
             if (cur.L > (uint32_t)kRegEntries) {  // rows longer than 32 entries
-                const uint16_t* col = reinterpret_cast<const uint16_t*>(ring + cur.rest) + j;
-                const Low* val = reinterpret_cast<const Low*>(ring + cur.rest + 2u * cur.L * cur.m) + j;
-                for (uint32_t k = kRegEntries; k < cur.L; ++k) s += (Acc)val[k * cur.m] * xs[col[k * cur.m]];
+                const unsigned char* ent = ring + cur.rest + (size_t)j * 2u * vb;
+                for (uint32_t k = kRegEntries; k < cur.L; ++k) {
+                    uint32_t c;
+                    Low v;
+                    ent_get(ent, k * cur.m, c, v);
+                    s += (Acc)v * xs[c];
+                }
             }
             Acc res;
             if (OP == OP_DIV || OP == OP_MUL) res = (cur.vin - s) * cur.dg;  // dg = 1/diag for OP_DIV
