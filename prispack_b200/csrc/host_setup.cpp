@@ -827,11 +827,15 @@ bool stream_layout(const Sweep<Low>& s, const std::vector<uint32_t>& start, uint
                 for (uint32_t k = sl.rowptr[p]; k < sl.rowptr[p + 1]; ++k) {
                     const uint32_t d = sl.col[k], e = (k - sl.rowptr[p]) * rec.m + j;
                     if (slot_in[d] != b || slot_of[d] == 0) return fail("a dependency without a value slot");
-                    // {slot word, value}: the slot in the low half of a word as wide as the value
-                    uint8_t* at = ent + (size_t)e * rec.eb;
-                    const uint64_t slot = slot_of[d];
-                    std::memcpy(at, &slot, 4);  // little-endian: the low bytes of the slot word
-                    std::memcpy(at + vb, &sl.val[k], vb);
+                    if (vb == 4) {  // {u32 slot, f32 value}
+                        const uint32_t slot = slot_of[d];
+                        std::memcpy(ent + (size_t)e * 8, &slot, 4);
+                        std::memcpy(ent + (size_t)e * 8 + 4, &sl.val[k], 4);
+                    } else {        // u16 slot; f64 value in the value section
+                        const uint16_t slot = (uint16_t)slot_of[d];
+                        std::memcpy(ent + (size_t)e * 2, &slot, 2);
+                        std::memcpy(base + rec.val + (size_t)e * 8, &sl.val[k], 8);
+                    }
                 }
             }
             for (uint32_t x = 0; x < X; ++x) {
@@ -916,14 +920,20 @@ std::string stream_layout_replay(const Sweep<Low>& s, const StreamLayout& L, con
                 const uint16_t* lrow = reinterpret_cast<const uint16_t*>(base + rec.lrow);
                 const uint16_t* oslot = reinterpret_cast<const uint16_t*>(base + rec.oslot);
                 const uint8_t* ent = base + rec.ent;
-                auto ent_slot = [&](uint32_t e) {
-                    uint64_t w = 0;
-                    std::memcpy(&w, ent + (size_t)e * rec.eb, vb);
+                auto ent_slot = [&](uint32_t e) -> uint64_t {
+                    if (vb == 4) {
+                        uint32_t w;
+                        std::memcpy(&w, ent + (size_t)e * 8, 4);
+                        return w;
+                    }
+                    uint16_t w;
+                    std::memcpy(&w, ent + (size_t)e * 2, 2);
                     return w;
                 };
                 auto ent_val = [&](uint32_t e) {
                     Low v;
-                    std::memcpy(&v, ent + (size_t)e * rec.eb + vb, vb);
+                    if (vb == 4) std::memcpy(&v, ent + (size_t)e * 8 + 4, 4);
+                    else std::memcpy(&v, base + rec.val + (size_t)e * 8, 8);
                     return v;
                 };
                 // the rows of a round run at once: all of them read before any writes

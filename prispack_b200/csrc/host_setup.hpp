@@ -124,9 +124,10 @@ void slab_layout(const Sweep<Low>& s, uint32_t num_ctas, uint32_t rows_per_cta, 
 //   f64 diag[m]      (1 / diag for the dividing operations)
 //   u16 lrow[m]      row - first row of the slab
 //   u16 oslot[m]     value slot of the row's result (0xFFFF: no reader in the slab)
-//   ent[L][m]        entry k of row j at k*m + j, one load each: the value slot of the
-//                    dependency (0: padding) and its coefficient (0: padding), as
-//                    {u32 slot, f32 value} (8 bytes) or {u64 slot, f64 value} (16 bytes)
+//   entries          entry k of row j at e = k*m + j: the value slot of the dependency
+//                    (0: padding) and its coefficient (0: padding).  Float values:
+//                    {u32 slot, f32 value} at ent + 8e, one load.  Double values:
+//                    u16 slot at ent + 2e and f64 value at val + 8e (val = ent + 2Lm).
 //   u32 xrow[X]      halo rows whose values this round copies in ...
 //   u16 xslot[X]     ... into these slots ...
 //   u16 xwait[X]     ... once this many rounds of the slab are done
@@ -142,7 +143,7 @@ void slab_layout(const Sweep<Low>& s, uint32_t num_ctas, uint32_t rows_per_cta, 
 constexpr uint32_t kRoundRows = 128;
 constexpr uint32_t kNoSlot = 0xFFFFu;
 struct RoundRec {
-    uint32_t m, in, diag, lrow, oslot, ent, eb, xrow, xslot, xwait, bytes;
+    uint32_t m, in, diag, lrow, oslot, ent, val, xrow, xslot, xwait, bytes;
 };
 PRISM_HD inline uint32_t pad16(uint32_t b) { return (b + 15u) & ~15u; }
 PRISM_HD inline RoundRec round_rec(uint32_t nr, uint32_t L, uint32_t X, uint32_t vb) {
@@ -153,8 +154,13 @@ PRISM_HD inline RoundRec round_rec(uint32_t nr, uint32_t L, uint32_t X, uint32_t
     r.lrow = 16u * r.m;
     r.oslot = 18u * r.m;
     r.ent = 20u * r.m;
-    r.eb = 2u * vb;  // slot word + value, each vb bytes
-    r.xrow = r.ent + r.eb * L * r.m;
+    if (vb == 4) {  // {u32 slot, f32 value} pairs
+        r.val = r.ent + 4u;
+        r.xrow = r.ent + 8u * L * r.m;
+    } else {        // u16 slots, then f64 values
+        r.val = r.ent + 2u * L * r.m;
+        r.xrow = r.val + 8u * L * r.m;
+    }
     r.xslot = r.xrow + pad16(4u * X);
     r.xwait = r.xslot + pad16(2u * X);
     r.bytes = r.xwait + pad16(2u * X);

@@ -343,23 +343,23 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
     const uint32_t j = threadIdx.x;
     constexpr int kRegEntries = 32;
     struct Row {
-        uint32_t nr, L, m, rest;        // rows, entries per row, stride, ring offset of entries past 32
+        uint32_t nr, L, m;              // rows, entries per row, stride
         uint32_t os, lr, base;
         Acc vin, dg;
         uint32_t c[kRegEntries];
         Low v[kRegEntries];
     };
     Row cur;
-    // record entry k of this thread: {slot, coefficient}; one 8-byte load for float values,
-    // the slot word's low half and the double for double values
-    auto ent_get = [](const unsigned char* ent, uint32_t k, uint32_t& c, Low& v) {
+    // record entry e of the round (this thread's entries: e = j, j + m, ...): {slot, coefficient};
+    // one 8-byte load for float values, a u16 slot and a double for double values
+    auto ent_get = [](const unsigned char* rbase, const RoundRec& rec, uint32_t e, uint32_t& c, Low& v) {
         if constexpr (sizeof(Low) == 4) {
-            const unsigned long long e = reinterpret_cast<const unsigned long long*>(ent)[k];
-            c = (uint32_t)e;
-            v = __uint_as_float((uint32_t)(e >> 32));
+            const unsigned long long w = reinterpret_cast<const unsigned long long*>(rbase + rec.ent)[e];
+            c = (uint32_t)w;
+            v = __uint_as_float((uint32_t)(w >> 32));
         } else {
-            c = reinterpret_cast<const uint32_t*>(ent)[4 * k];
-            v = reinterpret_cast<const double*>(ent)[2 * k + 1];
+            c = reinterpret_cast<const uint16_t*>(rbase + rec.ent)[e];
+            v = reinterpret_cast<const double*>(rbase + rec.val)[e];
         }
     };
     auto load_row = [&](uint32_t r, Row& w) {
@@ -369,10 +369,8 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
         const RoundRec rec = round_rec(w.nr, w.L, m.w, vb);
         w.base = ring_off[r % kStrMaxRounds];
         w.m = rec.m;
-        w.rest = w.base + rec.ent;
         if (j >= w.nr) return;
         const unsigned char* base = ring + w.base;
-        const unsigned char* ent = base + rec.ent + (size_t)j * rec.eb;
         w.vin = (Acc)reinterpret_cast<const double*>(base + rec.in)[j];
         w.dg = (Acc)reinterpret_cast<const double*>(base + rec.diag)[j];
         w.os = reinterpret_cast<const uint16_t*>(base + rec.oslot)[j];
@@ -384,7 +382,7 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
             for (int u = 0; u < N; ++u) {
                 w.c[u] = 0u;
                 w.v[u] = (Low)0;
-                if ((uint32_t)u < w.L) ent_get(ent, u * rec.m, w.c[u], w.v[u]);
+                if ((uint32_t)u < w.L) ent_get(base, rec, u * rec.m + j, w.c[u], w.v[u]);
             }
         };
         if (w.L <= 8) fill(std::integral_constant<int, 8>{});
@@ -424,11 +422,11 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
             else if (cur.L <= 28) s = dot_regs(cur, std::integral_constant<int, 28>{});
             else s = dot_regs(cur, std::integral_constant<int, 32>{});
             if (cur.L > (uint32_t)kRegEntries) {  // rows longer than 32 entries
-                const unsigned char* ent = ring + cur.rest + (size_t)j * 2u * vb;
+                const RoundRec rr = round_rec(cur.nr, cur.L, 0u, vb);  // entry sections do not depend on X
                 for (uint32_t k = kRegEntries; k < cur.L; ++k) {
                     uint32_t c;
                     Low v;
-                    ent_get(ent, k * cur.m, c, v);
+                    ent_get(ring + cur.base, rr, k * cur.m + j, c, v);
                     s += (Acc)v * xs[c];
                 }
             }
