@@ -43,10 +43,12 @@ AMSED = dict(levels=3, lanczos_steps=64, low_rank=32, eig_bound=0.8, lowrank_typ
 SEED = 2024
 # measured DRAM / algorithmic bytes of the level-0 lower sweep at 96^3, per sweep kernel (one ncu capture each;
 # profiles/k_sweep_level0_lower_96cube.md, profiles/k_sweep_stream_level0_lower_96cube.md)
-# DRAM / algorithmic bytes of one ncu capture of each sweep kernel on the 96^3 level-0 lower
-# sweep (profiles/): level order 181.2 MB, streamed with single-precision arithmetic 188.0 MB,
-# of 183.6 MB algorithmic
-TRAFFIC_RATIO = {"level-order": 181.2 / 183.6, "stream": 188.0 / 183.6}
+# DRAM / algorithmic bytes of each sweep kernel on the 96^3 level-0 lower sweep (183.6 MB
+# algorithmic): level order 181.2 MB (ncu capture); streamed with single-precision arithmetic
+# 188.0 MB captured with 6-byte record entries, plus the 49.9 MB the 8-byte {slot, value}
+# entries add to that sweep's records (175.1 -> 225.1 MB, computed from the layout; not
+# re-captured)
+TRAFFIC_RATIO = {"level-order": 181.2 / 183.6, "stream": (188.0 + 49.9) / 183.6}
 
 
 def workload(grid: int, tol: float, precond: str) -> str:
@@ -734,8 +736,10 @@ def main():
                          # of each sweep kernel on the 96^3 case, applied to this launch's algorithmic bytes
                          "traffic": round(statistics.mean(TRAFFIC_RATIO.get(i["kernel"], 1.0) * b_
                                                           for i, b_ in zip(sweep_infos, sweep_bytes))),
-                         "traffic_source": "ncu captures at 96^3 (level-order 181.2 MB, streamed single-precision "
-                                           "188.0 MB DRAM per 183.6 MB algorithmic), scaled by rows"},
+                         "traffic_source": "per 183.6 MB algorithmic at 96^3: level order 181.2 MB (ncu); streamed "
+                                           "237.9 MB = 188.0 MB ncu capture with 6-byte entries + 49.9 MB record "
+                                           "growth of the 8-byte entries (layout arithmetic, not re-captured); "
+                                           "scaled by rows"},
             "spmv": {"ms": round(statistics.median(spmv_ms), 4), "bytes": spmv_bytes, "GB/s": round(spmv_gbs, 1),
                      "frac": round(spmv_gbs / peak, 4)},
             "fp64_factor": fp64,
