@@ -17,6 +17,12 @@
 // ones) are copied into their slots by prefetcher warps as soon as they are
 // finished, while the slab is still working on earlier rounds.
 //
+// What a round costs (3D Poisson 128^3, level-0 factor, B200): about 0.7 us
+// with float arithmetic, in slabs with and without halo rows alike; about
+// half is the dot product, half the round's bookkeeping (record fields,
+// result, barrier, next record).  Each is a chain of dependent shared-memory
+// loads and arithmetic of some tens of cycles a link.
+//
 // Roles (352 threads; the polling warps sleep between polls so that the row
 // threads, which carry the dependency chain, keep the issue slots):
 //   warps 0..3    row threads: thread j computes row j of each round, then each
