@@ -560,8 +560,8 @@ int32_t prism_factor_create(int32_t kind, uint32_t n, const uint32_t* rowptr, co
         auto f = std::make_shared<prism::HostFactor>();
         std::string err;
         int rc = prism::build_triangular(kind, A, tol, lfill, precision != PRISM_FP64, *f, &err);
-        if (!rc) f->apply32 = precision == PRISM_FP32_APPLY;
         if (rc) return fail(rc, err);
+        f->apply32 = precision == PRISM_FP32_APPLY;
         *out = new prism_factor_s{std::move(f), nullptr};
         return PRISM_OK;
     });
