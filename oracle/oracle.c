@@ -59,6 +59,33 @@ void orc_spmv(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const dou
     }
 }
 
+/* One triangular sweep in gather form, in single precision: the arithmetic of
+ * the library's single-precision apply (PRISM_FP32_APPLY), which has no
+ * reference counterpart.  Row r (in dependency order: increasing for a lower
+ * sweep, decreasing for an upper one) sums its entries in order,
+ * s += val[k] * out[col[k]], each value, product and sum rounded to float, and
+ *   op 0: (in - s) / diag   op 1: (in - s) * diag   op 2: in - s   op 3: in / diag - s
+ * with in and diag rounded to float first; out holds the float results
+ * widened to double. */
+void orc_sweep_f32(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val,
+                   const double* diag, int op, int lower, const double* in, double* out) {
+    float* x = (float*)malloc(sizeof(float) * (n ? n : 1));
+    for (uint32_t t = 0; t < n; t++) {
+        const uint32_t r = lower ? t : n - 1 - t;
+        float s = 0.0f;
+        for (uint32_t k = rowptr[r]; k < rowptr[r + 1]; k++) s += (float)val[k] * x[col[k]];
+        const float b = (float)in[r], d = diag ? (float)diag[r] : 1.0f;
+        float res;
+        if (op == 0) res = (b - s) / d;
+        else if (op == 1) res = (b - s) * d;
+        else if (op == 2) res = b - s;
+        else res = b / d - s;
+        x[r] = res;
+        out[r] = (double)res;
+    }
+    free(x);
+}
+
 /* ---- AMSED ----------------------------------------------------------------- */
 static void ildlt_inplace(uint32_t n, const uint32_t* rp, const uint32_t* ci, const double* v, const double* D,
                           double* vec) {

@@ -66,6 +66,9 @@ void orc_laplacian(int nx, int ny, int nz, double ax, double ay, double az, doub
                    uint32_t* rowptr, uint32_t* col, double* val);
 void orc_spmv(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val,
               const double* x, double* y);
+/* a gather-form triangular sweep in single precision (see oracle.c) */
+void orc_sweep_f32(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val,
+                   const double* diag, int op, int lower, const double* in, double* out);
 void orc_precond_apply(const orc_precond* P, double* vec);
 void orc_cg(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val,
             const orc_precond* P, int flexible, double tol, uint32_t max_iter,

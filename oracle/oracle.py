@@ -54,6 +54,7 @@ def lib() -> C.CDLL:
         _LIB.orc_laplacian.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                        C.c_double, _u32p, _u32p, _f64p]
         _LIB.orc_spmv.argtypes = [C.c_uint32, _u32p, _u32p, _f64p, _f64p, _f64p]
+        _LIB.orc_sweep_f32.argtypes = [C.c_uint32, _u32p, _u32p, _f64p, C.c_void_p, C.c_int, C.c_int, _f64p, _f64p]
         _LIB.orc_precond_apply.argtypes = [C.POINTER(_Precond), _f64p]
         _LIB.orc_amsed_apply.argtypes = [C.POINTER(_Amsed), _f64p]
         _LIB.orc_cg.argtypes = [C.c_uint32, _u32p, _u32p, _f64p, C.POINTER(_Precond), C.c_int, C.c_double,
@@ -80,6 +81,18 @@ def spmv(rp, ci, v, x):
     y = np.zeros(len(rp) - 1)
     lib().orc_spmv(len(rp) - 1, rp, ci, v, np.ascontiguousarray(x, np.float64), y)
     return y
+
+
+def sweep_f32(rp, ci, v, b, *, diag=None, op=2, lower=True):
+    """Gather-form triangular sweep in single precision (the single-precision
+    apply's arithmetic); returns the float results widened to double."""
+    rp = np.ascontiguousarray(rp, np.uint32)
+    out = np.zeros(len(rp) - 1)
+    d = np.ascontiguousarray(diag, np.float64) if diag is not None else None
+    lib().orc_sweep_f32(len(rp) - 1, rp, np.ascontiguousarray(ci, np.uint32), np.ascontiguousarray(v, np.float64),
+                        d.ctypes.data if d is not None else None, int(op), int(bool(lower)),
+                        np.ascontiguousarray(b, np.float64), out)
+    return out
 
 
 class Precond:
