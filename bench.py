@@ -1,21 +1,30 @@
-"""Solve-phase benchmark: time-to-1e-10 relative residual on one B200 per rank.
+"""Solve-phase benchmark: time to a 1e-10 relative residual on one B200 per rank.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl prism|reference]
-                    [--precond amsed|ic] [--grid G]
+                    [--precond amsed|ic] [--grid G] [--config 1..5] [--no-secondary]
 
-Workload (default): 3D Poisson 7-point Laplacian 128^3 (n = 2,097,152,
+Headline workload: 3D Poisson 7-point Laplacian 128^3 (n = 2,097,152,
 nnz = 14,581,760; generateLaplacianCSR), b ~ N(0,1) from a fixed seed, x0 = 0,
-flexible CG + AMSED/MSLR (3 HID levels, local RCM, ILDLT(1e-3) blocks, ICT(1e-3)
-on the last level, low-rank correction of rank <= 32 per level from 64 classic
-generalized Lanczos steps, MSLR correction H = lambda/(1-lambda)), relative
-tolerance 1e-10, max 1000 iterations.  `--precond ic` runs FCG + ICT(1e-3) on
-the same system instead.  The preconditioner is set up once on the host
-(outside the timed region); one step is one complete device-resident solve.
-The headline is the mixed-precision solve: FP32 factor values and FP32
-arithmetic inside the streamed triangular sweeps (PRISM_FP32_APPLY), FP64
-Krylov vectors, scalars, SpMV and true residual.  Beside it: the reference's
-own <float,double> instantiation (FP32 values, FP64 arithmetic: PRISM_FP32)
-and the solve with FP64 factor values.
+flexible CG + AMSED/MSLR (3 HID levels, natural order inside each domain
+(MatrixReorderNo), ILDLT(1e-3) blocks, ICT(1e-3) on the last level, low-rank
+correction of rank <= 32 per level from 64 classic generalized Lanczos steps,
+MSLR correction H = lambda/(1-lambda)), relative tolerance 1e-10, max 1000
+iterations.  `--precond ic` runs FCG + ICT(1e-3) on the same system instead.
+The preconditioner is set up once on the host (outside the timed region); one
+step is one complete device-resident solve.  The headline is the
+mixed-precision solve: FP32 factor values and FP32 arithmetic inside the
+streamed triangular sweeps (PRISM_FP32_APPLY), FP64 Krylov vectors, scalars,
+SpMV and true residual.  Beside it: the reference's own <float,double>
+instantiation (FP32 values, FP64 arithmetic: PRISM_FP32), the solve with FP64
+factor values, and the forward error of both against the reference's own FP64
+solution of the same system.
+
+The default run (N = 1) also measures the other benchmark configurations as
+extra keys of the same line ("configs"), each with the reference's CPU solver
+timed beside it: 2D Poisson 64^2 FCG + ICT; 3D convection-diffusion 100^3
+FGMRES(50) + GMSLR; batched solves (64 right-hand sides on 2D Poisson 512^2,
+256 uneven 2D systems); the differentiable 64^3 variable-coefficient solve.
+`--config N` prints configuration N alone.
 
 Multi-GPU: replicas only (one independent system per rank, no collective on the
 data path); the process group is used for the barrier and the max over ranks.
@@ -25,6 +34,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import platform
 import statistics
 import subprocess
 import sys
@@ -41,14 +51,13 @@ METRIC = "time-to-1e-10 rel. residual, mixed FP32-factor / FP64-Krylov, 1 B200"
 # wavefronts of the RCM order at the same iteration count.
 AMSED = dict(levels=3, lanczos_steps=64, low_rank=32, eig_bound=0.8, lowrank_type=0, lanczos_type=0, reorder=0)
 SEED = 2024
-# measured DRAM / algorithmic bytes of the level-0 lower sweep at 96^3, per sweep kernel (one ncu capture each;
-# profiles/k_sweep_level0_lower_96cube.md, profiles/k_sweep_stream_level0_lower_96cube.md)
-# DRAM / algorithmic bytes of each sweep kernel on the 96^3 level-0 lower sweep (183.6 MB
-# algorithmic): level order 181.2 MB (ncu capture); streamed with single-precision arithmetic
-# 188.0 MB captured with 6-byte record entries, plus the 49.9 MB the 8-byte {slot, value}
-# entries add to that sweep's records (175.1 -> 225.1 MB, computed from the layout; not
-# re-captured)
-TRAFFIC_RATIO = {"level-order": 181.2 / 183.6, "stream": (188.0 + 49.9) / 183.6}
+# DRAM bytes / algorithmic bytes of the streamed sweep kernel's level-0 lower sweep (one ncu capture on the
+# 96^3 case, profiles/k_sweep_stream_fp32apply_level0_lower_96cube.md), applied to each launch's algorithmic bytes
+TRAFFIC_RATIO = {"level-order": 181.2 / 183.6, "stream": 188.0 / 183.6}
+TRAFFIC_SOURCE = ("ncu capture of the level-0 lower sweep at 96^3 (183.6 MB algorithmic): DRAM read + write "
+                  "bytes / algorithmic bytes, scaled to this launch")
+# the reference library's timing build (oracle/Makefile FAST_FLAGS)
+REF_BUILD = "g++ -O3 -ffast-math -march=x86-64-v3 (AVX2, FMA) -fopenmp, 4 OpenMP threads (THREAD_NUM)"
 
 
 def workload(grid: int, tol: float, precond: str) -> str:
@@ -75,15 +84,17 @@ def parse():
     p.add_argument("--precond", default="amsed", choices=["amsed", "ic"])
     p.add_argument("--tol", type=float, default=1e-10)
     p.add_argument("--no-fp64", action="store_true", help="skip the FP64-factor comparison solve")
-    p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--cpu-sample-s", type=float, default=15.0, help="target seconds of reference CPU work")
+    p.add_argument("--no-cpu-baseline", action="store_true", help="skip every reference CPU measurement")
+    p.add_argument("--no-secondary", action="store_true", help="headline line without the other configurations")
     p.add_argument("--only-sweep", default=None, choices=["global", "stream"],
                    help="profiling aid: set up the workload with this sweep layout forced, run the level-0 "
                         "lower sweep of the preconditioner four times and the SpMV twice, and exit (no JSON line)")
-    p.add_argument("--config", type=int, default=2, choices=[2, 3, 4, 5],
-                   help="2: the headline (3D Poisson, FCG + AMSED); 3: 3D convection-diffusion 100^3, "
-                        "FGMRES(50) + GMSLR; 4: batched solves (64 RHS on 2D 512^2 + 256 uneven 2D systems); "
-                        "5: differentiable 64^3 variable-coefficient diffusion")
+    p.add_argument("--config", type=int, default=2, choices=[1, 2, 3, 4, 5],
+                   help="2: the headline (3D Poisson, FCG + AMSED); 1: 2D Poisson 64^2, FCG + ICT; 3: 3D "
+                        "convection-diffusion 100^3, FGMRES(50) + GMSLR; 4: batched solves (64 RHS on 2D 512^2 "
+                        "+ 256 uneven 2D systems); 5: differentiable 64^3 variable-coefficient diffusion")
+    p.add_argument("--full-batch-reference", action="store_true",
+                   help="config 4: time the reference on all 64 right-hand sides instead of 16")
     return p.parse_args()
 
 
@@ -143,15 +154,27 @@ def measured_peak_gbs():
         return 6650.0, "fallback"
 
 
+def host_cpu() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return f"{line.split(':', 1)[1].strip()}, nproc {os.cpu_count()}"
+    except Exception:
+        pass
+    return f"{platform.processor() or 'unknown CPU'}, nproc {os.cpu_count()}"
+
+
 # ---------------------------------------------------------------------------
-# reference CPU solver (oracle/_ref fast build, else the oracle port)
+# reference CPU solver (oracle/_ref timing build, else the oracle port)
 # ---------------------------------------------------------------------------
 class CpuReference:
-    """The reference's CG<double> + IncompleteCholesky<float,double> on the host
-    cores (oracle/_ref, built from the reference's sources with its Release
-    flags; 4 OpenMP threads as THREAD_NUM hard-wires), else the oracle port.
-    Setup runs once in the constructor (so the solve's own setup() is a no-op,
-    IncompleteCholesky.cpp:105) and is excluded from the timings."""
+    """The reference's CG<double> + AMSEDPrecondition<float,double> (or
+    IncompleteCholesky<float,double>) on the host cores (oracle/_ref, built from
+    the reference's sources with its Release flags; 4 OpenMP threads as
+    THREAD_NUM hard-wires), else the oracle port.  Setup runs once in the
+    constructor (so the solve's own setup() is a no-op, AMSEDPrecondition.cpp:
+    1952) and is excluded from the timings."""
 
     def __init__(self, grid: int, tol: float, precond: str = "amsed"):
         from oracle import ref
@@ -168,7 +191,7 @@ class CpuReference:
                 self.P = ref.RefPrecond(self.A, ref.KIND_IC, True, 1e-3)
             self.P.setup()
             self.cores, self.kind = 4, "reference"
-            self._solve = lambda k: ref.cg_solve(self.A, self.P, self.b, tol=tol, maxit=k, flexible=True)[1]
+            self._solve = lambda: ref.cg_solve(self.A, self.P, self.b, tol=tol, maxit=1000, flexible=True)[1]
         else:
             import prispack_b200 as PB
             from oracle import oracle as orc
@@ -181,36 +204,46 @@ class CpuReference:
                 rp, ci, v, _ = F.arrays(0)
                 OP = orc.Precond(1, A.n, (rp, ci, v))
             self.cores, self.kind = 1, "port"
-            self._solve = lambda k: orc.cg(A.rowptr, A.col, A.val, self.b, OP, tol=tol, maxit=k)[1]
+            self._solve = lambda: orc.cg(A.rowptr, A.col, A.val, self.b, OP, tol=tol, maxit=1000)[1]
         self.setup_s = time.perf_counter() - t0
 
-    def run(self, k: int):
+    def full(self) -> dict:
+        """One complete solve to the tolerance, timed unscaled."""
         t = time.perf_counter()
-        it = self._solve(k)
-        return time.perf_counter() - t, it
+        it = self._solve()
+        s = time.perf_counter() - t
+        build = REF_BUILD if self.kind == "reference" else "the oracle's C port, 1 thread"
+        return {"value": s * 1e3, "unit": "ms", "cores": self.cores, "kind": self.kind, "iters": it,
+                "sample": f"one full FCG solve to {self.tol:g} ({it} iterations, {s:.2f} s) of the same system; host "
+                          f"setup {self.setup_s:.1f} s excluded; {build}; host {host_cpu()}"}
 
-    def sample(self, sample_s: float, full_iters: int | None):
-        """Times a bounded sample of the solve: maxIter = k iterations for a k taking
-        about `sample_s` seconds, scaled to `full_iters` (None: run to convergence)."""
-        t2, _ = self.run(2)
-        per_iter = max(t2 / 2.0, 1e-6)
-        k = 1000 if full_iters is None else int(max(3, min(sample_s / per_iter, full_iters)))
-        tk, itk = self.run(k)
-        per_iter = tk / max(itk - 1, 1)
-        iters = full_iters or itk
-        return {"value": per_iter * iters * 1e3, "unit": "ms", "cores": self.cores, "kind": self.kind,
-                "iters": itk,
-                "sample": f"{itk - 1} FCG iterations ({tk:.1f} s) of the same solve, scaled to {iters} iterations; "
-                          f"host setup {self.setup_s:.1f} s excluded"}
+
+def reference_fp64_solution(grid: int, tol: float, precond: str):
+    """The reference's own FP64 solve of the headline system (parity build: no fast-math),
+    untimed: (x, iterations), or None where the reference build is absent."""
+    from oracle import ref
+    if not ref.available():
+        return None
+    A = ref.RefCSR.laplacian(grid, grid, grid)
+    if precond == "amsed":
+        a = AMSED
+        P = ref.RefAmsed(A, a["levels"], a["lanczos_steps"], a["low_rank"], a["eig_bound"], a["reorder"],
+                         a["lowrank_type"], a["lanczos_type"], False)
+    else:
+        P = ref.RefPrecond(A, ref.KIND_IC, False, 1e-3)
+    P.setup()
+    b = np.random.default_rng(SEED).standard_normal(grid ** 3)
+    x, it, _, conv = ref.cg_solve(A, P, b, tol=tol, maxit=1000, flexible=True)
+    return (x, it) if conv else None
 
 
 # ---------------------------------------------------------------------------
-# secondary workloads (one GPU; rank 0 only under torchrun)
+# secondary configurations (one GPU; rank 0 only)
 # ---------------------------------------------------------------------------
 CONVDIFF = dict(grid=100, pe=50.0, levels=4, low_rank=24, restart=50)
 
 
-def _device_ms(S, stream, fn, steps, warm):
+def _device_ms(stream, fn, steps, warm):
     import torch
     for _ in range(warm):
         fn()
@@ -222,6 +255,52 @@ def _device_ms(S, stream, fn, steps, warm):
     ev1.record(stream)
     torch.cuda.synchronize()
     return ev0.elapsed_time(ev1) / steps, out
+
+
+def _ref_ready(args):
+    if args.no_cpu_baseline:
+        return None
+    from oracle import ref
+    return ref if ref.available(fast=True) else None
+
+
+def bench_config1(args, local):
+    """2D Poisson 64^2 (n = 4096), FCG + ICT(1e-3), b ~ U[-1,1] seeded, tol 1e-8, max
+    1000 iterations: the reference's own CPU case.  L2-resident: a latency figure."""
+    import torch
+    import prispack_b200 as PB
+    A = PB.CSRMatrix.laplacian(64, 64, 1)
+    b_host = np.random.default_rng(SEED).uniform(-1.0, 1.0, A.n)
+    S = PB.DeviceSystem(A, device=local)
+    stream = torch.cuda.current_stream()
+    S.set_stream(stream.cuda_stream)
+    S.set_precond(PB.PRECOND_IC, tol=1e-3)
+    b = torch.tensor(b_host, device="cuda")
+    x = torch.zeros_like(b)
+
+    def one():
+        x.zero_()
+        return S.solve(b, x, tol=1e-8, max_iter=1000)[1]
+
+    ms, sts = _device_ms(stream, one, max(args.steps, 5) * 4, 3)
+    out = {"workload": "2D Poisson 5-pt 64^2 (n=4096, nnz=20224), FCG + ICT(1e-3), tol 1e-8, b~U[-1,1] "
+                       f"seed {SEED}, FP64", "ms": round(ms, 4), "iterations": sts[-1].num_iter,
+           "true_rel_residual": sts[-1].true_rel_residual}
+    ref = _ref_ready(args)
+    if ref is not None:
+        RA = ref.RefCSR.laplacian(64, 64, 1, fast=True)
+        RP = ref.RefPrecond(RA, ref.KIND_IC, False, 1e-3)
+        RP.setup()
+        reps, t = 20, time.perf_counter()
+        for _ in range(reps):
+            xr, itr, _, _ = ref.cg_solve(RA, RP, b_host, tol=1e-8, maxit=1000, flexible=True)
+        cpu_ms = (time.perf_counter() - t) * 1e3 / reps
+        _, st = S.solve(b_host, tol=1e-8, max_iter=1000, x_ref=xr)
+        out.update({"cpu_baseline": {"value": round(cpu_ms, 3), "unit": "ms", "cores": 4, "kind": "reference",
+                                     "iters": itr, "sample": f"mean of {reps} full reference FCG + "
+                                     f"IncompleteCholesky<double,double> solves; {REF_BUILD}"},
+                    "forward_error_vs_reference": st.forward_error, "iteration_diff": sts[-1].num_iter - itr})
+    return out
 
 
 def bench_convdiff(args, local):
@@ -239,7 +318,7 @@ def bench_convdiff(args, local):
     b_host = np.random.default_rng(SEED).standard_normal(A.n)
     stream = torch.cuda.current_stream()
     res = {}
-    for name, prec in (("fp32", PB.PRISM_FP32), ("fp64", PB.PRISM_FP64)):
+    for name, prec in (("fp32", PB.PRISM_FP32_APPLY), ("fp64", PB.PRISM_FP64)):
         t0 = time.perf_counter()
         G = PB.HostGmslr(A, levels=c["levels"], low_rank=c["low_rank"], precision=prec)
         setup_s = time.perf_counter() - t0
@@ -253,55 +332,51 @@ def bench_convdiff(args, local):
             x.zero_()
             return S.solve(b, x, solver=PB.SOLVER_FGMRES, tol=args.tol, max_iter=1000, restart=c["restart"])[1]
 
-        ms, sts = _device_ms(S, stream, one, args.steps, args.warmup)
+        ms, sts = _device_ms(stream, one, max(1, args.steps // 2), 1)
         st = sts[-1]
         res[name] = {"ms": ms, "iters": st.num_iter, "true_rel_residual": st.true_rel_residual,
-                     "converged": bool(st.converged), "host_setup_s": round(setup_s, 2), "info": G.info()}
-        if name == "fp32":
-            pin_b = torch.from_numpy(b_host).pin_memory()
-            pin_x = torch.zeros(A.n, dtype=torch.float64).pin_memory()
-            bnp, xnp = pin_b.numpy(), pin_x.numpy()
+                     "converged": bool(st.converged), "host_setup_s": round(setup_s, 2), "info": G.info(),
+                     "S": S, "G": G}
+    S32 = res["fp32"]["S"]
+    pin_b = torch.from_numpy(b_host).pin_memory()
+    pin_x = torch.zeros(A.n, dtype=torch.float64).pin_memory()
+    bnp, xnp = pin_b.numpy(), pin_x.numpy()
 
-            def host_one():
-                xnp[:] = 0.0
-                return S.solve(bnp, xnp, solver=PB.SOLVER_FGMRES, tol=args.tol, max_iter=1000,
-                               restart=c["restart"])[1]
+    def host_one():
+        xnp[:] = 0.0
+        return S32.solve(bnp, xnp, solver=PB.SOLVER_FGMRES, tol=args.tol, max_iter=1000, restart=c["restart"])[1]
 
-            res["e2e_ms"], _ = _device_ms(S, stream, host_one, max(1, args.steps), 1)
-        del S, G
-    cpu = None
-    if not args.no_cpu_baseline:
-        from oracle import ref
-        if ref.available(fast=True):
-            RA = ref.RefCSR.from_arrays(A.rowptr, A.col, A.val, fast=True)
-            RG = ref.RefGmslr(RA, c["levels"], 20, c["low_rank"], low_precision=True)
-            RG.setup()
-            t = time.perf_counter()
-            _, it, err, conv = ref.gmres_solve(RA, RG, b_host, tol=args.tol, restart=c["restart"], flexible=True)
-            cpu = {"value": round((time.perf_counter() - t) * 1e3, 1), "unit": "ms", "cores": 4, "kind": "reference",
-                   "sample": f"one full reference FGMRES({c['restart']}) + GMSLR solve: {it} iterations, "
-                             f"error {err:.2e}, converged {conv}; host setup excluded"}
+    e2e_ms, _ = _device_ms(stream, host_one, 1, 1)
+    cpu, fwd = None, {}
+    ref = _ref_ready(args)
+    if ref is not None:
+        RA = ref.RefCSR.from_arrays(A.rowptr, A.col, A.val, fast=True)
+        RG = ref.RefGmslr(RA, c["levels"], 20, c["low_rank"], low_precision=True)
+        RG.setup()
+        t = time.perf_counter()
+        xr, it, err, conv = ref.gmres_solve(RA, RG, b_host, tol=args.tol, restart=c["restart"], flexible=True)
+        cpu = {"value": round((time.perf_counter() - t) * 1e3, 1), "unit": "ms", "cores": 4, "kind": "reference",
+               "iters": it, "sample": f"one full reference FGMRES({c['restart']}) + GMSLR<float,double> solve: {it} "
+                                      f"iterations, error {err:.2e}, converged {conv}; host setup excluded; {REF_BUILD}"}
+        for name in ("fp32", "fp64"):
+            _, st = res[name]["S"].solve(b_host, solver=PB.SOLVER_FGMRES, tol=args.tol, max_iter=1000,
+                                         restart=c["restart"], x_ref=xr)
+            fwd[name] = st.forward_error
     r32, r64 = res["fp32"], res["fp64"]
     info = r32["info"]
-    line = {"metric": "time-to-1e-10 rel. residual, FGMRES(50) + GMSLR, mixed FP32-factor / FP64-Arnoldi, 1 B200",
-            "value": round(r32["ms"], 3), "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": round(r32["ms"], 3), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64 (Krylov) / f32 (factor values)", "data": "synthetic",
-            "config": {"workload": f"3D convection-diffusion {g}^3 (n={A.n}, nnz={A.nnz}), central diffusion + "
-                                   f"first-order upwind convection, v=(1,0.5,0.25)*{pe:g}, FGMRES({c['restart']}) + "
-                                   f"GMSLR ({c['levels']} levels, rank {c['low_rank']}), tol {args.tol:g}, "
-                                   f"b~N(0,1) seed {SEED}",
-                       "iterations": r32["iters"], "true_rel_residual": r32["true_rel_residual"],
-                       "converged": r32["converged"], "host_setup_s": r32["host_setup_s"],
-                       "gmslr": {"nlev": info["nlev"], "lev_ptr": info["lev_ptr"].tolist(),
-                                 "ncomps": info["ncomps"].tolist(), "ranks": info["ranks"].tolist(),
-                                 "mnnz": info["mnnz"]}},
-            "e2e": {"value": round(res["e2e_ms"], 3), "unit": "ms", "h2d_bytes_per_step": 16 * A.n,
+    return {"workload": f"3D convection-diffusion {g}^3 (n={A.n}, nnz={A.nnz}), central diffusion + first-order "
+                        f"upwind convection, v=(1,0.5,0.25)*{pe:g}, FGMRES({c['restart']}) + GMSLR ({c['levels']} "
+                        f"levels, rank {c['low_rank']}), tol {args.tol:g}, b~N(0,1) seed {SEED}",
+            "ms": round(r32["ms"], 3), "precision": "PRISM_FP32_APPLY", "iterations": r32["iters"],
+            "true_rel_residual": r32["true_rel_residual"], "converged": r32["converged"],
+            "host_setup_s": r32["host_setup_s"],
+            "gmslr": {"nlev": info["nlev"], "lev_ptr": info["lev_ptr"].tolist(), "ranks": info["ranks"].tolist(),
+                      "mnnz": info["mnnz"]},
+            "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": 16 * A.n,
                     "d2h_bytes_per_step": 8 * A.n},
             "fp64_factor": {"ms": round(r64["ms"], 3), "iters": r64["iters"],
                             "true_rel_residual": r64["true_rel_residual"], "mixed_speedup": r64["ms"] / r32["ms"]},
-            "cpu_baseline": cpu}
-    emit(line)
+            "forward_error_vs_reference": fwd or None, "cpu_baseline": cpu}
 
 
 def bench_adjoint(args, local):
@@ -334,7 +409,7 @@ def bench_adjoint(args, local):
         loss.backward()
         return kap.grad
 
-    ms, grads = _device_ms(S, stream, step, args.steps, args.warmup)
+    ms, grads = _device_ms(stream, step, max(1, args.steps // 2), 1)
     grad = grads[-1].cpu().numpy()
     # central differences without cancellation: L+ - L- = d . (2 x- + d - 2 x*), d = x+ - x-
     cells = rng.choice(D.n, 64, replace=False)
@@ -356,15 +431,13 @@ def bench_adjoint(args, local):
         fd.append(float(d @ (2 * xm + d - 2 * xs_host)) / (2 * h))
     fd = np.array(fd)
     err = np.abs(fd - grad[cells]) / np.maximum(np.abs(grad[cells]), 1e-12 * np.abs(grad).max())
-    line = {"metric": "forward + adjoint solve time, variable-coefficient diffusion, 1 B200", "value": round(ms, 3),
-            "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
-            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "3D variable-coefficient diffusion 64^3 (n=262144), kappa=exp(g), g Gaussian "
-                                   "random field (sigma 1, correlation length 8 cells), loss ||x - x*||^2, FCG + IC "
-                                   "(factored once), tol 1e-13; grad wrt kappa and b by the adjoint",
-                       "fd_check": {"cells": 64, "h": h, "max_rel_err": float(err.max()),
-                                    "median_rel_err": float(np.median(err))}}}
-    emit(line)
+    return {"workload": "3D variable-coefficient diffusion 64^3 (n=262144), kappa=exp(g), g Gaussian random field "
+                        "(sigma 1, correlation length 8 cells), loss ||x - x*||^2, FCG + IC (factored once), tol "
+                        "1e-13; grad wrt kappa and b by the adjoint",
+            "ms": round(ms, 3), "unit": "ms forward + adjoint",
+            "fd_check": {"cells": 64, "h": h, "max_rel_err": float(err.max()), "median_rel_err": float(np.median(err)),
+                         "within_1e-6": int((err <= 1e-6).sum())},
+            "cpu_baseline": None, "note": "the reference has no adjoint or gradient path"}
 
 
 def bench_batched(args, local):
@@ -373,9 +446,9 @@ def bench_batched(args, local):
     one block solve (prism_solve_batched) against 64 solves one after another;
     (b) 256 independent 2D Poisson systems on grids with sides drawn uniformly
     from 32..256, assembled on the diagonal of one CSR and solved together
-    (prism_solve_segments) against solving a sample of them one by one.  The
-    reference solves one right-hand side and one system per call: its CPU time
-    is estimated from a sample of single solves."""
+    (prism_solve_segments).  The reference solves one right-hand side and one
+    system per call: it is timed on 16 of the 64 right-hand sides (all 64 with
+    --full-batch-reference) and on all 256 systems."""
     import torch
     import prispack_b200 as PB
     torch.cuda.set_device(local)
@@ -388,12 +461,13 @@ def bench_batched(args, local):
     S = PB.DeviceSystem(A, device=local)
     S.set_stream(stream.cuda_stream)
     S.set_precond(PB.PRECOND_IC, tol=1e-3, precision=PB.PRISM_FP32)
-    B = torch.tensor(rng.standard_normal((k, A.n)), device="cuda")
+    B_host = rng.standard_normal((k, A.n))
+    B = torch.tensor(B_host, device="cuda")
 
     def block():
         return S.solve_batched(B, tol=tol, max_iter=1000)[1]
 
-    block_ms, bst = _device_ms(S, stream, block, max(1, args.steps // 2), 1)
+    block_ms, bst = _device_ms(stream, block, max(1, args.steps // 2), 1)
     bst = bst[-1]
     x0 = torch.zeros(A.n, dtype=torch.float64, device="cuda")
 
@@ -401,7 +475,7 @@ def bench_batched(args, local):
         x0.zero_()
         return S.solve(B[0], x0, tol=tol, max_iter=1000)[1]
 
-    single_ms, sst = _device_ms(S, stream, single, max(1, args.steps), 1)
+    single_ms, _ = _device_ms(stream, single, max(1, args.steps), 1)
     # ---- (b) 256 uneven systems
     sides = rng.integers(32, 257, size=256)
     blocks = [PB.CSRMatrix.laplacian(int(q), int(q), 1) for q in sides]
@@ -411,80 +485,57 @@ def bench_batched(args, local):
     Sb.set_stream(stream.cuda_stream)
     Sb.set_precond(PB.PRECOND_IC, tol=1e-3, precision=PB.PRISM_FP32)
     setup_s = time.perf_counter() - t0
-    bb = torch.tensor(rng.standard_normal(Ab.n), device="cuda")
+    bb_host = rng.standard_normal(Ab.n)
+    bb = torch.tensor(bb_host, device="cuda")
     xb = torch.zeros_like(bb)
 
     def segs():
         xb.zero_()
         return Sb.solve_segments(seg, bb, xb, tol=tol, max_iter=1000)[1]
 
-    seg_ms, segst = _device_ms(Sb, stream, segs, max(1, args.steps // 2), 1)
+    seg_ms, segst = _device_ms(stream, segs, max(1, args.steps // 2), 1)
     segst = segst[-1]
-    # one-by-one on a sample of the systems (device solves, handles set up outside the timing)
-    sample = rng.choice(256, 24, replace=False)
-    one_ms, one_rows = 0.0, 0
-    for q in sample:
-        Sq = PB.DeviceSystem(blocks[q], device=local)
-        Sq.set_stream(stream.cuda_stream)
-        Sq.set_precond(PB.PRECOND_IC, tol=1e-3, precision=PB.PRISM_FP32)
-        bq = bb[seg[q]:seg[q + 1]].clone()
-        xq = torch.zeros_like(bq)
-
-        def one():
-            xq.zero_()
-            return Sq.solve(bq, xq, tol=tol, max_iter=1000)[1]
-
-        ms, _ = _device_ms(Sq, stream, one, 2, 1)
-        one_ms += ms
-        one_rows += blocks[q].n
-        del Sq
-    one_by_one_est = one_ms * Ab.n / one_rows
     cpu = None
-    if not args.no_cpu_baseline:
-        from oracle import ref
-        if ref.available(fast=True):
-            RA = ref.RefCSR.laplacian(512, 512, 1, fast=True)
-            RP = ref.RefPrecond(RA, ref.KIND_IC, True, 1e-3)
-            RP.setup()
+    ref = _ref_ready(args)
+    if ref is not None:
+        RA = ref.RefCSR.laplacian(512, 512, 1, fast=True)
+        RP = ref.RefPrecond(RA, ref.KIND_IC, True, 1e-3)
+        RP.setup()
+        kk = k if args.full_batch_reference else 16
+        t = time.perf_counter()
+        for c in range(kk):
+            ref.cg_solve(RA, RP, B_host[c], tol=tol, maxit=1000, flexible=True)
+        rhs_s = time.perf_counter() - t
+        sys_s = 0.0
+        for q, Bq in enumerate(blocks):
+            Rq = ref.RefCSR.from_arrays(Bq.rowptr, Bq.col, Bq.val, fast=True)
+            Pq = ref.RefPrecond(Rq, ref.KIND_IC, True, 1e-3)
+            Pq.setup()
             t = time.perf_counter()
-            it = ref.cg_solve(RA, RP, B[0].cpu().numpy(), tol=tol, maxit=1000, flexible=True)[1]
-            per_rhs = time.perf_counter() - t
-            cpu_rows, cpu_s = 0, 0.0
-            for q in sample[:8]:
-                Bq = blocks[q]
-                Rq = ref.RefCSR.from_arrays(Bq.rowptr, Bq.col, Bq.val, fast=True)
-                Pq = ref.RefPrecond(Rq, ref.KIND_IC, True, 1e-3)
-                Pq.setup()
-                t = time.perf_counter()
-                ref.cg_solve(Rq, Pq, bb[seg[q]:seg[q + 1]].cpu().numpy(), tol=tol, maxit=1000, flexible=True)
-                cpu_s += time.perf_counter() - t
-                cpu_rows += Bq.n
-            est = (per_rhs * k + cpu_s * Ab.n / cpu_rows) * 1e3
-            cpu = {"value": round(est, 1), "unit": "ms", "cores": 4, "kind": "reference",
-                   "sample": f"one reference FCG + ICT solve of the 512^2 system ({it} iterations, "
-                             f"{per_rhs:.2f} s) times 64, plus 8 of the uneven systems scaled by rows to all 256; "
-                             "setup excluded"}
-    total = block_ms + seg_ms
+            ref.cg_solve(Rq, Pq, bb_host[seg[q]:seg[q + 1]], tol=tol, maxit=1000, flexible=True)
+            sys_s += time.perf_counter() - t
+        cpu = {"value": round((rhs_s * k / kk + sys_s) * 1e3, 1), "unit": "ms", "cores": 4, "kind": "reference",
+               "block_rhs_measured": kk, "block_rhs_ms_measured": round(rhs_s * 1e3, 1),
+               "uneven_systems_ms_measured": round(sys_s * 1e3, 1),
+               "sample": f"reference FCG + IncompleteCholesky<float,double> solves timed one by one: {kk} of the 64 "
+                         f"right-hand sides ({rhs_s:.2f} s; the total counts {k}/{kk} times that) and all 256 uneven "
+                         f"systems ({sys_s:.2f} s); setups excluded; {REF_BUILD}"}
     its = [q.num_iter for q in segst]
-    line = {"metric": "batched time-to-1e-10: 64 RHS on 2D Poisson 512^2 + 256 uneven 2D Poisson systems, 1 B200",
-            "value": round(total, 3), "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": round(total, 3), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64 (Krylov) / f32 (factor values)", "data": "synthetic",
-            "config": {"workload": "FCG + ICT(1e-3), FP32 factor values, tol 1e-10; (a) 2D Poisson 512^2 "
-                                   "(n=262144) with 64 N(0,1) right-hand sides; (b) 256 2D Poisson systems, sides "
-                                   f"U{{32..256}} seed {SEED} (total n={Ab.n}, nnz={Ab.nnz})",
-                       "block_of_64": {"ms": round(block_ms, 3), "iters": [q.num_iter for q in bst][:4] + ["..."],
-                                       "all_converged": all(q.converged for q in bst),
-                                       "one_rhs_alone_ms": round(single_ms, 3),
-                                       "speedup_vs_64_single": round(64 * single_ms / block_ms, 2)},
-                       "uneven_256": {"ms": round(seg_ms, 3), "iters_min_max": [min(its), max(its)],
-                                      "all_converged": all(q.converged for q in segst),
-                                      "max_true_rel_residual": max(q.true_rel_residual for q in segst),
-                                      "one_by_one_est_ms": round(one_by_one_est, 1),
-                                      "speedup_vs_one_by_one": round(one_by_one_est / seg_ms, 2),
-                                      "host_setup_s": round(setup_s, 1)}},
+    return {"workload": "FCG + ICT(1e-3), FP32 factor values, tol 1e-10; (a) 2D Poisson 512^2 (n=262144) with 64 "
+                        f"N(0,1) right-hand sides; (b) 256 2D Poisson systems, sides U{{32..256}} seed {SEED} "
+                        f"(total n={Ab.n}, nnz={Ab.nnz})",
+            "ms": round(block_ms + seg_ms, 3),
+            "block_of_64": {"ms": round(block_ms, 3), "iters_first4": [q.num_iter for q in bst][:4],
+                            "all_converged": all(q.converged for q in bst), "one_rhs_alone_ms": round(single_ms, 3),
+                            "speedup_vs_64_single": round(64 * single_ms / block_ms, 2)},
+            "uneven_256": {"ms": round(seg_ms, 3), "iters_min_max": [min(its), max(its)],
+                           "all_converged": all(q.converged for q in segst),
+                           "max_true_rel_residual": max(q.true_rel_residual for q in segst),
+                           "host_setup_s": round(setup_s, 1)},
             "cpu_baseline": cpu}
-    emit(line)
+
+
+SECONDARY = {1: bench_config1, 3: bench_convdiff, 4: bench_batched, 5: bench_adjoint}
 
 
 # ---------------------------------------------------------------------------
@@ -506,6 +557,22 @@ def emit(obj):
     out.flush()
 
 
+def standalone_line(n: int, r: dict, args) -> dict:
+    """A secondary configuration as its own JSON line (--config N)."""
+    metric = {1: "time-to-1e-8 rel. residual, FCG + ICT, 2D Poisson 64^2, 1 B200",
+              3: "time-to-1e-10 rel. residual, FGMRES(50) + GMSLR, mixed FP32-factor / FP64-Arnoldi, 1 B200",
+              4: "batched time-to-1e-10: 64 RHS on 2D Poisson 512^2 + 256 uneven 2D Poisson systems, 1 B200",
+              5: "forward + adjoint solve time, variable-coefficient diffusion, 1 B200"}[n]
+    line = {"metric": metric, "value": r["ms"], "unit": "ms", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": r["ms"], "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if n in (1, 5) else "f64 (Krylov) / f32 (factor values)",
+            "data": "synthetic", "config": {k: v for k, v in r.items() if k not in ("ms", "cpu_baseline", "e2e")},
+            "cpu_baseline": r.get("cpu_baseline")}
+    if "e2e" in r:
+        line["e2e"] = r["e2e"]
+    return line
+
+
 def main():
     args = parse()
     quiet_stdout()
@@ -519,7 +586,9 @@ def main():
                 emit({"impl": "reference", "unavailable": "secondary configs carry their reference "
                       "timing in the prism line's cpu_baseline"})
             return
-        return {3: bench_convdiff, 4: bench_batched, 5: bench_adjoint}[args.config](args, local)
+        import torch
+        torch.cuda.set_device(local)
+        return emit(standalone_line(args.config, SECONDARY[args.config](args, local), args))
 
     if args.impl == "reference":
         return reference_arm(args, rank, world)
@@ -667,6 +736,21 @@ def main():
     spmv_bytes = 12 * A.nnz + 20 * n + 4
     spmv_gbs = spmv_bytes / (statistics.median(spmv_ms) * 1e-3) / 1e9
 
+    # ---- the reference's own FP64 solution of the same system (untimed): forward errors
+    xref = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            xref = reference_fp64_solution(g, args.tol, args.precond)
+        except Exception as e:  # reported, not fatal
+            print(f"reference FP64 solve failed: {e}", file=sys.stderr)
+    parity = None
+    if xref is not None:
+        xr_d = torch.tensor(xref[0], device="cuda")
+        x.zero_()
+        _, stp = S.solve(b, x, tol=args.tol, max_iter=1000, x_ref=xr_d)
+        parity = {"reference_fp64_iters": xref[1], "mixed": {"forward_error": stp.forward_error,
+                                                              "iteration_diff": stp.num_iter - xref[1]}}
+
     # ---- FP64-factor solve beside it
     fp64 = None
     fp32_storage = None
@@ -678,6 +762,10 @@ def main():
         ms64, stats64, _ = timed_solves(max(1, args.steps // 2), 1)
         fp64 = {"ms": ms64, "iters": stats64[-1][0], "true_rel_residual": stats64[-1][1],
                 "mixed_speedup": ms64 / ms32, "host_setup_s": setup64_s}
+        if xref is not None:
+            x.zero_()
+            _, stp = S.solve(b, x, tol=args.tol, max_iter=1000, x_ref=xr_d)
+            parity["fp64"] = {"forward_error": stp.forward_error, "iteration_diff": stp.num_iter - xref[1]}
         # the reference's <float,double> instantiation: float values, double arithmetic
         FS = build_precond(PB, A, args.precond, PB.PRISM_FP32)
         S.attach(FS)
@@ -694,12 +782,26 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            cpu = CpuReference(g, args.tol, args.precond).sample(args.cpu_sample_s, iters)
+            cpu = CpuReference(g, args.tol, args.precond).full()
             cpu.pop("iters", None)
         except Exception as e:  # reported, not fatal
             cpu = {"value": None, "unit": "ms", "cores": 0, "kind": "unavailable", "sample": str(e)[:200]}
 
+    configs = None
+    if rank == 0 and world == 1 and not args.no_secondary:
+        configs = {}
+        for k, fn in SECONDARY.items():
+            try:
+                configs[str(k)] = fn(args, local)
+            except Exception as e:  # reported, not fatal
+                configs[str(k)] = {"error": f"{type(e).__name__}: {e}"[:300]}
+
     if rank == 0:
+        amsed_info = None
+        if args.precond == "amsed":
+            amsed_info = {k: (v.tolist() if hasattr(v, "tolist") else v) for k, v in F32.info().items()}
+            amsed_info["note"] = ("ranks: the MSLR correction keeps the eigenpairs above the bound; rank 32 is a cap "
+                                  "that this operator does not reach")
         line = {
             "metric": METRIC,
             "value": round(ms32, 4),
@@ -713,10 +815,8 @@ def main():
             "vs_baseline": None,
             "dtype": "f64 (Krylov, SpMV, residual) / f32 (factor values and sweep arithmetic)",
             "data": "synthetic",
-            "config": {"workload": workload(g, args.tol, args.precond), "n": n, "nnz": A.nnz, "precond_nnz": F32.info()["mnnz"],
-                       "precision": "PRISM_FP32_APPLY",
-                       "amsed": ({k: (v.tolist() if hasattr(v, "tolist") else v) for k, v in F32.info().items()}
-                                 if args.precond == "amsed" else None),
+            "config": {"workload": workload(g, args.tol, args.precond), "n": n, "nnz": A.nnz,
+                       "precond_nnz": F32.info()["mnnz"], "precision": "PRISM_FP32_APPLY", "amsed": amsed_info,
                        "iterations": iters, "true_rel_residual": stats32[-1][1],
                        "converged": bool(stats32[-1][2]), "host_setup_s": round(setup32_s, 2),
                        "l2": "inputs larger than L2 (A 216 MB + factor > 600 MB per solve)",
@@ -731,22 +831,21 @@ def main():
                          "frac": round(achieved / peak, 4), "peak_source": peak_src,
                          "bytes_per_launch": sweep_bytes, "launch_ms": [round(t, 4) for t in sweep_ms],
                          "rows": [i["n"] for i in sweep_infos], "wavefronts": [i["levels"] for i in sweep_infos],
+                         "us_per_wavefront": [round(t * 1e3 / max(i["levels"], 1), 4)
+                                              for t, i in zip(sweep_ms, sweep_infos)],
                          "kernels": [i["kernel"] for i in sweep_infos],
-                         # DRAM bytes per launch: the ratio DRAM / algorithmic bytes of one ncu capture
-                         # of each sweep kernel on the 96^3 case, applied to this launch's algorithmic bytes
                          "traffic": round(statistics.mean(TRAFFIC_RATIO.get(i["kernel"], 1.0) * b_
                                                           for i, b_ in zip(sweep_infos, sweep_bytes))),
-                         "traffic_source": "per 183.6 MB algorithmic at 96^3: level order 181.2 MB (ncu); streamed "
-                                           "237.9 MB = 188.0 MB ncu capture with 6-byte entries + 49.9 MB record "
-                                           "growth of the 8-byte entries (layout arithmetic, not re-captured); "
-                                           "scaled by rows"},
+                         "traffic_source": TRAFFIC_SOURCE},
             "spmv": {"ms": round(statistics.median(spmv_ms), 4), "bytes": spmv_bytes, "GB/s": round(spmv_gbs, 1),
                      "frac": round(spmv_gbs / peak, 4)},
             "fp64_factor": fp64,
             "fp32_storage": fp32_storage,
+            "parity_vs_reference_fp64": parity,
             "cpu_baseline": cpu,
             "gpu_launches": int(launches / max(args.steps, 1)) * args.steps,
             "clocks": clk,
+            "configs": configs,
         }
         emit(line)
     if dist is not None:
@@ -766,20 +865,20 @@ def max_over_ranks(values, dist=None, device="cpu"):
 
 
 def reference_arm(args, rank, world):
-    """The reference's own CPU solver on the host cores (rank 0 only)."""
+    """The reference's own CPU solver on the host cores (rank 0 only): each step
+    one complete solve to the tolerance, timed unscaled."""
     if rank != 0:
         return
     from oracle import ref
     R = CpuReference(args.grid, args.tol, args.precond)
-    full = R.sample(0.0, None)          # one full solve: learns the iteration count (untimed warm-up)
-    full_iters = full["iters"]
-    vals, desc = [], full
-    for i in range(max(0, args.warmup - 1) + args.steps):
-        r = R.sample(args.cpu_sample_s, full_iters)
-        if i >= max(0, args.warmup - 1):
-            vals.append(r["value"])
-        desc = r
-    v = statistics.mean(vals)
+    first = R.full()  # untimed warm-up; also sizes the run
+    # every step is one full solve; at most about 150 s of them, so that the arm ends in minutes
+    steps = max(1, min(args.steps, int(150e3 / max(first["value"], 1.0))))
+    runs = [R.full() for _ in range(steps)]
+    v = statistics.mean(r["value"] for r in runs)
+    desc = runs[-1]
+    if steps < args.steps:
+        desc["sample"] += f"; mean of {steps} timed solves (of {args.steps} steps asked, to bound the run)"
     line = {"impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "ms", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(v, 3), "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64 (Krylov) / f32 (factor values)",

@@ -92,6 +92,10 @@ typedef struct prism_solve_opts {
     double tol;                   /* relative residual tolerance (CG.cpp:59, GMRES.cpp:194) */
     uint32_t max_iter;            /* CG: maxIter (CG.cpp:57); GMRES: 500 as MAX_ITER_NUM_SOLVER (config.h:25) */
     uint32_t restart;             /* GMRES restart m; 0 = no restart (setRestart(false, .)) */
+    const double* x_ref;          /* optional reference solution (device pointer for the *_device calls,
+                                     host pointer for the host-buffer calls; NULL: none): the solve then
+                                     reports its forward error against it.  Ignored by the adjoint, block
+                                     and batch solves.  No reference counterpart. */
 } prism_solve_opts;
 
 typedef struct prism_solve_stats {
@@ -102,6 +106,8 @@ typedef struct prism_solve_stats {
     uint32_t precond_applies;     /* number of M^{-1} applications performed */
     uint32_t spmv_count;          /* number of A x products performed */
     double device_ms;             /* device time of the solve (CUDA events on the handle's stream) */
+    double forward_error;         /* ||x - x_ref||_2 / ||x_ref||_2 in FP64 when opts.x_ref is given, else -1
+                                     (measured after the solve, outside device_ms) */
 } prism_solve_stats;
 
 typedef struct prism_handle_s* prism_handle;
@@ -133,6 +139,31 @@ int32_t prism_selftest_wait_timeout(int32_t device, uint64_t wait_ns, int32_t* d
 int32_t prism_selftest_stream_layout(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val,
                                      const double* diag, int32_t op, int32_t lower, int32_t precision,
                                      uint32_t num_ctas, uint32_t rows_per_cta, const double* in, double* out);
+
+/* The summation order of the streamed sweep kernel, for checking its
+ * arithmetic against the oracle.  For a gather-form triangular sweep given as
+ * for prism_selftest_stream_layout (row r lists its dependencies on one side
+ * of the diagonal) laid out in at most num_ctas slabs: for each row r,
+ * [eptr[r], eptr[r+1]) of edep/ecoef are its "early" positions and
+ * [kptr[r], kptr[r+1]) of kdep/kcoef its "late" ones, in the order the kernel
+ * sums them (dependency row, or 0xFFFFFFFF for a padding position with
+ * coefficient 0).  The kernel's sum of row r is
+ *   c_i = fma chains over early positions p = 4g + i  (c_i = fma(coef, x, c_i)),
+ *   s = (c0 + c1) + (c2 + c3), then s = fma(coef, x, s) over the late positions,
+ * in float for PRISM_FP32_APPLY, else in double; then op 0/1: (in - s) * d,
+ * 2: in - s, 3: in * d - s with d = 1 / diag (ops 0, 3) or diag (op 1).
+ * eptr and kptr (n + 1 each) are always filled; edep/ecoef/kdep/kcoef may be
+ * NULL (sizes only).  No reference counterpart (the reference sums each row
+ * in stored order, IncompleteLDLT.cpp:188-233). */
+int32_t prism_stream_sweep_order(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val,
+                                 const double* diag, int32_t op, int32_t lower, int32_t precision, uint32_t num_ctas,
+                                 uint32_t* eptr, uint32_t* edep, double* ecoef, uint32_t* kptr, uint32_t* kdep,
+                                 double* kcoef);
+/* Runs the streamed sweep kernel alone on `device` for the same sweep and
+ * slabs as prism_stream_sweep_order (host in and out): out = T^{-1} in. */
+int32_t prism_stream_sweep_run(int32_t device, uint32_t n, const uint32_t* rowptr, const uint32_t* col,
+                               const double* val, const double* diag, int32_t op, int32_t lower, int32_t precision,
+                               uint32_t num_ctas, const double* in, double* out);
 
 /* True residual norms of k right-hand sides without any allocation.  No
  * counterpart in the reference (its solvers only report the recursive
@@ -283,6 +314,18 @@ int32_t prism_precond_sweep_device(prism_handle h, int32_t sweep, const double* 
                                    int32_t prepare);
 int32_t prism_precond_sweep_info(prism_handle h, int32_t sweep, uint32_t* n, uint64_t* nnz,
                                  uint32_t* value_bytes, uint32_t* num_levels, uint32_t* kernel);
+
+/* The summation order of one of the handle's sweeps (numbered as for
+ * prism_precond_sweep_device) when it runs the streamed kernel, in the form of
+ * prism_stream_sweep_order, rows numbered as the sweep's, together with the
+ * sweep itself: diag (n, may be NULL) its per-row diagonal as stored (d of the
+ * sum's last step is 1 / diag for ops 0 and 3), *op and *lower (may be NULL).
+ * *n receives the sweep's rows; pass NULL eptr and kptr to query it alone.
+ * PRISM_ERR_UNSUPPORTED when the sweep runs another kernel.  No reference
+ * counterpart; for checking the kernel against the oracle. */
+int32_t prism_precond_sweep_order(prism_handle h, int32_t sweep, uint32_t* n, uint32_t* eptr, uint32_t* edep,
+                                  double* ecoef, uint32_t* kptr, uint32_t* kdep, double* kcoef, double* diag,
+                                  int32_t* op, int32_t* lower);
 
 /* ---- solvers ------------------------------------------------------------- */
 /* x is the in/out initial guess, as BaseSolver::solve (BaseSolver.h:16). */

@@ -59,14 +59,16 @@ void orc_spmv(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const dou
     }
 }
 
-/* One triangular sweep in gather form, in single precision: the arithmetic of
- * the library's single-precision apply (PRISM_FP32_APPLY), which has no
- * reference counterpart.  Row r (in dependency order: increasing for a lower
- * sweep, decreasing for an upper one) sums its entries in order,
- * s += val[k] * out[col[k]], each value, product and sum rounded to float, and
+/* One triangular sweep in gather form, in single precision, in the reference's
+ * order: row r (in dependency order: increasing for a lower sweep, decreasing
+ * for an upper one) sums its entries in stored order, as IncompleteLDLT.cpp:
+ * 188-233 and IncompleteCholesky.cpp:249-295 do, s += val[k] * out[col[k]],
+ * each value, product and sum rounded to float, and
  *   op 0: (in - s) / diag   op 1: (in - s) * diag   op 2: in - s   op 3: in / diag - s
  * with in and diag rounded to float first; out holds the float results
- * widened to double. */
+ * widened to double.  This is a tolerance reference for the library's
+ * single-precision apply, whose kernel sums in another order (see
+ * orc_sweep_ordered for that order). */
 void orc_sweep_f32(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val,
                    const double* diag, int op, int lower, const double* in, double* out) {
     float* x = (float*)malloc(sizeof(float) * (n ? n : 1));
@@ -84,6 +86,70 @@ void orc_sweep_f32(uint32_t n, const uint32_t* rowptr, const uint32_t* col, cons
         out[r] = (double)res;
     }
     free(x);
+}
+
+/* One triangular sweep in gather form in the summation order of the library's
+ * streamed sweep kernel (no reference counterpart: the reference sums each row
+ * in stored order).  For row r, [eptr[r], eptr[r+1]) of edep/ecoef are its
+ * "early" positions and [kptr[r], kptr[r+1]) of kdep/kcoef its "late" ones; a
+ * dependency of 0xFFFFFFFF is padding (value 0).  In the working precision
+ * (float when single != 0, else double), every product-sum one fused
+ * multiply-add:
+ *   c_i = fma(coef, x, c_i) over early positions p with p mod 4 == i, from 0,
+ *   s = (c0 + c1) + (c2 + c3),  then s = fma(coef, x, s) over the late positions,
+ *   op 0, 1: (in - s) * d    op 2: in - s    op 3: in * d - s,
+ * with in rounded to the working precision and d = 1 / diag (ops 0, 3, the
+ * division in double) or diag (op 1), then rounded.  Rows run in dependency
+ * order (increasing for a lower sweep, decreasing for an upper one); out holds
+ * the results widened to double. */
+void orc_sweep_ordered(uint32_t n, int single, int op, int lower, const uint32_t* eptr, const uint32_t* edep,
+                       const double* ecoef, const uint32_t* kptr, const uint32_t* kdep, const double* kcoef,
+                       const double* diag, const double* in, double* out) {
+    float* xf = single ? (float*)malloc(sizeof(float) * (n ? n : 1)) : NULL;
+    double* xd = single ? NULL : (double*)malloc(sizeof(double) * (n ? n : 1));
+    for (uint32_t t = 0; t < n; t++) {
+        const uint32_t r = lower ? t : n - 1 - t;
+        const double dd = op == 0 || op == 3 ? 1.0 / diag[r] : (op == 1 ? diag[r] : 1.0);
+        if (single) {
+            float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+            for (uint32_t p = eptr[r]; p < eptr[r + 1]; p++) {
+                const float x = edep[p] == 0xFFFFFFFFu ? 0.0f : xf[edep[p]];
+                c[(p - eptr[r]) & 3] = fmaf((float)ecoef[p], x, c[(p - eptr[r]) & 3]);
+            }
+            float s = (c[0] + c[1]) + (c[2] + c[3]);
+            for (uint32_t p = kptr[r]; p < kptr[r + 1]; p++) {
+                const float x = kdep[p] == 0xFFFFFFFFu ? 0.0f : xf[kdep[p]];
+                s = fmaf((float)kcoef[p], x, s);
+            }
+            const float b = (float)in[r], d = (float)dd;
+            float res;
+            if (op == 0 || op == 1) res = (b - s) * d;
+            else if (op == 2) res = b - s;
+            else res = b * d - s;
+            xf[r] = res;
+            out[r] = (double)res;
+        } else {
+            double c[4] = {0.0, 0.0, 0.0, 0.0};
+            for (uint32_t p = eptr[r]; p < eptr[r + 1]; p++) {
+                const double x = edep[p] == 0xFFFFFFFFu ? 0.0 : xd[edep[p]];
+                c[(p - eptr[r]) & 3] = fma(ecoef[p], x, c[(p - eptr[r]) & 3]);
+            }
+            double s = (c[0] + c[1]) + (c[2] + c[3]);
+            for (uint32_t p = kptr[r]; p < kptr[r + 1]; p++) {
+                const double x = kdep[p] == 0xFFFFFFFFu ? 0.0 : xd[kdep[p]];
+                s = fma(kcoef[p], x, s);
+            }
+            const double b = in[r];
+            double res;
+            if (op == 0 || op == 1) res = (b - s) * dd;
+            else if (op == 2) res = b - s;
+            else res = b * dd - s;
+            xd[r] = res;
+            out[r] = res;
+        }
+    }
+    free(xf);
+    free(xd);
 }
 
 /* ---- AMSED ----------------------------------------------------------------- */
@@ -122,9 +188,25 @@ static void ilut_inplace(uint32_t n, const uint32_t* lrp, const uint32_t* lci, c
 
 /* levelBlockInvSolve (AMSEDPrecondition.cpp:1690-1754, GMSLRDPrecondition.cpp:1170-1229):
  * x starts at the level's first row */
+/* the level's block solve as the two kernel-order sweeps (single-precision apply) */
+static void amsed_ordered_block_solve(const orc_amsed* S, const orc_amsed_level* L, double* x) {
+    const orc_sweep_order* lo = L->sweep_lo;
+    const orc_sweep_order* up = L->sweep_up;
+    double* t = malloc((size_t)(lo->n ? lo->n : 1) * sizeof(double));
+    orc_sweep_ordered(lo->n, S->single, lo->op, lo->lower, lo->eptr, lo->edep, lo->ecoef, lo->kptr, lo->kdep,
+                      lo->kcoef, lo->diag, x, t);
+    orc_sweep_ordered(up->n, S->single, up->op, up->lower, up->eptr, up->edep, up->ecoef, up->kptr, up->kdep,
+                      up->kcoef, up->diag, t, x);
+    free(t);
+}
+
 static void amsed_block_solve(const orc_amsed* S, uint32_t level, double* x) {
     const orc_amsed_level* L = &S->levels[level];
     const int last = level == S->nlev - 1;
+    if (L->sweep_lo) {
+        amsed_ordered_block_solve(S, L, x);
+        return;
+    }
     for (uint32_t b = 0; b < L->ncomps; b++) {
         double* seg = x + (L->dom_ptr[b] - L->dom_ptr[0]);
         uint32_t nb = L->dom_ptr[b + 1] - L->dom_ptr[b];
@@ -145,7 +227,9 @@ static void amsed_c_solve(const orc_amsed* S, int level, double* x) {
     const int next = level + 1;
     if (level == (int)S->nlev - 2) {
         const orc_amsed_level* LL = &S->levels[S->nlev - 1];
-        if (S->gmslr)
+        if (LL->sweep_lo)
+            amsed_ordered_block_solve(S, LL, x);
+        else if (S->gmslr)
             ilut_inplace(LL->dom_ptr[1] - LL->dom_ptr[0], LL->blk_rp[0], LL->blk_ci[0], LL->blk_val[0], LL->blk_rp1[0],
                          LL->blk_ci1[0], LL->blk_val1[0], LL->blk_diag[0], x);
         else

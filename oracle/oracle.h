@@ -13,6 +13,20 @@
 #define PRISM_ORACLE_H
 #include <stdint.h>
 
+/* A triangular sweep in the streamed kernel's summation order (arguments of
+ * orc_sweep_ordered); used by orc_amsed_apply for the single-precision apply. */
+typedef struct orc_sweep_order {
+    uint32_t n;
+    int op, lower;
+    const uint32_t* eptr;
+    const uint32_t* edep;
+    const double* ecoef;
+    const uint32_t* kptr;
+    const uint32_t* kdep;
+    const double* kcoef;
+    const double* diag;
+} orc_sweep_order;
+
 /* One level of an AMSED/MSLR hierarchy (LevelStructure,
  * include/Preconditioner/AMSEDPrecondition.h:75-85) in permuted numbering. */
 typedef struct orc_amsed_level {
@@ -35,11 +49,16 @@ typedef struct orc_amsed_level {
     const uint32_t* f_rp;
     const uint32_t* f_ci;
     const double* f_val;
+    /* when set, the level's block solve is these two kernel-order sweeps over its
+     * first sweep_lo->n rows (orc_amsed.single selects float arithmetic) */
+    const orc_sweep_order* sweep_lo;
+    const orc_sweep_order* sweep_up;
 } orc_amsed_level;
 
 typedef struct orc_amsed {
     uint32_t n, nlev;
     int gmslr;                        /* 0: AMSED, 1: GMSLR */
+    int single;                       /* kernel-order sweeps (levels' sweep_lo/up) in float */
     const uint32_t* pperm;            /* new -> original */
     const uint32_t* lev_ptr;          /* nlev + 1 */
     const orc_amsed_level* levels;
@@ -66,9 +85,13 @@ void orc_laplacian(int nx, int ny, int nz, double ax, double ay, double az, doub
                    uint32_t* rowptr, uint32_t* col, double* val);
 void orc_spmv(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val,
               const double* x, double* y);
-/* a gather-form triangular sweep in single precision (see oracle.c) */
+/* a gather-form triangular sweep in single precision, reference order (see oracle.c) */
 void orc_sweep_f32(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val,
                    const double* diag, int op, int lower, const double* in, double* out);
+/* a gather-form triangular sweep in the streamed kernel's summation order (see oracle.c) */
+void orc_sweep_ordered(uint32_t n, int single, int op, int lower, const uint32_t* eptr, const uint32_t* edep,
+                       const double* ecoef, const uint32_t* kptr, const uint32_t* kdep, const double* kcoef,
+                       const double* diag, const double* in, double* out);
 void orc_precond_apply(const orc_precond* P, double* vec);
 void orc_cg(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val,
             const orc_precond* P, int flexible, double tol, uint32_t max_iter,

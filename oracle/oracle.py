@@ -23,12 +23,19 @@ class _AmsedLevel(C.Structure):
                 ("e_rp", C.c_void_p), ("e_ci", C.c_void_p), ("e_val", C.c_void_p),
                 ("rank", C.c_uint32), ("W", C.c_void_p), ("H", C.c_void_p),
                 ("blk_rp1", C.c_void_p), ("blk_ci1", C.c_void_p), ("blk_val1", C.c_void_p),
-                ("f_rp", C.c_void_p), ("f_ci", C.c_void_p), ("f_val", C.c_void_p)]
+                ("f_rp", C.c_void_p), ("f_ci", C.c_void_p), ("f_val", C.c_void_p),
+                ("sweep_lo", C.c_void_p), ("sweep_up", C.c_void_p)]
+
+
+class _SweepOrder(C.Structure):
+    _fields_ = [("n", C.c_uint32), ("op", C.c_int), ("lower", C.c_int),
+                ("eptr", C.c_void_p), ("edep", C.c_void_p), ("ecoef", C.c_void_p),
+                ("kptr", C.c_void_p), ("kdep", C.c_void_p), ("kcoef", C.c_void_p), ("diag", C.c_void_p)]
 
 
 class _Amsed(C.Structure):
-    _fields_ = [("n", C.c_uint32), ("nlev", C.c_uint32), ("gmslr", C.c_int), ("pperm", C.c_void_p),
-                ("lev_ptr", C.c_void_p), ("levels", C.c_void_p)]
+    _fields_ = [("n", C.c_uint32), ("nlev", C.c_uint32), ("gmslr", C.c_int), ("single", C.c_int),
+                ("pperm", C.c_void_p), ("lev_ptr", C.c_void_p), ("levels", C.c_void_p)]
 
 
 class _Precond(C.Structure):
@@ -55,6 +62,8 @@ def lib() -> C.CDLL:
                                        C.c_double, _u32p, _u32p, _f64p]
         _LIB.orc_spmv.argtypes = [C.c_uint32, _u32p, _u32p, _f64p, _f64p, _f64p]
         _LIB.orc_sweep_f32.argtypes = [C.c_uint32, _u32p, _u32p, _f64p, C.c_void_p, C.c_int, C.c_int, _f64p, _f64p]
+        _LIB.orc_sweep_ordered.argtypes = [C.c_uint32, C.c_int, C.c_int, C.c_int, _u32p, _u32p, _f64p, _u32p, _u32p,
+                                           _f64p, C.c_void_p, _f64p, _f64p]
         _LIB.orc_precond_apply.argtypes = [C.POINTER(_Precond), _f64p]
         _LIB.orc_amsed_apply.argtypes = [C.POINTER(_Amsed), _f64p]
         _LIB.orc_cg.argtypes = [C.c_uint32, _u32p, _u32p, _f64p, C.POINTER(_Precond), C.c_int, C.c_double,
@@ -84,14 +93,29 @@ def spmv(rp, ci, v, x):
 
 
 def sweep_f32(rp, ci, v, b, *, diag=None, op=2, lower=True):
-    """Gather-form triangular sweep in single precision (the single-precision
-    apply's arithmetic); returns the float results widened to double."""
+    """Gather-form triangular sweep in single precision in the reference's order
+    (each row summed in stored order); returns the float results widened to double."""
     rp = np.ascontiguousarray(rp, np.uint32)
     out = np.zeros(len(rp) - 1)
     d = np.ascontiguousarray(diag, np.float64) if diag is not None else None
     lib().orc_sweep_f32(len(rp) - 1, rp, np.ascontiguousarray(ci, np.uint32), np.ascontiguousarray(v, np.float64),
                         d.ctypes.data if d is not None else None, int(op), int(bool(lower)),
                         np.ascontiguousarray(b, np.float64), out)
+    return out
+
+
+def sweep_ordered(order, b, *, diag=None, op=2, lower=True, single=True):
+    """Gather-form triangular sweep in the streamed kernel's summation order.  `order`
+    carries eptr/edep/ecoef and kptr/kdep/kcoef (per row: early then late positions,
+    padding 0xFFFFFFFF); float arithmetic when single, else double."""
+    n = len(order.eptr) - 1
+    out = np.zeros(n)
+    d = np.ascontiguousarray(diag, np.float64) if diag is not None else None
+    u = lambda a: np.ascontiguousarray(a if len(a) else np.zeros(1), np.uint32)
+    f = lambda a: np.ascontiguousarray(a if len(a) else np.zeros(1), np.float64)
+    lib().orc_sweep_ordered(n, int(bool(single)), int(op), int(bool(lower)), u(order.eptr), u(order.edep),
+                            f(order.ecoef), u(order.kptr), u(order.kdep), f(order.kcoef),
+                            d.ctypes.data if d is not None else None, np.ascontiguousarray(b, np.float64), out)
     return out
 
 
@@ -210,6 +234,26 @@ class Amsed:
         out = np.array(vec, np.float64, copy=True)
         lib().orc_amsed_apply(C.byref(self.s), out)
         return out
+
+    def use_sweep_orders(self, orders, single=True):
+        """Block solves as kernel-order sweeps: orders[2 l] / orders[2 l + 1] are level l's lower
+        and upper sweeps (objects with eptr/edep/ecoef/kptr/kdep/kcoef/diag/op/lower, such as a
+        device system's sweep_order()); `single` selects float arithmetic."""
+        def arr(a, dt):
+            a = np.ascontiguousarray(a if len(a) else np.zeros(1), dt)
+            self.keep.append(a)
+            return a.ctypes.data
+
+        for l in range(self.s.nlev):
+            for which, o in (("sweep_lo", orders[2 * l]), ("sweep_up", orders[2 * l + 1])):
+                so = _SweepOrder()
+                so.n, so.op, so.lower = len(o.eptr) - 1, int(o.op), int(bool(o.lower))
+                so.eptr, so.edep, so.ecoef = arr(o.eptr, np.uint32), arr(o.edep, np.uint32), arr(o.ecoef, np.float64)
+                so.kptr, so.kdep, so.kcoef = arr(o.kptr, np.uint32), arr(o.kdep, np.uint32), arr(o.kcoef, np.float64)
+                so.diag = arr(o.diag, np.float64)
+                self.keep.append(so)
+                setattr(self.levels[l], which, C.cast(C.pointer(so), C.c_void_p).value)
+        self.s.single = int(bool(single))
 
     def precond(self) -> "Precond":
         P = Precond(5, self.n)

@@ -39,7 +39,8 @@ class PrismError(RuntimeError):
 
 
 class SolveOpts(C.Structure):
-    _fields_ = [("solver", C.c_int32), ("tol", C.c_double), ("max_iter", C.c_uint32), ("restart", C.c_uint32)]
+    _fields_ = [("solver", C.c_int32), ("tol", C.c_double), ("max_iter", C.c_uint32), ("restart", C.c_uint32),
+                ("x_ref", C.c_void_p)]
 
 
 class AmsedOpts(C.Structure):
@@ -58,7 +59,7 @@ MatrixReorderNo, MatrixReorderAMD, MatrixReorderRCM = 0, 1, 2
 class SolveStats(C.Structure):
     _fields_ = [("num_iter", C.c_int32), ("converged", C.c_int32), ("final_error", C.c_double),
                 ("true_rel_residual", C.c_double), ("precond_applies", C.c_uint32),
-                ("spmv_count", C.c_uint32), ("device_ms", C.c_double)]
+                ("spmv_count", C.c_uint32), ("device_ms", C.c_double), ("forward_error", C.c_double)]
 
 
 _lib = None
@@ -74,6 +75,12 @@ _SIGS = {
     "prism_selftest_wait_timeout": (C.c_int32, [C.c_int32, C.c_uint64, C.POINTER(C.c_int32)]),
     "prism_selftest_stream_layout": (C.c_int32, [C.c_uint32, _u32p, _u32p, _f64p, _vp, C.c_int32, C.c_int32,
                                                  C.c_int32, C.c_uint32, C.c_uint32, _f64p, _f64p]),
+    "prism_stream_sweep_order": (C.c_int32, [C.c_uint32, _u32p, _u32p, _f64p, _vp, C.c_int32, C.c_int32, C.c_int32,
+                                             C.c_uint32, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "prism_stream_sweep_run": (C.c_int32, [C.c_int32, C.c_uint32, _u32p, _u32p, _f64p, _vp, C.c_int32, C.c_int32,
+                                           C.c_int32, C.c_uint32, _f64p, _f64p]),
+    "prism_precond_sweep_order": (C.c_int32, [_vp, C.c_int32, C.POINTER(C.c_uint32), _vp, _vp, _vp, _vp, _vp,
+                                              _vp, _vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "prism_laplacian_dims": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     "prism_laplacian_fill": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
                                          C.c_double, _u32p, _u32p, _f64p]),
@@ -191,6 +198,60 @@ def selftest_stream_layout(rowptr, col, val, in_, *, diag=None, op: int = 2, low
                                                np.ascontiguousarray(val, np.float64),
                                                d.ctypes.data if d is not None else None, op, int(lower), precision,
                                                num_ctas, rpc, np.ascontiguousarray(in_, np.float64), out))
+    return out
+
+
+class SweepOrder:
+    """The streamed sweep kernel's summation order (prism_stream_sweep_order): per row, its
+    early positions eptr[r]:eptr[r+1] of (edep, ecoef) and its late ones kptr[r]:kptr[r+1]
+    of (kdep, kcoef); a dependency of 0xFFFFFFFF is padding (coefficient 0)."""
+
+    PAD = 0xFFFFFFFF
+
+    def __init__(self, eptr, edep, ecoef, kptr, kdep, kcoef):
+        self.eptr, self.edep, self.ecoef = eptr, edep, ecoef
+        self.kptr, self.kdep, self.kcoef = kptr, kdep, kcoef
+        self.diag, self.op, self.lower = None, None, None  # filled for a handle's sweep
+
+
+def _fill_order(call, n):
+    """Two-call fill of a SweepOrder: sizes first, then the arrays."""
+    eptr = np.zeros(n + 1, np.uint32)
+    kptr = np.zeros(n + 1, np.uint32)
+    _check(call(eptr.ctypes.data, None, None, kptr.ctypes.data, None, None))
+    ne, nk = int(eptr[-1]), int(kptr[-1])
+    edep, ecoef = np.zeros(max(ne, 1), np.uint32), np.zeros(max(ne, 1))
+    kdep, kcoef = np.zeros(max(nk, 1), np.uint32), np.zeros(max(nk, 1))
+    _check(call(eptr.ctypes.data, edep.ctypes.data, ecoef.ctypes.data, kptr.ctypes.data, kdep.ctypes.data,
+                kcoef.ctypes.data))
+    return SweepOrder(eptr, edep[:ne], ecoef[:ne], kptr, kdep[:nk], kcoef[:nk])
+
+
+def stream_sweep_order(rowptr, col, val, *, diag=None, op: int = 2, lower: bool = True, precision: int = 0,
+                       num_ctas: int = 4) -> SweepOrder:
+    """Summation order of the streamed sweep kernel for a gather-form triangular sweep (host only)."""
+    rp = np.ascontiguousarray(rowptr, np.uint32)
+    ci = np.ascontiguousarray(col, np.uint32)
+    v = np.ascontiguousarray(val, np.float64)
+    d = np.ascontiguousarray(diag, np.float64) if diag is not None else None
+    n = len(rp) - 1
+    lib = load()
+    return _fill_order(lambda ep, ed, ec, kp, kd, kc: lib.prism_stream_sweep_order(
+        n, rp, ci, v, d.ctypes.data if d is not None else None, op, int(lower), precision, num_ctas,
+        ep, ed, ec, kp, kd, kc), n)
+
+
+def stream_sweep_run(rowptr, col, val, in_, *, diag=None, op: int = 2, lower: bool = True, precision: int = 0,
+                     num_ctas: int = 4, device: int = 0):
+    """Runs the streamed sweep kernel alone on the GPU (same slabs as stream_sweep_order)."""
+    rp = np.ascontiguousarray(rowptr, np.uint32)
+    n = len(rp) - 1
+    out = np.zeros(n)
+    d = np.ascontiguousarray(diag, np.float64) if diag is not None else None
+    _check(load().prism_stream_sweep_run(device, n, rp, np.ascontiguousarray(col, np.uint32),
+                                         np.ascontiguousarray(val, np.float64),
+                                         d.ctypes.data if d is not None else None, op, int(lower), precision,
+                                         num_ctas, np.ascontiguousarray(in_, np.float64), out))
     return out
 
 
@@ -562,6 +623,19 @@ class DeviceSystem:
         return {"n": n.value, "nnz": nnz.value, "value_bytes": vb.value, "levels": lv.value,
                 "kernel": {1: "level-order", 2: "slab", 3: "stream"}.get(kk.value, "?")}
 
+    def sweep_order(self, sweep: int) -> SweepOrder:
+        """Summation order of one of the preconditioner's sweeps when it runs the streamed kernel
+        (prism_precond_sweep_order); raises PrismError otherwise."""
+        n, op, lower = C.c_uint32(), C.c_int32(), C.c_int32()
+        _check(self.lib.prism_precond_sweep_order(self.h, sweep, C.byref(n), None, None, None, None, None, None,
+                                                  None, None, None))
+        lib, h = self.lib, self.h
+        diag = np.zeros(max(n.value, 1))
+        o = _fill_order(lambda ep, ed, ec, kp, kd, kc: lib.prism_precond_sweep_order(
+            h, sweep, C.byref(n), ep, ed, ec, kp, kd, kc, diag.ctypes.data, C.byref(op), C.byref(lower)), n.value)
+        o.diag, o.op, o.lower = diag[:n.value], op.value, bool(lower.value)
+        return o
+
     def apply(self, vec):
         """out = M^{-1} vec (MInvSolve(vecIN, vecOUT))."""
         if hasattr(vec, "is_cuda"):
@@ -585,7 +659,7 @@ class DeviceSystem:
     def adjoint(self, g, x=None, *, solver=SOLVER_FCG, tol=1e-10, max_iter=1000, restart=0):
         """lambda = A^{-T} g and, with x given, dL/dA on A's pattern (-lambda_i x_j);
         returns (lambda, grad_val or None, SolveStats)."""
-        opts = SolveOpts(solver, tol, max_iter, restart)
+        opts = SolveOpts(solver, tol, max_iter, restart, None)
         st = SolveStats()
         if hasattr(g, "is_cuda"):
             import torch
@@ -623,7 +697,7 @@ class DeviceSystem:
     def solve_batched(self, B, X=None, *, solver=SOLVER_FCG, tol=1e-8, max_iter=1000) -> tuple:
         """Solves A x_c = b_c for the k rows of B (shape (k, n), k <= 64) in one block
         solve; returns (X, [SolveStats] * k).  Device tensors or host arrays."""
-        opts = SolveOpts(solver, tol, max_iter, 0)
+        opts = SolveOpts(solver, tol, max_iter, 0, None)
         if hasattr(B, "is_cuda"):
             import torch
             Bc = B.contiguous()
@@ -644,7 +718,7 @@ class DeviceSystem:
         of A at once; returns (x, [SolveStats] per system).  Device tensors or host arrays."""
         sp = np.ascontiguousarray(seg_ptr, np.uint32)
         nseg = len(sp) - 1
-        opts = SolveOpts(solver, tol, max_iter, 0)
+        opts = SolveOpts(solver, tol, max_iter, 0, None)
         st = (SolveStats * nseg)()
         if hasattr(b, "is_cuda"):
             import torch
@@ -657,18 +731,25 @@ class DeviceSystem:
         _check(self.lib.prism_solve_segments(self.h, C.byref(opts), nseg, sp, bh, xh, st))
         return xh, list(st)
 
-    def solve(self, b, x=None, *, solver=SOLVER_FCG, tol=1e-8, max_iter=1000, restart=0) -> tuple:
-        """x (in/out initial guess) solved in place; returns (x, SolveStats)."""
-        opts = SolveOpts(solver, tol, max_iter, restart)
+    def solve(self, b, x=None, *, solver=SOLVER_FCG, tol=1e-8, max_iter=1000, restart=0, x_ref=None) -> tuple:
+        """x (in/out initial guess) solved in place; returns (x, SolveStats).  x_ref (same kind
+        as b: a CUDA tensor or a host array): a reference solution whose forward error the
+        stats then report (stats.forward_error, else -1)."""
+        opts = SolveOpts(solver, tol, max_iter, restart, None)
         st = SolveStats()
         if hasattr(b, "is_cuda"):
             import torch
             if x is None:
                 x = torch.zeros_like(b)
+            if x_ref is not None:
+                opts.x_ref = _ptr(x_ref)
             _check(self.lib.prism_solve_device(self.h, C.byref(opts), _ptr(b), _ptr(x), C.byref(st)))
             return x, st
         b = np.ascontiguousarray(b, np.float64)
         x = np.zeros(self.n) if x is None else np.array(x, np.float64, copy=True)
+        if x_ref is not None:
+            xr = np.ascontiguousarray(x_ref, np.float64)
+            opts.x_ref = xr.ctypes.data
         _check(self.lib.prism_solve(self.h, C.byref(opts), b, x, C.byref(st)))
         return x, st
 

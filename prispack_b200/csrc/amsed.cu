@@ -52,6 +52,63 @@ void upload_csr(DeviceCsr& d, uint32_t nrows, const std::vector<uint32_t>& rp, c
 }
 }  // namespace
 
+template <typename Low>
+void AmsedPrecond::level_sweeps(const AmsedSetup<Low>& S, uint32_t l, Sweep<Low>& lo, Sweep<Low>& up) const {
+    const AmsedLevel<Low>& L = S.levels[l];
+    const uint32_t nb = S.lev_ptr[l + 1] - S.lev_ptr[l];
+    const uint32_t nfac = l + 1 == nlev_ ? L.B[0].n : nb;  // rows with a factor
+    if (gmslr_) {
+        // ILUT blocks on every level (the last level: block 0 only, GMSLRDPrecondition.cpp:664-688)
+        const uint32_t nblk = l + 1 == nlev_ ? 1 : L.ncomps;
+        CsrT<Low> Lc, Uc;
+        std::vector<Low> Dc;
+        Lc.n = Uc.n = nfac;
+        Lc.rowptr.assign((size_t)nfac + 1, 0);
+        Uc.rowptr.assign((size_t)nfac + 1, 0);
+        for (uint32_t b = 0; b < nblk; ++b) {
+            const uint32_t off = L.dom_ptr[b] - L.dom_ptr[0];
+            const CsrT<Low>& fl = L.Lt[b];
+            const CsrT<Low>& fu = L.U[b];
+            for (uint32_t i = 0; i < fl.n; ++i) {
+                for (uint32_t k = fl.rowptr[i]; k < fl.rowptr[i + 1]; ++k) {
+                    Lc.col.push_back(fl.col[k] + off);
+                    Lc.val.push_back(fl.val[k]);
+                }
+                Lc.rowptr[off + i + 1] = (uint32_t)Lc.col.size();
+                for (uint32_t k = fu.rowptr[i]; k < fu.rowptr[i + 1]; ++k) {
+                    Uc.col.push_back(fu.col[k] + off);
+                    Uc.val.push_back(fu.val[k]);
+                }
+                Uc.rowptr[off + i + 1] = (uint32_t)Uc.col.size();
+            }
+            Dc.insert(Dc.end(), L.Dinv[b].begin(), L.Dinv[b].end());
+        }
+        ilut_sweeps<Low>(Lc, Uc, Dc, lo, up);
+    } else if (l + 1 == nlev_) {
+        // last level: IC of block 0 (the reference factors and applies only B_mat[0], :694-716, :1504-1508)
+        ic_sweeps<Low>(L.Lt[0], lo, up);
+    } else {
+        // block-diagonal ILDLT of all subdomains of the level
+        CsrT<Low> Lt;
+        std::vector<double> Dg;
+        Lt.n = nb;
+        Lt.rowptr.assign((size_t)nb + 1, 0);
+        for (uint32_t b = 0; b < L.ncomps; ++b) {
+            const uint32_t off = L.dom_ptr[b] - L.dom_ptr[0];
+            const CsrT<Low>& f = L.Lt[b];
+            for (uint32_t i = 0; i < f.n; ++i) {
+                for (uint32_t k = f.rowptr[i]; k < f.rowptr[i + 1]; ++k) {
+                    Lt.col.push_back(f.col[k] + off);
+                    Lt.val.push_back(f.val[k]);
+                }
+                Lt.rowptr[off + i + 1] = (uint32_t)Lt.col.size();
+            }
+            Dg.insert(Dg.end(), L.D[b].begin(), L.D[b].end());
+        }
+        ildlt_sweeps<Low>(Lt, Dg, lo, up);
+    }
+}
+
 AmsedPrecond::AmsedPrecond(Handle& h, std::shared_ptr<const HostAmsed> a) : h_(h), a_(std::move(a)) {
     gmslr_ = a_->opt.family == 4;
     if (a_->fp32) build(*a_->s32);
@@ -78,59 +135,8 @@ void AmsedPrecond::build(const AmsedSetup<Low>& S) {
         D.nb = S.lev_ptr[l + 1] - S.lev_ptr[l];
         D.nrem = S.n - S.lev_ptr[l + 1];
         Sweep<Low> lo, up;
-        if (gmslr_) {
-            // ILUT blocks on every level (the last level: block 0 only, GMSLRDPrecondition.cpp:664-688)
-            const uint32_t nblk = l + 1 == nlev_ ? 1 : L.ncomps;
-            D.nfac = l + 1 == nlev_ ? L.B[0].n : D.nb;
-            CsrT<Low> Lc, Uc;
-            std::vector<Low> Dc;
-            Lc.n = Uc.n = D.nfac;
-            Lc.rowptr.assign((size_t)D.nfac + 1, 0);
-            Uc.rowptr.assign((size_t)D.nfac + 1, 0);
-            for (uint32_t b = 0; b < nblk; ++b) {
-                const uint32_t off = L.dom_ptr[b] - L.dom_ptr[0];
-                const CsrT<Low>& fl = L.Lt[b];
-                const CsrT<Low>& fu = L.U[b];
-                for (uint32_t i = 0; i < fl.n; ++i) {
-                    for (uint32_t k = fl.rowptr[i]; k < fl.rowptr[i + 1]; ++k) {
-                        Lc.col.push_back(fl.col[k] + off);
-                        Lc.val.push_back(fl.val[k]);
-                    }
-                    Lc.rowptr[off + i + 1] = (uint32_t)Lc.col.size();
-                    for (uint32_t k = fu.rowptr[i]; k < fu.rowptr[i + 1]; ++k) {
-                        Uc.col.push_back(fu.col[k] + off);
-                        Uc.val.push_back(fu.val[k]);
-                    }
-                    Uc.rowptr[off + i + 1] = (uint32_t)Uc.col.size();
-                }
-                Dc.insert(Dc.end(), L.Dinv[b].begin(), L.Dinv[b].end());
-            }
-            ilut_sweeps<Low>(Lc, Uc, Dc, lo, up);
-        } else if (l + 1 == nlev_) {
-            // last level: IC of block 0 (the reference factors and applies only B_mat[0], :694-716, :1504-1508)
-            D.nfac = L.B[0].n;
-            ic_sweeps<Low>(L.Lt[0], lo, up);
-        } else {
-            // block-diagonal ILDLT of all subdomains of the level
-            CsrT<Low> Lt;
-            std::vector<double> Dg;
-            Lt.n = D.nb;
-            Lt.rowptr.assign((size_t)D.nb + 1, 0);
-            for (uint32_t b = 0; b < L.ncomps; ++b) {
-                const uint32_t off = L.dom_ptr[b] - L.dom_ptr[0];
-                const CsrT<Low>& f = L.Lt[b];
-                for (uint32_t i = 0; i < f.n; ++i) {
-                    for (uint32_t k = f.rowptr[i]; k < f.rowptr[i + 1]; ++k) {
-                        Lt.col.push_back(f.col[k] + off);
-                        Lt.val.push_back(f.val[k]);
-                    }
-                    Lt.rowptr[off + i + 1] = (uint32_t)Lt.col.size();
-                }
-                Dg.insert(Dg.end(), L.D[b].begin(), L.D[b].end());
-            }
-            D.nfac = D.nb;
-            ildlt_sweeps<Low>(Lt, Dg, lo, up);
-        }
+        level_sweeps<Low>(S, l, lo, up);
+        D.nfac = l + 1 == nlev_ ? L.B[0].n : D.nb;  // the last level factors block 0 only
         tune_sweep<Low>(h_, D.lower, lo, a_->apply32);
         tune_sweep<Low>(h_, D.upper, up, a_->apply32);
         if (l + 1 < nlev_) {
@@ -245,6 +251,21 @@ bool AmsedPrecond::sweep_info(int sweep, uint32_t* n, uint64_t* nnz, uint32_t* v
     if (levels) *levels = s.num_levels;
     if (kernel) *kernel = s.layout == LAYOUT_STREAM ? 3 : (s.layout == LAYOUT_SLAB ? 2 : 1);
     return true;
+}
+
+bool AmsedPrecond::sweep_order(int sweep, StreamOrder& o) const {
+    if (sweep < 0 || sweep >= (int)(2 * nlev_)) return false;
+    const Level& L = lv_[sweep / 2];
+    const DevSweep& d = (sweep & 1) ? L.upper : L.lower;
+    if (d.layout != LAYOUT_STREAM) return false;
+    if (a_->fp32) {
+        Sweep<float> lo, up;
+        level_sweeps<float>(*a_->s32, (uint32_t)sweep / 2, lo, up);
+        return d.stream_order<float>((sweep & 1) ? up : lo, o);
+    }
+    Sweep<double> lo, up;
+    level_sweeps<double>(*a_->s64, (uint32_t)sweep / 2, lo, up);
+    return d.stream_order<double>((sweep & 1) ? up : lo, o);
 }
 
 template void AmsedPrecond::build<double>(const AmsedSetup<double>&);

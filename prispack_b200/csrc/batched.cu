@@ -641,6 +641,7 @@ void batched_fcg_solve(Handle& h, const prism_solve_opts& o, uint32_t k, const d
             st[c].precond_applies = applies;
             st[c].spmv_count = spmvs;
             st[c].device_ms = ms;
+            st[c].forward_error = -1.0;  // no reference solution for block / batch solves
         }
     }
 }

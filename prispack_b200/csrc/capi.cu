@@ -110,10 +110,46 @@ static int32_t set_tri(prism_handle h, int kind, double tol, uint32_t lfill, int
     });
 }
 
+
+// A gather-form triangular sweep from caller arrays (dependencies on one side of the diagonal).
+template <typename Low>
+static void gather_sweep(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val,
+                         const double* diag, int op, bool lower, prism::Sweep<Low>& s) {
+    const uint64_t nnz = rowptr[n];
+    std::vector<uint32_t> rp(rowptr, rowptr + n + 1), ci(col, col + nnz);
+    std::vector<Low> v(nnz);
+    for (uint64_t k = 0; k < nnz; ++k) v[k] = (Low)val[k];
+    std::vector<double> d;
+    if (diag) d.assign(diag, diag + n);
+    prism::build_sweep<Low>(n, rp, ci, v, diag ? &d : nullptr, op, lower, s);
+}
+
+static int check_gather_form(uint32_t n, const uint32_t* rowptr, const uint32_t* col, int32_t lower) {
+    for (uint32_t r = 0; r < n; ++r) {
+        if (rowptr[r + 1] < rowptr[r]) return fail(PRISM_ERR_ARG, "row offsets decrease");
+        for (uint32_t k = rowptr[r]; k < rowptr[r + 1]; ++k)
+            if (col[k] >= n || (lower ? col[k] >= r : col[k] <= r))
+                return fail(PRISM_ERR_ARG, "dependency on the wrong side of the diagonal");
+    }
+    return PRISM_OK;
+}
+
+static int copy_order(const prism::StreamOrder& o, uint32_t n, uint32_t* eptr, uint32_t* edep, double* ecoef,
+                      uint32_t* kptr, uint32_t* kdep, double* kcoef) {
+    if (o.eptr.size() != (size_t)n + 1) return fail(PRISM_ERR_ARG, "order size");
+    std::memcpy(eptr, o.eptr.data(), o.eptr.size() * sizeof(uint32_t));
+    std::memcpy(kptr, o.kptr.data(), o.kptr.size() * sizeof(uint32_t));
+    if (edep) std::memcpy(edep, o.edep.data(), o.edep.size() * sizeof(uint32_t));
+    if (ecoef) std::memcpy(ecoef, o.ecoef.data(), o.ecoef.size() * sizeof(double));
+    if (kdep) std::memcpy(kdep, o.kdep.data(), o.kdep.size() * sizeof(uint32_t));
+    if (kcoef) std::memcpy(kcoef, o.kcoef.data(), o.kcoef.size() * sizeof(double));
+    return PRISM_OK;
+}
+
 template <typename Low>
 static int stream_selftest(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val,
                            const double* diag, int op, bool lower, uint32_t num_ctas, uint32_t rows_per_cta,
-                           const double* in, double* out) {
+                           uint32_t slot_bytes, const double* in, double* out) {
     const uint64_t nnz = rowptr[n];
     std::vector<uint32_t> rp(rowptr, rowptr + n + 1), ci(col, col + nnz);
     std::vector<Low> v(nnz);
@@ -133,7 +169,8 @@ static int stream_selftest(uint32_t n, const uint32_t* rowptr, const uint32_t* c
     }
     prism::StreamLayout L;
     std::string why;
-    if (!prism::stream_layout<Low>(s, start, prism::kNoSlot, L, &why)) return fail(PRISM_ERR_UNSUPPORTED, why);
+    if (!prism::stream_layout<Low>(s, start, prism::kNoSlot, slot_bytes, L, &why))
+        return fail(PRISM_ERR_UNSUPPORTED, why);
     why = prism::stream_layout_replay<Low>(s, L, in, out);
     if (!why.empty()) return fail(PRISM_ERR_ARG, "stream layout: " + why);
     return PRISM_OK;
@@ -159,6 +196,81 @@ int32_t prism_selftest_wait_timeout(int32_t device, uint64_t wait_ns, int32_t* d
     });
 }
 
+int32_t prism_stream_sweep_order(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val,
+                                 const double* diag, int32_t op, int32_t lower, int32_t precision, uint32_t num_ctas,
+                                 uint32_t* eptr, uint32_t* edep, double* ecoef, uint32_t* kptr, uint32_t* kdep,
+                                 double* kcoef) {
+    if (!rowptr || !col || !val || !eptr || !kptr || n == 0) return fail(PRISM_ERR_ARG, "null array or empty sweep");
+    if (op < 0 || op > 3 || (op != 2 && !diag)) return fail(PRISM_ERR_ARG, "bad op / missing diagonal");
+    if (!valid_precision(precision) || num_ctas == 0) return fail(PRISM_ERR_ARG, "bad precision or slab count");
+    return guarded([&]() -> int {
+        int rc = check_gather_form(n, rowptr, col, lower);
+        if (rc) return rc;
+        const uint32_t slot_bytes = precision == PRISM_FP32_APPLY ? 4 : 8;
+        const uint32_t ctas = prism::stream_slab_count(n, num_ctas, 32);
+        prism::StreamOrder o;
+        prism::StreamLayout L;
+        std::string why;
+        bool ok;
+        if (precision != PRISM_FP64) {
+            prism::Sweep<float> s;
+            gather_sweep<float>(n, rowptr, col, val, diag, op, lower != 0, s);
+            ok = prism::stream_layout<float>(s, prism::slab_ranges<float>(s, ctas), prism::kNoSlot, slot_bytes, L,
+                                             &why, &o);
+        } else {
+            prism::Sweep<double> s;
+            gather_sweep<double>(n, rowptr, col, val, diag, op, lower != 0, s);
+            ok = prism::stream_layout<double>(s, prism::slab_ranges<double>(s, ctas), prism::kNoSlot, 8, L, &why, &o);
+        }
+        if (!ok) return fail(PRISM_ERR_UNSUPPORTED, why);
+        return copy_order(o, n, eptr, edep, ecoef, kptr, kdep, kcoef);
+    });
+}
+
+int32_t prism_stream_sweep_run(int32_t device, uint32_t n, const uint32_t* rowptr, const uint32_t* col,
+                               const double* val, const double* diag, int32_t op, int32_t lower, int32_t precision,
+                               uint32_t num_ctas, const double* in, double* out) {
+    if (!rowptr || !col || !val || !in || !out || n == 0) return fail(PRISM_ERR_ARG, "null array or empty sweep");
+    if (op < 0 || op > 3 || (op != 2 && !diag)) return fail(PRISM_ERR_ARG, "bad op / missing diagonal");
+    if (!valid_precision(precision) || num_ctas == 0) return fail(PRISM_ERR_ARG, "bad precision or slab count");
+    return guarded([&]() -> int {
+        int rc = check_gather_form(n, rowptr, col, lower);
+        if (rc) return rc;
+        DeviceGuard g(device);
+        if (precision != PRISM_FP64) {
+            prism::Sweep<float> s;
+            gather_sweep<float>(n, rowptr, col, val, diag, op, lower != 0, s);
+            prism::stream_sweep_run<float>(device, s, precision == PRISM_FP32_APPLY, num_ctas, in, out);
+        } else {
+            prism::Sweep<double> s;
+            gather_sweep<double>(n, rowptr, col, val, diag, op, lower != 0, s);
+            prism::stream_sweep_run<double>(device, s, false, num_ctas, in, out);
+        }
+        return PRISM_OK;
+    });
+}
+
+int32_t prism_precond_sweep_order(prism_handle h, int32_t sweep, uint32_t* n, uint32_t* eptr, uint32_t* edep,
+                                  double* ecoef, uint32_t* kptr, uint32_t* kdep, double* kcoef, double* diag,
+                                  int32_t* op, int32_t* lower) {
+    if (!h || !n) return fail(PRISM_ERR_ARG, "null handle or size");
+    if (!h->P) return fail(PRISM_ERR_NOT_READY, "no preconditioner");
+    return guarded([&]() -> int {
+        uint32_t rows = 0;
+        if (!h->P->sweep_info(sweep, &rows, nullptr, nullptr, nullptr, nullptr))
+            return fail(PRISM_ERR_ARG, "no such sweep");
+        *n = rows;
+        if (!eptr && !kptr) return PRISM_OK;
+        if (!eptr || !kptr) return fail(PRISM_ERR_ARG, "eptr and kptr go together");
+        prism::StreamOrder o;
+        if (!h->P->sweep_order(sweep, o)) return fail(PRISM_ERR_UNSUPPORTED, "the sweep does not run the streamed kernel");
+        if (diag) std::memcpy(diag, o.diag.data(), o.diag.size() * sizeof(double));
+        if (op) *op = o.op;
+        if (lower) *lower = o.lower ? 1 : 0;
+        return copy_order(o, rows, eptr, edep, ecoef, kptr, kdep, kcoef);
+    });
+}
+
 int32_t prism_selftest_stream_layout(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val,
                                      const double* diag, int32_t op, int32_t lower, int32_t precision,
                                      uint32_t num_ctas, uint32_t rows_per_cta, const double* in, double* out) {
@@ -169,9 +281,12 @@ int32_t prism_selftest_stream_layout(uint32_t n, const uint32_t* rowptr, const u
             for (uint32_t k = rowptr[r]; k < rowptr[r + 1]; ++k)
                 if (col[k] >= n || (lower ? col[k] >= r : col[k] <= r))
                     return fail(PRISM_ERR_ARG, "dependency on the wrong side of the diagonal");
+        const uint32_t slot_bytes = precision == PRISM_FP32_APPLY ? 4 : 8;
         if (precision != PRISM_FP64)
-            return stream_selftest<float>(n, rowptr, col, val, diag, op, lower != 0, num_ctas, rows_per_cta, in, out);
-        return stream_selftest<double>(n, rowptr, col, val, diag, op, lower != 0, num_ctas, rows_per_cta, in, out);
+            return stream_selftest<float>(n, rowptr, col, val, diag, op, lower != 0, num_ctas, rows_per_cta,
+                                          slot_bytes, in, out);
+        return stream_selftest<double>(n, rowptr, col, val, diag, op, lower != 0, num_ctas, rows_per_cta, 8, in,
+                                       out);
     });
 }
 
@@ -677,10 +792,12 @@ int32_t prism_precond_sweep_info(prism_handle h, int32_t sweep, uint32_t* n, uin
 }
 
 // ---- solvers -------------------------------------------------------------------
+// xref: device pointer of the reference solution (or null)
 static void run_solver(prism::Handle& h, const prism_solve_opts& o, const double* b, double* x,
-                       prism_solve_stats* st) {
+                       prism_solve_stats* st, const double* xref) {
     if (o.solver == PRISM_SOLVER_FCG || o.solver == PRISM_SOLVER_CG) prism::fcg_solve(h, o, b, x, st);
     else prism::gmres_solve(h, o, b, x, st);
+    if (st) st->forward_error = xref ? prism::forward_error(h, x, xref) : -1.0;
 }
 
 static int check_opts(prism_handle h, const prism_solve_opts* o) {
@@ -700,7 +817,7 @@ int32_t prism_solve_device(prism_handle h, const prism_solve_opts* opts, const d
     if (!b_d || !x_d) return fail(PRISM_ERR_ARG, "null vector");
     return guarded([&]() -> int {
         DeviceGuard g(h->info.device);
-        run_solver(*h, *opts, b_d, x_d, stats);
+        run_solver(*h, *opts, b_d, x_d, stats, opts->x_ref);
         return PRISM_OK;
     });
 }
@@ -716,7 +833,14 @@ int32_t prism_solve(prism_handle h, const prism_solve_opts* opts, const double* 
         if (h->xb.size() < n) { h->xb.alloc(n); h->bb.alloc(n); }
         PRISM_CUDA(cudaMemcpyAsync(h->bb.get(), b, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
         PRISM_CUDA(cudaMemcpyAsync(h->xb.get(), x, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-        run_solver(*h, *opts, h->bb.get(), h->xb.get(), stats);
+        const double* xref = nullptr;
+        if (opts->x_ref) {
+            if (h->xr.size() < n) h->xr.alloc(n);
+            PRISM_CUDA(cudaMemcpyAsync(h->xr.get(), opts->x_ref, n * sizeof(double), cudaMemcpyHostToDevice,
+                                       h->stream));
+            xref = h->xr.get();
+        }
+        run_solver(*h, *opts, h->bb.get(), h->xb.get(), stats, xref);
         PRISM_CUDA(cudaMemcpyAsync(x, h->xb.get(), n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
         PRISM_CUDA(cudaStreamSynchronize(h->stream));
         return PRISM_OK;
@@ -761,7 +885,7 @@ static void adjoint(prism::Handle& h, const prism_solve_opts& o, const double* g
                                                   "transposed operator and preconditioner)");
     // A^T = A: lambda = A^{-1} g with the handle's own solver and preconditioner, from zero
     PRISM_CUDA(cudaMemsetAsync(lambda_d, 0, (size_t)h.A.n * sizeof(double), h.stream));
-    run_solver(h, o, g_d, lambda_d, st);
+    run_solver(h, o, g_d, lambda_d, st, nullptr);  // no reference solution for lambda
     if (grad_d) prism::launch_adjoint_outer(h, h.stream, lambda_d, x_d, grad_d);
     PRISM_CUDA(cudaStreamSynchronize(h.stream));
 }

@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstring>
 #include <numeric>
+#include <type_traits>
 
 namespace prism {
 
@@ -669,15 +670,84 @@ int build_triangular(int kind, const CsrHost& A, double tol, uint32_t lfill, boo
     return build_tri_t<double>(kind, A, tol, lfill, out, out.lower64, out.upper64, err);
 }
 
+namespace {
+// Positions for the entries of a group of rows that one shared-memory wavefront serves.
+// rows[i] lists (slot, source index) pairs; every row gets exactly P positions (entries
+// plus padding).  Position by position the rows take entries whose slots fall in banks no
+// other row uses there (the same slot twice is a broadcast, not a conflict); a row whose
+// remaining entries just fill its remaining positions must take one even if its bank is
+// taken.  Padding reads the zero slot of a bank left free (slot b holds 0.0 and sits in
+// bank b).  out[i][u] = index into rows[i] or -(1 + zero slot).
+void bank_order(const std::vector<std::vector<std::pair<uint32_t, uint32_t>>>& rows, uint32_t P, uint32_t nb,
+                std::vector<std::vector<int64_t>>& out) {
+    const size_t G = rows.size();
+    out.assign(G, std::vector<int64_t>(P, 0));
+    std::vector<std::vector<uint8_t>> taken(G);
+    std::vector<uint32_t> left(G);
+    for (size_t i = 0; i < G; ++i) {
+        taken[i].assign(rows[i].size(), 0);
+        left[i] = (uint32_t)rows[i].size();
+    }
+    std::vector<size_t> idx(G);
+    std::vector<int64_t> bank_slot(nb);
+    std::vector<uint8_t> padded(G);
+    for (uint32_t u = 0; u < P; ++u) {
+        std::fill(bank_slot.begin(), bank_slot.end(), -1);
+        std::iota(idx.begin(), idx.end(), 0);
+        // most constrained rows first: least slack between positions left and entries left
+        std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) { return left[a] > left[b]; });
+        for (size_t t = 0; t < G; ++t) {
+            const size_t i = idx[t];
+            padded[i] = 0;
+            if (left[i] == 0) {
+                padded[i] = 1;
+                continue;
+            }
+            const bool must = left[i] >= P - u;
+            int64_t pick = -1;
+            for (size_t e = 0; e < rows[i].size() && pick < 0; ++e) {
+                if (taken[i][e]) continue;
+                const uint32_t sl = rows[i][e].first, b = sl % nb;
+                if (bank_slot[b] < 0 || bank_slot[b] == (int64_t)sl) pick = (int64_t)e;
+            }
+            if (pick < 0 && must)
+                for (size_t e = 0; e < rows[i].size(); ++e)
+                    if (!taken[i][e]) {
+                        pick = (int64_t)e;
+                        break;
+                    }
+            if (pick < 0) {
+                padded[i] = 1;
+                continue;
+            }
+            taken[i][(size_t)pick] = 1;
+            --left[i];
+            const uint32_t sl = rows[i][(size_t)pick].first;
+            if (bank_slot[sl % nb] < 0) bank_slot[sl % nb] = sl;
+            out[i][u] = pick;
+        }
+        for (size_t i = 0; i < G; ++i) {
+            if (!padded[i]) continue;
+            uint32_t b = 0;
+            while (b < nb && bank_slot[b] >= 0 && bank_slot[b] != (int64_t)b) ++b;
+            if (b == nb) b = 0;  // every bank taken: the zero slot of bank 0 (a conflict at worst)
+            if (bank_slot[b] < 0) bank_slot[b] = b;
+            out[i][u] = -1 - (int64_t)b;
+        }
+    }
+}
+}  // namespace
+
 template <typename Low>
-bool stream_layout(const Sweep<Low>& s, const std::vector<uint32_t>& start, uint32_t max_slots, StreamLayout& out,
-                   std::string* why) {
+bool stream_layout(const Sweep<Low>& s, const std::vector<uint32_t>& start, uint32_t max_slots, uint32_t slot_bytes,
+                   StreamLayout& out, std::string* why, StreamOrder* order) {
     auto fail = [&](const std::string& m) {
         if (why) *why = m;
         return false;
     };
     const uint32_t n = s.n;
     if (n == 0 || start.size() < 2) return fail("empty sweep");
+    if (slot_bytes != 4 && slot_bytes != 8) return fail("slot width");
     const uint32_t num_ctas = (uint32_t)start.size() - 1;
     if (start[0] != 0 || start[num_ctas] != n) return fail("slabs do not cover the rows");
     for (uint32_t b = 0; b < num_ctas; ++b) {
@@ -685,6 +755,8 @@ bool stream_layout(const Sweep<Low>& s, const std::vector<uint32_t>& start, uint
         if (start[b + 1] - start[b] > 0xFFFFu) return fail("slab larger than 65535 rows");
     }
     if (max_slots > kNoSlot) max_slots = kNoSlot;
+    const uint32_t NZ = zero_slots(slot_bytes);
+    if (max_slots <= NZ) return fail("no room for value slots");
     Sweep<Low> sl;
     std::vector<uint32_t> cpos;
     slab_layout_ranges<Low>(s, start, cpos, sl);
@@ -692,13 +764,29 @@ bool stream_layout(const Sweep<Low>& s, const std::vector<uint32_t>& start, uint
     const bool recip = s.op == SWEEP_DIV || s.op == SWEEP_PREDIV;
     out = StreamLayout();
     out.num_ctas = num_ctas;
+    out.slot_bytes = slot_bytes;
     out.slab_start = start;
     out.cta_pos = cpos;
     out.cta_round.assign((size_t)num_ctas + 1, 0);
     out.in_slot.assign(n, 0);
+    out.halo_ptr.assign(1, 0);
+    if (order) {
+        order->eptr.assign((size_t)n + 1, 0);
+        order->kptr.assign((size_t)n + 1, 0);
+        order->diag.assign(n, 1.0);
+        for (uint32_t p = 0; p < n; ++p) order->diag[s.order[p]] = s.diag[p];
+        order->op = s.op;
+        order->lower = s.lower;
+    }
+    // per row: its (early, late) summation order, filled round by round, gathered at the end
+    std::vector<std::vector<std::pair<uint32_t, double>>> ord_e, ord_k;
+    if (order) {
+        ord_e.resize(n);
+        ord_k.resize(n);
+    }
 
     struct Round {
-        uint32_t p0, p1, L;
+        uint32_t p0, p1;
         std::vector<uint32_t> xrow, xslot, xwait;
     };
     constexpr uint32_t kNone = 0xFFFFFFFFu;
@@ -707,12 +795,12 @@ bool stream_layout(const Sweep<Low>& s, const std::vector<uint32_t>& start, uint
     std::vector<int64_t> last_use(n, -1);       // ... and the last round of that slab reading it
     std::vector<uint32_t> slot_of(n, kNoSlot);  // by row: its value slot in the slab being laid out
     std::vector<uint32_t> slot_in(n, kNone);    // by row: slab that slot_of refers to
+    const uint32_t G = slot_bytes == 4 ? 32u : 16u;  // rows one wavefront serves
     for (uint32_t b = 0; b < num_ctas; ++b) {
         const uint32_t rb = start[b], re = start[b + 1];
         const uint32_t P0 = cpos[b], P1 = cpos[b + 1];
         std::vector<Round> R;
         // 1. rounds: consecutive positions, at most kRoundRows, no dependency inside a round.
-        // A dependency has a lower level, hence an earlier position, so its round is known.
         for (uint32_t p = P0; p < P1;) {
             Round rd;
             rd.p0 = p;
@@ -728,9 +816,6 @@ bool stream_layout(const Sweep<Low>& s, const std::vector<uint32_t>& start, uint
                 ++p;
             }
             rd.p1 = p;
-            rd.L = 0;
-            for (uint32_t q = rd.p0; q < rd.p1; ++q) rd.L = std::max(rd.L, sl.rowptr[q + 1] - sl.rowptr[q]);
-            if (rd.L > 0xFFFFu) return fail("a row with more than 65535 entries");
             R.push_back(std::move(rd));
         }
         if (R.size() >= 0xFFFFu) return fail("more than 65534 rounds in a slab");
@@ -746,13 +831,15 @@ bool stream_layout(const Sweep<Low>& s, const std::vector<uint32_t>& start, uint
                     last_use[d] = std::max<int64_t>(last_use[d], r);
                 }
         // 3. slots: a value occupies its slot from the round that writes it (its own round for a
-        // slab row, its first reading round for a halo row) through its last reading round.  A
-        // slot released after round r takes a row result of round r + 1 or later; a halo value
-        // only from round r + 2 on, because the kernel copies round r + 2's halo in while round
-        // r + 1 computes, when only rounds up to r are known to be done.  Oldest first.
+        // slab row, its first reading round for a halo row) through its last reading round.
+        // Round r's reads happen while rounds r - 1 (early entries) and r (late ones) are
+        // computed, so its value is free once round r is done.  A row result of round r may
+        // take a slot whose last reader is round r - 1 or earlier.  A halo value read first in
+        // round r is read while round r - 1 is computed and copied in a round before that: its
+        // slot's last reader must be round r - 3 or earlier.  Oldest released slot first.
         std::vector<uint32_t> free_q;
         size_t free_head = 0;
-        std::vector<int64_t> slot_last{INT64_MAX};  // last reading round of the slot's value; slot 0 holds 0.0
+        std::vector<int64_t> slot_last(NZ, INT64_MAX);  // slots 0 .. NZ-1 hold 0.0
         std::vector<std::vector<uint32_t>> release(R.size());
         auto take = [&](int64_t last, uint32_t& slot, uint32_t& wait, int64_t free_by) -> bool {
             if (free_head < free_q.size() && slot_last[free_q[free_head]] <= free_by) {
@@ -770,22 +857,20 @@ bool stream_layout(const Sweep<Low>& s, const std::vector<uint32_t>& start, uint
         for (uint32_t r = 0; r < R.size(); ++r) {
             if (r > 0)
                 for (uint32_t q : release[r - 1]) free_q.push_back(q);
-            // halo rows first read in round r: copied in by a prefetcher
             for (uint32_t p = R[r].p0; p < R[r].p1; ++p)
                 for (uint32_t k = sl.rowptr[p]; k < sl.rowptr[p + 1]; ++k) {
                     const uint32_t d = sl.col[k];
                     if ((d >= rb && d < re) || slot_in[d] == b) continue;
                     uint32_t slot, wait;
-                    if (!take(last_use[d], slot, wait, (int64_t)r - 2))
+                    if (!take(last_use[d], slot, wait, (int64_t)r - 3))
                         return fail("more value slots than shared memory holds");
-                    if (wait > (r > 0 ? r - 1 : 0)) return fail("a prefetch would wait on its own or a later round");
+                    if (r >= 2 ? wait > r - 2 : wait > 0) return fail("a prefetch would wait on a later round");
                     slot_of[d] = slot;
                     slot_in[d] = b;
                     R[r].xrow.push_back(d);
                     R[r].xslot.push_back(slot);
                     R[r].xwait.push_back(wait);
                 }
-            // rows of round r read later in the slab: their results go to a slot
             for (uint32_t p = R[r].p0; p < R[r].p1; ++p) {
                 const uint32_t row = sl.order[p];
                 if (seen[row] == b && last_use[row] > (int64_t)r) {
@@ -804,82 +889,219 @@ bool stream_layout(const Sweep<Low>& s, const std::vector<uint32_t>& start, uint
         // 4. records of this slab's rounds
         for (uint32_t r = 0; r < R.size(); ++r) {
             const Round& rd = R[r];
-            const uint32_t nr = rd.p1 - rd.p0, X = (uint32_t)rd.xrow.size();
-            const RoundRec rec = round_rec(nr, rd.L, X, vb);
+            const uint32_t nr = rd.p1 - rd.p0;
+            // early / late entries of each row: (slot, index of the entry in the sweep)
+            std::vector<std::vector<std::pair<uint32_t, uint32_t>>> ear(nr), lat(nr);
+            uint32_t E = 0, K = 0;
+            for (uint32_t p = rd.p0; p < rd.p1; ++p) {
+                const uint32_t j = p - rd.p0;
+                for (uint32_t k = sl.rowptr[p]; k < sl.rowptr[p + 1]; ++k) {
+                    const uint32_t d = sl.col[k];
+                    if (slot_in[d] != b || slot_of[d] < NZ || slot_of[d] == kNoSlot)
+                        return fail("a dependency without a value slot");
+                    const bool late = d >= rb && d < re && r > 0 && round_of[d] == r - 1;
+                    (late ? lat : ear)[j].emplace_back(slot_of[d], k);
+                }
+                E = std::max<uint32_t>(E, (uint32_t)ear[j].size());
+                K = std::max<uint32_t>(K, (uint32_t)lat[j].size());
+            }
+            const uint32_t Eg = (E + 3) / 4, Kg = (K + 3) / 4;
+            if (Eg > 255 || Kg > 255) return fail("a row with more than 1020 entries");
+            const RoundRec rec = round_rec(nr, Eg, Kg, vb, slot_bytes);
             const uint64_t off = out.blob.size();
-            if ((off + rec.bytes) / 8 > 0xFFFFFFFFull) return fail("blob beyond 32 GB");
+            if ((off + rec.bytes) / 16 > 0xFFFFFFFFull || (off + rec.bytes) / slot_bytes > 0xFFFFFFFFull)
+                return fail("round records beyond the addressable blob");
             out.blob.resize(off + rec.bytes, 0);
             uint8_t* base = out.blob.data() + off;
-            double* diag = reinterpret_cast<double*>(base + rec.diag);
-            uint16_t* lrow = reinterpret_cast<uint16_t*>(base + rec.lrow);
-            uint16_t* oslot = reinterpret_cast<uint16_t*>(base + rec.oslot);
-            uint8_t* ent = base + rec.ent;
-            uint32_t* xrow = reinterpret_cast<uint32_t*>(base + rec.xrow);
-            uint16_t* xslot = reinterpret_cast<uint16_t*>(base + rec.xslot);
-            uint16_t* xwait = reinterpret_cast<uint16_t*>(base + rec.xwait);
             for (uint32_t p = rd.p0; p < rd.p1; ++p) {
                 const uint32_t j = p - rd.p0, row = sl.order[p];
-                diag[j] = recip ? 1.0 / sl.diag[p] : sl.diag[p];  // divisions become products
-                lrow[j] = (uint16_t)(row - rb);
-                oslot[j] = (uint16_t)(slot_in[row] == b && seen[row] == b && last_use[row] > (int64_t)r
-                                          ? slot_of[row] : kNoSlot);
-                out.in_slot[row] = (uint32_t)((off + rec.in) / 8 + j);
-                for (uint32_t k = sl.rowptr[p]; k < sl.rowptr[p + 1]; ++k) {
-                    const uint32_t d = sl.col[k], e = (k - sl.rowptr[p]) * rec.m + j;
-                    if (slot_in[d] != b || slot_of[d] == 0) return fail("a dependency without a value slot");
-                    if (vb == 4) {  // {u32 slot, f32 value}
-                        const uint32_t slot = slot_of[d];
-                        std::memcpy(ent + (size_t)e * 8, &slot, 4);
-                        std::memcpy(ent + (size_t)e * 8 + 4, &sl.val[k], 4);
-                    } else {        // u16 slot; f64 value in the value section
-                        const uint16_t slot = (uint16_t)slot_of[d];
-                        std::memcpy(ent + (size_t)e * 2, &slot, 2);
-                        std::memcpy(base + rec.val + (size_t)e * 8, &sl.val[k], 8);
-                    }
+                const uint32_t os = seen[row] == b && slot_in[row] == b && last_use[row] > (int64_t)r ? slot_of[row]
+                                                                                                      : kNoSlot;
+                const uint32_t lo = (row - rb) | (os << 16);
+                const double dg = recip ? 1.0 / sl.diag[p] : sl.diag[p];  // divisions become products
+                uint8_t* f = base + rec.fld + 16u * j;
+                if (slot_bytes == 4) {
+                    const float dgf = (float)dg;
+                    std::memcpy(f + 4, &dgf, 4);
+                    std::memcpy(f + 8, &lo, 4);
+                    out.in_slot[row] = (uint32_t)((off + rec.fld + 16u * j) / 4);
+                } else {
+                    std::memcpy(f + 8, &dg, 8);
+                    std::memcpy(base + rec.lo + 4u * j, &lo, 4);
+                    out.in_slot[row] = (uint32_t)((off + rec.fld + 16u * j) / 8);
                 }
             }
+            // entry order, one wavefront's rows at a time
+            auto place = [&](std::vector<std::vector<std::pair<uint32_t, uint32_t>>>& ent, uint32_t groups,
+                             uint32_t sec_s, uint32_t sec_c, std::vector<std::vector<std::pair<uint32_t, double>>>* ord) {
+                const uint32_t Pn = 4 * groups;
+                if (!Pn) return;
+                for (uint32_t g0 = 0; g0 < nr; g0 += G) {
+                    const uint32_t g1 = std::min(nr, g0 + G);
+                    std::vector<std::vector<std::pair<uint32_t, uint32_t>>> rows(ent.begin() + g0, ent.begin() + g1);
+                    std::vector<std::vector<int64_t>> pos;
+                    bank_order(rows, Pn, NZ, pos);
+                    for (uint32_t j = g0; j < g1; ++j) {
+                        const uint32_t row = sl.order[rd.p0 + j];
+                        for (uint32_t u = 0; u < Pn; ++u) {
+                            const int64_t e = pos[j - g0][u];
+                            uint16_t slot;
+                            Low coef;
+                            uint32_t dep = kNone;
+                            if (e >= 0) {
+                                const auto& pr = rows[j - g0][(size_t)e];
+                                slot = (uint16_t)pr.first;
+                                coef = sl.val[pr.second];
+                                dep = sl.col[pr.second];
+                            } else {
+                                slot = (uint16_t)(-1 - e);
+                                coef = (Low)0;
+                            }
+                            const uint32_t gi = u / 4, ci = u % 4;
+                            std::memcpy(base + sec_s + 8u * ((size_t)gi * rec.m + j) + 2u * ci, &slot, 2);
+                            std::memcpy(base + sec_c + 4u * vb * ((size_t)gi * rec.m + j) + vb * ci, &coef, vb);
+                            if (ord) (*ord)[row].emplace_back(dep, (double)coef);
+                        }
+                    }
+                }
+            };
+            place(ear, Eg, rec.es, rec.ec, order ? &ord_e : nullptr);
+            place(lat, Kg, rec.ls, rec.lc, order ? &ord_k : nullptr);
+            const uint32_t X = (uint32_t)rd.xrow.size();
             for (uint32_t x = 0; x < X; ++x) {
-                xrow[x] = rd.xrow[x];
-                xslot[x] = (uint16_t)rd.xslot[x];
-                xwait[x] = (uint16_t)rd.xwait[x];
+                out.halo_row.push_back(rd.xrow[x]);
+                out.halo_sw.push_back(rd.xslot[x] | (rd.xwait[x] << 16));
             }
+            out.halo_ptr.push_back((uint32_t)out.halo_row.size());
             out.meta.push_back((uint32_t)(off / 16));
             out.meta.push_back(rec.bytes);
-            out.meta.push_back(nr | (rd.L << 16));
-            out.meta.push_back(X);
+            out.meta.push_back(nr | (Eg << 8) | (Kg << 16) | ((X > 0 ? 1u : 0u) << 24));
+            out.meta.push_back(0);
             out.max_round_bytes = std::max(out.max_round_bytes, rec.bytes);
         }
     }
     out.num_rounds = out.cta_round[num_ctas];
+    if (order) {
+        for (uint32_t r = 0; r < n; ++r) {
+            order->eptr[r + 1] = order->eptr[r] + (uint32_t)ord_e[r].size();
+            order->kptr[r + 1] = order->kptr[r] + (uint32_t)ord_k[r].size();
+        }
+        order->edep.reserve(order->eptr[n]);
+        order->ecoef.reserve(order->eptr[n]);
+        order->kdep.reserve(order->kptr[n]);
+        order->kcoef.reserve(order->kptr[n]);
+        for (uint32_t r = 0; r < n; ++r) {
+            for (const auto& e : ord_e[r]) {
+                order->edep.push_back(e.first);
+                order->ecoef.push_back(e.second);
+            }
+            for (const auto& e : ord_k[r]) {
+                order->kdep.push_back(e.first);
+                order->kcoef.push_back(e.second);
+            }
+        }
+    }
     return true;
 }
 
-template <typename Low>
-std::string stream_layout_replay(const Sweep<Low>& s, const StreamLayout& L, const double* in, double* out) {
+namespace {
+template <typename A>
+struct Arith;
+template <>
+struct Arith<float> {
+    static float fma(float a, float b, float c) { return std::fmaf(a, b, c); }
+};
+template <>
+struct Arith<double> {
+    static double fma(double a, double b, double c) { return std::fma(a, b, c); }
+};
+
+// One row's sum and result in the kernel's arithmetic (Acc: float or double; -ffp-contract=off
+// keeps every other operation a separate rounding).
+template <typename Acc>
+Acc row_result(int op, Acc vin, Acc dg, const Acc* ex, const Acc* ec, uint32_t ne, const Acc* kx, const Acc* kc,
+               uint32_t nk) {
+    Acc c[4] = {(Acc)0, (Acc)0, (Acc)0, (Acc)0};
+    for (uint32_t u = 0; u < ne; ++u) c[u & 3] = Arith<Acc>::fma(ec[u], ex[u], c[u & 3]);
+    Acc s = (c[0] + c[1]) + (c[2] + c[3]);
+    for (uint32_t k = 0; k < nk; ++k) s = Arith<Acc>::fma(kc[k], kx[k], s);
+    if (op == SWEEP_DIV || op == SWEEP_MUL) return (vin - s) * dg;
+    if (op == SWEEP_NONE) return vin - s;
+    return vin * dg - s;
+}
+
+template <typename Low, typename Acc>
+std::string replay_impl(const Sweep<Low>& s, const StreamLayout& L, const double* in, double* out) {
     const uint32_t n = s.n;
-    const uint32_t vb = (uint32_t)sizeof(Low);
+    const uint32_t vb = (uint32_t)sizeof(Low), ab = (uint32_t)sizeof(Acc);
+    const uint32_t NZ = zero_slots(ab);
     const bool recip = s.op == SWEEP_DIV || s.op == SWEEP_PREDIV;
     std::vector<uint8_t> blob = L.blob;
     if (L.in_slot.size() != n) return "in_slot size";
     for (uint32_t r = 0; r < n; ++r) {
-        if ((uint64_t)L.in_slot[r] * 8 + 8 > blob.size()) return "in_slot beyond the blob";
-        std::memcpy(blob.data() + (uint64_t)L.in_slot[r] * 8, in + r, 8);
+        if ((uint64_t)L.in_slot[r] * ab + ab > blob.size()) return "in_slot beyond the blob";
+        const Acc v = (Acc)in[r];
+        std::memcpy(blob.data() + (uint64_t)L.in_slot[r] * ab, &v, ab);
     }
+    if (L.halo_ptr.size() != (size_t)L.num_rounds + 1 || L.halo_ptr.back() != L.halo_row.size() ||
+        L.halo_sw.size() != L.halo_row.size())
+        return "halo list sizes";
     std::vector<uint32_t> pos_of(n);
     for (uint32_t p = 0; p < n; ++p) pos_of[s.order[p]] = p;
     std::vector<uint8_t> done(n, 0);
+    std::vector<Acc> val(n, (Acc)0);   // finished results in the kernel's type
+    std::vector<uint32_t> rnd(n, 0);   // round of its slab in which a row was computed
     struct Cta {
-        uint32_t next = 0;
-        std::vector<double> xs;
-        std::vector<int64_t> owner;  // row whose value the slot holds (-1: none)
+        uint32_t next = 0;             // next round to compute
+        uint32_t copied = 0;           // halo copies made (in order)
+        std::vector<Acc> xs;
+        std::vector<int64_t> owner;    // row whose value the slot holds (-1: none, -2: zero)
     };
     std::vector<Cta> ctas(L.num_ctas);
     for (Cta& c : ctas) {
-        c.xs.assign(L.slots, 0.0);
+        c.xs.assign(L.slots, (Acc)0);
         c.owner.assign(L.slots, -1);
+        for (uint32_t z = 0; z < NZ && z < L.slots; ++z) c.owner[z] = -2;
     }
+    struct View {
+        uint32_t nr = 0, Eg = 0, Kg = 0, halo = 0;
+        RoundRec rec{};
+        const uint8_t* base = nullptr;
+    };
+    auto view = [&](uint32_t gr, View& v) -> std::string {
+        const uint64_t off = (uint64_t)L.meta[(size_t)gr * 4] * 16;
+        const uint32_t bytes = L.meta[(size_t)gr * 4 + 1], shape = L.meta[(size_t)gr * 4 + 2];
+        v.nr = shape & 0xFFu;
+        v.Eg = (shape >> 8) & 0xFFu;
+        v.Kg = (shape >> 16) & 0xFFu;
+        v.halo = shape >> 24;
+        v.rec = round_rec(v.nr, v.Eg, v.Kg, vb, ab);
+        if (off % 16 || v.rec.bytes != bytes || off + bytes > blob.size() || bytes > L.max_round_bytes)
+            return "round record outside the blob";
+        if (v.nr == 0 || v.nr > kRoundRows) return "round size";
+        if ((v.halo != 0) != (L.halo_ptr[gr + 1] > L.halo_ptr[gr])) return "halo flag";
+        v.base = blob.data() + off;
+        return std::string();
+    };
+    auto rd16 = [](const uint8_t* p) { uint16_t v; std::memcpy(&v, p, 2); return v; };
+    auto rd32 = [](const uint8_t* p) { uint32_t v; std::memcpy(&v, p, 4); return v; };
+    // entries of row j of a round in one section pair: slots and coefficients by position
+    auto entries = [&](const View& v, uint32_t j, uint32_t groups, uint32_t ss, uint32_t sc, std::vector<uint32_t>& sl,
+                       std::vector<Acc>& cf) {
+        sl.clear();
+        cf.clear();
+        for (uint32_t u = 0; u < 4 * groups; ++u) {
+            const size_t e = (size_t)(u / 4) * v.rec.m + j;
+            sl.push_back(rd16(v.base + ss + 8 * e + 2 * (u % 4)));
+            Low c;
+            std::memcpy(&c, v.base + sc + 4 * vb * e + vb * (u % 4), vb);
+            cf.push_back((Acc)c);
+        }
+    };
     uint32_t finished = 0;
-    const uint32_t total = L.cta_round[L.num_ctas];
+    const uint32_t total = L.num_rounds;
+    std::vector<uint32_t> sl;
+    std::vector<Acc> cf;
     while (finished < total) {
         bool progress = false;
         for (uint32_t b = 0; b < L.num_ctas; ++b) {
@@ -887,99 +1109,128 @@ std::string stream_layout_replay(const Sweep<Low>& s, const StreamLayout& L, con
             const uint32_t rb = L.slab_start[b];
             if (rb >= n) return "a slab beyond the rows";
             const uint32_t owned = L.slab_start[b + 1] - rb;
-            const uint32_t R = L.cta_round[b + 1] - L.cta_round[b];
+            const uint32_t g0 = L.cta_round[b], R = L.cta_round[b + 1] - g0;
+            // halo copies as early as their waits allow (rounds of this slab done >= wait and
+            // the halo row finished), in order
+            const uint32_t hbeg = L.halo_ptr[g0], hend = L.halo_ptr[g0 + R];
+            while (hbeg + c.copied < hend) {
+                const uint32_t x = hbeg + c.copied, row = L.halo_row[x];
+                const uint32_t slot = L.halo_sw[x] & 0xFFFFu, wait = L.halo_sw[x] >> 16;
+                if (row >= n) return "halo row out of range";
+                if (row >= rb && row < rb + owned) return "halo row inside the slab";
+                if (slot < NZ || slot >= L.slots) return "halo slot out of range";
+                if (c.next < wait || !done[row]) break;
+                c.xs[slot] = val[row];
+                c.owner[slot] = row;
+                ++c.copied;
+                progress = true;
+            }
             while (c.next < R) {
-                const uint32_t r = c.next, gr = L.cta_round[b] + r;
-                const uint64_t off = (uint64_t)L.meta[(size_t)gr * 4] * 16;
-                const uint32_t bytes = L.meta[(size_t)gr * 4 + 1], nr = L.meta[(size_t)gr * 4 + 2] & 0xFFFFu,
-                               Lr = L.meta[(size_t)gr * 4 + 2] >> 16, X = L.meta[(size_t)gr * 4 + 3];
-                const RoundRec rec = round_rec(nr, Lr, X, vb);
-                if (off % 16 || rec.bytes != bytes || off + bytes > blob.size() || bytes > L.max_round_bytes)
-                    return "round record outside the blob";
-                if (nr == 0 || nr > kRoundRows) return "round size";
-                const uint8_t* base = blob.data() + off;
-                const uint32_t* xrow = reinterpret_cast<const uint32_t*>(base + rec.xrow);
-                const uint16_t* xslot = reinterpret_cast<const uint16_t*>(base + rec.xslot);
-                const uint16_t* xwait = reinterpret_cast<const uint16_t*>(base + rec.xwait);
-                bool ready = true;
-                for (uint32_t x = 0; x < X && ready; ++x) {
-                    if (xrow[x] >= n) return "halo row out of range";
-                    if (xrow[x] >= rb && xrow[x] < rb + owned) return "halo row inside the slab";
-                    ready = done[xrow[x]] != 0;
+                const uint32_t r = c.next, gr = g0 + r;
+                View v;
+                std::string e = view(gr, v);
+                if (!e.empty()) return e;
+                // round r needs its own halo (its early entries are read while round r - 1 is computed)
+                if (hbeg + c.copied < L.halo_ptr[gr + 1]) break;  // an upstream slab first
+                for (uint32_t x = L.halo_ptr[gr]; x < L.halo_ptr[gr + 1]; ++x) {
+                    const uint32_t wait = L.halo_sw[x] >> 16;
+                    if (r >= 2 ? wait > r - 2 : wait > 0) return "a prefetch waits on its own or a later round";
                 }
-                if (!ready) break;  // an upstream slab first
-                for (uint32_t x = 0; x < X; ++x) {
-                    if (xslot[x] >= L.slots || xslot[x] == 0) return "halo slot out of range";
-                    // the kernel copies round r's halo in while round r - 1 computes
-                    if (xwait[x] > (r > 0 ? r - 1 : 0)) return "a prefetch waits on its own or a later round";
-                    c.xs[xslot[x]] = out[xrow[x]];
-                    c.owner[xslot[x]] = xrow[x];
-                }
-                const double* vin = reinterpret_cast<const double*>(base + rec.in);
-                const double* diag = reinterpret_cast<const double*>(base + rec.diag);
-                const uint16_t* lrow = reinterpret_cast<const uint16_t*>(base + rec.lrow);
-                const uint16_t* oslot = reinterpret_cast<const uint16_t*>(base + rec.oslot);
-                const uint8_t* ent = base + rec.ent;
-                auto ent_slot = [&](uint32_t e) -> uint64_t {
-                    if (vb == 4) {
-                        uint32_t w;
-                        std::memcpy(&w, ent + (size_t)e * 8, 4);
-                        return w;
-                    }
-                    uint16_t w;
-                    std::memcpy(&w, ent + (size_t)e * 2, 2);
-                    return w;
-                };
-                auto ent_val = [&](uint32_t e) {
-                    Low v;
-                    if (vb == 4) std::memcpy(&v, ent + (size_t)e * 8 + 4, 4);
-                    else std::memcpy(&v, base + rec.val + (size_t)e * 8, 8);
-                    return v;
-                };
-                // the rows of a round run at once: all of them read before any writes
-                std::vector<double> res(nr);
-                for (uint32_t j = 0; j < nr; ++j) {
-                    if (lrow[j] >= owned) return "row outside its slab";
-                    const uint32_t row = rb + lrow[j];
+                // reads of round r (early ones while round r - 1 is computed, late ones while
+                // round r is), checked against the slot owners
+                std::vector<Acc> res(v.nr);
+                std::vector<uint32_t> rows(v.nr);
+                std::vector<std::vector<uint32_t>> read_slots(v.nr);
+                std::vector<std::vector<int64_t>> read_owner(v.nr);
+                for (uint32_t j = 0; j < v.nr; ++j) {
+                    const uint8_t* f = v.base + v.rec.fld + 16 * j;
+                    const uint32_t lo = ab == 4 ? rd32(f + 8) : rd32(v.base + v.rec.lo + 4 * j);
+                    const uint32_t lrow = lo & 0xFFFFu;
+                    if (lrow >= owned) return "row outside its slab";
+                    const uint32_t row = rb + lrow;
+                    rows[j] = row;
                     if (done[row]) return "row visited twice";
                     const uint32_t p = pos_of[row];
-                    const uint32_t len = s.rowptr[p + 1] - s.rowptr[p];
-                    if (len > Lr) return "row longer than its round's entry table";
-                    if (diag[j] != (recip ? 1.0 / s.diag[p] : s.diag[p])) return "diagonal";
-                    double acc = 0.0;
-                    for (uint32_t t = 0; t < Lr; ++t) {
-                        const uint32_t e = t * rec.m + j;
-                        const uint64_t cs = ent_slot(e);
-                        const Low cv = ent_val(e);
-                        if (cs >= L.slots) return "dependency slot out of range";
-                        if (t >= len) {  // padding: slot 0 (0.0) times 0
-                            if (cs != 0 || cv != (Low)0) return "padding entry";
-                            continue;
+                    Acc vin, dg;
+                    std::memcpy(&vin, f, ab);
+                    std::memcpy(&dg, f + ab, ab);
+                    if (dg != (Acc)(recip ? 1.0 / s.diag[p] : s.diag[p])) return "diagonal";
+                    // the row's dependencies, each to be found exactly once among its entries
+                    std::vector<uint32_t> deps(s.col.begin() + s.rowptr[p], s.col.begin() + s.rowptr[p + 1]);
+                    std::vector<Low> cvals(s.val.begin() + s.rowptr[p], s.val.begin() + s.rowptr[p + 1]);
+                    std::vector<uint8_t> used(deps.size(), 0);
+                    std::vector<Acc> ex, ec, kx, kc;
+                    for (int part = 0; part < 2; ++part) {
+                        const bool late = part == 1;
+                        entries(v, j, late ? v.Kg : v.Eg, late ? v.rec.ls : v.rec.es, late ? v.rec.lc : v.rec.ec,
+                                sl, cf);
+                        for (size_t u = 0; u < sl.size(); ++u) {
+                            const uint32_t slot = sl[u];
+                            if (slot >= L.slots) return "dependency slot out of range";
+                            const int64_t ow = c.owner[slot];
+                            if (ow == -2) {
+                                if (cf[u] != (Acc)0) return "padding entry with a coefficient";
+                            } else {
+                                if (ow < 0) return "a slot read before anything was written to it";
+                                size_t t = 0;
+                                while (t < deps.size() && (used[t] || deps[t] != (uint32_t)ow || (Acc)cvals[t] != cf[u]))
+                                    ++t;
+                                if (t == deps.size()) return "a slot does not hold a dependency of the row";
+                                used[t] = 1;
+                                if (!done[(uint32_t)ow]) return "a dependency read before it was finished";
+                                const bool in_slab = (uint32_t)ow >= rb && (uint32_t)ow < rb + owned;
+                                if (late) {
+                                    if (!in_slab || rnd[(uint32_t)ow] + 1 != r)
+                                        return "a late entry not computed in the round before";
+                                } else if (in_slab && rnd[(uint32_t)ow] + 2 > r) {
+                                    return "an early entry computed in the round before";
+                                }
+                            }
+                            (late ? kx : ex).push_back(c.xs[slot]);
+                            (late ? kc : ec).push_back(cf[u]);
+                            read_slots[j].push_back(slot);
+                            read_owner[j].push_back(ow);
                         }
-                        const uint32_t k = s.rowptr[p] + t;
-                        if (cs == 0) return "a dependency in the zero slot";
-                        if (c.owner[cs] != (int64_t)s.col[k]) return "a slot does not hold the dependency";
-                        if (!done[s.col[k]]) return "a dependency read before it was finished";
-                        if (cv != s.val[k]) return "coefficient";
-                        acc += (double)cv * c.xs[cs];
                     }
-                    if (s.op == SWEEP_DIV || s.op == SWEEP_MUL) res[j] = (vin[j] - acc) * diag[j];
-                    else if (s.op == SWEEP_NONE) res[j] = vin[j] - acc;
-                    else res[j] = vin[j] * diag[j] - acc;
+                    for (size_t t = 0; t < deps.size(); ++t)
+                        if (!used[t]) return "a dependency missing from the row's entries";
+                    res[j] = row_result<Acc>(s.op, vin, dg, ex.data(), ec.data(), (uint32_t)ex.size(), kx.data(),
+                                             kc.data(), (uint32_t)kx.size());
                 }
-                for (uint32_t j = 0; j < nr; ++j) {
-                    const uint32_t row = rb + lrow[j];
-                    out[row] = res[j];
+                // the round's results, then the race check: a slower warp may still read the
+                // round's slots after a faster one wrote its results
+                for (uint32_t j = 0; j < v.nr; ++j) {
+                    const uint8_t* f = v.base + v.rec.fld + 16 * j;
+                    const uint32_t lo = ab == 4 ? rd32(f + 8) : rd32(v.base + v.rec.lo + 4 * j);
+                    const uint32_t os = lo >> 16;
+                    const uint32_t row = rows[j];
+                    val[row] = res[j];
+                    out[row] = (double)res[j];
                     done[row] = 1;
-                    if (oslot[j] != kNoSlot) {
-                        if (oslot[j] >= L.slots || oslot[j] == 0) return "result slot out of range";
-                        c.xs[oslot[j]] = res[j];
-                        c.owner[oslot[j]] = row;
+                    rnd[row] = r;
+                    if (os != kNoSlot) {
+                        if (os < NZ || os >= L.slots) return "result slot out of range";
+                        c.xs[os] = res[j];
+                        c.owner[os] = row;
                     }
                 }
+                for (uint32_t j = 0; j < v.nr; ++j)
+                    for (size_t t = 0; t < read_slots[j].size(); ++t)
+                        if (c.owner[read_slots[j][t]] != read_owner[j][t])
+                            return "a result overwrites a slot the same round reads";
                 ++c.next;
                 ++finished;
                 progress = true;
+                // copies allowed now that one more round is done
+                while (hbeg + c.copied < hend) {
+                    const uint32_t x = hbeg + c.copied, row = L.halo_row[x];
+                    const uint32_t slot = L.halo_sw[x] & 0xFFFFu, wait = L.halo_sw[x] >> 16;
+                    if (c.next < wait || !done[row]) break;
+                    if (slot < NZ || slot >= L.slots) return "halo slot out of range";
+                    c.xs[slot] = val[row];
+                    c.owner[slot] = row;
+                    ++c.copied;
+                }
             }
         }
         if (!progress) return "rounds wait on each other";
@@ -987,6 +1238,16 @@ std::string stream_layout_replay(const Sweep<Low>& s, const StreamLayout& L, con
     for (uint32_t r = 0; r < n; ++r)
         if (!done[r]) return "row never visited";
     return std::string();
+}
+}  // namespace
+
+template <typename Low>
+std::string stream_layout_replay(const Sweep<Low>& s, const StreamLayout& L, const double* in, double* out) {
+    if (L.slot_bytes == 4) {
+        if constexpr (std::is_same<Low, float>::value) return replay_impl<Low, float>(s, L, in, out);
+        return "4-byte slots need float factor values";
+    }
+    return replay_impl<Low, double>(s, L, in, out);
 }
 
 // ---- explicit instantiations ------------------------------------------------
@@ -1009,10 +1270,10 @@ template void slab_layout<double>(const Sweep<double>&, uint32_t, uint32_t, std:
 template void slab_layout<float>(const Sweep<float>&, uint32_t, uint32_t, std::vector<uint32_t>&, Sweep<float>&);
 template std::vector<uint32_t> slab_ranges<double>(const Sweep<double>&, uint32_t);
 template std::vector<uint32_t> slab_ranges<float>(const Sweep<float>&, uint32_t);
-template bool stream_layout<double>(const Sweep<double>&, const std::vector<uint32_t>&, uint32_t, StreamLayout&,
-                                    std::string*);
-template bool stream_layout<float>(const Sweep<float>&, const std::vector<uint32_t>&, uint32_t, StreamLayout&,
-                                   std::string*);
+template bool stream_layout<double>(const Sweep<double>&, const std::vector<uint32_t>&, uint32_t, uint32_t,
+                                    StreamLayout&, std::string*, StreamOrder*);
+template bool stream_layout<float>(const Sweep<float>&, const std::vector<uint32_t>&, uint32_t, uint32_t,
+                                   StreamLayout&, std::string*, StreamOrder*);
 template std::string stream_layout_replay<double>(const Sweep<double>&, const StreamLayout&, const double*,
                                                   double*);
 template std::string stream_layout_replay<float>(const Sweep<float>&, const StreamLayout&, const double*, double*);

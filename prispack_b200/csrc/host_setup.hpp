@@ -111,30 +111,47 @@ void slab_layout(const Sweep<Low>& s, uint32_t num_ctas, uint32_t rows_per_cta, 
 // positions, in (level, row) order, are cut greedily into rounds of at most
 // kRoundRows consecutive positions none of which depends on another row of
 // the same round, so a CTA can compute a round's rows all at once, one thread
-// per row.  Every value a round reads lives in a shared-memory value slot:
-// a row of the slab gets a slot when it has readers in the slab (its result
-// is written there), a row of another slab (a "halo" row) gets one for the
-// rounds that read it (a prefetcher copies it there from global memory).
-// Slots are reused once their value's last reader has run; for halo values
-// the prefetcher first waits until that round is done (xwait).  Slot 0 holds
-// 0.0 and pads short rows.  Each round is one 16-byte aligned record, with
-// m = nr rounded up to a multiple of 8 and L = the round's longest row:
+// per row.  Every value a round reads lives in a shared-memory value slot
+// (slot_bytes each: 4 for single-precision arithmetic, else 8): a row of the
+// slab gets a slot when it has readers in the slab (its result is written
+// there), a row of another slab (a "halo" row) gets one for the rounds that
+// read it (a prefetcher copies it there from global memory).  Slots are
+// reused once their value's last reader has run.  The first NZ slots (32 for
+// 4-byte slots, 16 for 8-byte ones: one per shared-memory bank) hold 0.0 and
+// pad short rows.
 //
-//   f64 in[m]        right-hand side of each row (written per call)
-//   f64 diag[m]      (1 / diag for the dividing operations)
-//   u16 lrow[m]      row - first row of the slab
-//   u16 oslot[m]     value slot of the row's result (0xFFFF: no reader in the slab)
-//   entries          entry k of row j at e = k*m + j: the value slot of the dependency
-//                    (0: padding) and its coefficient (0: padding).  Float values:
-//                    {u32 slot, f32 value} at ent + 8e, one load.  Double values:
-//                    u16 slot at ent + 2e and f64 value at val + 8e (val = ent + 2Lm).
-//   u32 xrow[X]      halo rows whose values this round copies in ...
-//   u16 xslot[X]     ... into these slots ...
-//   u16 xwait[X]     ... once this many rounds of the slab are done
+// The dependencies of a row of round r split in two: "late" ones, rows of the
+// slab computed in round r - 1, and "early" ones, everything else (rows of
+// rounds <= r - 2 and halo rows).  The kernel sums a round's early entries
+// while the round before it is still being computed, so only the late ones
+// (two or three per row on 3D stencils) sit on the chain of rounds.  Inside
+// each group of rows that one shared-memory wavefront serves (32 rows for
+// 4-byte slots, 16 for 8-byte ones) the entries of every row are ordered so
+// that, position by position, the rows read slots of distinct banks where the
+// pattern allows it (a greedy edge colouring, most constrained row first).
 //
-// (the halo sections padded to 16 bytes).  meta[r] = {offset / 16, bytes,
-// nr | L << 16, X}; the rounds of CTA b are [cta_round[b], cta_round[b+1]);
-// in_slot[row] indexes the row's `in` entry in the blob (in doubles).
+// Each round is one 16-byte aligned record; m = rows rounded up to 8,
+// Eg / Kg = groups of four early / late entries (the round's longest row):
+//
+//   fld  [m] x 16 B  4-byte slots: {f32 in, f32 diag, u32 lo, 0};
+//                    8-byte slots: {f64 in, f64 diag}
+//   lo   [m] x 4 B   8-byte slots only: row - first row of the slab (low 16
+//                    bits) | value slot of the row's result << 16 (0xFFFF: no
+//                    reader in the slab)
+//   es   [Eg][m] x 8 B       early slots, 4 x u16 per row and group
+//   ec   [Eg][m] x 4*vb B    their coefficients (vb = bytes of a factor value)
+//   ls   [Kg][m] x 8 B       late slots
+//   lc   [Kg][m] x 4*vb B    their coefficients
+//
+// diag holds 1 / diag for the dividing operations.  The sum of row j is
+//   P = (c0 + c1) + (c2 + c3),  c_i = fma chains over early positions 4g + i,
+//   s = P, then s = fma(coef, x, s) over the late positions in order,
+// padding included (slot of value 0.0, coefficient 0), in the slot type's
+// arithmetic.  meta[r] = {offset / 16, bytes, nr | Eg << 8 | Kg << 16 |
+// has_halo << 24, 0}; the rounds of CTA b are [cta_round[b], cta_round[b+1]);
+// round g's halo copies are [halo_ptr[g], halo_ptr[g+1]) of halo_row /
+// halo_sw (slot | rounds of the slab to finish first << 16); in_slot[row]
+// indexes the row's `in` field in the blob in units of slot_bytes.
 #ifdef __CUDACC__
 #define PRISM_HD __host__ __device__
 #else
@@ -143,34 +160,46 @@ void slab_layout(const Sweep<Low>& s, uint32_t num_ctas, uint32_t rows_per_cta, 
 constexpr uint32_t kRoundRows = 128;
 constexpr uint32_t kNoSlot = 0xFFFFu;
 struct RoundRec {
-    uint32_t m, in, diag, lrow, oslot, ent, val, xrow, xslot, xwait, bytes;
+    uint32_t m, fld, lo, es, ec, ls, lc, bytes;
 };
 PRISM_HD inline uint32_t pad16(uint32_t b) { return (b + 15u) & ~15u; }
-PRISM_HD inline RoundRec round_rec(uint32_t nr, uint32_t L, uint32_t X, uint32_t vb) {
+// vb: bytes of a factor value (coefficient), ab: bytes of a value slot
+PRISM_HD inline RoundRec round_rec(uint32_t nr, uint32_t Eg, uint32_t Kg, uint32_t vb, uint32_t ab) {
     RoundRec r;
     r.m = (nr + 7u) & ~7u;
-    r.in = 0;
-    r.diag = 8u * r.m;
-    r.lrow = 16u * r.m;
-    r.oslot = 18u * r.m;
-    r.ent = 20u * r.m;
-    if (vb == 4) {  // {u32 slot, f32 value} pairs
-        r.val = r.ent + 4u;
-        r.xrow = r.ent + 8u * L * r.m;
-    } else {        // u16 slots, then f64 values
-        r.val = r.ent + 2u * L * r.m;
-        r.xrow = r.val + 8u * L * r.m;
-    }
-    r.xslot = r.xrow + pad16(4u * X);
-    r.xwait = r.xslot + pad16(2u * X);
-    r.bytes = r.xwait + pad16(2u * X);
+    r.fld = 0;
+    uint32_t o = 16u * r.m;
+    r.lo = o;
+    if (ab == 8) o += pad16(4u * r.m);
+    r.es = o;
+    o += 8u * Eg * r.m;
+    r.ec = o;
+    o += 4u * vb * Eg * r.m;
+    r.ls = o;
+    o += 8u * Kg * r.m;
+    r.lc = o;
+    o += 4u * vb * Kg * r.m;
+    r.bytes = o;
     return r;
 }
+PRISM_HD inline uint32_t zero_slots(uint32_t slot_bytes) { return slot_bytes == 4 ? 32u : 16u; }
 struct StreamLayout {
     uint32_t num_ctas = 0, num_rounds = 0, max_round_bytes = 0, max_rounds_per_cta = 0;
-    uint32_t slots = 0;                // value slots of the CTA that needs most
+    uint32_t slots = 0;                // value slots of the CTA that needs most (zero slots included)
+    uint32_t slot_bytes = 8;
     std::vector<uint32_t> slab_start, cta_pos, cta_round, meta, in_slot;
+    std::vector<uint32_t> halo_ptr, halo_row, halo_sw;
     std::vector<uint8_t> blob;
+};
+// The order in which the kernel sums each row (for the oracle): per row of
+// the sweep (its own numbering), the early positions then the late ones, each
+// a dependency row (0xFFFFFFFF for padding) and its coefficient.
+struct StreamOrder {
+    std::vector<uint32_t> eptr, edep, kptr, kdep;  // eptr / kptr: n + 1
+    std::vector<double> ecoef, kcoef;
+    std::vector<double> diag;                      // per row: the sweep's diagonal (as given, not inverted)
+    int op = 0;                                    // SweepOp
+    bool lower = true;
 };
 // Slab boundaries for num_ctas CTAs (num_ctas + 1 entries, empty slabs
 // dropped): rows are first split where no dependency crosses (independent
@@ -179,19 +208,23 @@ struct StreamLayout {
 // each segment is split evenly.
 template <typename Low>
 std::vector<uint32_t> slab_ranges(const Sweep<Low>& s, uint32_t num_ctas);
-// Builds the records for slabs [start[b], start[b+1]).  For the dividing
-// operations (SWEEP_DIV, SWEEP_PREDIV) the record holds 1 / diag and the
-// kernel multiplies.  Returns false (and why) when the sweep does not fit the
-// record format or needs more than max_slots value slots in one slab.
+// Builds the records for slabs [start[b], start[b+1]) with slot_bytes-wide
+// value slots.  For the dividing operations (SWEEP_DIV, SWEEP_PREDIV) the
+// record holds 1 / diag and the kernel multiplies.  Returns false (and why)
+// when the sweep does not fit the record format or needs more than max_slots
+// value slots in one slab.  `order`, when given, receives the summation order.
 template <typename Low>
-bool stream_layout(const Sweep<Low>& s, const std::vector<uint32_t>& start, uint32_t max_slots, StreamLayout& out,
-                   std::string* why);
-// Replays k_sweep_stream on the host: stages `in` as the prep kernel does,
-// runs each slab's rounds in order (a round only once the halo rows it copies
-// in are finished), checks every offset, that each slot read holds the value
-// of the dependency it stands for, that no slot is overwritten before its last
-// reader ran and that no prefetch waits on its own or a later round, and
-// solves the sweep.  Returns an empty string, or what is wrong with the layout.
+bool stream_layout(const Sweep<Low>& s, const std::vector<uint32_t>& start, uint32_t max_slots, uint32_t slot_bytes,
+                   StreamLayout& out, std::string* why, StreamOrder* order = nullptr);
+// Replays k_sweep_stream on the host, in its arithmetic (float for 4-byte
+// slots): stages `in` as the prep kernel does and runs each slab's rounds in
+// the kernel's pipeline order -- round r's late entries and round r + 1's
+// early ones are read while round r is computed -- with every halo copy made
+// as early as its wait allows and every read checked after the writes that
+// may race with it.  Checks every offset, that each slot read holds the value
+// of the dependency it stands for and that no prefetch waits on its own or a
+// later round, and solves the sweep.  Returns an empty string, or what is
+// wrong with the layout.
 template <typename Low>
 std::string stream_layout_replay(const Sweep<Low>& s, const StreamLayout& L, const double* in, double* out);
 

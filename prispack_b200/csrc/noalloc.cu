@@ -30,11 +30,13 @@
 // which may take host memory for the text.
 //
 // Set-up.  The first call on a device, with that device current, resolves the
-// scratch address once with cudaGetSymbolAddress and caches it; later calls
-// only read the cache.  Make that first call before any stream capture
-// begins on the calling thread.
+// scratch address once with cudaGetSymbolAddress (under a mutex) and caches it
+// in an atomic per-device slot; later calls read the slot without taking the
+// mutex.  Make that first call before any stream capture begins on the
+// calling thread.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <mutex>
@@ -77,18 +79,22 @@ int na_cuda_fail(const char* what, cudaError_t e) {
 }
 
 std::mutex g_setup_mu;
-void* g_scratch_ptr[kNaMaxDevices] = {};
+std::atomic<void*> g_scratch_ptr[kNaMaxDevices] = {};
 
-// One-time set-up for `device`, which the caller has made current.
+// The scratch address on `device`, which the caller has made current; resolved
+// once per device (the only call that takes the mutex), then read lock-free.
 int scratch_for(int device, double** out) {
-    std::lock_guard<std::mutex> lock(g_setup_mu);
-    if (!g_scratch_ptr[device]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p) return na_cuda_fail("cudaGetSymbolAddress of the scratch", e);
-        g_scratch_ptr[device] = p;
+    void* p = g_scratch_ptr[device].load(std::memory_order_acquire);
+    if (!p) {
+        std::lock_guard<std::mutex> lock(g_setup_mu);
+        p = g_scratch_ptr[device].load(std::memory_order_relaxed);
+        if (!p) {
+            cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+            if (e != cudaSuccess || !p) return na_cuda_fail("cudaGetSymbolAddress of the scratch", e);
+            g_scratch_ptr[device].store(p, std::memory_order_release);
+        }
     }
-    *out = static_cast<double*>(g_scratch_ptr[device]);
+    *out = static_cast<double*>(p);
     return PRISM_OK;
 }
 
@@ -131,9 +137,10 @@ __global__ void __launch_bounds__(kNaThreads) k_residual_norms_noalloc(
     double acc[kNaVals];
 #pragma unroll
     for (int q = 0; q < kNaVals; ++q) acc[q] = 0.0;
-    // warp-uniform trip count: the full-mask shuffles below see all 32 lanes
-    for (uint32_t row0 = gid - sub; row0 < n; row0 += groups) {
-        const uint32_t row = row0 + sub;
+    // warp-uniform trip count: the full-mask shuffles below see all 32 lanes; 64-bit
+    // so that the stride cannot wrap past 2^32 for n close to it
+    for (uint64_t row0 = (uint64_t)(gid - sub); row0 < n; row0 += groups) {
+        const uint64_t row = row0 + sub;
         double s[kNaMaxCols];
 #pragma unroll
         for (int c = 0; c < kNaMaxCols; ++c) s[c] = 0.0;
@@ -144,7 +151,7 @@ __global__ void __launch_bounds__(kNaThreads) k_residual_norms_noalloc(
                 const uint64_t j = __ldg(col + e);
 #pragma unroll
                 for (int c = 0; c < kNaMaxCols; ++c)
-                    if (c < (int)k) s[c] += v * __ldg(x + c * ld + j);
+                    if (c < (int)k) s[c] += v * __ldg(x + (uint64_t)c * ld + j);
             }
         }
 #pragma unroll
@@ -152,7 +159,7 @@ __global__ void __launch_bounds__(kNaThreads) k_residual_norms_noalloc(
             if (c < (int)k) {
                 const double y = prism::group_sum<kNaG>(s[c]);
                 if (lane == 0 && row < n) {
-                    const double bi = __ldg(b + c * ld + row);
+                    const double bi = __ldg(b + (uint64_t)c * ld + row);
                     const double r = bi - y;
                     acc[2 * c] += r * r;
                     acc[2 * c + 1] += bi * bi;

@@ -263,6 +263,7 @@ void segmented_fcg_solve(Handle& h, const prism_solve_opts& o, uint32_t nseg, co
             st[q].precond_applies = applies;
             st[q].spmv_count = spmvs;
             st[q].device_ms = ms;
+            st[q].forward_error = -1.0;  // no reference solution for block / batch solves
         }
     }
 }

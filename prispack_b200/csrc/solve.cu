@@ -86,9 +86,14 @@ void launch_sweep_prepare(const Handle& h, cudaStream_t st, const DevSweep& s, c
         launch_fill(st, h, s.n, out);
         return;
     }
-    k_stream_prep<<<vec_grid(h, s.n), kBlock, 0, st>>>(s.n, s.str_in_slot.get(), in,
-                                                       reinterpret_cast<double*>(s.str_blob.get()),
-                                                       reinterpret_cast<unsigned long long*>(out));
+    if (s.acc32)
+        k_stream_prep<float><<<vec_grid(h, s.n), kBlock, 0, st>>>(s.n, s.str_in_slot.get(), in,
+                                                                  reinterpret_cast<float*>(s.str_blob.get()),
+                                                                  reinterpret_cast<unsigned long long*>(out));
+    else
+        k_stream_prep<double><<<vec_grid(h, s.n), kBlock, 0, st>>>(s.n, s.str_in_slot.get(), in,
+                                                                   reinterpret_cast<double*>(s.str_blob.get()),
+                                                                   reinterpret_cast<unsigned long long*>(out));
     PRISM_LAUNCHED();
 }
 
@@ -101,6 +106,9 @@ void launch_sweep_kernel(const Handle& h, cudaStream_t st, const DevSweep& s, co
         a.meta = reinterpret_cast<const uint4*>(s.str_meta.get());
         a.cta_round = s.str_cta_round.get();
         a.slab_start = s.str_slab_start.get();
+        a.halo_ptr = s.str_halo_ptr.get();
+        a.halo_row = s.str_halo_row.get();
+        a.halo_sw = s.str_halo_sw.get();
         a.n = s.n;
         a.ring_bytes = s.str_ring;
         a.meta_slots = s.str_meta_slots;
@@ -331,6 +339,7 @@ void DevSweep::release() {
     order.release(); rowptr.release(); col.release(); cta_pos.release();
     val64.release(); diag.release(); val32.release();
     str_blob.release(); str_meta.release(); str_cta_round.release(); str_slab_start.release(); str_in_slot.release();
+    str_halo_ptr.release(); str_halo_row.release(); str_halo_sw.release();
     num_ctas = rows_per_cta = smem_rows = 0;
     str_ctas = str_ring = str_meta_slots = str_slots = str_rounds = str_smem = 0;
     str_nnz = 0;
@@ -344,22 +353,21 @@ bool DevSweep::upload(const Sweep<Low>& s0, const DeviceInfo& info, int lay, cud
         // records stream through.
         const uint32_t nn = s0.n;
         if (nn == 0) return false;
-        uint32_t ctas = std::min<uint32_t>((uint32_t)info.sms, (nn + info.stream_min_rows - 1) / info.stream_min_rows);
-        if (ctas < 1) ctas = 1;
-        const std::vector<uint32_t> start = slab_ranges<Low>(s0, ctas);
-        ctas = (uint32_t)start.size() - 1;
+        const uint32_t ctas_req = stream_slab_count(nn, (uint32_t)info.sms, info.stream_min_rows);
+        const std::vector<uint32_t> start = slab_ranges<Low>(s0, ctas_req);
+        const uint32_t ctas = (uint32_t)start.size() - 1;
         const uint64_t smem = (uint64_t)info.max_smem_optin;
         StreamLayout L;
         const bool a32 = acc32 && std::is_same<Low, float>::value;
-        const uint64_t slot_bytes = a32 ? 4 : 8;  // one value slot
+        const uint32_t slot_bytes = a32 ? 4 : 8;  // one value slot
         const uint32_t slot_cap = (uint32_t)std::min<uint64_t>(kNoSlot, (smem - kStrFixedSmem) / slot_bytes / 2);
-        if (!stream_layout<Low>(s0, start, slot_cap, L, nullptr)) return false;
+        if (!stream_layout<Low>(s0, start, slot_cap, slot_bytes, L, nullptr)) return false;
         const uint64_t fixed = (uint64_t)kStrFixedSmem + (uint64_t)L.max_rounds_per_cta * 16 +
                                (((uint64_t)L.slots * slot_bytes + 127) & ~127ull);
-        // Round r + 1 must land while round r still occupies the ring (the row threads wait
-        // for it before finishing round r); wherever round r sits, a ring of three records
-        // has room for one more next to it.
-        if (fixed + 3ull * L.max_round_bytes > smem) return false;
+        // While round i is computed the row threads hold rounds i and i + 1 and wait for
+        // round i + 2's record: two live records and room for a third, which a circular ring
+        // of four of the largest records always has in one piece.
+        if (fixed + 4ull * L.max_round_bytes > smem) return false;
         const uint32_t ring = (uint32_t)((smem - fixed) & ~15ull);
         release();
         n = s0.n;
@@ -369,6 +377,8 @@ bool DevSweep::upload(const Sweep<Low>& s0, const DeviceInfo& info, int lay, cud
         acc32 = a32;
         layout = LAYOUT_STREAM;
         str_ctas = ctas;
+        str_ctas_req = ctas_req;
+        str_slot_bytes = slot_bytes;
         str_ring = ring;
         str_meta_slots = L.max_rounds_per_cta;
         str_slots = L.slots;
@@ -380,6 +390,11 @@ bool DevSweep::upload(const Sweep<Low>& s0, const DeviceInfo& info, int lay, cud
         str_cta_round.upload(L.cta_round.data(), L.cta_round.size(), st);
         str_slab_start.upload(L.slab_start.data(), L.slab_start.size(), st);
         str_in_slot.upload(L.in_slot.data(), L.in_slot.size(), st);
+        str_halo_ptr.upload(L.halo_ptr.data(), L.halo_ptr.size(), st);
+        str_halo_row.upload(L.halo_row.data(), L.halo_row.size(), st);
+        str_halo_sw.upload(L.halo_sw.data(), L.halo_sw.size(), st);
+        if (str_halo_row.size() == 0) str_halo_row.alloc(1);  // valid pointers for the kernel
+        if (str_halo_sw.size() == 0) str_halo_sw.alloc(1);
         PRISM_CUDA(cudaStreamSynchronize(st));
         return true;
     }
@@ -424,6 +439,48 @@ bool DevSweep::upload(const Sweep<Low>& s0, const DeviceInfo& info, int lay, cud
     PRISM_CUDA(cudaStreamSynchronize(st));
     return true;
 }
+
+uint32_t stream_slab_count(uint32_t n, uint32_t num_ctas, uint32_t min_rows) {
+    if (min_rows < 1) min_rows = 1;
+    uint32_t c = std::min<uint32_t>(num_ctas, (n + min_rows - 1) / min_rows);
+    return c < 1 ? 1 : c;
+}
+
+template <typename Low>
+bool DevSweep::stream_order(const Sweep<Low>& s, StreamOrder& o) const {
+    if (layout != LAYOUT_STREAM || s.n != n) return false;
+    StreamLayout L;
+    std::string why;
+    if (!stream_layout<Low>(s, slab_ranges<Low>(s, str_ctas_req), kNoSlot, str_slot_bytes, L, &why, &o))
+        throw Error(PRISM_ERR_CUDA, "streamed layout could not be rebuilt: " + why);
+    return true;
+}
+template bool DevSweep::stream_order<double>(const Sweep<double>&, StreamOrder&) const;
+template bool DevSweep::stream_order<float>(const Sweep<float>&, StreamOrder&) const;
+
+template <typename Low>
+void stream_sweep_run(int device, const Sweep<Low>& s, bool acc32, uint32_t num_ctas, const double* in,
+                      double* out) {
+    Handle h;
+    init_device_info(h.info, device);
+    h.info.sms = (int)std::min<uint32_t>(num_ctas, (uint32_t)h.info.sms);
+    h.info.stream_min_rows = 32;
+    PRISM_CUDA(cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking));
+    h.own_stream = true;
+    h.status.alloc(1);
+    PRISM_CUDA(cudaMemsetAsync(h.status.get(), 0, sizeof(int), h.stream));
+    DevSweep d;
+    d.acc32 = acc32 && std::is_same<Low, float>::value;
+    if (!d.upload(s, h.info, LAYOUT_STREAM, h.stream))
+        throw Error(PRISM_ERR_UNSUPPORTED, "the sweep does not fit the streamed layout");
+    DevBuf<double> din(s.n), dout(s.n);
+    din.upload(in, s.n, h.stream);
+    launch_sweep(h, h.stream, d, din.get(), dout.get());
+    PRISM_CUDA(cudaMemcpyAsync(out, dout.get(), s.n * sizeof(double), cudaMemcpyDeviceToHost, h.stream));
+    h.check_status();
+}
+template void stream_sweep_run<double>(int, const Sweep<double>&, bool, uint32_t, const double*, double*);
+template void stream_sweep_run<float>(int, const Sweep<float>&, bool, uint32_t, const double*, double*);
 
 // Sweep-kernel autotuner: uploads the sweep in each device layout in turn
 // (level order for k_sweep, slabs for k_sweep_slab, streamed rounds for
@@ -522,6 +579,12 @@ bool TriangularPrecond::sweep_info(int sweep, uint32_t* n, uint64_t* nnz, uint32
     if (vbytes) *vbytes = s.fp32 ? 4 : 8;
     if (levels) *levels = s.num_levels;
     return true;
+}
+
+bool TriangularPrecond::sweep_order(int sweep, StreamOrder& o) const {
+    const DevSweep& s = sweep == 0 ? lower_ : upper_;
+    if (f_->fp32) return s.stream_order<float>(sweep == 0 ? f_->lower32 : f_->upper32, o);
+    return s.stream_order<double>(sweep == 0 ? f_->lower64 : f_->upper64, o);
 }
 
 int export_host_factor(const HostFactor& f, int which, uint32_t* n, uint64_t* nnz, uint32_t* rowptr, uint32_t* col,
@@ -634,6 +697,19 @@ void fcg_solve(Handle& h, const prism_solve_opts& o, const double* b, double* x,
         st->spmv_count = spmvs;
         st->device_ms = ms;
     }
+}
+
+double forward_error(Handle& h, const double* x, const double* xref) {
+    const uint32_t n = h.A.n;
+    if (!n) return 0.0;
+    // { Σ xref_i^2, Σ (xref_i - x_i)^2 } into the two scratch scalars
+    k_residual<<<vec_grid(h, n), kBlock, 0, h.stream>>>(n, xref, x, nullptr, h.red.slot(SC_TMP));
+    PRISM_LAUNCHED();
+    double v[2] = {0.0, 0.0};
+    PRISM_CUDA(cudaMemcpyAsync(v, h.red.scalars.get() + SC_TMP, 2 * sizeof(double), cudaMemcpyDeviceToHost,
+                               h.stream));
+    PRISM_CUDA(cudaStreamSynchronize(h.stream));
+    return v[0] > 0.0 ? std::sqrt(v[1]) / std::sqrt(v[0]) : std::sqrt(v[1]);
 }
 
 }  // namespace prism

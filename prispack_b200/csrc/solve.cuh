@@ -76,6 +76,8 @@ struct DevSweep {
     uint64_t str_nnz = 0;
     DevBuf<unsigned char> str_blob;
     DevBuf<uint32_t> str_meta, str_cta_round, str_slab_start, str_in_slot;
+    DevBuf<uint32_t> str_halo_ptr, str_halo_row, str_halo_sw;
+    uint32_t str_ctas_req = 0, str_slot_bytes = 0;  // what the layout was built with (for its export)
     // Uploads the sweep in the given layout; false (nothing uploaded) when the
     // layout does not fit the sweep (stream layout only).
     template <typename Low>
@@ -84,6 +86,10 @@ struct DevSweep {
     bool self_filling() const { return layout == LAYOUT_STREAM; }
     uint64_t entries() const { return layout == LAYOUT_STREAM ? str_nnz : (fp32 ? val32.size() : val64.size()); }
     void release();
+    // the summation order of the streamed layout this sweep was uploaded with (s = the same
+    // host sweep); false for the other layouts
+    template <typename Low>
+    bool stream_order(const Sweep<Low>& s, StreamOrder& o) const;
     float tuned_ms = 0.f;          // time of the chosen kernel at setup (0: not tuned)
 };
 
@@ -108,6 +114,11 @@ class Precond {
     virtual bool sweep_info(int sweep, uint32_t* n, uint64_t* nnz, uint32_t* vbytes, uint32_t* levels,
                             uint32_t* kernel) const {
         (void)sweep; (void)n; (void)nnz; (void)vbytes; (void)levels; (void)kernel;
+        return false;
+    }
+    // summation order of a streamed sweep (see StreamOrder); false when the sweep runs another kernel
+    virtual bool sweep_order(int sweep, StreamOrder& o) const {
+        (void)sweep; (void)o;
         return false;
     }
     // factor export (parity checks)
@@ -135,6 +146,7 @@ class TriangularPrecond : public Precond {
     bool run_sweep(cudaStream_t st, int sweep, const double* in, double* out, int prepare) override;
     bool sweep_info(int sweep, uint32_t* n, uint64_t* nnz, uint32_t* vbytes, uint32_t* levels,
                     uint32_t* kernel) const override;
+    bool sweep_order(int sweep, StreamOrder& o) const override;
 
   private:
     Handle& h_;
@@ -169,6 +181,7 @@ class AmsedPrecond : public Precond {
     bool run_sweep(cudaStream_t st, int sweep, const double* in, double* out, int prepare) override;
     bool sweep_info(int sweep, uint32_t* n, uint64_t* nnz, uint32_t* vbytes, uint32_t* levels,
                     uint32_t* kernel) const override;
+    bool sweep_order(int sweep, StreamOrder& o) const override;
 
   private:
     struct Level {
@@ -179,6 +192,9 @@ class AmsedPrecond : public Precond {
     };
     template <typename Low>
     void build(const AmsedSetup<Low>& S);
+    // the block-diagonal lower / upper sweeps of level l, as build() uploads them
+    template <typename Low>
+    void level_sweeps(const AmsedSetup<Low>& S, uint32_t l, Sweep<Low>& lo, Sweep<Low>& up) const;
     void block_solve(cudaStream_t st, int level, const double* in, double* out);
     void c_solve(cudaStream_t st, int level, double* x);
     Handle& h_;
@@ -206,7 +222,7 @@ struct Handle {
     Reducer red;
     DevBuf<int> status;            // device status word of the bounded waits
     DevBuf<double> r, w, d, v, y;  // Krylov workspace (n each)
-    DevBuf<double> xb, bb;         // host-pointer API staging
+    DevBuf<double> xb, bb, xr;     // host-pointer API staging (xr: reference solution)
     DevBuf<double> V, Z, ksi;      // GMRES bases (n x (m+1), column-major) and LS coefficients
     double* pinned = nullptr;      // host mirror of scalars (pinned), kScalarCapacity entries
     static constexpr uint32_t kMaxKrylov = 1024;  // restart length limit
@@ -245,6 +261,14 @@ void tune_sweep(Handle& h, DevSweep& d, const Sweep<Low>& s, bool acc32 = false)
 // grad[k] = -lambda[row(k)] * x[col(k)] over A's stored entries
 void launch_adjoint_outer(const Handle& h, cudaStream_t st, const double* lambda, const double* x, double* grad);
 
+// Runs the streamed sweep kernel alone on `device` for sweep s laid out in at most num_ctas
+// slabs (the layout's own boundaries), single-precision arithmetic when acc32 (float values);
+// host input and output.  The summation order is stream_layout's with the same slabs.
+template <typename Low>
+void stream_sweep_run(int device, const Sweep<Low>& s, bool acc32, uint32_t num_ctas, const double* in, double* out);
+// slabs the streamed layout of an n-row sweep gets when at most num_ctas are wanted
+uint32_t stream_slab_count(uint32_t n, uint32_t num_ctas, uint32_t min_rows);
+
 // Runs the bounded-wait self test (see solve.cu); returns the device status the wait raised.
 int selftest_wait_timeout(int device, unsigned long long wait_ns, int* device_status);
 
@@ -252,6 +276,8 @@ int selftest_wait_timeout(int device, unsigned long long wait_ns, int* device_st
 void init_device_info(DeviceInfo& info, int device);
 
 void fcg_solve(Handle& h, const prism_solve_opts& o, const double* b, double* x, prism_solve_stats* st);
+// ||x - xref||_2 / ||xref||_2 (device vectors of the handle's size; synchronises)
+double forward_error(Handle& h, const double* x, const double* xref);
 void gmres_solve(Handle& h, const prism_solve_opts& o, const double* b, double* x, prism_solve_stats* st);
 // blocks of k <= 64 right-hand sides, column-major with leading dimension ld (batched.cu)
 void batched_apply(Handle& h, uint32_t k, const double* in_d, double* out_d, uint64_t ld);

@@ -1,43 +1,47 @@
 // Streamed round sweep: one triangular sweep (IncompleteCholesky /
 // IncompleteLDLT / IncompleteLU MSolve*UsePtr, IncompleteCholesky.cpp:249-295,
 // IncompleteLDLT.cpp:188-233, IncompleteLU.cpp:268-297) as one persistent
-// CTA per SM, each owning a slab of contiguous rows (StreamLayout).
+// CTA per SM, each owning a slab of contiguous rows (StreamLayout in
+// host_setup.hpp describes the records).
 //
 // Why.  A sweep is a chain of dependency wavefronts (about 2,000 for the
-// level-0 ILDLT factor of 3D Poisson 128^3).  When every dependency crosses
-// the L2 (k_sweep), each wavefront costs about two L2 round trips.  Here a
-// slab computes its rows in rounds of up to 128 mutually independent rows,
-// one thread per row, reading every dependency from a shared-memory value
-// slot, with an mbarrier between rounds, so the chain inside a slab costs a
-// few shared-memory reads and a barrier phase per round.  The L2 is kept off
-// the chain in two ways: the slab's round records stream from HBM into a
-// shared-memory ring by bulk copies (cp.async.bulk + mbarrier) well ahead of
-// their rounds, and values of rows owned by other slabs ("halo" rows, always
-// upstream: lower sweeps depend on lower rows only, upper sweeps on higher
-// ones) are copied into their slots by prefetcher warps as soon as they are
-// finished, while the slab is still working on earlier rounds.
+// level-0 ILDLT factor of 3D Poisson 128^3), so its time is the number of
+// wavefronts times the latency of one.  A slab computes its rows in rounds of
+// up to 128 mutually independent rows, one thread per row, reading every
+// dependency from a shared-memory value slot; the L2 stays off the chain: the
+// slab's round records stream from HBM into a shared-memory ring by bulk
+// copies (cp.async.bulk + mbarrier) well ahead of their rounds, and values of
+// rows owned by other slabs ("halo" rows, always upstream: lower sweeps depend
+// on lower rows only, upper sweeps on higher ones) are copied into their slots
+// by prefetcher warps as soon as they are finished.
 //
-// What a round costs (3D Poisson 128^3, level-0 factor, B200): about 0.7 us
-// with float arithmetic, in slabs with and without halo rows alike; about
-// half is the dot product, half the round's bookkeeping (record fields,
-// result, barrier, next record).  Each is a chain of dependent shared-memory
-// loads and arithmetic of some tens of cycles a link.
+// What sits on the chain.  Of a row's ~25 dependencies only two or three
+// ("late" entries) are rows of the round just before; the others ("early"
+// entries) were computed two or more rounds earlier or are halo values.  So
+// while round i is computed, each row thread also sums round i + 1's early
+// entries, and round i + 1 then only adds its late entries: one round on the
+// chain is a barrier, a few shared-memory loads and fused multiply-adds, the
+// result and its store.  The record of round i + 2 is loaded into registers
+// a round ahead of use, and the setup orders every row's entries so that the
+// 32 (16 for 8-byte slots) rows one wavefront serves read distinct banks.
 //
-// Roles (352 threads; the polling warps sleep between polls so that the row
-// threads, which carry the dependency chain, keep the issue slots):
-//   warps 0..3    row threads: thread j computes row j of each round, then each
-//                 warp arrives on the round's mbarrier and waits for it.  A
-//                 wavefront of a slab rarely holds more than 128 rows, so a
-//                 slab's chain of rounds is about as long as its chain of levels.
-//   warps 4..9    prefetchers: warp 4+k handles rounds k, k+6, ...: it waits
-//                 until the round's record has landed, polls each new halo row
-//                 in global memory until it is finished, waits until the slot's
-//                 previous value has had its last reader (xwait), writes the
-//                 slot and arrives on the barrier that ends the round before,
-//                 whose phase therefore also means "the next round's halo is in".
-//   warp 10       producer: issues the bulk copies of the records into the
-//                 ring in order, publishes how many have landed, and recycles
-//                 the ring space of finished rounds.
+// Roles (256 threads, two warps per SM sub-partition):
+//   warps 0..3    row threads: thread j computes row j of each round.  One
+//                 iteration (after the barrier that ends round i - 1): load round
+//                 i's late values; sum round i + 1's early entries; finish round
+//                 i (late entries, result into its slot and into global memory);
+//                 load round i + 2's record into registers; barrier (a named
+//                 barrier with an OR reduction, so that all four warps take the
+//                 same decision to leave).
+//   warps 4..6    prefetchers: warp 4+k handles the halo of rounds k, k+3, ...:
+//                 polls each halo row in global memory until it is finished,
+//                 waits until the slot's previous value has had its last reader,
+//                 writes the slot and raises the round's halo flag.  A row thread
+//                 that finds round i + 1's flag down sums its early entries after
+//                 the barrier instead, waiting for the flag there.
+//   warp 7        producer: issues the bulk copies of the records into the ring
+//                 in order, publishes how many have landed, and recycles the ring
+//                 space of finished rounds.
 //
 // Finished values are published in global memory with the kPending encoding
 // of k_sweep (the 8-byte word itself says whether it is finished); a prep
@@ -45,35 +49,40 @@
 // output pending before the sweep.
 //
 // Progress: rounds of a slab depend only on earlier rounds of the slab and on
-// upstream slabs, so the most upstream unfinished slab always progresses
-// (its halo rows are finished, its records need only ring space that its own
-// finished rounds release).  All CTAs are co-resident (cooperative launch,
-// one per SM).  There is no hardware barrier: every wait is a bounded poll
-// (wait_ns); on expiry the kernel raises status 6 and tells the CTA to leave,
-// the producer waits (again bounded) for its copies in flight, and every
-// warp returns.
+// upstream slabs, so the most upstream unfinished slab always progresses.  All
+// CTAs are co-resident (cooperative launch, one per SM).  Every wait is a
+// bounded poll (wait_ns); on expiry the kernel raises status 6 and tells the
+// CTA to leave; the row warps leave together after their next barrier, and the
+// producer waits (bounded, much longer than any copy takes) for its copies in
+// flight before it returns.
 #pragma once
 
 #include <type_traits>
 
+#include "host_setup.hpp"
 #include "kernels.cuh"
 
 namespace prism {
 
 constexpr int kStrRowWarps = (int)kRoundRows / 32;     // row threads: one per row of a round
-constexpr int kStrPrefetchWarps = 6;                   // warps kStrRowWarps .. kStrProducer - 1
+constexpr int kStrPrefetchWarps = 3;                   // warps kStrRowWarps .. kStrProducer - 1
 constexpr int kStrProducer = kStrRowWarps + kStrPrefetchWarps;
 constexpr int kStrThreads = 32 * (kStrProducer + 1);
-constexpr uint32_t kStrMaxRounds = 64;                 // rounds in flight (ring table slots)
-// copy barriers, round barriers, start barrier (+pad), ring offsets, words
-constexpr uint32_t kStrFixedSmem = 64 * 8 + 64 * 8 + 16 + 64 * 4 + 32;
+constexpr uint32_t kStrMaxRounds = 64;                 // rounds in flight (ring table and halo flag slots)
+// copy barriers, halo flags, ring offsets, words
+constexpr uint32_t kStrFixedSmem = 64 * 8 + 64 * 4 + 64 * 4 + 32;
+constexpr unsigned long long kStrDrainNs = 2000000000ull;  // bound of the final wait for copies in flight
 static_assert(kStrThreads <= 1024, "warp roles");
+static_assert(kStrFixedSmem % 16 == 0, "round table alignment");
 
 struct StreamArgs {
     const unsigned char* blob;
-    const uint4* meta;            // per round: {offset / 16, bytes, nr | L << 16, X}
+    const uint4* meta;            // per round: {offset / 16, bytes, nr | Eg << 8 | Kg << 16 | halo << 24, 0}
     const uint32_t* cta_round;    // num_ctas + 1
     const uint32_t* slab_start;   // num_ctas + 1: CTA b owns rows [slab_start[b], slab_start[b+1])
+    const uint32_t* halo_ptr;     // rounds + 1
+    const uint32_t* halo_row;     // per halo copy: row
+    const uint32_t* halo_sw;      // per halo copy: slot | wait << 16
     uint32_t n, ring_bytes, meta_slots, slots;
     double* out;
     int* status;
@@ -92,9 +101,6 @@ __device__ __forceinline__ void st_release_shared_u32(uint32_t* p, uint32_t v) {
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
 }
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
-}
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
 }
@@ -109,17 +115,6 @@ __device__ __forceinline__ bool mbar_test_parity(uint64_t* bar, uint32_t parity)
         : "memory");
     return ok != 0;
 }
-__device__ __forceinline__ bool mbar_try_parity(uint64_t* bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_addr(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
 // global -> shared bulk copy completing on an mbarrier (16-byte aligned, size % 16 == 0)
 __device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
@@ -127,53 +122,95 @@ __device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32
                  "l"(src), "r"(bytes), "r"(smem_addr(bar))
                  : "memory");
 }
+// Barrier 1 over the row threads with an OR reduction: every row thread gets the
+// same answer, so all of them leave at the same barrier or none does.
+__device__ __forceinline__ bool row_barrier_or(bool pred) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 q, %1, 0;\n\t"
+        "bar.red.or.pred p, 1, %2, q;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)pred), "n"(kStrRowWarps * 32)
+        : "memory");
+    return r != 0;
+}
 
-// Prep: each row's right-hand side into its record, the output marked pending.
-// Safe for in == out (each row is read, then written, by one thread).
+// Correctly rounded arithmetic in the sweep's type, never contracted.
+__device__ __forceinline__ float acc_fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double acc_fma(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float acc_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double acc_add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float acc_sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double acc_sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float acc_mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double acc_mul(double a, double b) { return __dmul_rn(a, b); }
+
+// four coefficients of one entry group (16-byte aligned)
+template <typename Low>
+__device__ __forceinline__ void load_coef4(const unsigned char* p, Low (&c)[4]) {
+    if constexpr (sizeof(Low) == 4) {
+        const float4 v = *reinterpret_cast<const float4*>(p);
+        c[0] = v.x;
+        c[1] = v.y;
+        c[2] = v.z;
+        c[3] = v.w;
+    } else {
+        const double2 v0 = *reinterpret_cast<const double2*>(p);
+        const double2 v1 = *reinterpret_cast<const double2*>(p + 16);
+        c[0] = v0.x;
+        c[1] = v0.y;
+        c[2] = v1.x;
+        c[3] = v1.y;
+    }
+}
+
+// Prep: each row's right-hand side into its record (in the sweep's type), the output
+// marked pending.  Safe for in == out (each row is read, then written, by one thread).
+template <typename Acc>
 static __global__ void __launch_bounds__(kBlock) k_stream_prep(uint32_t n, const uint32_t* __restrict__ in_slot,
-                                                               const double* in, double* __restrict__ blob64,
+                                                               const double* in, Acc* __restrict__ blob,
                                                                unsigned long long* out) {
     for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
         const double v = in[r];
-        blob64[__ldg(in_slot + r)] = v;
+        blob[__ldg(in_slot + r)] = (Acc)v;
         out[r] = kPending;
     }
 }
 
-// Acc: the arithmetic type of the sweep (double; float for the single-precision apply,
-// whose value slots, products and sums are float and whose results are widened to double).
+// Low: factor value type; Acc: the arithmetic type of the sweep (double; float for the
+// single-precision apply, whose value slots, products and sums are float and whose
+// results are widened to double).
 template <typename Low, int OP, typename Acc>
 static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const StreamArgs a) {
     extern __shared__ __align__(128) unsigned char sm[];
-    uint64_t* tma_bar = reinterpret_cast<uint64_t*>(sm);                     // [64] record copies
-    uint64_t* round_bar = tma_bar + 64;                                      // [64] end of round r (r % 64)
-    uint64_t* start_bar = round_bar + 64;                                    // round 0's halo in place
-    uint32_t* ring_off = reinterpret_cast<uint32_t*>(sm + 64 * 8 * 2 + 16);  // [64]
-    uint32_t* words = ring_off + 64;  // landed, rounds done, abort
-    uint4* meta_s = reinterpret_cast<uint4*>(sm + kStrFixedSmem);            // [meta_slots]
-    Acc* xs = reinterpret_cast<Acc*>(meta_s + a.meta_slots);                 // [slots]; xs[0] = 0
+    uint64_t* tma_bar = reinterpret_cast<uint64_t*>(sm);                       // [64] record copies
+    uint32_t* hflag = reinterpret_cast<uint32_t*>(sm + 64 * 8);                // [64] round q's halo in: q + 1
+    uint32_t* ring_off = hflag + 64;                                           // [64]
+    uint32_t* words = ring_off + 64;                                           // landed, rounds done, abort
+    uint4* meta_s = reinterpret_cast<uint4*>(sm + kStrFixedSmem);              // [meta_slots]
+    Acc* xs = reinterpret_cast<Acc*>(meta_s + a.meta_slots);                   // [slots]; zero slots first
     unsigned char* ring = reinterpret_cast<unsigned char*>(xs) + ((a.slots * (uint32_t)sizeof(Acc) + 127u) & ~127u);
+    constexpr uint32_t vb = sizeof(Low), ab = sizeof(Acc);
+    constexpr uint32_t NZ = ab == 4 ? 32u : 16u;
     const uint32_t b = blockIdx.x;
     const uint32_t rb = a.slab_start[b];
-    const uint32_t r0 = a.cta_round[b];
-    const uint32_t R = a.cta_round[b + 1] - r0;
-    constexpr uint32_t vb = sizeof(Low);
+    const uint32_t g0 = a.cta_round[b];
+    const uint32_t R = a.cta_round[b + 1] - g0;
 
-    for (uint32_t i = threadIdx.x; i < R; i += blockDim.x) meta_s[i] = __ldg(a.meta + r0 + i);
+    for (uint32_t i = threadIdx.x; i < R; i += blockDim.x) meta_s[i] = __ldg(a.meta + g0 + i);
+    for (uint32_t i = threadIdx.x; i < NZ; i += blockDim.x) xs[i] = (Acc)0;
+    for (uint32_t i = threadIdx.x; i < kStrMaxRounds; i += blockDim.x) hflag[i] = 0;
     if (threadIdx.x == 0) {
-        xs[0] = (Acc)0;
         words[0] = 0;  // records landed
         words[1] = 0;  // rounds done
         words[2] = 0;  // abort
-
-        for (uint32_t i = 0; i < kStrMaxRounds; ++i) {
-            mbar_init(tma_bar + i, 1);
-            mbar_init(round_bar + i, kStrRowWarps + 1);  // the row warps + the next round's prefetcher
-        }
-        mbar_init(start_bar, 1);
+        for (uint32_t i = 0; i < kStrMaxRounds; ++i) mbar_init(tma_bar + i, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
+    if (R == 0) return;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     int* status = a.status;
@@ -188,6 +225,17 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
             return true;
         }
         return false;
+    };
+    // bounded wait until rounds done >= need (polling warps sleep between polls)
+    auto wait_done = [&](uint32_t need) {
+        if (ld_acquire_shared_u32(words + 1) >= need) return true;
+        const unsigned long long t0 = globaltimer_ns();
+        unsigned spins = 0;
+        while (ld_acquire_shared_u32(words + 1) < need) {
+            __nanosleep(32);
+            if (give_up(spins, t0)) return false;
+        }
+        return true;
     };
 
     if (warp == kStrProducer) {
@@ -206,7 +254,7 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
             }
             // ring: live records [freed, issued) occupy [tail, head) circularly
             const uint32_t tail = freed < issued ? ring_off[freed % kStrMaxRounds] : head;
-            while (issued < R && issued - freed < kStrMaxRounds) {
+            while (issued < R && issued - freed < kStrMaxRounds && vwords[2] == 0) {
                 const uint4 m = meta_s[issued];
                 const uint32_t bytes = m.y;
                 uint32_t off;
@@ -250,10 +298,12 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
             }
         }
         if (failed) {
-            // no copy may still be writing into this CTA's shared memory when it exits
+            // no new copy was issued after the failure; wait for those in flight so that none
+            // is still writing into this CTA's shared memory when it exits
             const unsigned long long t0 = globaltimer_ns();
-            while (landed < issued && globaltimer_ns() - t0 < wait_ns) {
+            while (landed < issued && globaltimer_ns() - t0 < kStrDrainNs) {
                 if (mbar_test_parity(tma_bar + landed % kStrMaxRounds, (landed / kStrMaxRounds) & 1u)) ++landed;
+                else __nanosleep(256);
             }
         }
         return;
@@ -261,69 +311,37 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
 
     if (warp >= kStrRowWarps) {
         // ------------------------------------------------------------------ prefetchers
-        // Warp k copies in the halo of rounds k, k + 6, ... and then arrives on the barrier
-        // that ends the round before (start_bar for round 0).  That barrier's previous phase
-        // (64 rounds earlier) is over: the record of round q is in the ring only once round
-        // q - 64 is done.  Round R is a stand-in that only arrives.
-        for (uint32_t q = (uint32_t)(warp - kStrRowWarps); q <= R; q += kStrPrefetchWarps) {
+        // Warp k copies in the halo of rounds k, k + 3, ... and raises each round's flag.
+        // Round q's halo is read while round q - 1 is computed (rounds done = q - 1); each
+        // slot's wait (<= q - 2) lets the copy happen a round before that.
+        for (uint32_t q = (uint32_t)(warp - kStrRowWarps); q < R; q += kStrPrefetchWarps) {
+            if ((meta_s[q].z >> 24) == 0u) continue;
+            const uint32_t x0 = __ldg(a.halo_ptr + g0 + q), x1 = __ldg(a.halo_ptr + g0 + q + 1);
             bool ok = true;
-            unsigned long long t0 = globaltimer_ns();
-            unsigned spins = 0;
-            if (q == R) {
-                while (R >= kStrMaxRounds && ld_acquire_shared_u32(words + 1) + kStrMaxRounds < R + 1) {
-                    __nanosleep(spins < 16 ? 64 : 256);  // polling warps leave issue slots to the row threads
-                    if (give_up(spins, t0)) {
+            for (uint32_t xb = x0; xb < x1; xb += 64) {
+                // two halo rows per lane in flight at once
+                unsigned long long v[2];
+                uint32_t idx[2], row[2], sw[2];
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    idx[u] = xb + (uint32_t)lane + 32u * u;
+                    row[u] = idx[u] < x1 ? __ldg(a.halo_row + idx[u]) : 0u;
+                    sw[u] = idx[u] < x1 ? __ldg(a.halo_sw + idx[u]) : 0u;
+                    v[u] = idx[u] < x1 ? ld_relaxed_u64(a.out + row[u]) : 0ull;
+                }
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    if (idx[u] >= x1 || !ok) continue;
+                    if (v[u] == kPending) {
+                        const double* p = a.out + row[u];
+                        ok = spin_ready([&] { return ld_relaxed_u64(p); }, v[u], status, wait_ns);
+                        if (!ok) break;
+                    }
+                    if (!wait_done(sw[u] >> 16)) {
                         ok = false;
                         break;
                     }
-                }
-                if (__all_sync(0xFFFFFFFFu, ok) && lane == 0) mbar_arrive(round_bar + (R - 1) % kStrMaxRounds);
-                break;
-            }
-            while (ld_acquire_shared_u32(words) <= q) {
-                __nanosleep(spins < 16 ? 64 : 256);  // polling warps leave issue slots to the row threads
-                if (give_up(spins, t0)) {
-                    ok = false;
-                    break;
-                }
-            }
-            if (!__all_sync(0xFFFFFFFFu, ok)) return;
-            const uint4 m = meta_s[q];
-            const uint32_t X = m.w;
-            const RoundRec rec = round_rec(m.z & 0xFFFFu, m.z >> 16, X, vb);
-            const unsigned char* base = ring + ring_off[q % kStrMaxRounds];
-            const uint32_t* xrow = reinterpret_cast<const uint32_t*>(base + rec.xrow);
-            const uint16_t* xslot = reinterpret_cast<const uint16_t*>(base + rec.xslot);
-            const uint16_t* xwait = reinterpret_cast<const uint16_t*>(base + rec.xwait);
-            for (uint32_t x0 = 0; x0 < X; x0 += 64) {
-                // two halo rows per lane in flight at once
-                unsigned long long v[2];
-                uint32_t idx[2];
-#pragma unroll
-                for (int u = 0; u < 2; ++u) {
-                    idx[u] = x0 + (uint32_t)lane + 32u * u;
-                    v[u] = idx[u] < X ? ld_relaxed_u64(a.out + xrow[idx[u]]) : 0ull;
-                }
-#pragma unroll
-                for (int u = 0; u < 2; ++u) {
-                    if (idx[u] >= X || !ok) continue;
-                    if (v[u] == kPending) {
-                        const double* p = a.out + xrow[idx[u]];
-                        ok = spin_ready([&] { return ld_relaxed_u64(p); }, v[u], status, wait_ns);
-                    }
-                    const uint32_t need = xwait[idx[u]];
-                    if (ok && ld_acquire_shared_u32(words + 1) < need) {
-                        t0 = globaltimer_ns();
-                        spins = 0;
-                        while (ld_acquire_shared_u32(words + 1) < need) {
-                            __nanosleep(spins < 16 ? 64 : 256);  // polling warps leave issue slots to the row threads
-                            if (give_up(spins, t0)) {
-                                ok = false;
-                                break;
-                            }
-                        }
-                    }
-                    if (ok) xs[xslot[idx[u]]] = (Acc)__longlong_as_double((long long)v[u]);
+                    xs[sw[u] & 0xFFFFu] = (Acc)__longlong_as_double((long long)v[u]);
                 }
             }
             if (!__all_sync(0xFFFFFFFFu, ok)) {
@@ -333,144 +351,231 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
                 }
                 return;
             }
-            if (lane == 0) mbar_arrive(q == 0 ? start_bar : round_bar + (q - 1) % kStrMaxRounds);
+            __syncwarp();
+            if (lane == 0) {
+                // the flag's slot last served round q - 64, whose readers are done with it
+                // once round q - 63 is done
+                if (!wait_done(q >= 63 ? q - 63 : 0)) return;
+                st_release_shared_u32(hflag + q % kStrMaxRounds, q + 1);
+            }
         }
         return;
     }
 
     // ---------------------------------------------------------------------- row threads
-    // Thread j computes row j of each round: its entries ({slot, coefficient}, one load
-    // each) sit at j, j + m, j + 2m, ...
-    // of the round's entry table (m = rows rounded up to 8), padded with slot 0 (0.0)
-    // to the round's longest row.  Before waiting for the barrier that ends round r,
-    // each thread reads round r+1's record -- up to 32 entries, right-hand side,
-    // diagonal, slots -- into registers; after it only the value-slot reads (all
-    // independent, issued back to back), the sums and the result remain on the chain.
     const uint32_t j = threadIdx.x;
-    constexpr int kRegEntries = 32;
-    struct Row {
-        uint32_t nr, L, m;              // rows, entries per row, stride
-        uint32_t os, lr, base;
-        Acc vin, dg;
-        uint32_t c[kRegEntries];
-        Low v[kRegEntries];
+    constexpr int EGR = ab == 4 ? 8 : 4;  // early entry groups held in registers (the rest: from the record)
+    // One round as a row thread holds it: fields, the first group of late entries and,
+    // once summed, its early part P.
+    struct Fld {
+        Acc vin, dg, P;
+        uint32_t lo, shape, base;
+        uint32_t ls0, ls1;
+        Low lc[4];
     };
-    Row cur;
-    // record entry e of the round (this thread's entries: e = j, j + m, ...): {slot, coefficient};
-    // one 8-byte load for float values, a u16 slot and a double for double values
-    auto ent_get = [](const unsigned char* rbase, const RoundRec& rec, uint32_t e, uint32_t& c, Low& v) {
-        if constexpr (sizeof(Low) == 4) {
-            const unsigned long long w = reinterpret_cast<const unsigned long long*>(rbase + rec.ent)[e];
-            c = (uint32_t)w;
-            v = __uint_as_float((uint32_t)(w >> 32));
+    uint32_t es[EGR][2];  // early slots of the round whose early part comes next (4 x u16 per group)
+    Low ec[EGR][4];       // and their coefficients
+    auto nr_of = [](uint32_t shape) { return shape & 0xFFu; };
+    auto eg_of = [](uint32_t shape) { return (shape >> 8) & 0xFFu; };
+    auto kg_of = [](uint32_t shape) { return (shape >> 16) & 0xFFu; };
+    auto rec_of = [&](const Fld& F) {
+        return round_rec(nr_of(F.shape), eg_of(F.shape), kg_of(F.shape), vb, ab);
+    };
+    auto load_fields = [&](uint32_t q, Fld& F) {
+        const uint4 m = meta_s[q];
+        F.shape = m.z;
+        F.base = ring_off[q % kStrMaxRounds];
+        F.P = (Acc)0;
+        if (j >= nr_of(m.z)) return;
+        const RoundRec rec = rec_of(F);
+        const unsigned char* base = ring + F.base;
+        if constexpr (ab == 4) {
+            const uint4 f = *reinterpret_cast<const uint4*>(base + rec.fld + 16u * j);
+            F.vin = __uint_as_float(f.x);
+            F.dg = __uint_as_float(f.y);
+            F.lo = f.z;
         } else {
-            c = reinterpret_cast<const uint16_t*>(rbase + rec.ent)[e];
-            v = reinterpret_cast<const double*>(rbase + rec.val)[e];
+            const double2 f = *reinterpret_cast<const double2*>(base + rec.fld + 16u * j);
+            F.vin = f.x;
+            F.dg = f.y;
+            F.lo = *reinterpret_cast<const uint32_t*>(base + rec.lo + 4u * j);
+        }
+        if (kg_of(m.z) > 0u) {
+            const uint2 s2 = *reinterpret_cast<const uint2*>(base + rec.ls + 8u * j);
+            F.ls0 = s2.x;
+            F.ls1 = s2.y;
+            load_coef4<Low>(base + rec.lc + 4u * vb * j, F.lc);
         }
     };
-    auto load_row = [&](uint32_t r, Row& w) {
-        const uint4 m = meta_s[r];
-        w.nr = m.z & 0xFFFFu;
-        w.L = m.z >> 16;
-        const RoundRec rec = round_rec(w.nr, w.L, m.w, vb);
-        w.base = ring_off[r % kStrMaxRounds];
-        w.m = rec.m;
-        if (j >= w.nr) return;
-        const unsigned char* base = ring + w.base;
-        w.vin = (Acc)reinterpret_cast<const double*>(base + rec.in)[j];
-        w.dg = (Acc)reinterpret_cast<const double*>(base + rec.diag)[j];
-        w.os = reinterpret_cast<const uint16_t*>(base + rec.oslot)[j];
-        w.lr = reinterpret_cast<const uint16_t*>(base + rec.lrow)[j];
-        // only as many register entries as the round's longest row needs (8, 16, 24, 28 or 32)
-        auto fill = [&](auto nconst) {
-            constexpr int N = decltype(nconst)::value;
+    auto load_early = [&](const Fld& F) {
+        const uint32_t Eg = eg_of(F.shape);
+        if (j >= nr_of(F.shape)) return;
+        const RoundRec rec = rec_of(F);
+        const unsigned char* base = ring + F.base;
 #pragma unroll
-            for (int u = 0; u < N; ++u) {
-                w.c[u] = 0u;
-                w.v[u] = (Low)0;
-                if ((uint32_t)u < w.L) ent_get(base, rec, u * rec.m + j, w.c[u], w.v[u]);
+        for (int g = 0; g < EGR; ++g) {
+            if ((uint32_t)g < Eg) {
+                const uint32_t e = (uint32_t)g * rec.m + j;
+                const uint2 s2 = *reinterpret_cast<const uint2*>(base + rec.es + 8u * e);
+                es[g][0] = s2.x;
+                es[g][1] = s2.y;
+                load_coef4<Low>(base + rec.ec + 4u * vb * e, ec[g]);
             }
-        };
-        if (w.L <= 8) fill(std::integral_constant<int, 8>{});
-        else if (w.L <= 16) fill(std::integral_constant<int, 16>{});
-        else if (w.L <= 24) fill(std::integral_constant<int, 24>{});
-        else if (w.L <= 28) fill(std::integral_constant<int, 28>{});
-        else fill(std::integral_constant<int, 32>{});
+        }
     };
-    // sum of the first N register entries (N a multiple of 4): value reads first, then four chains
-    auto dot_regs = [&](const Row& w, auto nconst) {
-        constexpr int N = decltype(nconst)::value;
-        Acc x[N];
+    // P = (c0 + c1) + (c2 + c3), c_i the fma chain over early positions 4g + i
+    auto early_sum = [&](Fld& F) {
+        const uint32_t Eg = eg_of(F.shape);
+        if (j >= nr_of(F.shape)) return;
+        Acc x[EGR][4];
 #pragma unroll
-        for (int u = 0; u < N; ++u) x[u] = xs[w.c[u]];
-        Acc acc[4] = {(Acc)0, (Acc)0, (Acc)0, (Acc)0};
+        for (int g = 0; g < EGR; ++g) {
+            if ((uint32_t)g < Eg) {
+                x[g][0] = xs[es[g][0] & 0xFFFFu];
+                x[g][1] = xs[es[g][0] >> 16];
+                x[g][2] = xs[es[g][1] & 0xFFFFu];
+                x[g][3] = xs[es[g][1] >> 16];
+            }
+        }
+        Acc c[4] = {(Acc)0, (Acc)0, (Acc)0, (Acc)0};
 #pragma unroll
-        for (int u = 0; u < N; ++u) acc[u & 3] += (Acc)w.v[u] * x[u];
-        return (acc[0] + acc[1]) + (acc[2] + acc[3]);
+        for (int g = 0; g < EGR; ++g) {
+            if ((uint32_t)g < Eg) {
+#pragma unroll
+                for (int i = 0; i < 4; ++i) c[i] = acc_fma((Acc)ec[g][i], x[g][i], c[i]);
+            }
+        }
+        if (Eg > (uint32_t)EGR) {  // rows longer than the register groups: the rest from the record
+            const RoundRec rec = rec_of(F);
+            const unsigned char* base = ring + F.base;
+            for (uint32_t g = EGR; g < Eg; ++g) {
+                const uint32_t e = g * rec.m + j;
+                const uint2 s2 = *reinterpret_cast<const uint2*>(base + rec.es + 8u * e);
+                Low cf[4];
+                load_coef4<Low>(base + rec.ec + 4u * vb * e, cf);
+                c[0] = acc_fma((Acc)cf[0], xs[s2.x & 0xFFFFu], c[0]);
+                c[1] = acc_fma((Acc)cf[1], xs[s2.x >> 16], c[1]);
+                c[2] = acc_fma((Acc)cf[2], xs[s2.y & 0xFFFFu], c[2]);
+                c[3] = acc_fma((Acc)cf[3], xs[s2.y >> 16], c[3]);
+            }
+        }
+        F.P = acc_add(acc_add(c[0], c[1]), acc_add(c[2], c[3]));
     };
-    auto wait_phase = [&](uint64_t* bar, uint32_t parity) {
-        if (mbar_try_parity(bar, parity)) return true;
+    auto late_load = [&](const Fld& F, Acc (&xl)[4]) {
+        if (j < nr_of(F.shape) && kg_of(F.shape) > 0u) {
+            xl[0] = xs[F.ls0 & 0xFFFFu];
+            xl[1] = xs[F.ls0 >> 16];
+            xl[2] = xs[F.ls1 & 0xFFFFu];
+            xl[3] = xs[F.ls1 >> 16];
+        }
+    };
+    auto finish = [&](const Fld& F, const Acc (&xl)[4]) {
+        const uint32_t Kg = kg_of(F.shape);
+        if (j >= nr_of(F.shape)) return;
+        Acc s = F.P;
+        if (Kg > 0u) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) s = acc_fma((Acc)F.lc[i], xl[i], s);
+        }
+        if (Kg > 1u) {  // more than four late entries: the rest from the record
+            const RoundRec rec = rec_of(F);
+            const unsigned char* base = ring + F.base;
+            for (uint32_t g = 1; g < Kg; ++g) {
+                const uint32_t e = g * rec.m + j;
+                const uint2 s2 = *reinterpret_cast<const uint2*>(base + rec.ls + 8u * e);
+                Low cf[4];
+                load_coef4<Low>(base + rec.lc + 4u * vb * e, cf);
+                s = acc_fma((Acc)cf[0], xs[s2.x & 0xFFFFu], s);
+                s = acc_fma((Acc)cf[1], xs[s2.x >> 16], s);
+                s = acc_fma((Acc)cf[2], xs[s2.y & 0xFFFFu], s);
+                s = acc_fma((Acc)cf[3], xs[s2.y >> 16], s);
+            }
+        }
+        Acc res;
+        if (OP == OP_DIV || OP == OP_MUL) res = acc_mul(acc_sub(F.vin, s), F.dg);  // dg = 1/diag for OP_DIV
+        else if (OP == OP_NONE) res = acc_sub(F.vin, s);
+        else res = acc_sub(acc_mul(F.vin, F.dg), s);                                 // dg = 1/diag
+        const double rd = (double)res;
+        unsigned long long rbits = (unsigned long long)__double_as_longlong(rd);
+        if (rd != rd) rbits = kCanonicalNaN;
+        const uint32_t os = F.lo >> 16;
+        if (os != kNoSlot) xs[os] = res;
+        st_relaxed_u64(a.out + rb + (F.lo & 0xFFFFu), rbits);
+    };
+    auto wait_landed = [&](uint32_t q) {
+        if (ld_acquire_shared_u32(words) > q) return true;
         const unsigned long long t0 = globaltimer_ns();
         unsigned spins = 0;
-        while (!mbar_try_parity(bar, parity))
+        while (ld_acquire_shared_u32(words) <= q)
             if (give_up(spins, t0)) return false;
         return true;
     };
-    if (!wait_phase(start_bar, 0)) return;
-    load_row(0, cur);
-    uint32_t landed_seen = 1;
-    for (uint32_t r = 0; r < R; ++r) {
-        if (j < cur.nr) {
-            Acc s;
-            if (cur.L <= 8) s = dot_regs(cur, std::integral_constant<int, 8>{});
-            else if (cur.L <= 16) s = dot_regs(cur, std::integral_constant<int, 16>{});
-            else if (cur.L <= 24) s = dot_regs(cur, std::integral_constant<int, 24>{});
-            else if (cur.L <= 28) s = dot_regs(cur, std::integral_constant<int, 28>{});
-            else s = dot_regs(cur, std::integral_constant<int, 32>{});
-            if (cur.L > (uint32_t)kRegEntries) {  // rows longer than 32 entries
-                const RoundRec rr = round_rec(cur.nr, cur.L, 0u, vb);  // entry sections do not depend on X
-                for (uint32_t k = kRegEntries; k < cur.L; ++k) {
-                    uint32_t c;
-                    Low v;
-                    ent_get(ring + cur.base, rr, k * cur.m + j, c, v);
-                    s += (Acc)v * xs[c];
-                }
+    auto halo_in = [&](uint32_t q) { return ld_acquire_shared_u32(hflag + q % kStrMaxRounds) == q + 1; };
+    auto wait_halo = [&](uint32_t q) {
+        if (halo_in(q)) return true;
+        const unsigned long long t0 = globaltimer_ns();
+        unsigned spins = 0;
+        while (!halo_in(q))
+            if (give_up(spins, t0)) return false;
+        return true;
+    };
+    auto has_halo = [](const Fld& F) { return (F.shape >> 24) != 0u; };
+
+    bool bad = false;
+    Fld F0, F1;
+    F0.shape = F1.shape = 0u;
+    // prologue: round 0 with its early part summed, round 1's record in registers
+    if (!wait_landed(0)) bad = true;
+    if (!bad) {
+        load_fields(0, F0);
+        load_early(F0);
+        if (has_halo(F0) && !wait_halo(0)) bad = true;
+    }
+    if (!bad) early_sum(F0);
+    if (!bad && R > 1) {
+        if (!wait_landed(1)) bad = true;
+        else {
+            load_fields(1, F1);
+            load_early(F1);
+        }
+    }
+    // One iteration: cur = round i (early part summed), nxt = round i + 1 (record in
+    // registers); once round i is finished, cur receives round i + 2.  Returns true when
+    // the row threads leave.
+    auto step = [&](uint32_t i, Fld& cur, Fld& nxt) -> bool {
+        Acc xl[4] = {(Acc)0, (Acc)0, (Acc)0, (Acc)0};
+        if (!bad) late_load(cur, xl);
+        const bool more = i + 1 < R, more2 = i + 2 < R;
+        bool pend = false;
+        if (more && !bad) {
+            if (!has_halo(nxt) || halo_in(i + 1)) early_sum(nxt);
+            else pend = true;  // its halo is not in yet: sum it after the barrier
+        }
+        if (!bad) finish(cur, xl);
+        if (more2 && !bad) {
+            if (!wait_landed(i + 2)) bad = true;
+            else {
+                load_fields(i + 2, cur);
+                if (!pend) load_early(cur);
             }
-            Acc res;
-            if (OP == OP_DIV || OP == OP_MUL) res = (cur.vin - s) * cur.dg;  // dg = 1/diag for OP_DIV
-            else if (OP == OP_NONE) res = cur.vin - s;
-            else res = cur.vin * cur.dg - s;                                  // dg = 1/diag
-            const double rd = (double)res;
-            unsigned long long rbits = (unsigned long long)__double_as_longlong(rd);
-            if (rd != rd) rbits = kCanonicalNaN;
-            if (cur.os != kNoSlot) {
-                if constexpr (sizeof(Acc) == 8) xs[cur.os] = __longlong_as_double((long long)rbits);
-                else xs[cur.os] = res;
-            }
-            st_relaxed_u64(a.out + rb + cur.lr, rbits);
         }
         __syncwarp();
-        if (lane == 0) mbar_arrive(round_bar + r % kStrMaxRounds);
-        const bool more = r + 1 < R;
-        if (more) {
-            if (landed_seen <= r + 1) {
-                // the next record normally landed long ago; otherwise wait for it here
-                const unsigned long long t0 = globaltimer_ns();
-                unsigned spins = 0;
-                bool ok = true;
-                do {
-                    uint32_t l = 0;
-                    if (lane == 0) l = ld_acquire_shared_u32(words);
-                    landed_seen = __shfl_sync(0xFFFFFFFFu, l, 0);
-                    if (landed_seen > r + 1) break;
-                    ok = !give_up(spins, t0);
-                } while (__all_sync(0xFFFFFFFFu, ok));
-                if (!__all_sync(0xFFFFFFFFu, ok)) return;
+        const bool stop = row_barrier_or(bad || vwords[2] != 0u);
+        if (threadIdx.x == 0) st_release_shared_u32(words + 1, i + 1);
+        if (stop) return true;
+        if (pend) {
+            if (!wait_halo(i + 1)) {
+                bad = true;
+            } else {
+                early_sum(nxt);
+                if (more2) load_early(cur);
             }
-            load_row(r + 1, cur);
         }
-        if (!wait_phase(round_bar + r % kStrMaxRounds, (r / kStrMaxRounds) & 1u)) return;
-        if (threadIdx.x == 0) st_release_shared_u32(words + 1, r + 1);
+        return false;
+    };
+    for (uint32_t i = 0; i < R; i += 2) {
+        if (step(i, F0, F1)) break;
+        if (i + 1 >= R || step(i + 1, F1, F0)) break;
     }
 }
 

@@ -103,3 +103,52 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
     assert rc == PRISM_ERR_ARG
     rc = _noalloc(lib, dev, A_d, X, X, 2, A.n - 1, norms, None)
     assert rc == PRISM_ERR_ARG and b"leading dimension" in lib.prism_last_error()
+
+
+def test_noalloc_calls_take_no_device_memory():
+    """After the first call on a device (which resolves the scratch address),
+    a batch of calls leaves the device's free memory exactly where it was."""
+    import torch
+
+    lib = P.load()
+    dev = torch.cuda.current_device()
+    A = P.CSRMatrix.laplacian(32, 32, 32, 0.0, 0.0, 0.0)
+    A_d = (torch.from_numpy(A.rowptr.view(np.int32)).cuda(), torch.from_numpy(A.col.view(np.int32)).cuda(),
+           torch.from_numpy(A.val).cuda())
+    rng = np.random.default_rng(12)
+    X = torch.from_numpy(rng.standard_normal(4 * A.n)).cuda()
+    B = torch.from_numpy(rng.standard_normal(4 * A.n)).cuda()
+    norms = torch.zeros(8, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    assert _noalloc(lib, dev, A_d, X, B, 4, A.n, norms, stream) == PRISM_OK
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info(dev)
+    for _ in range(20):
+        assert _noalloc(lib, dev, A_d, X, B, 4, A.n, norms, stream) == PRISM_OK
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info(dev)
+    assert free1 == free0
+
+
+def test_noalloc_on_a_device_that_is_not_current():
+    """With more than one GPU visible: a call naming another device runs there
+    (its own scratch) and leaves the calling thread's current device as it was."""
+    import torch
+
+    if torch.cuda.device_count() < 2:
+        pytest.skip("needs two visible GPUs")
+    lib = P.load()
+    cur = torch.cuda.current_device()
+    other = (cur + 1) % torch.cuda.device_count()
+    A = P.CSRMatrix.laplacian(16, 16, 16, 0.0, 0.0, 0.0)
+    with torch.cuda.device(other):
+        A_d = (torch.from_numpy(A.rowptr.view(np.int32)).cuda(), torch.from_numpy(A.col.view(np.int32)).cuda(),
+               torch.from_numpy(A.val).cuda())
+        x = torch.from_numpy(np.random.default_rng(13).standard_normal(A.n)).cuda()
+        b = torch.from_numpy(np.random.default_rng(14).standard_normal(A.n)).cuda()
+        norms = torch.zeros(2, dtype=torch.float64, device="cuda")
+    assert _noalloc(lib, other, A_d, x, b, 1, 0, norms, None) == PRISM_OK, lib.prism_last_error()
+    assert torch.cuda.current_device() == cur
+    torch.cuda.synchronize(other)
+    r = b.cpu().numpy() - A.to_scipy() @ x.cpu().numpy()
+    np.testing.assert_allclose(norms.cpu().numpy()[0], np.linalg.norm(r), rtol=1e-10)
