@@ -34,6 +34,8 @@
  *   prism_laplacian_*                 generateLaplacianCSR
  *                                     (include/MatrixClass/ModelProblem.h:45-52,
  *                                      source/MatrixClass/ModelProblem.cpp:68-133)
+ *   prism_mtx_read*                   HOST::ReadMtxTools::loadMatrix / loadRightHand
+ *                                     (source/utils/TestTools/ReadMtxTools.cpp:50-453)
  */
 #ifndef PRISM_SOLVE_H
 #define PRISM_SOLVE_H
@@ -194,6 +196,21 @@ int32_t prism_laplacian_dims(int32_t nx, int32_t ny, int32_t nz, uint32_t* n, ui
  * generateLaplacianCOO + transCOO2CSR (ModelProblem.cpp:68-133, MatrixTools.h:16-62) */
 int32_t prism_laplacian_fill(int32_t nx, int32_t ny, int32_t nz, double alphax, double alphay,
                              double alphaz, double shift, uint32_t* rowptr, uint32_t* col, double* val);
+
+/* ---- Matrix Market files (host) ------------------------------------------
+ * HOST::ReadMtxTools::loadMatrix / loadRightHand
+ * (source/utils/TestTools/ReadMtxTools.cpp:50-453) restated: a "coordinate"
+ * real file (complex: part 0 the real part, part 1 the imaginary part, each
+ * with its own pattern; pattern and integer files are refused), entries with
+ * |value| <= 10 * DBL_EPSILON not stored, indices shifted by `base` (1 for
+ * Matrix Market), "symmetric" files expanded to the full matrix and
+ * "skew-symmetric" ones mirrored with the opposite sign, each row ordered by
+ * column (transCOO2CSR, include/MatrixClass/MatrixTools.h:16-62).  Pass NULL
+ * arrays to get the sizes first.  prism_mtx_read_dense reads an "array" real
+ * file (right-hand sides), rows x cols values in column order. */
+int32_t prism_mtx_read(const char* path, int32_t base, int32_t part, uint32_t* rows, uint32_t* cols, uint64_t* nnz,
+                       uint32_t* rowptr, uint32_t* col, double* val);
+int32_t prism_mtx_read_dense(const char* path, uint32_t* rows, uint32_t* cols, double* values);
 
 /* ---- operator ------------------------------------------------------------ */
 /* Copies the host CSR to device `device`.  The structure is validated

@@ -50,6 +50,8 @@ def load(fast: bool = False) -> C.CDLL:
     lib.ref_csr_from_arrays.restype = vp
     lib.ref_csr_from_arrays.argtypes = [C.c_uint, _u32p, _u32p, _f64p]
     lib.ref_csr_dims.argtypes = [vp, C.POINTER(C.c_uint), C.POINTER(C.c_uint)]
+    lib.ref_read_mtx.restype = vp
+    lib.ref_read_mtx.argtypes = [C.c_char_p, C.c_int]
     lib.ref_csr_copy.argtypes = [vp, _u32p, _u32p, _f64p]
     lib.ref_csr_free.argtypes = [vp]
     lib.ref_spmv.argtypes = [vp, _f64p, _f64p]
@@ -99,6 +101,13 @@ class RefCSR:
     def laplacian(cls, nx, ny, nz, ax=0.0, ay=0.0, az=0.0, shift=0.0, fast=False):
         lib = load(fast)
         return cls(lib.ref_csr_laplacian(nx, ny, nz, ax, ay, az, shift), lib)
+
+    @classmethod
+    def from_mtx(cls, path, part=0, fast=False):
+        """HOST::ReadMtxTools<double>::loadMatrix of a Matrix Market file (part 1: a complex
+        file's imaginary part)."""
+        lib = load(fast)
+        return cls(lib.ref_read_mtx(os.fsencode(path), part), lib)
 
     @classmethod
     def from_arrays(cls, rowptr, col, val, fast=False):

@@ -25,6 +25,7 @@
 #include "utils/ExternalTools/MatrixReorderTools.h"
 #include "utils/ExternalTools/MetisTools.h"
 #include "utils/TestTools/WriteMtxTools.h"
+#include "utils/TestTools/ReadMtxTools.h"
 #include "utils/TestTools/checkTools.hpp"
 #define private public
 #define protected public
@@ -133,6 +134,22 @@ void ref_csr_copy(void* h, unsigned* rowptr, unsigned* col, double* val) {
 }
 
 void ref_csr_free(void* h) { delete static_cast<CSRd*>(h); }
+
+// HOST::ReadMtxTools<double>::loadMatrix of a Matrix Market file (1-based), part 0: the real
+// matrix (or a complex file's real part), 1: a complex file's imaginary part.  The reader
+// changes the working directory to dirname(binaryPath): "./" keeps it.
+void* ref_read_mtx(const char* path, int part) {
+    char here[] = "./reader";
+    ReadMtxTools<FLOAT64> rd(here, path, 1);
+    auto* A = new CSRd();
+    if (part == 0) {
+        rd.loadMatrix(*A);
+    } else {
+        CSRd re;
+        rd.loadMatrix(re, *A);
+    }
+    return A;
+}
 
 void ref_spmv(void* h, const double* x, double* y) {
     auto* A = static_cast<CSRd*>(h);

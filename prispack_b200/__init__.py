@@ -81,6 +81,9 @@ _SIGS = {
                                            C.c_int32, C.c_uint32, _f64p, _f64p]),
     "prism_precond_sweep_order": (C.c_int32, [_vp, C.c_int32, C.POINTER(C.c_uint32), _vp, _vp, _vp, _vp, _vp,
                                               _vp, _vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "prism_mtx_read": (C.c_int32, [C.c_char_p, C.c_int32, C.c_int32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                   C.POINTER(C.c_uint64), _vp, _vp, _vp]),
+    "prism_mtx_read_dense": (C.c_int32, [C.c_char_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), _vp]),
     "prism_laplacian_dims": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     "prism_laplacian_fill": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
                                          C.c_double, _u32p, _u32p, _f64p]),
@@ -255,6 +258,18 @@ def stream_sweep_run(rowptr, col, val, in_, *, diag=None, op: int = 2, lower: bo
     return out
 
 
+def read_mtx_dense(path: str):
+    """A Matrix Market "array real" file (right-hand sides, HOST::ReadMtxTools::loadRightHand):
+    returns an array of shape (cols, rows), one right-hand side per row."""
+    lib = load()
+    rows, cols = C.c_uint32(), C.c_uint32()
+    bpath = os.fsencode(path)
+    _check(lib.prism_mtx_read_dense(bpath, C.byref(rows), C.byref(cols), None))
+    v = np.zeros(max(rows.value * cols.value, 1))
+    _check(lib.prism_mtx_read_dense(bpath, C.byref(rows), C.byref(cols), v.ctypes.data))
+    return v[:rows.value * cols.value].reshape(cols.value, rows.value)
+
+
 def _ptr(t) -> int:
     """Device pointer of a torch CUDA tensor (float64, contiguous)."""
     import torch
@@ -283,6 +298,38 @@ class CSRMatrix:
 
     def getRowNum(self) -> int:
         return self.n
+
+    @classmethod
+    def from_mtx(cls, path: str, base: int = 1, part: int = 0) -> "CSRMatrix":
+        """A Matrix Market "coordinate" file (HOST::ReadMtxTools::loadMatrix,
+        source/utils/TestTools/ReadMtxTools.cpp): symmetric files expanded, near-zero
+        entries dropped, rows ordered by column; complex files: part 0 real, 1 imaginary.
+        The matrix must be square to be solved."""
+        lib = load()
+        rows, cols, nnz = C.c_uint32(), C.c_uint32(), C.c_uint64()
+        bpath = os.fsencode(path)
+        _check(lib.prism_mtx_read(bpath, base, part, C.byref(rows), C.byref(cols), C.byref(nnz), None, None, None))
+        rp = np.zeros(rows.value + 1, np.uint32)
+        ci = np.zeros(max(nnz.value, 1), np.uint32)
+        v = np.zeros(max(nnz.value, 1), np.float64)
+        _check(lib.prism_mtx_read(bpath, base, part, C.byref(rows), C.byref(cols), C.byref(nnz), rp.ctypes.data,
+                                  ci.ctypes.data, v.ctypes.data))
+        m = cls(rp, ci[:nnz.value], v[:nnz.value])
+        m.ncols = cols.value
+        return m
+
+    def write_mtx(self, path: str, symmetric: bool = False, comment: str = ""):
+        """Writes the matrix as a Matrix Market "coordinate real" file (1-based; with
+        symmetric=True only the lower triangle, as HOST::WriteMtxTools stores symmetric ones)."""
+        rows = np.repeat(np.arange(self.n), np.diff(self.rowptr.astype(np.int64)))
+        keep = rows >= self.col if symmetric else np.ones(len(rows), bool)
+        with open(path, "w") as f:
+            f.write(f"%%MatrixMarket matrix coordinate real {'symmetric' if symmetric else 'general'}\n")
+            if comment:
+                f.write(f"% {comment}\n")
+            f.write(f"{self.n} {getattr(self, 'ncols', self.n)} {int(keep.sum())}\n")
+            for r, c, v in zip(rows[keep], self.col[keep], self.val[keep]):
+                f.write(f"{int(r) + 1} {int(c) + 1} {float(v)!r}\n")
 
     @classmethod
     def laplacian(cls, nx, ny, nz, alphax=0.0, alphay=0.0, alphaz=0.0, shift=0.0) -> "CSRMatrix":

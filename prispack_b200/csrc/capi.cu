@@ -290,6 +290,42 @@ int32_t prism_selftest_stream_layout(uint32_t n, const uint32_t* rowptr, const u
     });
 }
 
+int32_t prism_mtx_read(const char* path, int32_t base, int32_t part, uint32_t* rows, uint32_t* cols, uint64_t* nnz,
+                       uint32_t* rowptr, uint32_t* col, double* val) {
+    if (!path || !rows || !cols || !nnz) return fail(PRISM_ERR_ARG, "null argument");
+    if (base < 0 || (part != 0 && part != 1)) return fail(PRISM_ERR_ARG, "index base must be >= 0, part 0 or 1");
+    return guarded([&]() -> int {
+        uint32_t r = 0, c = 0;
+        std::vector<uint32_t> rp, ci;
+        std::vector<double> v;
+        std::string err;
+        int rc = prism::read_mtx(path, (uint32_t)base, part, r, c, rp, ci, v, &err);
+        if (rc) return fail(PRISM_ERR_ARG, "Matrix Market: " + err);
+        *rows = r;
+        *cols = c;
+        *nnz = ci.size();
+        if (rowptr) std::memcpy(rowptr, rp.data(), rp.size() * sizeof(uint32_t));
+        if (col) std::memcpy(col, ci.data(), ci.size() * sizeof(uint32_t));
+        if (val) std::memcpy(val, v.data(), v.size() * sizeof(double));
+        return PRISM_OK;
+    });
+}
+
+int32_t prism_mtx_read_dense(const char* path, uint32_t* rows, uint32_t* cols, double* values) {
+    if (!path || !rows || !cols) return fail(PRISM_ERR_ARG, "null argument");
+    return guarded([&]() -> int {
+        uint32_t r = 0, c = 0;
+        std::vector<double> v;
+        std::string err;
+        int rc = prism::read_mtx_dense(path, r, c, v, &err);
+        if (rc) return fail(PRISM_ERR_ARG, "Matrix Market: " + err);
+        *rows = r;
+        *cols = c;
+        if (values) std::memcpy(values, v.data(), v.size() * sizeof(double));
+        return PRISM_OK;
+    });
+}
+
 int32_t prism_laplacian_dims(int32_t nx, int32_t ny, int32_t nz, uint32_t* n, uint32_t* nnz) {
     if (!n || !nnz) return fail(PRISM_ERR_ARG, "null output pointer");
     if (!prism::laplacian_dims(nx, ny, nz, n, nnz)) return fail(PRISM_ERR_ARG, "grid dimensions out of range");

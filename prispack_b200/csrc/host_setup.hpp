@@ -46,6 +46,18 @@ bool laplacian_dims(int32_t nx, int32_t ny, int32_t nz, uint32_t* n, uint32_t* n
 void laplacian_fill(int32_t nx, int32_t ny, int32_t nz, double ax, double ay, double az, double shift,
                     uint32_t* rowptr, uint32_t* col, double* val);
 
+// ---- Matrix Market files (mtx.cpp) -----------------------------------------
+// A sparse "coordinate" file as HOST::ReadMtxTools::loadMatrix reads it
+// (source/utils/TestTools/ReadMtxTools.cpp): real values (complex files: part
+// 0 the real part, part 1 the imaginary part, each with its own pattern),
+// near-zero entries dropped, symmetric / skew-symmetric files expanded, rows
+// ordered by column.  base: index base of the file (1 for Matrix Market).
+int read_mtx(const std::string& path, uint32_t base, int part, uint32_t& rows, uint32_t& cols,
+             std::vector<uint32_t>& rowptr, std::vector<uint32_t>& col, std::vector<double>& val, std::string* err);
+// A dense "array" file (a right-hand side block): rows x cols values, column-major.
+int read_mtx_dense(const std::string& path, uint32_t& rows, uint32_t& cols, std::vector<double>& values,
+                   std::string* err);
+
 // Structural validation of a caller CSR: monotone offsets, columns < n and
 // strictly increasing inside a row.  Returns an empty string when valid.
 std::string validate_csr(uint32_t n, const uint32_t* rowptr, const uint32_t* col);

@@ -12,6 +12,12 @@ parity build) on seeded model problems and stores their outputs:
 * CG (FlexibleCG, NormalCG) and GMRES (FlexibleGMRES with restart) results:
   iteration count, reported error, convergence flag and solution.
 
+* Matrix Market files read by HOST::ReadMtxTools (section ``mtx``): small
+  files written here (mtx/*.mtx: general with explicit zeros, comments,
+  duplicates and unsorted entries, symmetric, skew-symmetric, complex,
+  hermitian, rectangular, a right-hand-side array) and the CSR arrays the
+  reference's reader makes of them (mtx_cases.npz).
+
 * AMSED / MSLR and GMSLR hierarchies (permutation, level pointers, block
   factor digests, low-rank spectra), their MInvSolve on a seeded vector and a
   preconditioned FCG / FGMRES solve.
@@ -74,7 +80,7 @@ def main(sections):
         raise SystemExit("oracle/_ref/libprism_ref.so not built: run `make -C oracle ref` where the reference exists")
     path = os.path.join(HERE, "manifest.json")
     manifest = {}
-    if os.path.exists(path) and set(sections) != {"basic", "amsed", "gmslr"}:
+    if os.path.exists(path) and set(sections) != {"basic", "amsed", "gmslr", "mtx"}:
         with open(path) as f:
             manifest = json.load(f)
     if "basic" in sections:
@@ -83,6 +89,8 @@ def main(sections):
         amsed_section(manifest)
     if "gmslr" in sections:
         gmslr_section(manifest)
+    if "mtx" in sections:
+        mtx_section(manifest)
     manifest["_seed"] = SEED
     manifest["_generator"] = "tests/golden/make_golden.py via oracle/_ref/libprism_ref.so (reference sources, parity flags)"
     with open(path, "w") as f:
@@ -216,5 +224,86 @@ def gmslr_section(manifest):
     manifest["_gmslr"] = gm
 
 
+def write_mtx_fixtures(d: str):
+    """Small Matrix Market files exercising what ReadMtxTools handles (seeded)."""
+    os.makedirs(d, exist_ok=True)
+    rng = np.random.default_rng(SEED + 7)
+
+    def entries(n, m, k, lower=None):
+        rows = rng.integers(0, n, k)
+        cols = rng.integers(0, m, k)
+        if lower == "incl":
+            rows, cols = np.maximum(rows, cols), np.minimum(rows, cols)
+        elif lower == "strict":
+            keep = rows != cols
+            rows, cols = np.maximum(rows, cols)[keep], np.minimum(rows, cols)[keep]
+        return rows, cols
+
+    files = {}
+    # general, 1-based, explicit zeros (exact and below 10 eps), duplicates, unsorted, comments, blank lines
+    r, c = entries(30, 30, 160)
+    v = rng.standard_normal(len(r))
+    v[::17] = 0.0
+    v[5::23] = 1e-16
+    lines = ["%%MatrixMarket matrix coordinate real general", "% seeded fixture", "%",
+             f"30 30 {len(r) + 3}"]
+    for i, (a, b, x) in enumerate(zip(r, c, v)):
+        lines.append(f"{a + 1} {b + 1} {float(x)!r}")
+        if i == 40:
+            lines.append("")
+            lines.append("% a comment between entries")
+    lines += [f"{r[0] + 1} {c[0] + 1} 2.5", "7 7 -3.25", "30 1 4e-3"]  # a duplicate and extra entries
+    files["general"] = "\n".join(lines) + "\n"
+    # symmetric (lower triangle with diagonal), keyword case mixed as some writers do
+    r, c = entries(25, 25, 90, lower="incl")
+    v = rng.standard_normal(len(r))
+    files["symmetric"] = "\n".join(["%%MatrixMarket Matrix Coordinate Real Symmetric", f"25 25 {len(r)}"] +
+                                    [f"{a + 1} {b + 1} {float(x)!r}" for a, b, x in zip(r, c, v)]) + "\n"
+    # skew-symmetric (strictly lower)
+    r, c = entries(20, 20, 70, lower="strict")
+    v = rng.standard_normal(len(r))
+    files["skew"] = "\n".join(["%%MatrixMarket matrix coordinate real skew-symmetric", f"20 20 {len(r)}"] +
+                               [f"{a + 1} {b + 1} {float(x)!r}" for a, b, x in zip(r, c, v)]) + "\n"
+    # complex general: real and imaginary parts, some zero in one part only
+    r, c = entries(18, 18, 60)
+    re, im = rng.standard_normal(len(r)), rng.standard_normal(len(r))
+    re[::7] = 0.0
+    im[3::5] = 0.0
+    files["complex"] = "\n".join(["%%MatrixMarket matrix coordinate complex general", f"18 18 {len(r)}"] +
+                                  [f"{a + 1} {b + 1} {float(x)!r} {float(y)!r}" for a, b, x, y in zip(r, c, re, im)]) + "\n"
+    # hermitian: taken as stored
+    r, c = entries(16, 16, 40, lower="incl")
+    re, im = rng.standard_normal(len(r)), rng.standard_normal(len(r))
+    files["hermitian"] = "\n".join(["%%MatrixMarket matrix coordinate complex hermitian", f"16 16 {len(r)}"] +
+                                    [f"{a + 1} {b + 1} {float(x)!r} {float(y)!r}" for a, b, x, y in zip(r, c, re, im)]) + "\n"
+    # rectangular general
+    r, c = entries(12, 21, 50)
+    v = rng.standard_normal(len(r))
+    files["rect"] = "\n".join(["%%MatrixMarket matrix coordinate real general", f"12 21 {len(r)}"] +
+                               [f"{a + 1} {b + 1} {float(x)!r}" for a, b, x in zip(r, c, v)]) + "\n"
+    # right-hand sides: 30 x 2 array, column order
+    vals = rng.standard_normal(60)
+    files["rhs"] = "\n".join(["%%MatrixMarket matrix array real general", "% two right-hand sides", "30 2"] +
+                              [repr(float(x)) for x in vals]) + "\n"
+    for name, text in files.items():
+        with open(os.path.join(d, f"{name}.mtx"), "w") as f:
+            f.write(text)
+    return files
+
+
+def mtx_section(manifest):
+    d = os.path.join(HERE, "mtx")
+    write_mtx_fixtures(d)
+    out = {}
+    for name, parts in (("general", (0,)), ("symmetric", (0,)), ("skew", (0,)), ("complex", (0, 1)),
+                        ("hermitian", (0, 1)), ("rect", (0,))):
+        for part in parts:
+            A = ref.RefCSR.from_mtx(os.path.join(d, f"{name}.mtx"), part)
+            rp, ci, v = A.arrays()
+            out[f"{name}.{part}.rowptr"], out[f"{name}.{part}.col"], out[f"{name}.{part}.val"] = rp, ci, v
+    np.savez_compressed(os.path.join(HERE, "mtx_cases.npz"), **out)
+    manifest["_mtx"] = {"files": sorted(os.listdir(d)), "reader": "HOST::ReadMtxTools<double>::loadMatrix"}
+
+
 if __name__ == "__main__":
-    main(sys.argv[1:] or ["basic", "amsed", "gmslr"])
+    main(sys.argv[1:] or ["basic", "amsed", "gmslr", "mtx"])
