@@ -905,7 +905,8 @@ bool stream_layout(const Sweep<Low>& s, const std::vector<uint32_t>& start, uint
                 E = std::max<uint32_t>(E, (uint32_t)ear[j].size());
                 K = std::max<uint32_t>(K, (uint32_t)lat[j].size());
             }
-            const uint32_t Eg = (E + 3) / 4, Kg = (K + 3) / 4;
+            const uint32_t Eg = std::max((E + 3) / 4, stream_early_groups(slot_bytes));
+            const uint32_t Kg = std::max<uint32_t>((K + 3) / 4, 1);
             if (Eg > 255 || Kg > 255) return fail("a row with more than 1020 entries");
             const RoundRec rec = round_rec(nr, Eg, Kg, vb, slot_bytes);
             const uint64_t off = out.blob.size();

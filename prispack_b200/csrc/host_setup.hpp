@@ -143,7 +143,8 @@ void slab_layout(const Sweep<Low>& s, uint32_t num_ctas, uint32_t rows_per_cta, 
 // pattern allows it (a greedy edge colouring, most constrained row first).
 //
 // Each round is one 16-byte aligned record; m = rows rounded up to 8,
-// Eg / Kg = groups of four early / late entries (the round's longest row):
+// Eg / Kg = groups of four early / late entries (the round's longest row, at
+// least stream_early_groups / 1):
 //
 //   fld  [m] x 16 B  4-byte slots: {f32 in, f32 diag, u32 lo, 0};
 //                    8-byte slots: {f64 in, f64 diag}
@@ -195,6 +196,10 @@ PRISM_HD inline RoundRec round_rec(uint32_t nr, uint32_t Eg, uint32_t Kg, uint32
     return r;
 }
 PRISM_HD inline uint32_t zero_slots(uint32_t slot_bytes) { return slot_bytes == 4 ? 32u : 16u; }
+// Early entry groups the kernel holds in registers: every round is padded to at least this
+// many (and to at least one late group), so that the kernel loads a fixed count with
+// straight-line code; rows with more entries continue from the record.
+PRISM_HD constexpr uint32_t stream_early_groups(uint32_t slot_bytes) { return slot_bytes == 4 ? 7u : 5u; }
 struct StreamLayout {
     uint32_t num_ctas = 0, num_rounds = 0, max_round_bytes = 0, max_rounds_per_cta = 0;
     uint32_t slots = 0;                // value slots of the CTA that needs most (zero slots included)

@@ -64,6 +64,7 @@
 
 namespace prism {
 
+
 constexpr int kStrRowWarps = (int)kRoundRows / 32;     // row threads: one per row of a round
 constexpr int kStrPrefetchWarps = 3;                   // warps kStrRowWarps .. kStrProducer - 1
 constexpr int kStrProducer = kStrRowWarps + kStrPrefetchWarps;
@@ -74,6 +75,22 @@ constexpr uint32_t kStrFixedSmem = 64 * 8 + 64 * 4 + 64 * 4 + 32;
 constexpr unsigned long long kStrDrainNs = 2000000000ull;  // bound of the final wait for copies in flight
 static_assert(kStrThreads <= 1024, "warp roles");
 static_assert(kStrFixedSmem % 16 == 0, "round table alignment");
+
+// Dynamic shared memory of one CTA, in bytes from its start: copy barriers, halo flags,
+// ring offsets and words (kStrFixedSmem), the round table (16 B per round), the value
+// slots (rounded up to 128 B), then the ring.  The host sizes the launch with the same
+// function.
+struct StrSmem {
+    uint32_t meta, xs, ring, total;
+};
+PRISM_HD inline StrSmem stream_smem(uint32_t meta_slots, uint32_t slots, uint32_t slot_bytes, uint32_t ring_bytes) {
+    StrSmem m;
+    m.meta = kStrFixedSmem;
+    m.xs = m.meta + 16u * meta_slots;
+    m.ring = m.xs + ((slots * slot_bytes + 127u) & ~127u);
+    m.total = m.ring + ring_bytes;
+    return m;
+}
 
 struct StreamArgs {
     const unsigned char* blob;
@@ -166,6 +183,28 @@ __device__ __forceinline__ void load_coef4(const unsigned char* p, Low (&c)[4]) 
     }
 }
 
+// Value loads of a round's first EG early entry groups (slots: 4 x u16 per group), all
+// issued before any is used.
+template <int EG, int EGR, typename Acc>
+__device__ __forceinline__ void gather_groups(const Acc* xs, const uint32_t (&es)[EGR][2], Acc (&x)[EGR][4]) {
+#pragma unroll
+    for (int g = 0; g < EG; ++g) {
+        x[g][0] = xs[es[g][0] & 0xFFFFu];
+        x[g][1] = xs[es[g][0] >> 16];
+        x[g][2] = xs[es[g][1] & 0xFFFFu];
+        x[g][3] = xs[es[g][1] >> 16];
+    }
+}
+// c_i += coefficient * value over early positions 4g + i of the first EG groups
+template <int EG, int EGR, typename Acc, typename Low>
+__device__ __forceinline__ void fma_groups(const Low (&ec)[EGR][4], const Acc (&x)[EGR][4], Acc (&c)[4]) {
+#pragma unroll
+    for (int g = 0; g < EG; ++g) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) c[i] = acc_fma((Acc)ec[g][i], x[g][i], c[i]);
+    }
+}
+
 // Prep: each row's right-hand side into its record (in the sweep's type), the output
 // marked pending.  Safe for in == out (each row is read, then written, by one thread).
 template <typename Acc>
@@ -189,9 +228,10 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
     uint32_t* hflag = reinterpret_cast<uint32_t*>(sm + 64 * 8);                // [64] round q's halo in: q + 1
     uint32_t* ring_off = hflag + 64;                                           // [64]
     uint32_t* words = ring_off + 64;                                           // landed, rounds done, abort
-    uint4* meta_s = reinterpret_cast<uint4*>(sm + kStrFixedSmem);              // [meta_slots]
-    Acc* xs = reinterpret_cast<Acc*>(meta_s + a.meta_slots);                   // [slots]; zero slots first
-    unsigned char* ring = reinterpret_cast<unsigned char*>(xs) + ((a.slots * (uint32_t)sizeof(Acc) + 127u) & ~127u);
+    const StrSmem lay = stream_smem(a.meta_slots, a.slots, (uint32_t)sizeof(Acc), a.ring_bytes);
+    uint4* meta_s = reinterpret_cast<uint4*>(sm + lay.meta);                   // [meta_slots]
+    Acc* xs = reinterpret_cast<Acc*>(sm + lay.xs);                             // [slots]; zero slots first
+    unsigned char* ring = sm + lay.ring;
     constexpr uint32_t vb = sizeof(Low), ab = sizeof(Acc);
     constexpr uint32_t NZ = ab == 4 ? 32u : 16u;
     const uint32_t b = blockIdx.x;
@@ -364,7 +404,7 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
 
     // ---------------------------------------------------------------------- row threads
     const uint32_t j = threadIdx.x;
-    constexpr int EGR = ab == 4 ? 8 : 4;  // early entry groups held in registers (the rest: from the record)
+    constexpr int EGR = (int)stream_early_groups(ab);  // early entry groups in registers (every round has them)
     // One round as a row thread holds it: fields, the first group of late entries and,
     // once summed, its early part P.
     struct Fld {
@@ -400,52 +440,31 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
             F.dg = f.y;
             F.lo = *reinterpret_cast<const uint32_t*>(base + rec.lo + 4u * j);
         }
-        if (kg_of(m.z) > 0u) {
-            const uint2 s2 = *reinterpret_cast<const uint2*>(base + rec.ls + 8u * j);
-            F.ls0 = s2.x;
-            F.ls1 = s2.y;
-            load_coef4<Low>(base + rec.lc + 4u * vb * j, F.lc);
-        }
+        const uint2 s2 = *reinterpret_cast<const uint2*>(base + rec.ls + 8u * j);  // late group 0
+        F.ls0 = s2.x;
+        F.ls1 = s2.y;
+        load_coef4<Low>(base + rec.lc + 4u * vb * j, F.lc);
     };
+    // the early entries of a round (its first EGR groups) into registers
     auto load_early = [&](const Fld& F) {
-        const uint32_t Eg = eg_of(F.shape);
+        constexpr int EG = EGR;
         if (j >= nr_of(F.shape)) return;
         const RoundRec rec = rec_of(F);
         const unsigned char* base = ring + F.base;
 #pragma unroll
-        for (int g = 0; g < EGR; ++g) {
-            if ((uint32_t)g < Eg) {
-                const uint32_t e = (uint32_t)g * rec.m + j;
-                const uint2 s2 = *reinterpret_cast<const uint2*>(base + rec.es + 8u * e);
-                es[g][0] = s2.x;
-                es[g][1] = s2.y;
-                load_coef4<Low>(base + rec.ec + 4u * vb * e, ec[g]);
-            }
+        for (int g = 0; g < EG; ++g) {
+            const uint32_t e = (uint32_t)g * rec.m + j;
+            const uint2 s2 = *reinterpret_cast<const uint2*>(base + rec.es + 8u * e);
+            es[g][0] = s2.x;
+            es[g][1] = s2.y;
+            load_coef4<Low>(base + rec.ec + 4u * vb * e, ec[g]);
         }
     };
-    // P = (c0 + c1) + (c2 + c3), c_i the fma chain over early positions 4g + i
-    auto early_sum = [&](Fld& F) {
+    // P = (c0 + c1) + (c2 + c3): c holds the register groups' chains; entry groups beyond
+    // the register groups (rows longer than 4 * EGR entries) continue from the record
+    auto close_early = [&](Acc c0, Acc c1, Acc c2, Acc c3, Fld& F) {
         const uint32_t Eg = eg_of(F.shape);
-        if (j >= nr_of(F.shape)) return;
-        Acc x[EGR][4];
-#pragma unroll
-        for (int g = 0; g < EGR; ++g) {
-            if ((uint32_t)g < Eg) {
-                x[g][0] = xs[es[g][0] & 0xFFFFu];
-                x[g][1] = xs[es[g][0] >> 16];
-                x[g][2] = xs[es[g][1] & 0xFFFFu];
-                x[g][3] = xs[es[g][1] >> 16];
-            }
-        }
-        Acc c[4] = {(Acc)0, (Acc)0, (Acc)0, (Acc)0};
-#pragma unroll
-        for (int g = 0; g < EGR; ++g) {
-            if ((uint32_t)g < Eg) {
-#pragma unroll
-                for (int i = 0; i < 4; ++i) c[i] = acc_fma((Acc)ec[g][i], x[g][i], c[i]);
-            }
-        }
-        if (Eg > (uint32_t)EGR) {  // rows longer than the register groups: the rest from the record
+        if (Eg > (uint32_t)EGR) {
             const RoundRec rec = rec_of(F);
             const unsigned char* base = ring + F.base;
             for (uint32_t g = EGR; g < Eg; ++g) {
@@ -453,30 +472,28 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
                 const uint2 s2 = *reinterpret_cast<const uint2*>(base + rec.es + 8u * e);
                 Low cf[4];
                 load_coef4<Low>(base + rec.ec + 4u * vb * e, cf);
-                c[0] = acc_fma((Acc)cf[0], xs[s2.x & 0xFFFFu], c[0]);
-                c[1] = acc_fma((Acc)cf[1], xs[s2.x >> 16], c[1]);
-                c[2] = acc_fma((Acc)cf[2], xs[s2.y & 0xFFFFu], c[2]);
-                c[3] = acc_fma((Acc)cf[3], xs[s2.y >> 16], c[3]);
+                c0 = acc_fma((Acc)cf[0], xs[s2.x & 0xFFFFu], c0);
+                c1 = acc_fma((Acc)cf[1], xs[s2.x >> 16], c1);
+                c2 = acc_fma((Acc)cf[2], xs[s2.y & 0xFFFFu], c2);
+                c3 = acc_fma((Acc)cf[3], xs[s2.y >> 16], c3);
             }
         }
-        F.P = acc_add(acc_add(c[0], c[1]), acc_add(c[2], c[3]));
+        F.P = acc_add(acc_add(c0, c1), acc_add(c2, c3));
     };
-    auto late_load = [&](const Fld& F, Acc (&xl)[4]) {
-        if (j < nr_of(F.shape) && kg_of(F.shape) > 0u) {
-            xl[0] = xs[F.ls0 & 0xFFFFu];
-            xl[1] = xs[F.ls0 >> 16];
-            xl[2] = xs[F.ls1 & 0xFFFFu];
-            xl[3] = xs[F.ls1 >> 16];
-        }
+    // the whole early part of a round at once (prologue, and a round whose halo came late)
+    auto early_sum = [&](Fld& F) {
+        if (j >= nr_of(F.shape)) return;
+        Acc x[EGR][4];
+        Acc c[4] = {(Acc)0, (Acc)0, (Acc)0, (Acc)0};
+        gather_groups<EGR, EGR, Acc>(xs, es, x);
+        fma_groups<EGR, EGR, Acc, Low>(ec, x, c);
+        close_early(c[0], c[1], c[2], c[3], F);
     };
     auto finish = [&](const Fld& F, const Acc (&xl)[4]) {
-        const uint32_t Kg = kg_of(F.shape);
-        if (j >= nr_of(F.shape)) return;
+        const uint32_t Kg = kg_of(F.shape);  // >= 1: every round has a late group (padding where empty)
         Acc s = F.P;
-        if (Kg > 0u) {
 #pragma unroll
-            for (int i = 0; i < 4; ++i) s = acc_fma((Acc)F.lc[i], xl[i], s);
-        }
+        for (int i = 0; i < 4; ++i) s = acc_fma((Acc)F.lc[i], xl[i], s);
         if (Kg > 1u) {  // more than four late entries: the rest from the record
             const RoundRec rec = rec_of(F);
             const unsigned char* base = ring + F.base;
@@ -543,15 +560,29 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
     // registers); once round i is finished, cur receives round i + 2.  Returns true when
     // the row threads leave.
     auto step = [&](uint32_t i, Fld& cur, Fld& nxt) -> bool {
-        Acc xl[4] = {(Acc)0, (Acc)0, (Acc)0, (Acc)0};
-        if (!bad) late_load(cur, xl);
         const bool more = i + 1 < R, more2 = i + 2 < R;
-        bool pend = false;
-        if (more && !bad) {
-            if (!has_halo(nxt) || halo_in(i + 1)) early_sum(nxt);
-            else pend = true;  // its halo is not in yet: sum it after the barrier
+        // round i + 1's early part now unless its halo is not in yet (then after the barrier)
+        const bool pend = more && !bad && has_halo(nxt) && !halo_in(i + 1);
+        const bool live = !bad && j < nr_of(cur.shape);
+        const bool early = more && !bad && !pend && j < nr_of(nxt.shape);
+        {
+            // every value load first: round i's late values, round i + 1's early ones
+            Acc xl[4] = {(Acc)0, (Acc)0, (Acc)0, (Acc)0};
+            if (live) {
+                xl[0] = xs[cur.ls0 & 0xFFFFu];
+                xl[1] = xs[cur.ls0 >> 16];
+                xl[2] = xs[cur.ls1 & 0xFFFFu];
+                xl[3] = xs[cur.ls1 >> 16];
+            }
+            Acc x[EGR][4];
+            if (early) gather_groups<EGR, EGR, Acc>(xs, es, x);
+            if (live) finish(cur, xl);
+            if (early) {
+                Acc c[4] = {(Acc)0, (Acc)0, (Acc)0, (Acc)0};
+                fma_groups<EGR, EGR, Acc, Low>(ec, x, c);
+                close_early(c[0], c[1], c[2], c[3], nxt);
+            }
         }
-        if (!bad) finish(cur, xl);
         if (more2 && !bad) {
             if (!wait_landed(i + 2)) bad = true;
             else {
