@@ -53,7 +53,7 @@ AMSED = dict(levels=3, lanczos_steps=64, low_rank=32, eig_bound=0.8, lowrank_typ
 SEED = 2024
 # DRAM bytes / algorithmic bytes of the streamed sweep kernel's level-0 lower sweep (one ncu capture on the
 # 96^3 case, profiles/k_sweep_stream_fp32apply_level0_lower_96cube.md), applied to each launch's algorithmic bytes
-TRAFFIC_RATIO = {"level-order": 181.2 / 183.6, "stream": 188.0 / 183.6}
+TRAFFIC_RATIO = {"level-order": 181.2 / 183.6, "stream": 229.6 / 183.6}
 TRAFFIC_SOURCE = ("ncu capture of the level-0 lower sweep at 96^3 (183.6 MB algorithmic): DRAM read + write "
                   "bytes / algorithmic bytes, scaled to this launch")
 # the reference library's timing build (oracle/Makefile FAST_FLAGS)
@@ -336,8 +336,15 @@ def bench_convdiff(args, local):
         st = sts[-1]
         res[name] = {"ms": ms, "iters": st.num_iter, "true_rel_residual": st.true_rel_residual,
                      "converged": bool(st.converged), "host_setup_s": round(setup_s, 2), "info": G.info(),
-                     "S": S, "G": G}
+                     "S": S, "G": G, "host_syncs": st.host_syncs, "graph_nodes": st.graph_nodes}
     S32 = res["fp32"]["S"]
+
+    def plain_one():
+        x.zero_()
+        return S32.solve(b, x, solver=PB.SOLVER_FGMRES, tol=args.tol, max_iter=1000, restart=c["restart"],
+                         launch_mode=PB.LAUNCH_STREAM)[1]
+
+    plain_ms, plain_sts = _device_ms(stream, plain_one, max(1, args.steps // 2), 1)
     pin_b = torch.from_numpy(b_host).pin_memory()
     pin_x = torch.zeros(A.n, dtype=torch.float64).pin_memory()
     bnp, xnp = pin_b.numpy(), pin_x.numpy()
@@ -376,6 +383,10 @@ def bench_convdiff(args, local):
                     "d2h_bytes_per_step": 8 * A.n},
             "fp64_factor": {"ms": round(r64["ms"], 3), "iters": r64["iters"],
                             "true_rel_residual": r64["true_rel_residual"], "mixed_speedup": r64["ms"] / r32["ms"]},
+            "launches": {"cycle_graph": {"ms": round(r32["ms"], 3), "host_syncs": r32["host_syncs"],
+                                         "graph_nodes_per_arnoldi_step": r32["graph_nodes"]},
+                         "plain": {"ms": round(plain_ms, 3), "host_syncs": plain_sts[-1].host_syncs,
+                                   "iters": plain_sts[-1].num_iter}},
             "forward_error_vs_reference": fwd or None, "cpu_baseline": cpu}
 
 

@@ -89,6 +89,13 @@ typedef enum prism_solver_kind {
     PRISM_SOLVER_GMRES = 3        /* GMRES with NormalGMRES (no preconditioner applied, GMRES.cpp:164) */
 } prism_solver_kind;
 
+typedef enum prism_launch_mode {
+    PRISM_LAUNCH_AUTO = 0,        /* GMRES: each restart cycle runs as one CUDA graph whose loop over the
+                                     Arnoldi steps ends on the device (one host read per cycle), with
+                                     plain launches where the runtime cannot build that graph */
+    PRISM_LAUNCH_STREAM = 1       /* plain launches, one host read per Arnoldi step */
+} prism_launch_mode;
+
 typedef struct prism_solve_opts {
     int32_t solver;               /* prism_solver_kind */
     double tol;                   /* relative residual tolerance (CG.cpp:59, GMRES.cpp:194) */
@@ -98,6 +105,8 @@ typedef struct prism_solve_opts {
                                      host pointer for the host-buffer calls; NULL: none): the solve then
                                      reports its forward error against it.  Ignored by the adjoint, block
                                      and batch solves.  No reference counterpart. */
+    int32_t launch_mode;          /* prism_launch_mode (GMRES solvers; CG ignores it).  No reference
+                                     counterpart. */
 } prism_solve_opts;
 
 typedef struct prism_solve_stats {
@@ -110,6 +119,12 @@ typedef struct prism_solve_stats {
     double device_ms;             /* device time of the solve (CUDA events on the handle's stream) */
     double forward_error;         /* ||x - x_ref||_2 / ||x_ref||_2 in FP64 when opts.x_ref is given, else -1
                                      (measured after the solve, outside device_ms) */
+    uint32_t host_syncs;          /* times the host waited for the device between the solve's first
+                                     and last device operation (CG: once per iteration; GMRES: once
+                                     per restart cycle with the cycle graph, once per Arnoldi step
+                                     with plain launches; block and batch solves: 0, not counted) */
+    uint32_t graph_nodes;         /* GMRES: nodes of the captured Arnoldi step replayed by the cycle
+                                     graph (0: plain launches) */
 } prism_solve_stats;
 
 typedef struct prism_handle_s* prism_handle;

@@ -26,6 +26,7 @@ class DeviceSolver : public BaseSolver<T> {
         opts_.max_iter = maxIter;
         opts_.restart = restart;
         opts_.x_ref = nullptr;
+        opts_.launch_mode = PRISM_LAUNCH_AUTO;
     }
 
     void solve(const HOST::CSRMatrix<T>& matA, const HostVector<T>& b, HostVector<T>& x) override {

@@ -23,6 +23,7 @@ PRISM_FP64, PRISM_FP32 = 0, 1
 PRISM_FP32_APPLY = 2
 PRECOND_NONE, PRECOND_IC, PRECOND_ILUT, PRECOND_ILDLT, PRECOND_GMSLR, PRECOND_AMSED = range(6)
 SOLVER_FCG, SOLVER_CG, SOLVER_FGMRES, SOLVER_GMRES = range(4)
+LAUNCH_AUTO, LAUNCH_STREAM = range(2)
 # reference spellings (include/Solver/CG.h:14-18, include/Solver/GMRES.h:15-18)
 NormalCG, FlexibleCG = "NormalCG", "FlexibleCG"
 NormalGMRES, FlexibleGMRES = "NormalGMRES", "FlexibleGMRES"
@@ -40,7 +41,7 @@ class PrismError(RuntimeError):
 
 class SolveOpts(C.Structure):
     _fields_ = [("solver", C.c_int32), ("tol", C.c_double), ("max_iter", C.c_uint32), ("restart", C.c_uint32),
-                ("x_ref", C.c_void_p)]
+                ("x_ref", C.c_void_p), ("launch_mode", C.c_int32)]
 
 
 class AmsedOpts(C.Structure):
@@ -59,7 +60,8 @@ MatrixReorderNo, MatrixReorderAMD, MatrixReorderRCM = 0, 1, 2
 class SolveStats(C.Structure):
     _fields_ = [("num_iter", C.c_int32), ("converged", C.c_int32), ("final_error", C.c_double),
                 ("true_rel_residual", C.c_double), ("precond_applies", C.c_uint32),
-                ("spmv_count", C.c_uint32), ("device_ms", C.c_double), ("forward_error", C.c_double)]
+                ("spmv_count", C.c_uint32), ("device_ms", C.c_double), ("forward_error", C.c_double),
+                ("host_syncs", C.c_uint32), ("graph_nodes", C.c_uint32)]
 
 
 _lib = None
@@ -778,11 +780,14 @@ class DeviceSystem:
         _check(self.lib.prism_solve_segments(self.h, C.byref(opts), nseg, sp, bh, xh, st))
         return xh, list(st)
 
-    def solve(self, b, x=None, *, solver=SOLVER_FCG, tol=1e-8, max_iter=1000, restart=0, x_ref=None) -> tuple:
+    def solve(self, b, x=None, *, solver=SOLVER_FCG, tol=1e-8, max_iter=1000, restart=0, x_ref=None,
+              launch_mode=LAUNCH_AUTO) -> tuple:
         """x (in/out initial guess) solved in place; returns (x, SolveStats).  x_ref (same kind
         as b: a CUDA tensor or a host array): a reference solution whose forward error the
-        stats then report (stats.forward_error, else -1)."""
-        opts = SolveOpts(solver, tol, max_iter, restart, None)
+        stats then report (stats.forward_error, else -1).  launch_mode (GMRES solvers):
+        LAUNCH_AUTO runs each restart cycle as one CUDA graph, LAUNCH_STREAM as plain
+        launches with a host read after every Arnoldi step."""
+        opts = SolveOpts(solver, tol, max_iter, restart, None, launch_mode)
         st = SolveStats()
         if hasattr(b, "is_cuda"):
             import torch

@@ -642,6 +642,8 @@ void batched_fcg_solve(Handle& h, const prism_solve_opts& o, uint32_t k, const d
             st[c].spmv_count = spmvs;
             st[c].device_ms = ms;
             st[c].forward_error = -1.0;  // no reference solution for block / batch solves
+            st[c].host_syncs = 0;  // not counted for block / batch solves
+            st[c].graph_nodes = 0;
         }
     }
 }

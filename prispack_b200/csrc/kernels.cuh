@@ -448,26 +448,6 @@ static __global__ void __launch_bounds__(kBlock) k_scale(uint32_t n, const doubl
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[i] = src[i] * alpha;
 }
 
-// Modified Gram-Schmidt link i of Arnoldi step j (GMRES.cpp:174-180):
-//   w -= h_prev * v_prev   (h_prev from device memory; skipped when v_prev is null)
-//   out = { Σ w_i * v_next_i }  (or Σ w_i^2 when v_next is null: the new norm)
-static __global__ void __launch_bounds__(kBlock) k_mgs(uint32_t n, double* __restrict__ w,
-                                                       const double* __restrict__ v_prev,
-                                                       const double* __restrict__ h_prev,
-                                                       const double* __restrict__ v_next, ReduceSlot slot) {
-    const double h = v_prev ? *h_prev : 0.0;
-    double acc[1] = {0.0};
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        double wi = w[i];
-        if (v_prev) {
-            wi = wi + -1.0 * (h * v_prev[i]);
-            w[i] = wi;
-        }
-        acc[0] += v_next ? wi * v_next[i] : wi * wi;
-    }
-    grid_reduce<1>(acc, slot);
-}
-
 // x += B * ksi over ncols columns of a column-major n x ncols block, summed
 // column by column per element (DenseMatrix::MatVec, DenseMatrix.cpp:208-243).
 static __global__ void __launch_bounds__(kBlock) k_gemv_add(uint32_t n, const double* __restrict__ B, uint32_t ncols,

@@ -264,6 +264,8 @@ void segmented_fcg_solve(Handle& h, const prism_solve_opts& o, uint32_t nseg, co
             st[q].spmv_count = spmvs;
             st[q].device_ms = ms;
             st[q].forward_error = -1.0;  // no reference solution for block / batch solves
+            st[q].host_syncs = 0;  // not counted for block / batch solves
+            st[q].graph_nodes = 0;
         }
     }
 }

@@ -544,6 +544,11 @@ void tune_sweep(Handle& h, DevSweep& d, const Sweep<Low>& s, bool acc32) {
 template void tune_sweep<double>(Handle&, DevSweep&, const Sweep<double>&, bool);
 template void tune_sweep<float>(Handle&, DevSweep&, const Sweep<float>&, bool);
 
+namespace {
+std::atomic<uint64_t> g_precond_uid{0};
+}
+Precond::Precond() : uid(++g_precond_uid) {}
+
 TriangularPrecond::TriangularPrecond(Handle& h, std::shared_ptr<const HostFactor> f) : h_(h), f_(std::move(f)) {
     if (f_->fp32) {
         tune_sweep(h_, lower_, f_->lower32, f_->apply32);
@@ -552,6 +557,7 @@ TriangularPrecond::TriangularPrecond(Handle& h, std::shared_ptr<const HostFactor
         tune_sweep(h_, lower_, f_->lower64);
         tune_sweep(h_, upper_, f_->upper64);
     }
+    tmp_.alloc(h_.A.n);  // here rather than at the first apply, which may be under graph capture
 }
 
 void TriangularPrecond::apply(cudaStream_t st, const double* in, double* out) {
@@ -629,7 +635,7 @@ void fcg_solve(Handle& h, const prism_solve_opts& o, const double* b, double* x,
     double* y = h.y.get();
     double* sc = h.red.scalars.get();
     const int vg = vec_grid(h, n);
-    uint32_t applies = 0, spmvs = 0;
+    uint32_t applies = 0, spmvs = 0, syncs = 0;
 
     PRISM_CUDA(cudaEventRecord(h.ev0, s));
     // r = b - A x ; Σ b²
@@ -650,6 +656,7 @@ void fcg_solve(Handle& h, const prism_solve_opts& o, const double* b, double* x,
 
     PRISM_CUDA(cudaMemcpyAsync(h.pinned, sc, kNumScalars * sizeof(double), cudaMemcpyDeviceToHost, s));
     h.check_status();
+    ++syncs;
     const double norm_b = std::sqrt(h.pinned[SC_BB]);
     uint32_t m = o.max_iter;
     double norm = -1.0;
@@ -658,6 +665,7 @@ void fcg_solve(Handle& h, const prism_solve_opts& o, const double* b, double* x,
         if (i > 1) {
             PRISM_CUDA(cudaMemcpyAsync(h.pinned + SC_RR, sc + SC_RR, sizeof(double), cudaMemcpyDeviceToHost, s));
             h.check_status();
+            ++syncs;
         }
         norm = std::sqrt(h.pinned[SC_RR]) / norm_b;
         if (!std::isfinite(norm)) throw Error(PRISM_ERR_NONFINITE, "non-finite residual norm in CG iteration " + std::to_string(i));
@@ -687,6 +695,7 @@ void fcg_solve(Handle& h, const prism_solve_opts& o, const double* b, double* x,
     PRISM_CUDA(cudaEventRecord(h.ev1, s));
     PRISM_CUDA(cudaMemcpyAsync(h.pinned, sc, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
     h.check_status();
+    ++syncs;
     float ms = 0.f;
     PRISM_CUDA(cudaEventElapsedTime(&ms, h.ev0, h.ev1));
     if (st) {
@@ -697,6 +706,8 @@ void fcg_solve(Handle& h, const prism_solve_opts& o, const double* b, double* x,
         st->precond_applies = applies;
         st->spmv_count = spmvs;
         st->device_ms = ms;
+        st->host_syncs = syncs;
+        st->graph_nodes = 0;
     }
 }
 

@@ -45,7 +45,6 @@ enum Scalar : int {
     SC_DV = 4, SC_DR = 5,    // written together by k_spmv<.,.,2>: Σ v·d, Σ d·r
     SC_TMP = 6, SC_TMP2 = 7,
     SC_DR2 = 8,
-    SC_H0 = 16,              // GMRES Hessenberg column h_0 .. h_{j+1}
     kNumScalars = 16
 };
 
@@ -95,7 +94,11 @@ struct DevSweep {
 
 class Precond {
   public:
+    Precond();
     virtual ~Precond() = default;
+    // distinct for every preconditioner object of the process (never reused), so that work
+    // captured from one (a GMRES cycle graph) is never replayed against another
+    const uint64_t uid;
     virtual int kind() const = 0;
     virtual uint64_t mnnz() const = 0;
     // out = M^{-1} in; in != out not required.
@@ -211,6 +214,8 @@ struct BatchWork;                  // block-of-RHS workspace (batched.cu)
 void batch_release(BatchWork* w);
 struct SegWork;                    // batch-of-systems workspace (segments.cu)
 void seg_release(SegWork* w);
+struct GmresWork;                  // device GMRES scalars and scratch (gmres.cu)
+void gmres_release(GmresWork* w);
 
 struct Handle {
     DeviceInfo info;
@@ -223,13 +228,14 @@ struct Handle {
     DevBuf<int> status;            // device status word of the bounded waits
     DevBuf<double> r, w, d, v, y;  // Krylov workspace (n each)
     DevBuf<double> xb, bb, xr;     // host-pointer API staging (xr: reference solution)
-    DevBuf<double> V, Z, ksi;      // GMRES bases (n x (m+1), column-major) and LS coefficients
+    DevBuf<double> V, Z;           // GMRES bases (n x (m+1), column-major)
     double* pinned = nullptr;      // host mirror of scalars (pinned), kScalarCapacity entries
     static constexpr uint32_t kMaxKrylov = 1024;  // restart length limit
     static constexpr uint32_t kScalarCapacity = kNumScalars + kMaxKrylov + 2;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::unique_ptr<BatchWork, void (*)(BatchWork*)> batch{nullptr, batch_release};
     std::unique_ptr<SegWork, void (*)(SegWork*)> seg{nullptr, seg_release};
+    std::unique_ptr<GmresWork, void (*)(GmresWork*)> gmres{nullptr, gmres_release};
     int symmetric = -1;            // A == A^T exactly: -1 not yet checked, 0 no, 1 yes
 
     ~Handle();
