@@ -454,7 +454,10 @@ def bench_adjoint(args, local):
 def bench_batched(args, local):
     """Batched solves, FCG + ICT(1e-3) with FP32 factor values, tol 1e-10:
     (a) 2D Poisson 512^2 with a block of 64 random-normal right-hand sides,
-    one block solve (prism_solve_batched) against 64 solves one after another;
+    one block solve (prism_solve_batched) against 64 solves one after another,
+    and the same block with AMSED / MSLR (FP32 factor values; block sweeps per
+    level; the low-rank block products on the tensor cores in BF16 with FP32
+    accumulation);
     (b) 256 independent 2D Poisson systems on grids with sides drawn uniformly
     from 32..256, assembled on the diagonal of one CSR and solved together
     (prism_solve_segments).  The reference solves one right-hand side and one
@@ -487,6 +490,20 @@ def bench_batched(args, local):
         return S.solve(B[0], x0, tol=tol, max_iter=1000)[1]
 
     single_ms, _ = _device_ms(stream, single, max(1, args.steps), 1)
+    # ---- (a') the same block with AMSED / MSLR, FP32 factor values: block sweeps per level and
+    # the low-rank block products on the tensor cores (BF16 operands, FP32 accumulation)
+    t0 = time.perf_counter()
+    HA = PB.HostAmsed(A, precision=PB.PRISM_FP32, **AMSED)
+    amsed_setup_s = time.perf_counter() - t0
+    SA = PB.DeviceSystem(A, device=local)
+    SA.set_stream(stream.cuda_stream)
+    SA.attach(HA)
+
+    def block_amsed():
+        return SA.solve_batched(B, tol=tol, max_iter=1000)[1]
+
+    am_ms, amst = _device_ms(stream, block_amsed, max(1, args.steps // 2), 1)
+    amst = amst[-1]
     # ---- (b) 256 uneven systems
     sides = rng.integers(32, 257, size=256)
     blocks = [PB.CSRMatrix.laplacian(int(q), int(q), 1) for q in sides]
@@ -507,6 +524,7 @@ def bench_batched(args, local):
     seg_ms, segst = _device_ms(stream, segs, max(1, args.steps // 2), 1)
     segst = segst[-1]
     cpu = None
+    cpu_amsed = None
     ref = _ref_ready(args)
     if ref is not None:
         RA = ref.RefCSR.laplacian(512, 512, 1, fast=True)
@@ -517,6 +535,18 @@ def bench_batched(args, local):
         for c in range(kk):
             ref.cg_solve(RA, RP, B_host[c], tol=tol, maxit=1000, flexible=True)
         rhs_s = time.perf_counter() - t
+        a = AMSED
+        RM = ref.RefAmsed(RA, a["levels"], a["lanczos_steps"], a["low_rank"], a["eig_bound"], a["reorder"],
+                          a["lowrank_type"], a["lanczos_type"], True)
+        RM.setup()
+        t = time.perf_counter()
+        for c in range(kk):
+            ref.cg_solve(RA, RM, B_host[c], tol=tol, maxit=1000, flexible=True)
+        am_rhs_s = time.perf_counter() - t
+        cpu_amsed = {"value": round(am_rhs_s * k / kk * 1e3, 1), "unit": "ms", "cores": 4, "kind": "reference",
+                     "sample": f"reference FCG + AMSEDPrecondition<float,double> solves timed one by one: {kk} of "
+                               f"the 64 right-hand sides ({am_rhs_s:.2f} s; the total counts {k}/{kk} times that); "
+                               f"setup excluded; {REF_BUILD}"}
         sys_s = 0.0
         for q, Bq in enumerate(blocks):
             Rq = ref.RefCSR.from_arrays(Bq.rowptr, Bq.col, Bq.val, fast=True)
@@ -539,6 +569,14 @@ def bench_batched(args, local):
             "block_of_64": {"ms": round(block_ms, 3), "iters_first4": [q.num_iter for q in bst][:4],
                             "all_converged": all(q.converged for q in bst), "one_rhs_alone_ms": round(single_ms, 3),
                             "speedup_vs_64_single": round(64 * single_ms / block_ms, 2)},
+            "block_of_64_amsed": {"ms": round(am_ms, 3), "iters_first4": [q.num_iter for q in amst][:4],
+                                  "all_converged": all(q.converged for q in amst),
+                                  "max_true_rel_residual": max(q.true_rel_residual for q in amst),
+                                  "precond": "AMSED/MSLR (3 levels, natural local order), FP32 factor values, block "
+                                             "sweeps per level, low-rank W (H o (W^T X)) on the tensor cores "
+                                             "(mma.sync m16n8k16, BF16 operands, FP32 accumulation)",
+                                  "ranks": HA.info()["ranks"].tolist(), "host_setup_s": round(amsed_setup_s, 2),
+                                  "cpu_baseline": cpu_amsed},
             "uneven_256": {"ms": round(seg_ms, 3), "iters_min_max": [min(its), max(its)],
                            "all_converged": all(q.converged for q in segst),
                            "max_true_rel_residual": max(q.true_rel_residual for q in segst),

@@ -157,6 +157,19 @@ int32_t prism_selftest_stream_layout(uint32_t n, const uint32_t* rowptr, const u
                                      const double* diag, int32_t op, int32_t lower, int32_t precision,
                                      uint32_t num_ctas, uint32_t rows_per_cta, const double* in, double* out);
 
+/* The low-rank correction of an AMSED / MSLR level on a block of k <= 64
+ * right-hand sides, alone on `device` with host arrays: Y += W (H o (W^T X)),
+ * W column-major nrem x rank (rank <= 128), H of length rank, X and Y
+ * interleaved (X[i * k + c]).  tensor != 0: W, X and the intermediate
+ * T = H o (W^T X) rounded to BF16 (through float, round to nearest even),
+ * both products on the tensor cores with FP32 accumulation, Y updated in FP64
+ * (the block apply's path with FP32 factor values); tensor == 0: FP64
+ * throughout (the path with FP64 factor values).  Reference:
+ * AMSEDPrecondition.cpp:1557-1574 (DenseMatrix::transposeVec / MatVec,
+ * DenseMatrix.cpp:208-267), one column at a time. */
+int32_t prism_lowrank_block_run(int32_t device, uint32_t nrem, uint32_t rank, uint32_t k, const double* W,
+                                const double* H, const double* X, double* Y, int32_t tensor);
+
 /* The summation order of the streamed sweep kernel, for checking its
  * arithmetic against the oracle.  For a gather-form triangular sweep given as
  * for prism_selftest_stream_layout (row r lists its dependencies on one side

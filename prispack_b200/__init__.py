@@ -75,6 +75,8 @@ _SIGS = {
     "prism_version": (C.c_int32, []),
     "prism_kernel_launch_count": (C.c_uint64, []),
     "prism_selftest_wait_timeout": (C.c_int32, [C.c_int32, C.c_uint64, C.POINTER(C.c_int32)]),
+    "prism_lowrank_block_run": (C.c_int32, [C.c_int32, C.c_uint32, C.c_uint32, C.c_uint32, _f64p, _f64p, _f64p, _f64p,
+                                            C.c_int32]),
     "prism_selftest_stream_layout": (C.c_int32, [C.c_uint32, _u32p, _u32p, _f64p, _vp, C.c_int32, C.c_int32,
                                                  C.c_int32, C.c_uint32, C.c_uint32, _f64p, _f64p]),
     "prism_stream_sweep_order": (C.c_int32, [C.c_uint32, _u32p, _u32p, _f64p, _vp, C.c_int32, C.c_int32, C.c_int32,
@@ -187,6 +189,18 @@ def selftest_wait_timeout(device: int = 0, wait_ns: int = 50_000_000) -> int:
     st = C.c_int32(-1)
     _check(load().prism_selftest_wait_timeout(device, wait_ns, C.byref(st)))
     return st.value
+
+
+def lowrank_block_run(W, H, X, Y, *, tensor: bool, device: int = 0):
+    """Y + W (H o (W^T X)) for W (nrem, rank), H (rank,), X and Y (nrem, k), k <= 64, on
+    `device` (prism_lowrank_block_run): BF16 tensor cores when tensor, else FP64."""
+    W = np.asarray(W, np.float64)
+    nrem, rank = W.shape
+    X = np.ascontiguousarray(X, np.float64)
+    out = np.array(Y, np.float64, copy=True, order="C")
+    _check(load().prism_lowrank_block_run(device, nrem, rank, X.shape[1], np.ascontiguousarray(W.T),
+                                          np.ascontiguousarray(H, np.float64), X, out, int(bool(tensor))))
+    return out
 
 
 def selftest_stream_layout(rowptr, col, val, in_, *, diag=None, op: int = 2, lower: bool = True,

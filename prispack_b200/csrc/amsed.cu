@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <cstring>
 
+#include "amsed_block.cuh"
 #include "amsed_setup.hpp"
 #include "kernels.cuh"
 #include "solve.cuh"
@@ -223,6 +224,247 @@ void AmsedPrecond::apply(cudaStream_t st, const double* in, double* out) {
     else c_solve(st, -1, X_.get());
     k_permute<<<vg, kBlock, 0, st>>>(n_, pperm_.get(), X_.get(), out, 1);
     PRISM_LAUNCHED();
+}
+
+// ============================================================================
+// Block apply: k <= 64 interleaved columns (X[row * k + c])
+// ============================================================================
+void launch_bt_fill(cudaStream_t st, const Handle& h, uint64_t count, double* p);
+void launch_bt_sweep(const Handle& h, cudaStream_t st, const DevSweep& s, uint32_t k, const double* in, double* out);
+
+namespace {
+// float -> BF16, round to nearest even (NaN kept quiet)
+uint16_t bf16_bits(float f) {
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    if ((u & 0x7F800000u) == 0x7F800000u && (u & 0x007FFFFFu)) return (uint16_t)((u >> 16) | 0x40u);
+    u += 0x7FFFu + ((u >> 16) & 1u);
+    return (uint16_t)(u >> 16);
+}
+
+int bk_grid(const Handle& h, uint64_t items, uint32_t per_block) {
+    uint64_t want = (items + per_block - 1) / per_block;
+    const uint64_t cap = (uint64_t)h.info.sms * 4;
+    if (want < 1) want = 1;
+    return (int)(want < cap ? want : cap);
+}
+}  // namespace
+
+void AmsedPrecond::prepare_block(uint32_t k) {
+    if (bk_ >= k && !blv_.empty()) return;
+    cudaStream_t st = h_.stream;
+    tensor_lowrank_ = a_->fp32;
+    const bool first = blv_.empty();
+    if (first) blv_.resize(nlev_);
+    size_t part64 = 1, part32 = 1, t64 = 1, t32 = 1;
+    uint32_t max_nfac = 1;
+    for (uint32_t l = 0; l < nlev_; ++l) {
+        Level& L = lv_[l];
+        BlockLevel& B = blv_[l];
+        if (first) {
+            // level-order copies of the sweeps (the block sweep kernel's layout)
+            if (a_->fp32) {
+                Sweep<float> lo, up;
+                level_sweeps<float>(*a_->s32, l, lo, up);
+                B.lower.upload(lo, h_.info, LAYOUT_LEVEL, st);
+                B.upper.upload(up, h_.info, LAYOUT_LEVEL, st);
+            } else {
+                Sweep<double> lo, up;
+                level_sweeps<double>(*a_->s64, l, lo, up);
+                B.lower.upload(lo, h_.info, LAYOUT_LEVEL, st);
+                B.upper.upload(up, h_.info, LAYOUT_LEVEL, st);
+            }
+            if (L.rank && tensor_lowrank_) {
+                const std::vector<double>& W = a_->fp32 ? a_->s32->levels[l].W : a_->s64->levels[l].W;
+                const std::vector<double>& Hh = a_->fp32 ? a_->s32->levels[l].H : a_->s64->levels[l].H;
+                B.rpad = (L.rank + 15) / 16 * 16;
+                B.ldw = (L.nrem + 15) / 16 * 16;
+                std::vector<uint16_t> wc((size_t)B.rpad * B.ldw, 0), wr((size_t)B.ldw * B.rpad, 0);
+                for (uint32_t q = 0; q < L.rank; ++q)
+                    for (uint32_t i = 0; i < L.nrem; ++i) {
+                        const uint16_t v = bf16_bits((float)W[(size_t)q * L.nrem + i]);
+                        wc[(size_t)q * B.ldw + i] = v;
+                        wr[(size_t)i * B.rpad + q] = v;
+                    }
+                std::vector<float> h32(B.rpad, 0.f);
+                for (uint32_t q = 0; q < L.rank; ++q) h32[q] = (float)Hh[q];
+                B.Wc.upload(wc.data(), wc.size(), st);
+                B.Wr.upload(wr.data(), wr.size(), st);
+                B.H32.upload(h32.data(), h32.size(), st);
+            }
+        }
+        max_nfac = std::max(max_nfac, L.nfac);
+        if (l + 1 < nlev_) {
+            B.xc.alloc(std::max<size_t>((size_t)L.nrem * k, 1));
+            B.tmp.alloc(std::max<size_t>((size_t)L.nb * k, 1));
+            B.tmp2.alloc(std::max<size_t>((size_t)L.nb * k, 1));
+            if (L.rank) {
+                part64 = std::max(part64, (size_t)bk_grid(h_, L.nrem, 64) * L.rank * kLrMaxK);
+                t64 = std::max(t64, (size_t)L.rank * kLrMaxK);
+                if (tensor_lowrank_) {
+                    part32 = std::max(part32, (size_t)bk_grid(h_, B.ldw / 16, kBlock / 32) * B.rpad * kLrMaxK);
+                    t32 = std::max(t32, (size_t)B.rpad * kLrMaxK);
+                }
+            }
+        }
+    }
+    Xk_.alloc((size_t)n_ * k);
+    sweep_tmpk_.alloc((size_t)max_nfac * k);
+    lr_part64_.alloc(part64);
+    lr_t64_.alloc(t64);
+    lr_part32_.alloc(part32);
+    lr_t32_.alloc(t32);
+    if (lr_ticket_.size() == 0) {
+        lr_ticket_.alloc(1);
+        PRISM_CUDA(cudaMemsetAsync(lr_ticket_.get(), 0, sizeof(unsigned), st));
+    }
+    bk_ = k;
+    PRISM_CUDA(cudaStreamSynchronize(st));
+}
+
+// out = B_level^{-1} in over the level's rows, k columns (in == out allowed)
+void AmsedPrecond::block_solve_k(cudaStream_t st, int level, uint32_t k, const double* in, double* out) {
+    Level& L = lv_[level];
+    BlockLevel& B = blv_[level];
+    if (L.nfac < L.nb && in != out)
+        PRISM_CUDA(cudaMemcpyAsync(out + (size_t)L.nfac * k, in + (size_t)L.nfac * k,
+                                   (size_t)(L.nb - L.nfac) * k * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    const uint64_t cnt = (uint64_t)L.nfac * k;
+    launch_bt_fill(st, h_, cnt, sweep_tmpk_.get());
+    if (in != out) launch_bt_fill(st, h_, cnt, out);
+    launch_bt_sweep(h_, st, B.lower, k, in, sweep_tmpk_.get());
+    if (in == out) launch_bt_fill(st, h_, cnt, out);
+    launch_bt_sweep(h_, st, B.upper, k, sweep_tmpk_.get(), out);
+}
+
+// x2 += W (H o (W^T xc)) on k columns
+void AmsedPrecond::lowrank_k(cudaStream_t st, int level, uint32_t k, const double* xc, double* y) {
+    Level& L = lv_[level];
+    BlockLevel& B = blv_[level];
+    if (tensor_lowrank_) {
+        const int g = bk_grid(h_, B.ldw / 16, kBlock / 32);
+        k_lr_dots_tc<<<g, kBlock, 0, st>>>(L.nrem, B.ldw, k, B.rpad, reinterpret_cast<const __nv_bfloat16*>(B.Wc.get()),
+                                           B.H32.get(), xc, lr_part32_.get(), lr_ticket_.get(), lr_t32_.get());
+        PRISM_LAUNCHED();
+        const size_t smem = (size_t)(B.rpad / 2) * kLrMaxK * sizeof(uint32_t);
+        k_lr_add_tc<<<g, kBlock, smem, st>>>(L.nrem, B.ldw, k, B.rpad, reinterpret_cast<const __nv_bfloat16*>(B.Wr.get()),
+                                             lr_t32_.get(), y);
+        PRISM_LAUNCHED();
+    } else {
+        const int g = bk_grid(h_, L.nrem, 64);
+        k_lr_dots_f64<<<g, kBlock, 0, st>>>(L.nrem, k, L.rank, L.W.get(), L.H.get(), xc, lr_part64_.get(),
+                                            lr_ticket_.get(), lr_t64_.get());
+        PRISM_LAUNCHED();
+        k_lr_add_f64<<<bk_grid(h_, (uint64_t)L.nrem * k, kBlock), kBlock, 0, st>>>(L.nrem, k, L.rank, L.W.get(),
+                                                                                   lr_t64_.get(), y);
+        PRISM_LAUNCHED();
+    }
+}
+
+// levelCInvRecursiveSolve(level, x) on k columns; x is the C block of `level`
+void AmsedPrecond::c_solve_k(cudaStream_t st, int level, uint32_t k, double* x) {
+    const int next = level + 1;
+    if (level == (int)nlev_ - 2) {
+        block_solve_k(st, next, k, x, x);
+        return;
+    }
+    Level& L = lv_[next];
+    BlockLevel& B = blv_[next];
+    double* x2 = x + (size_t)L.nb * k;
+    // x1 = B^{-1} x1
+    block_solve_k(st, next, k, x, x);
+    // x2 -= E^T x1
+    k_bk_csr<1><<<bk_grid(h_, L.nrem, kBlock / 32), kBlock, 0, st>>>(L.nrem, k, L.Et.rowptr.get(), L.Et.col.get(),
+                                                                      L.Et.val.get(), x, x2);
+    PRISM_LAUNCHED();
+    // xc = x2 ; x2 = C^{-1} x2
+    PRISM_CUDA(cudaMemcpyAsync(B.xc.get(), x2, (size_t)L.nrem * k * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    c_solve_k(st, next, k, x2);
+    // x2 += W (H o (W^T xc))
+    if (L.rank) lowrank_k(st, next, k, B.xc.get(), x2);
+    // x1 -= B^{-1} (E x2)
+    k_bk_csr<0><<<bk_grid(h_, L.nb, kBlock / 32), kBlock, 0, st>>>(L.nb, k, L.E.rowptr.get(), L.E.col.get(),
+                                                                    L.E.val.get(), x2, B.tmp.get());
+    PRISM_LAUNCHED();
+    block_solve_k(st, next, k, B.tmp.get(), B.tmp2.get());
+    k_bk_sub<<<bk_grid(h_, (uint64_t)L.nb * k, kBlock), kBlock, 0, st>>>((uint64_t)L.nb * k, B.tmp2.get(), x);
+    PRISM_LAUNCHED();
+}
+
+void AmsedPrecond::apply_batched(cudaStream_t st, uint32_t k, const double* in, double* out) {
+    if (k == 0 || k > (uint32_t)kLrMaxK) throw Error(PRISM_ERR_ARG, "a block holds 1 to 64 columns");
+    prepare_block(k);
+    const int g = bk_grid(h_, (uint64_t)n_ * k, kBlock);
+    k_bk_permute<<<g, kBlock, 0, st>>>(n_, k, pperm_.get(), in, Xk_.get(), 0);
+    PRISM_LAUNCHED();
+    if (nlev_ == 1) block_solve_k(st, 0, k, Xk_.get(), Xk_.get());
+    else c_solve_k(st, -1, k, Xk_.get());
+    k_bk_permute<<<g, kBlock, 0, st>>>(n_, k, pperm_.get(), Xk_.get(), out, 1);
+    PRISM_LAUNCHED();
+}
+
+// The block low-rank correction alone on `device` (host arrays): Y += W (H o (W^T X)).
+void lowrank_block_run(int device, uint32_t nrem, uint32_t rank, uint32_t k, const double* W, const double* H,
+                       const double* X, double* Y, bool tensor) {
+    DeviceInfo info;
+    init_device_info(info, device);
+    cudaStream_t st;
+    PRISM_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    struct StreamGuard {
+        cudaStream_t s;
+        ~StreamGuard() { cudaStreamDestroy(s); }
+    } guard{st};
+    const size_t nk = (size_t)nrem * k;
+    DevBuf<double> dX, dY;
+    dX.upload(X, nk, st);
+    dY.upload(Y, nk, st);
+    DevBuf<unsigned> ticket(1);
+    PRISM_CUDA(cudaMemsetAsync(ticket.get(), 0, sizeof(unsigned), st));
+    auto grid = [&](uint64_t items, uint32_t per) {
+        uint64_t want = (items + per - 1) / per;
+        const uint64_t cap = (uint64_t)info.sms * 4;
+        return (int)std::max<uint64_t>(1, std::min(want, cap));
+    };
+    if (tensor) {
+        const uint32_t rpad = (rank + 15) / 16 * 16, ldw = (nrem + 15) / 16 * 16;
+        std::vector<uint16_t> wc((size_t)rpad * ldw, 0), wr((size_t)ldw * rpad, 0);
+        for (uint32_t q = 0; q < rank; ++q)
+            for (uint32_t i = 0; i < nrem; ++i) {
+                const uint16_t v = bf16_bits((float)W[(size_t)q * nrem + i]);
+                wc[(size_t)q * ldw + i] = v;
+                wr[(size_t)i * rpad + q] = v;
+            }
+        std::vector<float> h32(rpad, 0.f);
+        for (uint32_t q = 0; q < rank; ++q) h32[q] = (float)H[q];
+        DevBuf<uint16_t> dWc, dWr;
+        DevBuf<float> dH, dT((size_t)rpad * kLrMaxK);
+        dWc.upload(wc.data(), wc.size(), st);
+        dWr.upload(wr.data(), wr.size(), st);
+        dH.upload(h32.data(), h32.size(), st);
+        const int g = grid(ldw / 16, kBlock / 32);
+        DevBuf<float> part((size_t)g * rpad * kLrMaxK);
+        k_lr_dots_tc<<<g, kBlock, 0, st>>>(nrem, ldw, k, rpad, reinterpret_cast<const __nv_bfloat16*>(dWc.get()),
+                                           dH.get(), dX.get(), part.get(), ticket.get(), dT.get());
+        PRISM_LAUNCHED();
+        k_lr_add_tc<<<g, kBlock, (size_t)(rpad / 2) * kLrMaxK * sizeof(uint32_t), st>>>(
+            nrem, ldw, k, rpad, reinterpret_cast<const __nv_bfloat16*>(dWr.get()), dT.get(), dY.get());
+        PRISM_LAUNCHED();
+        PRISM_CUDA(cudaMemcpyAsync(Y, dY.get(), nk * sizeof(double), cudaMemcpyDeviceToHost, st));
+        PRISM_CUDA(cudaStreamSynchronize(st));
+    } else {
+        DevBuf<double> dW, dH, dT((size_t)rank * kLrMaxK);
+        dW.upload(W, (size_t)rank * nrem, st);
+        dH.upload(H, rank, st);
+        const int g = grid(nrem, 64);
+        DevBuf<double> part((size_t)g * rank * kLrMaxK);
+        k_lr_dots_f64<<<g, kBlock, 0, st>>>(nrem, k, rank, dW.get(), dH.get(), dX.get(), part.get(), ticket.get(),
+                                            dT.get());
+        PRISM_LAUNCHED();
+        k_lr_add_f64<<<grid(nk, kBlock), kBlock, 0, st>>>(nrem, k, rank, dW.get(), dT.get(), dY.get());
+        PRISM_LAUNCHED();
+        PRISM_CUDA(cudaMemcpyAsync(Y, dY.get(), nk * sizeof(double), cudaMemcpyDeviceToHost, st));
+        PRISM_CUDA(cudaStreamSynchronize(st));
+    }
 }
 
 uint32_t AmsedPrecond::levels(int sweep) const {

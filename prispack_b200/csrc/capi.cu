@@ -196,6 +196,17 @@ int32_t prism_selftest_wait_timeout(int32_t device, uint64_t wait_ns, int32_t* d
     });
 }
 
+int32_t prism_lowrank_block_run(int32_t device, uint32_t nrem, uint32_t rank, uint32_t k, const double* W,
+                                const double* H, const double* X, double* Y, int32_t tensor) {
+    if (!W || !H || !X || !Y || nrem == 0) return fail(PRISM_ERR_ARG, "null array or empty block");
+    if (rank == 0 || rank > 128 || k == 0 || k > 64) return fail(PRISM_ERR_ARG, "rank must be in [1, 128], k in [1, 64]");
+    return guarded([&]() -> int {
+        DeviceGuard g(device);
+        prism::lowrank_block_run(device, nrem, rank, k, W, H, X, Y, tensor != 0);
+        return PRISM_OK;
+    });
+}
+
 int32_t prism_stream_sweep_order(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val,
                                  const double* diag, int32_t op, int32_t lower, int32_t precision, uint32_t num_ctas,
                                  uint32_t* eptr, uint32_t* edep, double* ecoef, uint32_t* kptr, uint32_t* kdep,

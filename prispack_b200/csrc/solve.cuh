@@ -179,6 +179,10 @@ class AmsedPrecond : public Precond {
     int kind() const override { return gmslr_ ? PRISM_PRECOND_GMSLR : PRISM_PRECOND_AMSED; }
     uint64_t mnnz() const override;
     void apply(cudaStream_t st, const double* in, double* out) override;
+    // k <= 64 interleaved columns: block sweeps per level, k-column couplings, and the
+    // low-rank correction as two matrix products (BF16 tensor cores with FP32 factor
+    // values, FP64 otherwise); see amsed_block.cuh
+    void apply_batched(cudaStream_t st, uint32_t k, const double* in, double* out) override;
     uint32_t levels(int sweep) const override;
     // sweeps are numbered 2*level + (0: lower, 1: upper) over the HID levels
     bool run_sweep(cudaStream_t st, int sweep, const double* in, double* out, int prepare) override;
@@ -200,6 +204,24 @@ class AmsedPrecond : public Precond {
     void level_sweeps(const AmsedSetup<Low>& S, uint32_t l, Sweep<Low>& lo, Sweep<Low>& up) const;
     void block_solve(cudaStream_t st, int level, const double* in, double* out);
     void c_solve(cudaStream_t st, int level, double* x);
+    // block apply (built on first use for a given k)
+    struct BlockLevel {
+        DevSweep lower, upper;            // level-order copies of the level's sweeps
+        uint32_t rpad = 0, ldw = 0;       // rank rounded up to 16, rows rounded up to 16
+        DevBuf<uint16_t> Wc, Wr;          // BF16 W: column-major rpad x ldw, row-major ldw x rpad
+        DevBuf<float> H32;                // [rpad], zero padded
+        DevBuf<double> xc, tmp, tmp2;     // nrem x k, nb x k, nb x k
+    };
+    void prepare_block(uint32_t k);
+    void block_solve_k(cudaStream_t st, int level, uint32_t k, const double* in, double* out);
+    void c_solve_k(cudaStream_t st, int level, uint32_t k, double* x);
+    void lowrank_k(cudaStream_t st, int level, uint32_t k, const double* xc, double* y);
+    std::vector<BlockLevel> blv_;
+    uint32_t bk_ = 0;                     // columns the block workspace holds
+    bool tensor_lowrank_ = false;         // BF16 tensor-core low-rank products (FP32 factor values)
+    DevBuf<double> Xk_, sweep_tmpk_, lr_t64_, lr_part64_;
+    DevBuf<float> lr_t32_, lr_part32_;
+    DevBuf<unsigned> lr_ticket_;
     Handle& h_;
     std::shared_ptr<const HostAmsed> a_;
     bool gmslr_ = false;
@@ -274,6 +296,11 @@ template <typename Low>
 void stream_sweep_run(int device, const Sweep<Low>& s, bool acc32, uint32_t num_ctas, const double* in, double* out);
 // slabs the streamed layout of an n-row sweep gets when at most num_ctas are wanted
 uint32_t stream_slab_count(uint32_t n, uint32_t num_ctas, uint32_t min_rows);
+
+// The AMSED block low-rank correction alone (amsed.cu): Y += W (H o (W^T X)), W column-major
+// nrem x rank, X and Y interleaved nrem x k (k <= 64); BF16 tensor cores when tensor, else FP64.
+void lowrank_block_run(int device, uint32_t nrem, uint32_t rank, uint32_t k, const double* W, const double* H,
+                       const double* X, double* Y, bool tensor);
 
 // Runs the bounded-wait self test (see solve.cu); returns the device status the wait raised.
 int selftest_wait_timeout(int device, unsigned long long wait_ns, int* device_status);
