@@ -832,11 +832,12 @@ bool stream_layout(const Sweep<Low>& s, const std::vector<uint32_t>& start, uint
                 }
         // 3. slots: a value occupies its slot from the round that writes it (its own round for a
         // slab row, its first reading round for a halo row) through its last reading round.
-        // Round r's reads happen while rounds r - 1 (early entries) and r (late ones) are
-        // computed, so its value is free once round r is done.  A row result of round r may
-        // take a slot whose last reader is round r - 1 or earlier.  A halo value read first in
-        // round r is read while round r - 1 is computed and copied in a round before that: its
-        // slot's last reader must be round r - 3 or earlier.  Oldest released slot first.
+        // Round r's early entries are read once rounds <= r - kStreamLate - 1 are done and before
+        // round r starts, its late ones while round r is computed, so its values are free once
+        // round r is done.  A row result of round r may take a slot whose last reader is round
+        // r - 1 or earlier.  A halo value read first in round r is copied in once rounds
+        // <= r - kStreamLate - 1 are done at the latest: its slot's last reader must be round
+        // r - kStreamLate - 1 or earlier.  Oldest released slot first.
         std::vector<uint32_t> free_q;
         size_t free_head = 0;
         std::vector<int64_t> slot_last(NZ, INT64_MAX);  // slots 0 .. NZ-1 hold 0.0
@@ -862,9 +863,10 @@ bool stream_layout(const Sweep<Low>& s, const std::vector<uint32_t>& start, uint
                     const uint32_t d = sl.col[k];
                     if ((d >= rb && d < re) || slot_in[d] == b) continue;
                     uint32_t slot, wait;
-                    if (!take(last_use[d], slot, wait, (int64_t)r - 3))
+                    if (!take(last_use[d], slot, wait, (int64_t)r - kStreamLate - 1))
                         return fail("more value slots than shared memory holds");
-                    if (r >= 2 ? wait > r - 2 : wait > 0) return fail("a prefetch would wait on a later round");
+                    if (r >= kStreamLate ? wait > r - kStreamLate : wait > 0)
+                        return fail("a prefetch would wait on a later round");
                     slot_of[d] = slot;
                     slot_in[d] = b;
                     R[r].xrow.push_back(d);
@@ -899,7 +901,7 @@ bool stream_layout(const Sweep<Low>& s, const std::vector<uint32_t>& start, uint
                     const uint32_t d = sl.col[k];
                     if (slot_in[d] != b || slot_of[d] < NZ || slot_of[d] == kNoSlot)
                         return fail("a dependency without a value slot");
-                    const bool late = d >= rb && d < re && r > 0 && round_of[d] == r - 1;
+                    const bool late = d >= rb && d < re && round_of[d] < r && round_of[d] + kStreamLate >= r;
                     (late ? lat : ear)[j].emplace_back(slot_of[d], k);
                 }
                 E = std::max<uint32_t>(E, (uint32_t)ear[j].size());
@@ -1131,14 +1133,16 @@ std::string replay_impl(const Sweep<Low>& s, const StreamLayout& L, const double
                 View v;
                 std::string e = view(gr, v);
                 if (!e.empty()) return e;
-                // round r needs its own halo (its early entries are read while round r - 1 is computed)
+                // round r needs its own halo (its early entries are read once rounds
+                // <= r - kStreamLate - 1 are done)
                 if (hbeg + c.copied < L.halo_ptr[gr + 1]) break;  // an upstream slab first
                 for (uint32_t x = L.halo_ptr[gr]; x < L.halo_ptr[gr + 1]; ++x) {
                     const uint32_t wait = L.halo_sw[x] >> 16;
-                    if (r >= 2 ? wait > r - 2 : wait > 0) return "a prefetch waits on its own or a later round";
+                    if (r >= kStreamLate ? wait > r - kStreamLate : wait > 0)
+                        return "a prefetch waits on its own or a later round";
                 }
-                // reads of round r (early ones while round r - 1 is computed, late ones while
-                // round r is), checked against the slot owners
+                // reads of round r (early ones before round r starts, late ones while round r
+                // is computed), checked against the slot owners
                 std::vector<Acc> res(v.nr);
                 std::vector<uint32_t> rows(v.nr);
                 std::vector<std::vector<uint32_t>> read_slots(v.nr);
@@ -1181,10 +1185,10 @@ std::string replay_impl(const Sweep<Low>& s, const StreamLayout& L, const double
                                 if (!done[(uint32_t)ow]) return "a dependency read before it was finished";
                                 const bool in_slab = (uint32_t)ow >= rb && (uint32_t)ow < rb + owned;
                                 if (late) {
-                                    if (!in_slab || rnd[(uint32_t)ow] + 1 != r)
-                                        return "a late entry not computed in the round before";
-                                } else if (in_slab && rnd[(uint32_t)ow] + 2 > r) {
-                                    return "an early entry computed in the round before";
+                                    if (!in_slab || rnd[(uint32_t)ow] >= r || rnd[(uint32_t)ow] + kStreamLate < r)
+                                        return "a late entry not computed in the rounds just before";
+                                } else if (in_slab && rnd[(uint32_t)ow] + kStreamLate + 1 > r) {
+                                    return "an early entry computed in the rounds just before";
                                 }
                             }
                             (late ? kx : ex).push_back(c.xs[slot]);

@@ -171,6 +171,10 @@ void slab_layout(const Sweep<Low>& s, uint32_t num_ctas, uint32_t rows_per_cta, 
 #define PRISM_HD
 #endif
 constexpr uint32_t kRoundRows = 128;
+// A dependency of a row of round r is "late" when it is a row of the slab computed in one of
+// the kStreamLate rounds before r; every other dependency (rounds <= r - kStreamLate - 1,
+// halo rows) is "early" and is summed before round r starts.
+constexpr uint32_t kStreamLate = 2;
 constexpr uint32_t kNoSlot = 0xFFFFu;
 struct RoundRec {
     uint32_t m, fld, lo, es, ec, ls, lc, bytes;

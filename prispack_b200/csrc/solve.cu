@@ -360,11 +360,13 @@ bool DevSweep::upload(const Sweep<Low>& s0, const DeviceInfo& info, int lay, cud
         StreamLayout L;
         const bool a32 = acc32 && std::is_same<Low, float>::value;
         const uint32_t slot_bytes = a32 ? 4 : 8;  // one value slot
-        if (smem <= (uint64_t)kStrFixedSmem) return false;
-        const uint32_t slot_cap = (uint32_t)std::min<uint64_t>(kNoSlot, (smem - kStrFixedSmem) / slot_bytes / 2);
+        const uint32_t vb = (uint32_t)sizeof(Low);
+        const uint64_t base_smem = stream_smem(0, 0, slot_bytes, vb, 0).total;  // everything but table and slots
+        if (smem <= base_smem) return false;
+        const uint32_t slot_cap = (uint32_t)std::min<uint64_t>(kNoSlot, (smem - base_smem) / slot_bytes / 2);
         if (!stream_layout<Low>(s0, start, slot_cap, slot_bytes, L, nullptr)) return false;
         if (L.max_rounds_per_cta > smem / 16 || L.slots > kNoSlot) return false;
-        const uint64_t fixed = stream_smem(L.max_rounds_per_cta, L.slots, slot_bytes, 0).total;
+        const uint64_t fixed = stream_smem(L.max_rounds_per_cta, L.slots, slot_bytes, vb, 0).total;
         // While round i is computed the row threads hold rounds i and i + 1 and wait for
         // round i + 2's record: two live records and room for a third, which a circular ring
         // of four of the largest records always has in one piece.
@@ -384,7 +386,7 @@ bool DevSweep::upload(const Sweep<Low>& s0, const DeviceInfo& info, int lay, cud
         str_meta_slots = L.max_rounds_per_cta;
         str_slots = L.slots;
         str_rounds = L.num_rounds;
-        str_smem = stream_smem(L.max_rounds_per_cta, L.slots, slot_bytes, ring).total;  // <= smem
+        str_smem = stream_smem(L.max_rounds_per_cta, L.slots, slot_bytes, vb, ring).total;  // <= smem
         str_nnz = s0.val.size();
         str_blob.upload(L.blob.data(), L.blob.size(), st);
         str_meta.upload(L.meta.data(), L.meta.size(), st);

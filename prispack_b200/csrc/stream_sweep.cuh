@@ -15,31 +15,34 @@
 // on lower rows only, upper sweeps on higher ones) are copied into their slots
 // by prefetcher warps as soon as they are finished.
 //
-// What sits on the chain.  Of a row's ~25 dependencies only two or three
-// ("late" entries) are rows of the round just before; the others ("early"
-// entries) were computed two or more rounds earlier or are halo values.  So
-// while round i is computed, each row thread also sums round i + 1's early
-// entries, and round i + 1 then only adds its late entries: one round on the
-// chain is a barrier, a few shared-memory loads and fused multiply-adds, the
-// result and its store.  The record of round i + 2 is loaded into registers
-// a round ahead of use, and the setup orders every row's entries so that the
-// 32 (16 for 8-byte slots) rows one wavefront serves read distinct banks.
+// What sits on the chain.  Of a row's ~25 dependencies only a few ("late"
+// entries) are rows of the kStreamLate rounds just before; the others ("early"
+// entries) were computed earlier or are halo values.  Helper warps sum every
+// row's early entries of round q as soon as rounds <= q - kStreamLate - 1 are
+// done, and hand the row threads a packet per row (the early sum P, the
+// right-hand side, the diagonal, the result slot and the first four late
+// entries).  One round on the chain is then: the packet, a few shared-memory
+// loads and fused multiply-adds, the result and its stores, and a barrier of
+// the four row warps; the early sums of the next rounds overlap it on other
+// warps.  The setup orders every row's entries so that the 32 (16 for 8-byte
+// slots) rows one wavefront serves read distinct banks.
 //
-// Roles (256 threads, two warps per SM sub-partition):
-//   warps 0..3    row threads: thread j computes row j of each round.  One
-//                 iteration (after the barrier that ends round i - 1): load round
-//                 i's late values; sum round i + 1's early entries; finish round
-//                 i (late entries, result into its slot and into global memory);
-//                 load round i + 2's record into registers; barrier (a named
-//                 barrier with an OR reduction, so that all four warps take the
-//                 same decision to leave).
-//   warps 4..6    prefetchers: warp 4+k handles the halo of rounds k, k+3, ...:
+// Roles (384 threads, three warps per SM sub-partition):
+//   warps 0..3    row threads: thread j computes row j of each round.  Round i:
+//                 wait for its packets, load the late values, add them to P one
+//                 fused multiply-add at a time, the result into its slot and into
+//                 global memory; barrier (a named barrier with an OR reduction, so
+//                 that all four warps take the same decision to leave); thread 0
+//                 publishes "rounds done".
+//   warps 4..7    helpers: warp 4+h handles rounds h, h+4, ...: waits until rounds
+//                 <= q - kStreamLate - 1 are done, round q's record has landed and
+//                 its halo is in, then sums the early entries of every row of round
+//                 q (slices of 32 rows) and publishes the round's packets.
+//   warps 8..10   prefetchers: warp 8+k handles the halo of rounds k, k+3, ...:
 //                 polls each halo row in global memory until it is finished,
 //                 waits until the slot's previous value has had its last reader,
-//                 writes the slot and raises the round's halo flag.  A row thread
-//                 that finds round i + 1's flag down sums its early entries after
-//                 the barrier instead, waiting for the flag there.
-//   warp 7        producer: issues the bulk copies of the records into the ring
+//                 writes the slot and raises the round's halo flag.
+//   warp 11       producer: issues the bulk copies of the records into the ring
 //                 in order, publishes how many have landed, and recycles the ring
 //                 space of finished rounds.
 //
@@ -52,8 +55,8 @@
 // upstream slabs, so the most upstream unfinished slab always progresses.  All
 // CTAs are co-resident (cooperative launch, one per SM).  Every wait is a
 // bounded poll (wait_ns); on expiry the kernel raises status 6 and tells the
-// CTA to leave; the row warps leave together after their next barrier, and the
-// producer waits (bounded, much longer than any copy takes) for its copies in
+// CTA to leave; the row warps leave together after their next barrier, the
+// helpers and prefetchers at their next wait, and the producer waits (bounded, much longer than any copy takes) for its copies in
 // flight before it returns.
 #pragma once
 
@@ -66,28 +69,49 @@ namespace prism {
 
 
 constexpr int kStrRowWarps = (int)kRoundRows / 32;     // row threads: one per row of a round
-constexpr int kStrPrefetchWarps = 3;                   // warps kStrRowWarps .. kStrProducer - 1
-constexpr int kStrProducer = kStrRowWarps + kStrPrefetchWarps;
+constexpr int kStrHelperWarps = 4;                     // early sums: warps kStrRowWarps ..
+constexpr int kStrPrefetchWarps = 3;                   // halo copies
+constexpr int kStrPrefetch0 = kStrRowWarps + kStrHelperWarps;
+constexpr int kStrProducer = kStrPrefetch0 + kStrPrefetchWarps;
 constexpr int kStrThreads = 32 * (kStrProducer + 1);
 constexpr uint32_t kStrMaxRounds = 64;                 // rounds in flight (ring table and halo flag slots)
-// copy barriers, halo flags, ring offsets, words
-constexpr uint32_t kStrFixedSmem = 64 * 8 + 64 * 4 + 64 * 4 + 32;
+constexpr uint32_t kStrPackets = 4;                    // rounds of packets in shared memory
+static_assert(kStrPackets > kStreamLate, "a packet slot is refilled only after its round is done");
+// copy barriers, halo flags, ring offsets, words, packet flags, packet round info
+constexpr uint32_t kStrFixedSmem = 64 * 8 + 64 * 4 + 64 * 4 + 32 + kStrPackets * 4 + kStrPackets * 8 + 16;
 constexpr unsigned long long kStrDrainNs = 2000000000ull;  // bound of the final wait for copies in flight
 static_assert(kStrThreads <= 1024, "warp roles");
 static_assert(kStrFixedSmem % 16 == 0, "round table alignment");
 
-// Dynamic shared memory of one CTA, in bytes from its start: copy barriers, halo flags,
-// ring offsets and words (kStrFixedSmem), the round table (16 B per round), the value
-// slots (rounded up to 128 B), then the ring.  The host sizes the launch with the same
-// function.
-struct StrSmem {
-    uint32_t meta, xs, ring, total;
+// What a helper hands the row thread of one row of a round: the early sum, the
+// right-hand side, the diagonal (or its reciprocal), the row (low 16 bits) and result
+// slot (high 16 bits), the first group of late slots (4 x u16) and their coefficients.
+template <typename Low, typename Acc>
+struct alignas(16) StrPacket {
+    Acc P, vin, dg;
+    uint32_t lo, ls0, ls1;
+    Low lc[4];
 };
-PRISM_HD inline StrSmem stream_smem(uint32_t meta_slots, uint32_t slots, uint32_t slot_bytes, uint32_t ring_bytes) {
+// 16-byte words of a packet for factor values of vb bytes and value slots of ab bytes
+PRISM_HD constexpr uint32_t stream_packet_words(uint32_t vb, uint32_t ab) { return ab == 4 ? 3u : (vb == 4 ? 4u : 5u); }
+static_assert(sizeof(StrPacket<float, float>) == 16 * stream_packet_words(4, 4), "packet words");
+static_assert(sizeof(StrPacket<float, double>) == 16 * stream_packet_words(4, 8), "packet words");
+static_assert(sizeof(StrPacket<double, double>) == 16 * stream_packet_words(8, 8), "packet words");
+
+// Dynamic shared memory of one CTA, in bytes from its start: copy barriers, halo flags,
+// ring offsets, words and packet flags (kStrFixedSmem), the round table (16 B per round),
+// the value slots (rounded up to 128 B), the packets (kStrPackets rounds, one 16-byte word
+// array per packet word), then the ring.  The host sizes the launch with the same function.
+struct StrSmem {
+    uint32_t meta, xs, pk, ring, total;
+};
+PRISM_HD inline StrSmem stream_smem(uint32_t meta_slots, uint32_t slots, uint32_t slot_bytes, uint32_t factor_bytes,
+                                    uint32_t ring_bytes) {
     StrSmem m;
     m.meta = kStrFixedSmem;
     m.xs = m.meta + 16u * meta_slots;
-    m.ring = m.xs + ((slots * slot_bytes + 127u) & ~127u);
+    m.pk = m.xs + ((slots * slot_bytes + 127u) & ~127u);
+    m.ring = m.pk + kStrPackets * kRoundRows * 16u * stream_packet_words(factor_bytes, slot_bytes);
     m.total = m.ring + ring_bytes;
     return m;
 }
@@ -228,11 +252,15 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
     uint32_t* hflag = reinterpret_cast<uint32_t*>(sm + 64 * 8);                // [64] round q's halo in: q + 1
     uint32_t* ring_off = hflag + 64;                                           // [64]
     uint32_t* words = ring_off + 64;                                           // landed, rounds done, abort
-    const StrSmem lay = stream_smem(a.meta_slots, a.slots, (uint32_t)sizeof(Acc), a.ring_bytes);
+    uint32_t* pflag = words + 8;                                               // [kStrPackets] round q's packets: q + 1
+    uint2* pinfo = reinterpret_cast<uint2*>(pflag + kStrPackets);              // [kStrPackets] {ring offset, shape}
+    constexpr uint32_t vb = sizeof(Low), ab = sizeof(Acc);
+    constexpr uint32_t PW = stream_packet_words(vb, ab);
+    const StrSmem lay = stream_smem(a.meta_slots, a.slots, ab, vb, a.ring_bytes);
     uint4* meta_s = reinterpret_cast<uint4*>(sm + lay.meta);                   // [meta_slots]
     Acc* xs = reinterpret_cast<Acc*>(sm + lay.xs);                             // [slots]; zero slots first
+    uint4* pkw = reinterpret_cast<uint4*>(sm + lay.pk);                        // [PW][kStrPackets * kRoundRows]
     unsigned char* ring = sm + lay.ring;
-    constexpr uint32_t vb = sizeof(Low), ab = sizeof(Acc);
     constexpr uint32_t NZ = ab == 4 ? 32u : 16u;
     const uint32_t b = blockIdx.x;
     const uint32_t rb = a.slab_start[b];
@@ -242,6 +270,7 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
     for (uint32_t i = threadIdx.x; i < R; i += blockDim.x) meta_s[i] = __ldg(a.meta + g0 + i);
     for (uint32_t i = threadIdx.x; i < NZ; i += blockDim.x) xs[i] = (Acc)0;
     for (uint32_t i = threadIdx.x; i < kStrMaxRounds; i += blockDim.x) hflag[i] = 0;
+    for (uint32_t i = threadIdx.x; i < kStrPackets; i += blockDim.x) pflag[i] = 0;
     if (threadIdx.x == 0) {
         words[0] = 0;  // records landed
         words[1] = 0;  // rounds done
@@ -349,12 +378,12 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
         return;
     }
 
-    if (warp >= kStrRowWarps) {
+    if (warp >= kStrPrefetch0) {
         // ------------------------------------------------------------------ prefetchers
         // Warp k copies in the halo of rounds k, k + 3, ... and raises each round's flag.
-        // Round q's halo is read while round q - 1 is computed (rounds done = q - 1); each
-        // slot's wait (<= q - 2) lets the copy happen a round before that.
-        for (uint32_t q = (uint32_t)(warp - kStrRowWarps); q < R; q += kStrPrefetchWarps) {
+        // Round q's halo is read by its helper once rounds <= q - kStreamLate - 1 are done;
+        // each slot's wait (<= q - kStreamLate) lets the copy happen by then.
+        for (uint32_t q = (uint32_t)(warp - kStrPrefetch0); q < R; q += kStrPrefetchWarps) {
             if ((meta_s[q].z >> 24) == 0u) continue;
             const uint32_t x0 = __ldg(a.halo_ptr + g0 + q), x1 = __ldg(a.halo_ptr + g0 + q + 1);
             bool ok = true;
@@ -402,211 +431,165 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
         return;
     }
 
-    // ---------------------------------------------------------------------- row threads
-    const uint32_t j = threadIdx.x;
-    constexpr int EGR = (int)stream_early_groups(ab);  // early entry groups in registers (every round has them)
-    // One round as a row thread holds it: fields, the first group of late entries and,
-    // once summed, its early part P.
-    struct Fld {
-        Acc vin, dg, P;
-        uint32_t lo, shape, base;
-        uint32_t ls0, ls1;
-        Low lc[4];
-    };
-    uint32_t es[EGR][2];  // early slots of the round whose early part comes next (4 x u16 per group)
-    Low ec[EGR][4];       // and their coefficients
     auto nr_of = [](uint32_t shape) { return shape & 0xFFu; };
     auto eg_of = [](uint32_t shape) { return (shape >> 8) & 0xFFu; };
     auto kg_of = [](uint32_t shape) { return (shape >> 16) & 0xFFu; };
-    auto rec_of = [&](const Fld& F) {
-        return round_rec(nr_of(F.shape), eg_of(F.shape), kg_of(F.shape), vb, ab);
-    };
-    auto load_fields = [&](uint32_t q, Fld& F) {
-        const uint4 m = meta_s[q];
-        F.shape = m.z;
-        F.base = ring_off[q % kStrMaxRounds];
-        F.P = (Acc)0;
-        if (j >= nr_of(m.z)) return;
-        const RoundRec rec = rec_of(F);
-        const unsigned char* base = ring + F.base;
-        if constexpr (ab == 4) {
-            const uint4 f = *reinterpret_cast<const uint4*>(base + rec.fld + 16u * j);
-            F.vin = __uint_as_float(f.x);
-            F.dg = __uint_as_float(f.y);
-            F.lo = f.z;
-        } else {
-            const double2 f = *reinterpret_cast<const double2*>(base + rec.fld + 16u * j);
-            F.vin = f.x;
-            F.dg = f.y;
-            F.lo = *reinterpret_cast<const uint32_t*>(base + rec.lo + 4u * j);
-        }
-        const uint2 s2 = *reinterpret_cast<const uint2*>(base + rec.ls + 8u * j);  // late group 0
-        F.ls0 = s2.x;
-        F.ls1 = s2.y;
-        load_coef4<Low>(base + rec.lc + 4u * vb * j, F.lc);
-    };
-    // the early entries of a round (its first EGR groups) into registers
-    auto load_early = [&](const Fld& F) {
-        constexpr int EG = EGR;
-        if (j >= nr_of(F.shape)) return;
-        const RoundRec rec = rec_of(F);
-        const unsigned char* base = ring + F.base;
-#pragma unroll
-        for (int g = 0; g < EG; ++g) {
-            const uint32_t e = (uint32_t)g * rec.m + j;
-            const uint2 s2 = *reinterpret_cast<const uint2*>(base + rec.es + 8u * e);
-            es[g][0] = s2.x;
-            es[g][1] = s2.y;
-            load_coef4<Low>(base + rec.ec + 4u * vb * e, ec[g]);
-        }
-    };
-    // P = (c0 + c1) + (c2 + c3): c holds the register groups' chains; entry groups beyond
-    // the register groups (rows longer than 4 * EGR entries) continue from the record
-    auto close_early = [&](Acc c0, Acc c1, Acc c2, Acc c3, Fld& F) {
-        const uint32_t Eg = eg_of(F.shape);
-        if (Eg > (uint32_t)EGR) {
-            const RoundRec rec = rec_of(F);
-            const unsigned char* base = ring + F.base;
-            for (uint32_t g = EGR; g < Eg; ++g) {
-                const uint32_t e = g * rec.m + j;
-                const uint2 s2 = *reinterpret_cast<const uint2*>(base + rec.es + 8u * e);
-                Low cf[4];
-                load_coef4<Low>(base + rec.ec + 4u * vb * e, cf);
-                c0 = acc_fma((Acc)cf[0], xs[s2.x & 0xFFFFu], c0);
-                c1 = acc_fma((Acc)cf[1], xs[s2.x >> 16], c1);
-                c2 = acc_fma((Acc)cf[2], xs[s2.y & 0xFFFFu], c2);
-                c3 = acc_fma((Acc)cf[3], xs[s2.y >> 16], c3);
-            }
-        }
-        F.P = acc_add(acc_add(c0, c1), acc_add(c2, c3));
-    };
-    // the whole early part of a round at once (prologue, and a round whose halo came late)
-    auto early_sum = [&](Fld& F) {
-        if (j >= nr_of(F.shape)) return;
-        Acc x[EGR][4];
-        Acc c[4] = {(Acc)0, (Acc)0, (Acc)0, (Acc)0};
-        gather_groups<EGR, EGR, Acc>(xs, es, x);
-        fma_groups<EGR, EGR, Acc, Low>(ec, x, c);
-        close_early(c[0], c[1], c[2], c[3], F);
-    };
-    auto finish = [&](const Fld& F, const Acc (&xl)[4]) {
-        const uint32_t Kg = kg_of(F.shape);  // >= 1: every round has a late group (padding where empty)
-        Acc s = F.P;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) s = acc_fma((Acc)F.lc[i], xl[i], s);
-        if (Kg > 1u) {  // more than four late entries: the rest from the record
-            const RoundRec rec = rec_of(F);
-            const unsigned char* base = ring + F.base;
-            for (uint32_t g = 1; g < Kg; ++g) {
-                const uint32_t e = g * rec.m + j;
-                const uint2 s2 = *reinterpret_cast<const uint2*>(base + rec.ls + 8u * e);
-                Low cf[4];
-                load_coef4<Low>(base + rec.lc + 4u * vb * e, cf);
-                s = acc_fma((Acc)cf[0], xs[s2.x & 0xFFFFu], s);
-                s = acc_fma((Acc)cf[1], xs[s2.x >> 16], s);
-                s = acc_fma((Acc)cf[2], xs[s2.y & 0xFFFFu], s);
-                s = acc_fma((Acc)cf[3], xs[s2.y >> 16], s);
-            }
-        }
-        Acc res;
-        if (OP == OP_DIV || OP == OP_MUL) res = acc_mul(acc_sub(F.vin, s), F.dg);  // dg = 1/diag for OP_DIV
-        else if (OP == OP_NONE) res = acc_sub(F.vin, s);
-        else res = acc_sub(acc_mul(F.vin, F.dg), s);                                 // dg = 1/diag
-        const double rd = (double)res;
-        unsigned long long rbits = (unsigned long long)__double_as_longlong(rd);
-        if (rd != rd) rbits = kCanonicalNaN;
-        const uint32_t os = F.lo >> 16;
-        if (os != kNoSlot) xs[os] = res;
-        st_relaxed_u64(a.out + rb + (F.lo & 0xFFFFu), rbits);
-    };
-    auto wait_landed = [&](uint32_t q) {
-        if (ld_acquire_shared_u32(words) > q) return true;
-        const unsigned long long t0 = globaltimer_ns();
-        unsigned spins = 0;
-        while (ld_acquire_shared_u32(words) <= q)
-            if (give_up(spins, t0)) return false;
-        return true;
-    };
-    auto halo_in = [&](uint32_t q) { return ld_acquire_shared_u32(hflag + q % kStrMaxRounds) == q + 1; };
-    auto wait_halo = [&](uint32_t q) {
-        if (halo_in(q)) return true;
-        const unsigned long long t0 = globaltimer_ns();
-        unsigned spins = 0;
-        while (!halo_in(q))
-            if (give_up(spins, t0)) return false;
-        return true;
-    };
-    auto has_halo = [](const Fld& F) { return (F.shape >> 24) != 0u; };
+    constexpr uint32_t PKN = kStrPackets * kRoundRows;  // packets of one word array
+    using Packet = StrPacket<Low, Acc>;
 
+    if (warp >= kStrRowWarps) {
+        // ------------------------------------------------------------------ helpers
+        constexpr int EGR = (int)stream_early_groups(ab);  // early entry groups in registers (every round has them)
+        const uint32_t l = (uint32_t)lane;
+        // tight bounded spin on a shared word (the helpers are on the round chain's critical path)
+        auto spin_until = [&](auto ready) {
+            if (ready()) return true;
+            const unsigned long long t0 = globaltimer_ns();
+            unsigned spins = 0;
+            while (!ready())
+                if (give_up(spins, t0)) return false;
+            return true;
+        };
+        for (uint32_t q = (uint32_t)(warp - kStrRowWarps); q < R; q += kStrHelperWarps) {
+            const uint32_t need = q > kStreamLate ? q - kStreamLate : 0u;  // rounds <= q - kStreamLate - 1 done
+            bool ok = spin_until([&] { return ld_acquire_shared_u32(words + 1) >= need; }) &&
+                      spin_until([&] { return ld_acquire_shared_u32(words) > q; });
+            // the halo of every round <= q: round q may read halo rows that an earlier round copied
+            // in first; rounds <= q - kStreamLate - 1 are done, so their helpers saw their flags.
+            // A flag slot only grows (round h + 1, then h + 65, ... once round h is done), so a
+            // value >= h + 1 says round h's halo is in.
+            for (uint32_t h = q > kStreamLate ? q - kStreamLate : 0u; ok && h <= q; ++h)
+                if ((meta_s[h].z >> 24) != 0u)
+                    ok = spin_until([&] { return ld_acquire_shared_u32(hflag + h % kStrMaxRounds) >= h + 1; });
+            const uint32_t shape = meta_s[q].z;
+            if (!__all_sync(0xFFFFFFFFu, ok)) return;  // the CTA is leaving (status raised by give_up)
+            const uint32_t nr = nr_of(shape), Eg = eg_of(shape), Kg = kg_of(shape);
+            const uint32_t off = ring_off[q % kStrMaxRounds];
+            const RoundRec rec = round_rec(nr, Eg, Kg, vb, ab);
+            const unsigned char* base = ring + off;
+            uint4* dst = pkw + (q % kStrPackets) * kRoundRows;
+            for (uint32_t s0 = 0; s0 < nr; s0 += 32) {  // the same for the whole warp
+                const uint32_t r = s0 + l;
+                if (r < nr) {
+                    union {
+                        Packet p;
+                        uint4 w[PW];
+                    } u;
+                    if constexpr (ab == 4) {
+                        const uint4 f = *reinterpret_cast<const uint4*>(base + rec.fld + 16u * r);
+                        u.p.vin = __uint_as_float(f.x);
+                        u.p.dg = __uint_as_float(f.y);
+                        u.p.lo = f.z;
+                    } else {
+                        const double2 f = *reinterpret_cast<const double2*>(base + rec.fld + 16u * r);
+                        u.p.vin = f.x;
+                        u.p.dg = f.y;
+                        u.p.lo = *reinterpret_cast<const uint32_t*>(base + rec.lo + 4u * r);
+                    }
+                    const uint2 l2 = *reinterpret_cast<const uint2*>(base + rec.ls + 8u * r);  // late group 0
+                    u.p.ls0 = l2.x;
+                    u.p.ls1 = l2.y;
+                    load_coef4<Low>(base + rec.lc + 4u * vb * r, u.p.lc);
+                    // early part: fma chains c_i over positions 4g + i, P = (c0 + c1) + (c2 + c3)
+                    uint32_t es[EGR][2];
+                    Low ec[EGR][4];
+#pragma unroll
+                    for (int g = 0; g < EGR; ++g) {
+                        const uint32_t e = (uint32_t)g * rec.m + r;
+                        const uint2 s2 = *reinterpret_cast<const uint2*>(base + rec.es + 8u * e);
+                        es[g][0] = s2.x;
+                        es[g][1] = s2.y;
+                        load_coef4<Low>(base + rec.ec + 4u * vb * e, ec[g]);
+                    }
+                    Acc x[EGR][4];
+                    gather_groups<EGR, EGR, Acc>(xs, es, x);
+                    Acc c[4] = {(Acc)0, (Acc)0, (Acc)0, (Acc)0};
+                    fma_groups<EGR, EGR, Acc, Low>(ec, x, c);
+                    for (uint32_t g = EGR; g < Eg; ++g) {  // more groups than registers: the rest from the record
+                        const uint32_t e = g * rec.m + r;
+                        const uint2 s2 = *reinterpret_cast<const uint2*>(base + rec.es + 8u * e);
+                        Low cf[4];
+                        load_coef4<Low>(base + rec.ec + 4u * vb * e, cf);
+                        c[0] = acc_fma((Acc)cf[0], xs[s2.x & 0xFFFFu], c[0]);
+                        c[1] = acc_fma((Acc)cf[1], xs[s2.x >> 16], c[1]);
+                        c[2] = acc_fma((Acc)cf[2], xs[s2.y & 0xFFFFu], c[2]);
+                        c[3] = acc_fma((Acc)cf[3], xs[s2.y >> 16], c[3]);
+                    }
+                    u.p.P = acc_add(acc_add(c[0], c[1]), acc_add(c[2], c[3]));
+#pragma unroll
+                    for (uint32_t w = 0; w < PW; ++w) dst[w * PKN + r] = u.w[w];
+                }
+            }
+            __syncwarp();
+            if (lane == 0) {
+                pinfo[q % kStrPackets] = make_uint2(off, shape);
+                st_release_shared_u32(pflag + q % kStrPackets, q + 1);
+            }
+        }
+        return;
+    }
+
+    // ---------------------------------------------------------------------- row threads
+    const uint32_t j = threadIdx.x;
     bool bad = false;
-    Fld F0, F1;
-    F0.shape = F1.shape = 0u;
-    // prologue: round 0 with its early part summed, round 1's record in registers
-    if (!wait_landed(0)) bad = true;
-    if (!bad) {
-        load_fields(0, F0);
-        load_early(F0);
-        if (has_halo(F0) && !wait_halo(0)) bad = true;
-    }
-    if (!bad) early_sum(F0);
-    if (!bad && R > 1) {
-        if (!wait_landed(1)) bad = true;
-        else {
-            load_fields(1, F1);
-            load_early(F1);
+    for (uint32_t i = 0; i < R; ++i) {
+        const uint32_t ps = i % kStrPackets;
+        if (!bad && ld_acquire_shared_u32(pflag + ps) != i + 1) {
+            const unsigned long long t0 = globaltimer_ns();
+            unsigned spins = 0;
+            while (ld_acquire_shared_u32(pflag + ps) != i + 1)
+                if (give_up(spins, t0)) {
+                    bad = true;
+                    break;
+                }
         }
-    }
-    // One iteration: cur = round i (early part summed), nxt = round i + 1 (record in
-    // registers); once round i is finished, cur receives round i + 2.  Returns true when
-    // the row threads leave.
-    auto step = [&](uint32_t i, Fld& cur, Fld& nxt) -> bool {
-        const bool more = i + 1 < R, more2 = i + 2 < R;
-        // round i + 1's early part now unless its halo is not in yet (then after the barrier)
-        const bool pend = more && !bad && has_halo(nxt) && !halo_in(i + 1);
-        const bool live = !bad && j < nr_of(cur.shape);
-        const bool early = more && !bad && !pend && j < nr_of(nxt.shape);
-        {
-            // every value load first: round i's late values, round i + 1's early ones
-            Acc xl[4] = {(Acc)0, (Acc)0, (Acc)0, (Acc)0};
-            if (live) {
-                xl[0] = xs[cur.ls0 & 0xFFFFu];
-                xl[1] = xs[cur.ls0 >> 16];
-                xl[2] = xs[cur.ls1 & 0xFFFFu];
-                xl[3] = xs[cur.ls1 >> 16];
+        const uint32_t shape = meta_s[i].z;
+        if (!bad && j < nr_of(shape)) {
+            union {
+                Packet p;
+                uint4 w[PW];
+            } u;
+            const uint4* src = pkw + ps * kRoundRows + j;
+#pragma unroll
+            for (uint32_t w = 0; w < PW; ++w) u.w[w] = src[w * PKN];
+            Acc xl[4];
+            xl[0] = xs[u.p.ls0 & 0xFFFFu];
+            xl[1] = xs[u.p.ls0 >> 16];
+            xl[2] = xs[u.p.ls1 & 0xFFFFu];
+            xl[3] = xs[u.p.ls1 >> 16];
+            Acc s = u.p.P;
+#pragma unroll
+            for (int t = 0; t < 4; ++t) s = acc_fma((Acc)u.p.lc[t], xl[t], s);
+            const uint32_t Kg = kg_of(shape);  // >= 1: every round has a late group (padding where empty)
+            if (Kg > 1u) {                     // more than four late entries: the rest from the record
+                const RoundRec rec = round_rec(nr_of(shape), eg_of(shape), Kg, vb, ab);
+                const unsigned char* base = ring + pinfo[ps].x;
+                for (uint32_t g = 1; g < Kg; ++g) {
+                    const uint32_t e = g * rec.m + j;
+                    const uint2 s2 = *reinterpret_cast<const uint2*>(base + rec.ls + 8u * e);
+                    Low cf[4];
+                    load_coef4<Low>(base + rec.lc + 4u * vb * e, cf);
+                    s = acc_fma((Acc)cf[0], xs[s2.x & 0xFFFFu], s);
+                    s = acc_fma((Acc)cf[1], xs[s2.x >> 16], s);
+                    s = acc_fma((Acc)cf[2], xs[s2.y & 0xFFFFu], s);
+                    s = acc_fma((Acc)cf[3], xs[s2.y >> 16], s);
+                }
             }
-            Acc x[EGR][4];
-            if (early) gather_groups<EGR, EGR, Acc>(xs, es, x);
-            if (live) finish(cur, xl);
-            if (early) {
-                Acc c[4] = {(Acc)0, (Acc)0, (Acc)0, (Acc)0};
-                fma_groups<EGR, EGR, Acc, Low>(ec, x, c);
-                close_early(c[0], c[1], c[2], c[3], nxt);
-            }
-        }
-        if (more2 && !bad) {
-            if (!wait_landed(i + 2)) bad = true;
-            else {
-                load_fields(i + 2, cur);
-                if (!pend) load_early(cur);
-            }
+            Acc res;
+            if (OP == OP_DIV || OP == OP_MUL) res = acc_mul(acc_sub(u.p.vin, s), u.p.dg);  // dg = 1/diag for OP_DIV
+            else if (OP == OP_NONE) res = acc_sub(u.p.vin, s);
+            else res = acc_sub(acc_mul(u.p.vin, u.p.dg), s);                                 // dg = 1/diag
+            const double rd = (double)res;
+            unsigned long long rbits = (unsigned long long)__double_as_longlong(rd);
+            if (rd != rd) rbits = kCanonicalNaN;
+            const uint32_t os = u.p.lo >> 16;
+            if (os != kNoSlot) xs[os] = res;
+            st_relaxed_u64(a.out + rb + (u.p.lo & 0xFFFFu), rbits);
         }
         __syncwarp();
         const bool stop = row_barrier_or(bad || vwords[2] != 0u);
         if (threadIdx.x == 0) st_release_shared_u32(words + 1, i + 1);
-        if (stop) return true;
-        if (pend) {
-            if (!wait_halo(i + 1)) {
-                bad = true;
-            } else {
-                early_sum(nxt);
-                if (more2) load_early(cur);
-            }
-        }
-        return false;
-    };
-    for (uint32_t i = 0; i < R; i += 2) {
-        if (step(i, F0, F1)) break;
-        if (i + 1 >= R || step(i + 1, F1, F0)) break;
+        if (stop) break;
     }
 }
 
