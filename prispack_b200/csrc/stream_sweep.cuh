@@ -75,25 +75,27 @@ constexpr int kStrPrefetch0 = kStrRowWarps + kStrHelperWarps;
 constexpr int kStrProducer = kStrPrefetch0 + kStrPrefetchWarps;
 constexpr int kStrThreads = 32 * (kStrProducer + 1);
 constexpr uint32_t kStrMaxRounds = 64;                 // rounds in flight (ring table and halo flag slots)
-constexpr uint32_t kStrPackets = 4;                    // rounds of packets in shared memory
+constexpr uint32_t kStrPackets = 3;                    // rounds of packets in shared memory
 static_assert(kStrPackets > kStreamLate, "a packet slot is refilled only after its round is done");
-// copy barriers, halo flags, ring offsets, words, packet flags, packet round info
-constexpr uint32_t kStrFixedSmem = 64 * 8 + 64 * 4 + 64 * 4 + 32 + kStrPackets * 4 + kStrPackets * 8 + 16;
+// copy barriers, halo flags, ring offsets, words, packet flags [4], packet round info [4]
+static_assert(kStrPackets <= 4, "packet flag space");
+constexpr uint32_t kStrFixedSmem = 64 * 8 + 64 * 4 + 64 * 4 + 32 + 4 * 4 + 4 * 8 + 16;
 constexpr unsigned long long kStrDrainNs = 2000000000ull;  // bound of the final wait for copies in flight
 static_assert(kStrThreads <= 1024, "warp roles");
 static_assert(kStrFixedSmem % 16 == 0, "round table alignment");
 
 // What a helper hands the row thread of one row of a round: the early sum, the
 // right-hand side, the diagonal (or its reciprocal), the row (low 16 bits) and result
-// slot (high 16 bits), the first group of late slots (4 x u16) and their coefficients.
+// slot (high 16 bits), the first two groups of late slots (4 x u16 each; the second
+// unused when the round has one) and their coefficients.
 template <typename Low, typename Acc>
 struct alignas(16) StrPacket {
     Acc P, vin, dg;
-    uint32_t lo, ls0, ls1;
-    Low lc[4];
+    uint32_t lo, ls[4];
+    Low lc[8];
 };
 // 16-byte words of a packet for factor values of vb bytes and value slots of ab bytes
-PRISM_HD constexpr uint32_t stream_packet_words(uint32_t vb, uint32_t ab) { return ab == 4 ? 3u : (vb == 4 ? 4u : 5u); }
+PRISM_HD constexpr uint32_t stream_packet_words(uint32_t vb, uint32_t ab) { return ab == 4 ? 4u : (vb == 4 ? 5u : 7u); }
 static_assert(sizeof(StrPacket<float, float>) == 16 * stream_packet_words(4, 4), "packet words");
 static_assert(sizeof(StrPacket<float, double>) == 16 * stream_packet_words(4, 8), "packet words");
 static_assert(sizeof(StrPacket<double, double>) == 16 * stream_packet_words(8, 8), "packet words");
@@ -253,7 +255,7 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
     uint32_t* ring_off = hflag + 64;                                           // [64]
     uint32_t* words = ring_off + 64;                                           // landed, rounds done, abort
     uint32_t* pflag = words + 8;                                               // [kStrPackets] round q's packets: q + 1
-    uint2* pinfo = reinterpret_cast<uint2*>(pflag + kStrPackets);              // [kStrPackets] {ring offset, shape}
+    uint2* pinfo = reinterpret_cast<uint2*>(pflag + 4);                        // [kStrPackets] {ring offset, shape}
     constexpr uint32_t vb = sizeof(Low), ab = sizeof(Acc);
     constexpr uint32_t PW = stream_packet_words(vb, ab);
     const StrSmem lay = stream_smem(a.meta_slots, a.slots, ab, vb, a.ring_bytes);
@@ -486,10 +488,22 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
                         u.p.dg = f.y;
                         u.p.lo = *reinterpret_cast<const uint32_t*>(base + rec.lo + 4u * r);
                     }
-                    const uint2 l2 = *reinterpret_cast<const uint2*>(base + rec.ls + 8u * r);  // late group 0
-                    u.p.ls0 = l2.x;
-                    u.p.ls1 = l2.y;
-                    load_coef4<Low>(base + rec.lc + 4u * vb * r, u.p.lc);
+                    // late groups 0 and 1
+                    const uint2 l2 = *reinterpret_cast<const uint2*>(base + rec.ls + 8u * r);
+                    u.p.ls[0] = l2.x;
+                    u.p.ls[1] = l2.y;
+                    load_coef4<Low>(base + rec.lc + 4u * vb * r, *reinterpret_cast<Low(*)[4]>(u.p.lc));
+                    if (Kg > 1u) {
+                        const uint32_t e = rec.m + r;
+                        const uint2 m2 = *reinterpret_cast<const uint2*>(base + rec.ls + 8u * e);
+                        u.p.ls[2] = m2.x;
+                        u.p.ls[3] = m2.y;
+                        load_coef4<Low>(base + rec.lc + 4u * vb * e, *reinterpret_cast<Low(*)[4]>(u.p.lc + 4));
+                    } else {
+                        u.p.ls[2] = u.p.ls[3] = 0u;
+#pragma unroll
+                        for (int t = 4; t < 8; ++t) u.p.lc[t] = (Low)0;
+                    }
                     // early part: fma chains c_i over positions 4g + i, P = (c0 + c1) + (c2 + c3)
                     uint32_t es[EGR][2];
                     Low ec[EGR][4];
@@ -532,63 +546,84 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
     // ---------------------------------------------------------------------- row threads
     const uint32_t j = threadIdx.x;
     bool bad = false;
-    for (uint32_t i = 0; i < R; ++i) {
+    union Pk {
+        Packet p;
+        uint4 w[PW];
+    };
+    auto wait_packet = [&](uint32_t i) {
         const uint32_t ps = i % kStrPackets;
-        if (!bad && ld_acquire_shared_u32(pflag + ps) != i + 1) {
-            const unsigned long long t0 = globaltimer_ns();
-            unsigned spins = 0;
-            while (ld_acquire_shared_u32(pflag + ps) != i + 1)
-                if (give_up(spins, t0)) {
-                    bad = true;
-                    break;
-                }
+        if (ld_acquire_shared_u32(pflag + ps) == i + 1) return true;
+        const unsigned long long t0 = globaltimer_ns();
+        unsigned spins = 0;
+        while (ld_acquire_shared_u32(pflag + ps) != i + 1)
+            if (give_up(spins, t0)) return false;
+        return true;
+    };
+    auto load_packet = [&](uint32_t i, Pk& u) {
+        const uint4* src = pkw + (i % kStrPackets) * kRoundRows + j;
+#pragma unroll
+        for (uint32_t w = 0; w < PW; ++w) u.w[w] = src[w * PKN];
+    };
+    // row j of round i from its packet: the result into its slot; returns the encoded result
+    // for global memory, which the caller stores after publishing the round (a release
+    // would otherwise wait for that store to reach L2)
+    auto compute = [&](uint32_t i, uint32_t shape, const Pk& u) -> unsigned long long {
+        const uint32_t Kg = kg_of(shape);  // >= 1: every round has a late group (padding where empty)
+        Acc xl[8];
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+            const uint32_t sl = (u.p.ls[t / 2] >> (16 * (t & 1))) & 0xFFFFu;
+            if (t < 4 || Kg > 1u) xl[t] = xs[sl];
         }
-        const uint32_t shape = meta_s[i].z;
-        if (!bad && j < nr_of(shape)) {
-            union {
-                Packet p;
-                uint4 w[PW];
-            } u;
-            const uint4* src = pkw + ps * kRoundRows + j;
+        Acc s = u.p.P;
 #pragma unroll
-            for (uint32_t w = 0; w < PW; ++w) u.w[w] = src[w * PKN];
-            Acc xl[4];
-            xl[0] = xs[u.p.ls0 & 0xFFFFu];
-            xl[1] = xs[u.p.ls0 >> 16];
-            xl[2] = xs[u.p.ls1 & 0xFFFFu];
-            xl[3] = xs[u.p.ls1 >> 16];
-            Acc s = u.p.P;
+        for (int t = 0; t < 4; ++t) s = acc_fma((Acc)u.p.lc[t], xl[t], s);
+        if (Kg > 1u) {  // the second late group (warp-uniform)
 #pragma unroll
-            for (int t = 0; t < 4; ++t) s = acc_fma((Acc)u.p.lc[t], xl[t], s);
-            const uint32_t Kg = kg_of(shape);  // >= 1: every round has a late group (padding where empty)
-            if (Kg > 1u) {                     // more than four late entries: the rest from the record
-                const RoundRec rec = round_rec(nr_of(shape), eg_of(shape), Kg, vb, ab);
-                const unsigned char* base = ring + pinfo[ps].x;
-                for (uint32_t g = 1; g < Kg; ++g) {
-                    const uint32_t e = g * rec.m + j;
-                    const uint2 s2 = *reinterpret_cast<const uint2*>(base + rec.ls + 8u * e);
-                    Low cf[4];
-                    load_coef4<Low>(base + rec.lc + 4u * vb * e, cf);
-                    s = acc_fma((Acc)cf[0], xs[s2.x & 0xFFFFu], s);
-                    s = acc_fma((Acc)cf[1], xs[s2.x >> 16], s);
-                    s = acc_fma((Acc)cf[2], xs[s2.y & 0xFFFFu], s);
-                    s = acc_fma((Acc)cf[3], xs[s2.y >> 16], s);
-                }
+            for (int t = 4; t < 8; ++t) s = acc_fma((Acc)u.p.lc[t], xl[t], s);
+        }
+        if (Kg > 2u) {  // more than eight late entries: the rest from the record
+            const RoundRec rec = round_rec(nr_of(shape), eg_of(shape), Kg, vb, ab);
+            const unsigned char* base = ring + pinfo[i % kStrPackets].x;
+            for (uint32_t g = 2; g < Kg; ++g) {
+                const uint32_t e = g * rec.m + j;
+                const uint2 s2 = *reinterpret_cast<const uint2*>(base + rec.ls + 8u * e);
+                Low cf[4];
+                load_coef4<Low>(base + rec.lc + 4u * vb * e, cf);
+                s = acc_fma((Acc)cf[0], xs[s2.x & 0xFFFFu], s);
+                s = acc_fma((Acc)cf[1], xs[s2.x >> 16], s);
+                s = acc_fma((Acc)cf[2], xs[s2.y & 0xFFFFu], s);
+                s = acc_fma((Acc)cf[3], xs[s2.y >> 16], s);
             }
-            Acc res;
-            if (OP == OP_DIV || OP == OP_MUL) res = acc_mul(acc_sub(u.p.vin, s), u.p.dg);  // dg = 1/diag for OP_DIV
-            else if (OP == OP_NONE) res = acc_sub(u.p.vin, s);
-            else res = acc_sub(acc_mul(u.p.vin, u.p.dg), s);                                 // dg = 1/diag
-            const double rd = (double)res;
-            unsigned long long rbits = (unsigned long long)__double_as_longlong(rd);
-            if (rd != rd) rbits = kCanonicalNaN;
-            const uint32_t os = u.p.lo >> 16;
-            if (os != kNoSlot) xs[os] = res;
-            st_relaxed_u64(a.out + rb + (u.p.lo & 0xFFFFu), rbits);
+        }
+        Acc res;
+        if (OP == OP_DIV || OP == OP_MUL) res = acc_mul(acc_sub(u.p.vin, s), u.p.dg);  // dg = 1/diag for OP_DIV
+        else if (OP == OP_NONE) res = acc_sub(u.p.vin, s);
+        else res = acc_sub(acc_mul(u.p.vin, u.p.dg), s);                                 // dg = 1/diag
+        const double rd = (double)res;
+        unsigned long long rbits = (unsigned long long)__double_as_longlong(rd);
+        if (rd != rd) rbits = kCanonicalNaN;
+        const uint32_t os = u.p.lo >> 16;
+        if (os != kNoSlot) xs[os] = res;
+        return rbits;
+    };
+    for (uint32_t i = 0; i < R; ++i) {
+        const uint32_t shape = meta_s[i].z;
+        if (!bad && !wait_packet(i)) bad = true;
+        bool mine = false;
+        unsigned long long rbits = 0;
+        uint32_t orow = 0;
+        if (!bad && j < nr_of(shape)) {
+            Pk u;
+            load_packet(i, u);
+            rbits = compute(i, shape, u);
+            orow = u.p.lo & 0xFFFFu;
+            mine = true;
         }
         __syncwarp();
         const bool stop = row_barrier_or(bad || vwords[2] != 0u);
         if (threadIdx.x == 0) st_release_shared_u32(words + 1, i + 1);
+        if (mine) st_relaxed_u64(a.out + rb + orow, rbits);
         if (stop) break;
     }
 }
