@@ -381,9 +381,21 @@ int32_t prism_solve(prism_handle h, const prism_solve_opts* opts, const double* 
 
 /* ---- new values on the same pattern, and the adjoint solve ---------------
  * prism_update_values*: A's values replaced (same rowptr/col); the
- * preconditioner is kept as it was until a prism_set_precond_* call refactors
- * it (a solve stays exact with a stale preconditioner, only slower).  No
- * reference counterpart: the reference builds a new CSRMatrix.
+ * preconditioner is kept as it was until a prism_set_precond_* call sets it
+ * up again or prism_refactor recomputes it (a solve stays exact with a stale
+ * preconditioner, only slower).  No reference counterpart: the reference
+ * builds a new CSRMatrix.
+ *
+ * prism_refactor: the IC / ILDLT factor recomputed on the device for A's
+ * current values, on the factor's own pattern (no new fill, no dropping), in
+ * the operation order of the host factorisation (IncompleteCholesky::setup,
+ * IncompleteCholesky.cpp:96-246; IncompleteLDLT::setup,
+ * IncompleteLDLT.cpp:39-186), which the host recorded when it built the
+ * factor: with the values the factor was built from, the result is the host
+ * factor bit for bit.  The new values go into every device layout of the
+ * preconditioner's sweeps.  PRISM_ERR_NOT_SPD / PRISM_ERR_ZERO_PIVOT as the
+ * host factorisation reports them; PRISM_ERR_UNSUPPORTED for ILUT, AMSED and
+ * GMSLR.
  *
  * prism_adjoint_solve*: the backward pass of x = A^{-1} b for a scalar loss L
  * with g = dL/dx:  lambda = A^{-T} g  (= dL/db), solved with the handle's
@@ -393,6 +405,7 @@ int32_t prism_solve(prism_handle h, const prism_solve_opts* opts, const double* 
  * of values; PRISM_ERR_UNSUPPORTED otherwise).  No reference counterpart. */
 int32_t prism_update_values(prism_handle h, const double* val);
 int32_t prism_update_values_device(prism_handle h, const double* val_d);
+int32_t prism_refactor(prism_handle h);
 int32_t prism_adjoint_solve_device(prism_handle h, const prism_solve_opts* opts, const double* g_d, const double* x_d,
                                    double* lambda_d, double* grad_val_d, prism_solve_stats* stats);
 int32_t prism_adjoint_solve(prism_handle h, const prism_solve_opts* opts, const double* g, const double* x,

@@ -152,6 +152,101 @@ void orc_sweep_ordered(uint32_t n, int single, int op, int lower, const uint32_t
     free(xd);
 }
 
+/* Numeric refactorisation of an IC (kind 1) or ILDLT (kind 3) factor on a given
+ * pattern: IncompleteCholesky::setup (IncompleteCholesky.cpp:96-246) and
+ * IncompleteLDLT::setup (IncompleteLDLT.cpp:39-186) with their drop test
+ * (|L_ij| >= threshold * sum of |A_ij|) replaced by "L_ij is kept when (i, j) is in
+ * the pattern".  Column j accumulates the entries of row j of A at or below the
+ * diagonal, then subtracts L_ik * L_jk (* d_k) for each finished column k of its row
+ * list (the reference's vNonZeroRow / vNextIdxRow linked lists), divides the kept
+ * entries by the pivot (sqrt of it for IC) and stores them rounded to float when
+ * single != 0.  lt_rowptr / lt_col: the pattern of L^T by rows (IC: the diagonal
+ * first, ILDLT: no diagonal), rows in increasing order; lt_val receives the values,
+ * D (ILDLT) the pivots.  Returns 0, 4 (IC: non-positive pivot) or 3 (ILDLT: zero
+ * pivot). */
+int orc_refactor(uint32_t n, int kind, const uint32_t* a_rowptr, const uint32_t* a_col, const double* a_val,
+                 const uint32_t* lt_rowptr, const uint32_t* lt_col, int single, double* lt_val, double* D) {
+    const int ldlt = kind == 3;
+    uint8_t* used = (uint8_t*)calloc(n ? n : 1, 1);
+    double* colv = (double*)calloc(n ? n : 1, sizeof(double));
+    uint32_t* nz_row = (uint32_t*)malloc(sizeof(uint32_t) * (n ? n : 1));
+    uint32_t* next_idx = (uint32_t*)malloc(sizeof(uint32_t) * (n ? n : 1));
+    uint32_t* touched = (uint32_t*)malloc(sizeof(uint32_t) * (n ? n : 1));
+    int rc = 0;
+    for (uint32_t i = 0; i < n; i++) nz_row[i] = UINT32_MAX;
+#define STORE(x) (single ? (double)(float)(x) : (x))
+    for (uint32_t j = 0; j < n && !rc; j++) {
+        uint32_t cnt = 0;
+        for (uint32_t p = a_rowptr[j]; p < a_rowptr[j + 1]; p++) {
+            const uint32_t i = a_col[p];
+            if (i >= j) {
+                if (!used[i]) {
+                    colv[i] = 0.0;
+                    used[i] = 1;
+                    touched[cnt++] = i;
+                }
+                colv[i] += a_val[p];
+            }
+        }
+        uint32_t k = nz_row[j];
+        while (k != UINT32_MAX) {
+            uint32_t start = next_idx[k];
+            const double Ljk = lt_val[start];
+            const double dk = ldlt ? D[k] : 0.0;
+            for (uint32_t p = start; p < lt_rowptr[k + 1]; p++) {
+                const uint32_t i = lt_col[p];
+                if (!used[i]) {
+                    used[i] = 1;
+                    colv[i] = 0.0;
+                    touched[cnt++] = i;
+                }
+                if (ldlt) colv[i] -= lt_val[p] * Ljk * dk;
+                else colv[i] -= lt_val[p] * Ljk;
+            }
+            start += 1;
+            const uint32_t knext = nz_row[k];
+            if (start < lt_rowptr[k + 1]) {
+                next_idx[k] = start;
+                const uint32_t i = lt_col[start];
+                nz_row[k] = nz_row[i];
+                nz_row[i] = k;
+            }
+            k = knext;
+        }
+        double piv = colv[j];
+        uint32_t w = lt_rowptr[j];
+        if (ldlt) {
+            if (fabs(piv) < 1e-15) rc = 3;
+            D[j] = piv;
+            next_idx[j] = w;
+        } else {
+            if (piv <= 0.0) rc = 4;
+            piv = sqrt(piv);
+            lt_val[w++] = STORE(piv);
+            next_idx[j] = w;
+        }
+        /* the kept entries in increasing row order (the pattern's own order) */
+        int first = 1;
+        for (uint32_t q = w; q < lt_rowptr[j + 1]; q++) {
+            const uint32_t i = lt_col[q];
+            if (first) {
+                first = 0;
+                nz_row[j] = nz_row[i];
+                nz_row[i] = j;
+            }
+            lt_val[q] = STORE(colv[i] / piv);
+        }
+        for (uint32_t t = 0; t < cnt; t++) used[touched[t]] = 0;
+    }
+#undef STORE
+    free(used);
+    free(colv);
+    free(nz_row);
+    free(next_idx);
+    free(touched);
+    return rc;
+}
+
 /* ---- AMSED ----------------------------------------------------------------- */
 static void ildlt_inplace(uint32_t n, const uint32_t* rp, const uint32_t* ci, const double* v, const double* D,
                           double* vec) {

@@ -92,6 +92,9 @@ void orc_sweep_f32(uint32_t n, const uint32_t* rowptr, const uint32_t* col, cons
 void orc_sweep_ordered(uint32_t n, int single, int op, int lower, const uint32_t* eptr, const uint32_t* edep,
                        const double* ecoef, const uint32_t* kptr, const uint32_t* kdep, const double* kcoef,
                        const double* diag, const double* in, double* out);
+/* IC (kind 1) / ILDLT (kind 3) factor values recomputed on a given pattern (see oracle.c) */
+int orc_refactor(uint32_t n, int kind, const uint32_t* a_rowptr, const uint32_t* a_col, const double* a_val,
+                 const uint32_t* lt_rowptr, const uint32_t* lt_col, int single, double* lt_val, double* D);
 void orc_precond_apply(const orc_precond* P, double* vec);
 void orc_cg(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val,
             const orc_precond* P, int flexible, double tol, uint32_t max_iter,

@@ -65,6 +65,8 @@ def lib() -> C.CDLL:
         _LIB.orc_sweep_ordered.argtypes = [C.c_uint32, C.c_int, C.c_int, C.c_int, _u32p, _u32p, _f64p, _u32p, _u32p,
                                            _f64p, C.c_void_p, _f64p, _f64p]
         _LIB.orc_precond_apply.argtypes = [C.POINTER(_Precond), _f64p]
+        _LIB.orc_refactor.argtypes = [C.c_uint32, C.c_int, _u32p, _u32p, _f64p, _u32p, _u32p, C.c_int, _f64p, _f64p]
+        _LIB.orc_refactor.restype = C.c_int
         _LIB.orc_amsed_apply.argtypes = [C.POINTER(_Amsed), _f64p]
         _LIB.orc_cg.argtypes = [C.c_uint32, _u32p, _u32p, _f64p, C.POINTER(_Precond), C.c_int, C.c_double,
                                 C.c_uint32, _f64p, _f64p, C.POINTER(C.c_int32), C.POINTER(C.c_double),
@@ -102,6 +104,20 @@ def sweep_f32(rp, ci, v, b, *, diag=None, op=2, lower=True):
                         d.ctypes.data if d is not None else None, int(op), int(bool(lower)),
                         np.ascontiguousarray(b, np.float64), out)
     return out
+
+
+def refactor(kind, A_rowptr, A_col, A_val, lt_rowptr, lt_col, *, single=False):
+    """IC (kind 1) / ILDLT (kind 3) factor values on the pattern (lt_rowptr, lt_col) for the
+    matrix values A_val: returns (status, lt_val, D)."""
+    n = len(A_rowptr) - 1
+    lt_val = np.zeros(max(len(lt_col), 1))
+    D = np.zeros(max(n, 1))
+    rc = lib().orc_refactor(n, int(kind), np.ascontiguousarray(A_rowptr, np.uint32),
+                            np.ascontiguousarray(A_col, np.uint32), np.ascontiguousarray(A_val, np.float64),
+                            np.ascontiguousarray(lt_rowptr, np.uint32),
+                            np.ascontiguousarray(lt_col if len(lt_col) else np.zeros(1), np.uint32),
+                            int(bool(single)), lt_val, D)
+    return rc, lt_val[:len(lt_col)], D[:n]
 
 
 def sweep_ordered(order, b, *, diag=None, op=2, lower=True, single=True):

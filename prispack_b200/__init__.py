@@ -146,6 +146,7 @@ _SIGS = {
     "prism_solve_segments": (C.c_int32, [_vp, C.POINTER(SolveOpts), C.c_uint32, _u32p, _f64p, _f64p,
                                          C.POINTER(SolveStats)]),
     "prism_update_values": (C.c_int32, [_vp, _f64p]),
+    "prism_refactor": (C.c_int32, [_vp]),
     "prism_update_values_device": (C.c_int32, [_vp, _vp]),
     "prism_adjoint_solve_device": (C.c_int32, [_vp, C.POINTER(SolveOpts), _vp, _vp, _vp, _vp, C.POINTER(SolveStats)]),
     "prism_adjoint_solve": (C.c_int32, [_vp, C.POINTER(SolveOpts), _f64p, _f64p, _f64p, _vp, C.POINTER(SolveStats)]),
@@ -718,6 +719,11 @@ class DeviceSystem:
             _check(self.lib.prism_update_values_device(self.h, _ptr(val.contiguous())))
         else:
             _check(self.lib.prism_update_values(self.h, np.ascontiguousarray(val, np.float64)))
+
+    def refactor(self):
+        """IC / ILDLT: the factor recomputed on the device for A's current values, on its own
+        pattern, in the host factorisation's operation order (prism_refactor)."""
+        _check(self.lib.prism_refactor(self.h))
 
     def adjoint(self, g, x=None, *, solver=SOLVER_FCG, tol=1e-10, max_iter=1000, restart=0):
         """lambda = A^{-T} g and, with x given, dL/dA on A's pattern (-lambda_i x_j);

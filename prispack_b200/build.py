@@ -19,7 +19,7 @@ OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libprism_solve.so")
 BUILD = os.path.join(OUT_DIR, "obj")
 
-CU_SOURCES = ["solve.cu", "gmres.cu", "amsed.cu", "batched.cu", "segments.cu", "capi.cu", "noalloc.cu"]
+CU_SOURCES = ["solve.cu", "gmres.cu", "amsed.cu", "batched.cu", "segments.cu", "capi.cu", "noalloc.cu", "refactor.cu"]
 CPP_SOURCES = ["host_setup.cpp", "amsed_setup.cpp", "partition.cpp", "mtx.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

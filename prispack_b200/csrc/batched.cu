@@ -494,6 +494,7 @@ void TriangularPrecond::apply_batched(cudaStream_t st, uint32_t k, const double*
         if (mine.n != tuned.n) {
             if (f_->fp32) mine.upload(lower ? f_->lower32 : f_->upper32, h_.info, LAYOUT_LEVEL, h_.stream);
             else mine.upload(lower ? f_->lower64 : f_->upper64, h_.info, LAYOUT_LEVEL, h_.stream);
+            refresh_level_copy(mine, lower);  // after a device refactorisation: its values
         }
         return mine;
     };

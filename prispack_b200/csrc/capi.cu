@@ -924,6 +924,16 @@ int32_t prism_update_values_device(prism_handle h, const double* val_d) {
     });
 }
 
+int32_t prism_refactor(prism_handle h) {
+    if (!h) return fail(PRISM_ERR_ARG, "null handle");
+    if (!h->P) return fail(PRISM_ERR_NOT_READY, "no preconditioner set");
+    return guarded([&]() -> int {
+        DeviceGuard g(h->info.device);
+        h->P->refactor();
+        return PRISM_OK;
+    });
+}
+
 static void adjoint(prism::Handle& h, const prism_solve_opts& o, const double* g_d, const double* x_d,
                     double* lambda_d, double* grad_d, prism_solve_stats* st) {
     if (h.symmetric < 0) h.symmetric = prism::csr_symmetric(h.A_host) ? 1 : 0;

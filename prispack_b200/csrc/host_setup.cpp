@@ -109,7 +109,8 @@ constexpr uint32_t kNone = 0xFFFFFFFFu;
 // the list of row j.  `ldlt` selects the IncompleteLDLT variant (no sqrt,
 // pivot kept in D, unit L^T stored without its diagonal).
 template <typename Low, bool ldlt>
-int left_looking(const CsrHost& A, double thr, CsrT<Low>& Lt, std::vector<double>* D, std::string* err) {
+int left_looking(const CsrHost& A, double thr, CsrT<Low>& Lt, std::vector<double>* D, std::string* err,
+                 RefactorPlan* plan) {
     const uint32_t n = A.n;
     std::vector<uint8_t> used(n, 0);
     std::vector<uint32_t> touched(n);
@@ -123,6 +124,13 @@ int left_looking(const CsrHost& A, double thr, CsrT<Low>& Lt, std::vector<double
     Lt.col.reserve(A.nnz() * 4);
     Lt.val.reserve(A.nnz() * 4);
     if (ldlt) D->assign(n, 0.0);
+    if (plan) {
+        *plan = RefactorPlan();
+        plan->n = n;
+        plan->ldlt = ldlt;
+        plan->a_ptr.assign(1, 0);
+        plan->up_ptr.assign(1, 0);
+    }
 
     for (uint32_t j = 0; j < n; ++j) {
         uint32_t cnt = 0;
@@ -132,6 +140,7 @@ int left_looking(const CsrHost& A, double thr, CsrT<Low>& Lt, std::vector<double
             const uint32_t i = A.col[p];
             const double a = A.val[p];
             if (i >= j) {
+                if (plan) plan->a_pos.push_back(p);
                 colThr += std::fabs(a);
                 if (!used[i]) { acc[i] = 0.0; used[i] = 1; touched[cnt++] = i; }
                 acc[i] += a;
@@ -142,6 +151,10 @@ int left_looking(const CsrHost& A, double thr, CsrT<Low>& Lt, std::vector<double
         uint32_t k = link[j];
         while (k != kNone) {
             uint32_t start = next[k];
+            if (plan) {
+                plan->up_k.push_back(k);
+                plan->up_start.push_back(start);
+            }
             const double Ljk = (double)Lt.val[start];
             const double dk = ldlt ? (*D)[k] : 0.0;
             const uint32_t stop = Lt.rowptr[k + 1];
@@ -201,6 +214,11 @@ int left_looking(const CsrHost& A, double thr, CsrT<Low>& Lt, std::vector<double
             used[i] = 0;
         }
         Lt.rowptr[j + 1] = (uint32_t)Lt.col.size();
+        if (plan) {
+            plan->a_ptr.push_back((uint32_t)plan->a_pos.size());
+            plan->up_ptr.push_back((uint32_t)plan->up_k.size());
+            plan->max_col = std::max<uint32_t>(plan->max_col, Lt.rowptr[j + 1] - Lt.rowptr[j] + (ldlt ? 1u : 0u));
+        }
     }
     return SETUP_OK;
 }
@@ -243,13 +261,14 @@ void qsplit_select(T* a, int32_t* ind, int32_t n, int32_t ncut_count) {
 }  // namespace
 
 template <typename Low>
-int ict_factor(const CsrHost& A, double threshold, CsrT<Low>& Lt, std::string* err) {
-    return left_looking<Low, false>(A, threshold, Lt, nullptr, err);
+int ict_factor(const CsrHost& A, double threshold, CsrT<Low>& Lt, std::string* err, RefactorPlan* plan) {
+    return left_looking<Low, false>(A, threshold, Lt, nullptr, err, plan);
 }
 
 template <typename Low>
-int ildlt_factor(const CsrHost& A, double tol, CsrT<Low>& Lt, std::vector<double>& D, std::string* err) {
-    return left_looking<Low, true>(A, tol, Lt, &D, err);
+int ildlt_factor(const CsrHost& A, double tol, CsrT<Low>& Lt, std::vector<double>& D, std::string* err,
+                 RefactorPlan* plan) {
+    return left_looking<Low, true>(A, tol, Lt, &D, err, plan);
 }
 
 template <typename Low>
@@ -615,6 +634,22 @@ template void ic_sweeps<float>(const CsrT<float>&, Sweep<float>&, Sweep<float>&)
 template void ildlt_sweeps<double>(const CsrT<double>&, const std::vector<double>&, Sweep<double>&, Sweep<double>&);
 template void ildlt_sweeps<float>(const CsrT<float>&, const std::vector<double>&, Sweep<float>&, Sweep<float>&);
 
+void factor_index_sweeps(const HostFactor& f, Sweep<double>& lo, Sweep<double>& up) {
+    CsrT<double> Lt;
+    Lt.n = f.f0.n;
+    Lt.rowptr = f.f0.rowptr;
+    Lt.col = f.f0.col;
+    Lt.val.resize(f.f0.col.size());
+    for (size_t e = 0; e < Lt.val.size(); ++e) Lt.val[e] = (double)e;
+    if (f.kind == 1) {
+        ic_sweeps<double>(Lt, lo, up);
+    } else {
+        std::vector<double> rows(Lt.n);
+        for (uint32_t r = 0; r < Lt.n; ++r) rows[r] = (double)r;
+        ildlt_sweeps<double>(Lt, rows, lo, up);
+    }
+}
+
 namespace {
 template <typename Low>
 int build_tri_t(int kind, const CsrHost& A, double tol, uint32_t lfill, HostFactor& F, Sweep<Low>& lo,
@@ -624,8 +659,10 @@ int build_tri_t(int kind, const CsrHost& A, double tol, uint32_t lfill, HostFact
         // IC: L^T rows hold the diagonal first.  Lower sweep = gather over L
         // (transpose of the strictly upper part), upper sweep = gather over L^T.
         CsrT<Low> Lt;
-        int rc = ict_factor<Low>(A, tol, Lt, err);
+        auto plan = std::make_shared<RefactorPlan>();
+        int rc = ict_factor<Low>(A, tol, Lt, err, plan.get());
         if (rc) return rc;
+        F.plan = plan;
         ic_sweeps<Low>(Lt, lo, up);
         F.mnnz = Lt.nnz() * 2 + n;  // IncompleteCholesky.cpp:245
         widen_csr(Lt, F.f0);
@@ -635,8 +672,10 @@ int build_tri_t(int kind, const CsrHost& A, double tol, uint32_t lfill, HostFact
         // ILDLT: unit L^T without diagonal, D separate; D^{-1} folded into the upper sweep.
         CsrT<Low> Lt;
         std::vector<double> D;
-        int rc = ildlt_factor<Low>(A, tol, Lt, D, err);
+        auto plan = std::make_shared<RefactorPlan>();
+        int rc = ildlt_factor<Low>(A, tol, Lt, D, err, plan.get());
         if (rc) return rc;
+        F.plan = plan;
         ildlt_sweeps<Low>(Lt, D, lo, up);
         F.mnnz = Lt.nnz() * 2 + n;  // IncompleteLDLT.cpp:185
         widen_csr(Lt, F.f0);
@@ -740,7 +779,7 @@ void bank_order(const std::vector<std::vector<std::pair<uint32_t, uint32_t>>>& r
 
 template <typename Low>
 bool stream_layout(const Sweep<Low>& s, const std::vector<uint32_t>& start, uint32_t max_slots, uint32_t slot_bytes,
-                   StreamLayout& out, std::string* why, StreamOrder* order) {
+                   StreamLayout& out, std::string* why, StreamOrder* order, std::vector<uint32_t>* coef_map) {
     auto fail = [&](const std::string& m) {
         if (why) *why = m;
         return false;
@@ -760,6 +799,29 @@ bool stream_layout(const Sweep<Low>& s, const std::vector<uint32_t>& start, uint
     Sweep<Low> sl;
     std::vector<uint32_t> cpos;
     slab_layout_ranges<Low>(s, start, cpos, sl);
+    // coef_map: which entry of s each entry of the slab-ordered copy is
+    std::vector<uint32_t> sweep_entry;
+    if (coef_map) {
+        coef_map->clear();
+        Sweep<double> si;
+        si.n = s.n;
+        si.op = s.op;
+        si.lower = s.lower;
+        si.num_levels = s.num_levels;
+        si.level_ptr = s.level_ptr;
+        si.order = s.order;
+        si.rowptr = s.rowptr;
+        si.col = s.col;
+        si.diag = s.diag;
+        si.level = s.level;
+        si.val.resize(s.val.size());
+        for (size_t e = 0; e < si.val.size(); ++e) si.val[e] = (double)e;
+        Sweep<double> sli;
+        std::vector<uint32_t> cp2;
+        slab_layout_ranges<double>(si, start, cp2, sli);
+        sweep_entry.resize(sli.val.size());
+        for (size_t e = 0; e < sli.val.size(); ++e) sweep_entry[e] = (uint32_t)sli.val[e];
+    }
     const uint32_t vb = (uint32_t)sizeof(Low);
     const bool recip = s.op == SWEEP_DIV || s.op == SWEEP_PREDIV;
     out = StreamLayout();
@@ -956,6 +1018,11 @@ bool stream_layout(const Sweep<Low>& s, const std::vector<uint32_t>& start, uint
                                 slot = (uint16_t)pr.first;
                                 coef = sl.val[pr.second];
                                 dep = sl.col[pr.second];
+                                if (coef_map) {
+                                    const uint64_t at = off + sec_c + 4u * vb * ((size_t)(u / 4) * rec.m + j) + vb * (u % 4);
+                                    coef_map->push_back((uint32_t)(at / vb));
+                                    coef_map->push_back(sweep_entry[pr.second]);
+                                }
                             } else {
                                 slot = (uint16_t)(-1 - e);
                                 coef = (Low)0;
@@ -1256,10 +1323,12 @@ std::string stream_layout_replay(const Sweep<Low>& s, const StreamLayout& L, con
 }
 
 // ---- explicit instantiations ------------------------------------------------
-template int ict_factor<double>(const CsrHost&, double, CsrT<double>&, std::string*);
-template int ict_factor<float>(const CsrHost&, double, CsrT<float>&, std::string*);
-template int ildlt_factor<double>(const CsrHost&, double, CsrT<double>&, std::vector<double>&, std::string*);
-template int ildlt_factor<float>(const CsrHost&, double, CsrT<float>&, std::vector<double>&, std::string*);
+template int ict_factor<double>(const CsrHost&, double, CsrT<double>&, std::string*, RefactorPlan*);
+template int ict_factor<float>(const CsrHost&, double, CsrT<float>&, std::string*, RefactorPlan*);
+template int ildlt_factor<double>(const CsrHost&, double, CsrT<double>&, std::vector<double>&, std::string*,
+                                  RefactorPlan*);
+template int ildlt_factor<float>(const CsrHost&, double, CsrT<float>&, std::vector<double>&, std::string*,
+                                 RefactorPlan*);
 template int ilut_factor<double>(const CsrHost&, uint32_t, double, CsrT<double>&, CsrT<double>&,
                                  std::vector<double>&, std::string*);
 template int ilut_factor<float>(const CsrHost&, uint32_t, double, CsrT<float>&, CsrT<float>&,
@@ -1276,9 +1345,9 @@ template void slab_layout<float>(const Sweep<float>&, uint32_t, uint32_t, std::v
 template std::vector<uint32_t> slab_ranges<double>(const Sweep<double>&, uint32_t);
 template std::vector<uint32_t> slab_ranges<float>(const Sweep<float>&, uint32_t);
 template bool stream_layout<double>(const Sweep<double>&, const std::vector<uint32_t>&, uint32_t, uint32_t,
-                                    StreamLayout&, std::string*, StreamOrder*);
+                                    StreamLayout&, std::string*, StreamOrder*, std::vector<uint32_t>*);
 template bool stream_layout<float>(const Sweep<float>&, const std::vector<uint32_t>&, uint32_t, uint32_t,
-                                   StreamLayout&, std::string*, StreamOrder*);
+                                   StreamLayout&, std::string*, StreamOrder*, std::vector<uint32_t>*);
 template std::string stream_layout_replay<double>(const Sweep<double>&, const StreamLayout&, const double*,
                                                   double*);
 template std::string stream_layout_replay<float>(const Sweep<float>&, const StreamLayout&, const double*, double*);

@@ -9,6 +9,7 @@
 #pragma once
 
 #include <cstdint>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -65,15 +66,32 @@ std::string validate_csr(uint32_t n, const uint32_t* rowptr, const uint32_t* col
 bool csr_symmetric(const CsrHost& A);
 
 // ---- incomplete factorisations ---------------------------------------------
+// The operation order of one left-looking factorisation on its own pattern, recorded
+// while it runs, so that the factor values can be computed again for new matrix values
+// on the same pattern (device numeric refactorisation) with every floating-point
+// operation in the same order.  Column j: its accumulator starts from the matrix
+// entries a_pos[a_ptr[j] .. a_ptr[j+1]) (positions in A's value array, row j with
+// column >= j, in stored order), then subtracts, for each finished column k listed in
+// up_k[up_ptr[j] .. up_ptr[j+1]) in that order, L_ik * L_jk (* D_k) over the entries of
+// column k from position up_start (L_jk) to its end.
+struct RefactorPlan {
+    uint32_t n = 0;
+    bool ldlt = false;
+    std::vector<uint32_t> a_ptr, a_pos;
+    std::vector<uint32_t> up_ptr, up_k, up_start;
+    uint32_t max_col = 0;  // longest column of the factor, diagonal included
+};
+
 // IncompleteCholesky<Low,double>::setup (source/Preconditioner/IncompleteCholesky.cpp:96-246):
 // left-looking threshold Cholesky; Lt holds L^T by rows, diagonal first.
 template <typename Low>
-int ict_factor(const CsrHost& A, double threshold, CsrT<Low>& Lt, std::string* err);
+int ict_factor(const CsrHost& A, double threshold, CsrT<Low>& Lt, std::string* err, RefactorPlan* plan = nullptr);
 
 // IncompleteLDLT<Low,double>::setup (source/Preconditioner/IncompleteLDLT.cpp:39-186):
 // unit L^T by rows without the diagonal; D (double) separately.
 template <typename Low>
-int ildlt_factor(const CsrHost& A, double tol, CsrT<Low>& Lt, std::vector<double>& D, std::string* err);
+int ildlt_factor(const CsrHost& A, double tol, CsrT<Low>& Lt, std::vector<double>& D, std::string* err,
+                 RefactorPlan* plan = nullptr);
 
 // IncompleteLU<Low,double>::setup (source/Preconditioner/IncompleteLU.cpp:38-266):
 // Saad's ILUT(lfill, tol); L unit strictly lower, U strictly upper (columns in
@@ -234,9 +252,12 @@ std::vector<uint32_t> slab_ranges(const Sweep<Low>& s, uint32_t num_ctas);
 // record holds 1 / diag and the kernel multiplies.  Returns false (and why)
 // when the sweep does not fit the record format or needs more than max_slots
 // value slots in one slab.  `order`, when given, receives the summation order.
+// `coef_map`, when given, receives one pair per coefficient written from the sweep:
+// (position in the blob in units of the factor value, index of the sweep entry).
 template <typename Low>
 bool stream_layout(const Sweep<Low>& s, const std::vector<uint32_t>& start, uint32_t max_slots, uint32_t slot_bytes,
-                   StreamLayout& out, std::string* why, StreamOrder* order = nullptr);
+                   StreamLayout& out, std::string* why, StreamOrder* order = nullptr,
+                   std::vector<uint32_t>* coef_map = nullptr);
 // Replays k_sweep_stream on the host, in its arithmetic (float for 4-byte
 // slots): stages `in` as the prep kernel does and runs each slab's rounds in
 // the kernel's pipeline order -- round r's late entries and round r + 1's
@@ -278,7 +299,12 @@ struct HostFactor {
     std::vector<double> diag;      // ILDLT: D; ILUT: Dinv
     Sweep<double> lower64, upper64;
     Sweep<float> lower32, upper32;
+    std::shared_ptr<const RefactorPlan> plan;  // IC / ILDLT: the factorisation's operation order
 };
+// The two sweeps of an IC / ILDLT factor's pattern whose values are the indices of the
+// factor entries they come from (entries of f0, as doubles); diag holds, per position,
+// the index of the diagonal entry (IC) or the row (ILDLT: an index into D).
+void factor_index_sweeps(const HostFactor& f, Sweep<double>& lo, Sweep<double>& up);
 
 // The two device sweeps of an IC factor (L^T with diagonal first) and of an
 // ILDLT factor (unit L^T without diagonal, pivots D).

@@ -343,6 +343,7 @@ void DevSweep::release() {
     num_ctas = rows_per_cta = smem_rows = 0;
     str_ctas = str_ring = str_meta_slots = str_slots = str_rounds = str_smem = 0;
     str_nnz = 0;
+    n = num_levels = 0;  // empty: nothing launches on a released sweep
 }
 
 template <typename Low>
@@ -611,6 +612,7 @@ int export_host_factor(const HostFactor& f, int which, uint32_t* n, uint64_t* nn
 
 int TriangularPrecond::export_factor(int which, uint32_t* n, uint64_t* nnz, uint32_t* rowptr, uint32_t* col,
                                      double* val, double* diag) const {
+    if (rf_) return export_refactored(which, n, nnz, rowptr, col, val, diag);
     return export_host_factor(*f_, which, n, nnz, rowptr, col, val, diag);
 }
 

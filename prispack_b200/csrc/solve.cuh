@@ -84,7 +84,7 @@ struct DevSweep {
     // the stream layout marks its own output pending; the others need launch_fill first
     bool self_filling() const { return layout == LAYOUT_STREAM; }
     uint64_t entries() const { return layout == LAYOUT_STREAM ? str_nnz : (fp32 ? val32.size() : val64.size()); }
-    void release();
+    void release();                // frees the arrays; n = 0 afterwards
     // the summation order of the streamed layout this sweep was uploaded with (s = the same
     // host sweep); false for the other layouts
     template <typename Low>
@@ -124,6 +124,8 @@ class Precond {
         (void)sweep; (void)o;
         return false;
     }
+    // numeric refactorisation for the operator's current values on the factor's own pattern
+    virtual void refactor() { throw Error(PRISM_ERR_UNSUPPORTED, "this preconditioner has no device refactorisation"); }
     // factor export (parity checks)
     virtual int export_factor(int which, uint32_t* n, uint64_t* nnz, uint32_t* rowptr, uint32_t* col, double* val,
                               double* diag) const {
@@ -133,6 +135,8 @@ class Precond {
 };
 
 struct Handle;
+struct RefactorState;              // device refactorisation of an IC / ILDLT factor (refactor.cu)
+void refactor_release(RefactorState* r);
 
 // IC / ILDLT / ILUT: two sweeps on the device (ILDLT's D^{-1} is folded into
 // its upper sweep).  Built from a host factor, which it keeps for export.
@@ -150,13 +154,21 @@ class TriangularPrecond : public Precond {
     bool sweep_info(int sweep, uint32_t* n, uint64_t* nnz, uint32_t* vbytes, uint32_t* levels,
                     uint32_t* kernel) const override;
     bool sweep_order(int sweep, StreamOrder& o) const override;
+    // IC / ILDLT: the factor's values recomputed on the device for the operator's current
+    // values (same pattern, the host factorisation's operation order), then written into
+    // every device layout of the two sweeps
+    void refactor() override;
 
   private:
+    int export_refactored(int which, uint32_t* n, uint64_t* nnz, uint32_t* rowptr, uint32_t* col, double* val,
+                          double* diag) const;
+    void refresh_level_copy(DevSweep& d, bool lower);
     Handle& h_;
     std::shared_ptr<const HostFactor> f_;
     DevSweep lower_, upper_;
     DevSweep lower_lv_, upper_lv_;   // level-order copies for the block sweeps when the tuner chose slabs
     DevBuf<double> tmp_, tmpk_;
+    std::unique_ptr<RefactorState, void (*)(RefactorState*)> rf_{nullptr, refactor_release};
 };
 
 // Factor export shared by the device preconditioner and the host-only factor object.

@@ -72,10 +72,12 @@ def test_noalloc_residual_norms_match_existing_entry_points():
 
     for got in results:
         for c in range(K):
-            np.testing.assert_allclose(got[2 * c], want[c][0], rtol=1e-10)
+            # column 0 is a converged solution: its residual is a difference of nearly equal
+            # vectors, so two SpMV summation orders differ by about eps * ||b||, not relative
+            np.testing.assert_allclose(got[2 * c], want[c][0], rtol=1e-10, atol=1e-13 * want[c][1])
             np.testing.assert_allclose(got[2 * c + 1], want[c][1], rtol=1e-12)
         # column 0 against the solver's own true residual
-        np.testing.assert_allclose(got[0] / got[1], st.true_rel_residual, rtol=1e-10)
+        np.testing.assert_allclose(got[0] / got[1], st.true_rel_residual, rtol=1e-10, atol=1e-13)
     # same inputs, same fixed grid and reduction order: identical bits
     assert np.array_equal(results[0], results[1])
 
