@@ -26,7 +26,10 @@ from . import (CSRMatrix, DeviceSystem, PRECOND_IC, PRISM_FP64, SOLVER_FCG)
 
 class SolveSpec:
     """How the forward and adjoint solves run: solver, tolerance, and whether the
-    preconditioner is refactored from the new values on every forward call."""
+    preconditioner is refactored from the new values on every forward call
+    (refactor=True: a new host setup; "device": the IC / ILDLT factor recomputed on
+    the device on its own pattern, prism_refactor; False: the caller's preconditioner
+    stays)."""
 
     def __init__(self, solver=SOLVER_FCG, tol=1e-12, max_iter=5000, restart=0, precond=PRECOND_IC,
                  precond_tol=1e-3, precision=PRISM_FP64, refactor=True):
@@ -42,7 +45,9 @@ def _function():
         def forward(ctx, values, b, system, spec):
             v = values.detach().contiguous()
             system.update_values(v)
-            if spec.refactor:  # otherwise the caller's preconditioner stays (a stale one still gives the exact x)
+            if spec.refactor == "device":
+                system.refactor()
+            elif spec.refactor:  # otherwise the caller's preconditioner stays (a stale one still gives the exact x)
                 system.set_precond(spec.precond, tol=spec.precond_tol, precision=spec.precision)
             x, st = system.solve(b.detach().contiguous(), solver=spec.solver, tol=spec.tol, max_iter=spec.max_iter,
                                  restart=spec.restart)
