@@ -302,7 +302,7 @@ typedef struct prism_amsed_opts {
     int32_t low_rank;         /* lowRankSize (AMSED_RANK = 16): cap of the MSLR (basic) rank */
     double eig_bound;         /* eigCorrectBound (AMSED_EIGVAL_CORRECTION = 0.8) */
     int32_t lowrank_type;     /* 0 AMSEDBasic (MSLR), 1 AMSEDEigenvalueDeflation */
-    int32_t lanczos_type;     /* 0 UseClassicLanczos (the restarted variant is not provided) */
+    int32_t lanczos_type;     /* 0 UseClassicLanczos, 1 UseRestartLanczos (Krylov-Schur, up to 3 restarts) */
     int32_t reorder;          /* 0 MatrixReorderNo, 2 MatrixReorderRCM (AMD is not provided) */
     double factor_tol;        /* AMSED_FACTOR_TOLRANCE = 1e-3 */
     uint32_t minsep;          /* AMSED_MINSEP = 3 */

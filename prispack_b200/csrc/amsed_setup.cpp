@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <limits>
 #include <numeric>
 #include <random>
 
@@ -406,15 +407,31 @@ double dot_host(size_t n, const double* a, const double* b) {
 }
 
 // Eigen-decomposition of the symmetric tridiagonal matrix (diagonal d[0..m),
-// off-diagonal e[0..m-1)): implicit-shift QL with Givens rotations accumulated
-// into the eigenvector matrix; eigenvalues returned ascending, eigenvectors as
-// unit columns of Y (column-major, m x m).  Same contract as LAPACK dstevx with
-// RANGE = 'A' (AMSEDPrecondition.cpp:975-1006); eigenvectors are unique up to
-// sign, which the correction W H W^T does not see.
-void tridiag_eig(int m, const double* d_in, const double* e_in, double* mu, double* Y) {
-    std::vector<double> d(d_in, d_in + m), e(m, 0.0), z((size_t)m * m, 0.0);
+// off-diagonal e[0..m-1)), with the contract of LAPACK dstevx, RANGE = 'A'
+// (AMSEDPrecondition.cpp:975-1006): eigenvalues ascending in mu, unit
+// eigenvectors as the columns of Y (column-major, m x m), the first component of
+// largest magnitude of each made positive (the sign dstevx's inverse iteration,
+// dstein, leaves).  Eigenvalues by implicit-shift QL.
+//
+// Eigenvectors: with inverse_iteration false, from the QL rotations accumulated
+// (accurate to eps |T| in each component).  With inverse_iteration true, by
+// inverse iteration on T - mu_j I, the method dstevx uses with a positive
+// ABSTOL: an LU factorisation with partial pivoting (zero pivots replaced by
+// eps |T|), four solves from a fixed start, each followed, inside a cluster
+// (eigenvalues closer than 1e-3 |T|_1), by modified Gram-Schmidt against the
+// cluster's earlier vectors.  Inverse iteration gives the small components of an
+// eigenvector to high relative accuracy; the restarted Lanczos builds its Givens
+// rotations from the last components of converged Ritz vectors, 1e-20 and below,
+// and needs them.  The classic process only compares those components with
+// 1e-15 / |beta_k|; there the accumulated rotations are kept.
+void tridiag_eig(int m, const double* d_in, const double* e_in, double* mu, double* Y, bool inverse_iteration) {
+    if (m <= 0) return;
+    std::vector<double> d(d_in, d_in + m), e(m, 0.0), z;
     for (int i = 0; i + 1 < m; ++i) e[i] = e_in[i];
-    for (int i = 0; i < m; ++i) z[(size_t)i * m + i] = 1.0;
+    if (!inverse_iteration) {
+        z.assign((size_t)m * m, 0.0);
+        for (int i = 0; i < m; ++i) z[(size_t)i * m + i] = 1.0;
+    }
     for (int l = 0; l < m; ++l) {
         for (int iter = 0; iter < 60; ++iter) {
             int k = l;
@@ -446,10 +463,12 @@ void tridiag_eig(int m, const double* d_in, const double* e_in, double* mu, doub
                 p = s * r;
                 d[i + 1] = g + p;
                 g = c * r - b;
-                for (int q = 0; q < m; ++q) {  // rotate columns i, i+1 of z
-                    f = z[(size_t)(i + 1) * m + q];
-                    z[(size_t)(i + 1) * m + q] = s * z[(size_t)i * m + q] + c * f;
-                    z[(size_t)i * m + q] = c * z[(size_t)i * m + q] - s * f;
+                if (!inverse_iteration) {
+                    for (int q = 0; q < m; ++q) {  // rotate columns i, i+1 of z
+                        f = z[(size_t)(i + 1) * m + q];
+                        z[(size_t)(i + 1) * m + q] = s * z[(size_t)i * m + q] + c * f;
+                        z[(size_t)i * m + q] = c * z[(size_t)i * m + q] - s * f;
+                    }
                 }
             }
             if (r == 0.0 && i >= l) continue;
@@ -461,9 +480,108 @@ void tridiag_eig(int m, const double* d_in, const double* e_in, double* mu, doub
     std::vector<int> idx(m);
     std::iota(idx.begin(), idx.end(), 0);
     std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return d[a] < d[b]; });
+    for (int j = 0; j < m; ++j) mu[j] = d[idx[j]];
+    auto store = [&](int j, const double* v) {  // with dstein's sign
+        int big = 0;
+        for (int q = 1; q < m; ++q)
+            if (std::fabs(v[q]) > std::fabs(v[big])) big = q;
+        const double sg = v[big] < 0 ? -1.0 : 1.0;
+        for (int q = 0; q < m; ++q) Y[(size_t)j * m + q] = sg * v[q];
+    };
+    if (!inverse_iteration) {
+        for (int j = 0; j < m; ++j) store(j, z.data() + (size_t)idx[j] * m);
+        return;
+    }
+
+    const double eps = std::numeric_limits<double>::epsilon();
+    double tnorm = 0.0;  // |T|_1
+    for (int i = 0; i < m; ++i) {
+        const double col = std::fabs(d_in[i]) + (i > 0 ? std::fabs(e_in[i - 1]) : 0.0) +
+                           (i + 1 < m ? std::fabs(e_in[i]) : 0.0);
+        tnorm = std::max(tnorm, col);
+    }
+    const double ortol = 1e-3 * tnorm, tiny = eps * std::max(tnorm, std::numeric_limits<double>::min());
+    std::vector<double> dg(m), du(m), du2(m), ml(m), x(m);
+    std::vector<char> swp(m);
+    int cluster = 0;
+    double prev = 0.0;
     for (int j = 0; j < m; ++j) {
-        mu[j] = d[idx[j]];
-        for (int q = 0; q < m; ++q) Y[(size_t)j * m + q] = z[(size_t)idx[j] * m + q];
+        double lam = mu[j];
+        if (j > 0) {
+            if (mu[j] - mu[j - 1] > ortol) cluster = j;
+            const double pert = 10.0 * std::fabs(eps * lam);  // separate equal shifts
+            if (lam - prev < pert) lam = prev + pert;
+        }
+        prev = lam;
+        // T - lam I = P L U, U with two superdiagonals
+        for (int i = 0; i < m; ++i) {
+            dg[i] = d_in[i] - lam;
+            du[i] = i + 1 < m ? e_in[i] : 0.0;
+            du2[i] = 0.0;
+        }
+        for (int i = 0; i + 1 < m; ++i) {
+            const double sub = e_in[i];
+            if (std::fabs(dg[i]) >= std::fabs(sub)) {
+                swp[i] = 0;
+                if (dg[i] == 0.0) dg[i] = tiny;
+                ml[i] = sub / dg[i];
+                dg[i + 1] -= ml[i] * du[i];
+            } else {
+                swp[i] = 1;
+                ml[i] = dg[i] / sub;
+                dg[i] = sub;
+                const double t = dg[i + 1];
+                dg[i + 1] = du[i] - ml[i] * t;
+                if (i + 2 < m) {
+                    du2[i] = du[i + 1];
+                    du[i + 1] = -ml[i] * du[i + 1];
+                }
+                du[i] = t;
+            }
+        }
+        for (int i = 0; i < m; ++i)
+            if (std::fabs(dg[i]) < tiny) dg[i] = dg[i] < 0 ? -tiny : tiny;
+        uint32_t lcg = 12345u + 7919u * (uint32_t)j;  // fixed start in [-1, 1)
+        for (int i = 0; i < m; ++i) {
+            lcg = lcg * 1664525u + 1013904223u;
+            x[i] = (double)(lcg >> 8) / 8388608.0 - 1.0;
+        }
+        for (int it = 0; it < 4; ++it) {
+            for (int i = 0; i + 1 < m; ++i) {
+                if (swp[i]) {
+                    const double t = x[i];
+                    x[i] = x[i + 1];
+                    x[i + 1] = t - ml[i] * x[i];
+                } else {
+                    x[i + 1] -= ml[i] * x[i];
+                }
+            }
+            for (int i = m - 1; i >= 0; --i) {
+                double v = x[i];
+                if (i + 1 < m) v -= du[i] * x[i + 1];
+                if (i + 2 < m) v -= du2[i] * x[i + 2];
+                x[i] = v / dg[i];
+            }
+            for (int q = cluster; q < j; ++q) {
+                const double* yq = Y + (size_t)q * m;
+                double dot = 0.0;
+                for (int i = 0; i < m; ++i) dot += yq[i] * x[i];
+                for (int i = 0; i < m; ++i) x[i] -= dot * yq[i];
+            }
+            double nrm = 0.0, big = 0.0;
+            for (int i = 0; i < m; ++i) big = std::max(big, std::fabs(x[i]));
+            if (big == 0.0) {
+                x[j] = 1.0;
+                big = 1.0;
+            }
+            for (int i = 0; i < m; ++i) {
+                x[i] /= big;
+                nrm += x[i] * x[i];
+            }
+            nrm = std::sqrt(nrm);
+            for (int i = 0; i < m; ++i) x[i] /= nrm;
+        }
+        store(j, x.data());
     }
 }
 }  // namespace
@@ -586,7 +704,7 @@ void classic_lanczos(AmsedSetup<Low>& S, int level, const AmsedOptions& opt, uns
     }
     S.lanczos_steps_done[level] = actual;
     std::vector<double> mu(actual), Y((size_t)actual * actual);
-    tridiag_eig(actual, D.data(), E.data(), mu.data(), Y.data());
+    tridiag_eig(actual, D.data(), E.data(), mu.data(), Y.data(), false);
     // converged Ritz pairs: |beta_k| |Y(last, i)| <= AMSED_EXIT_ZERO
     std::vector<int> conv;
     const double betak = E[actual - 1];
@@ -630,6 +748,244 @@ void classic_lanczos(AmsedSetup<Low>& S, int level, const AmsedOptions& opt, uns
     S.mnnz += lr;
     S.lowrank_nnz += lr;
 }
+
+// The low-rank terms of a level from its converged Ritz pairs (AMSEDPrecondition.cpp:1204-1267):
+// the top m of mu (ascending), W = V Y over the `actual` Lanczos vectors.
+template <typename Low>
+void lowrank_from_ritz(AmsedSetup<Low>& S, AmsedLevel<Low>& L, const AmsedOptions& opt, uint32_t nr, int actual,
+                       const std::vector<double>& mu, const std::vector<double>& Y, const std::vector<double>& V) {
+    const int m = opt.lowrank_type == 0 ? std::min(actual, opt.low_rank) : actual;
+    std::vector<int> chosen;
+    L.H.clear();
+    if (opt.lowrank_type == 0) {
+        for (int i = 0; i < m; ++i) {
+            const int idx = actual - i - 1;
+            chosen.push_back(idx);
+            L.H.push_back(mu[idx] / (1.0 - mu[idx]));
+        }
+    } else {
+        const double eps = opt.eig_bound, para = 1.0 - eps;
+        int count = 0;
+        for (int i = 0; i < m; ++i) {
+            if (mu[actual - i - 1] <= para || count >= opt.lanczos_steps) break;
+            ++count;
+        }
+        for (int i = 0; i < count; ++i) {
+            const int idx = actual - i - 1;
+            chosen.push_back(idx);
+            const double lambda = 1.0 - mu[idx];
+            L.H.push_back((eps - lambda) / lambda);
+        }
+    }
+    const uint32_t r = (uint32_t)chosen.size();
+    L.rank = r;
+    L.rank_reported = r;
+    L.W.assign((size_t)nr * r, 0.0);
+    for (uint32_t i = 0; i < r; ++i) {
+        double* wc = L.W.data() + (size_t)i * nr;
+        const double* yc = Y.data() + (size_t)chosen[i] * actual;
+        for (int c = 0; c < actual; ++c) {
+            const double* vc = V.data() + (size_t)c * nr;
+            for (uint32_t j = 0; j < nr; ++j) wc[j] += vc[j] * yc[c];
+        }
+    }
+    const uint64_t lr = 2ull * r * nr + r;
+    S.mnnz += lr;
+    S.lowrank_nnz += lr;
+}
+
+// expandReorthogonalLanczos (AMSEDPrecondition.cpp:1275-1351): steps from..to-1 of the
+// generalized Lanczos process with full reorthogonalization, V and Z column-major (nr).
+template <typename Low>
+void expand_lanczos(AmsedSetup<Low>& S, int level, std::vector<double>& D, std::vector<double>& E,
+                    std::vector<double>& V, std::vector<double>& Z, int from, int to, int& actual) {
+    const AmsedLevel<Low>& L = S.levels[level];
+    const uint32_t n_local = S.lev_ptr[level + 1] - S.lev_ptr[level];
+    const uint32_t nr = S.n - S.lev_ptr[level + 1];
+    std::vector<double> u(nr), w(nr), ut(n_local);
+    actual = from;
+    size_t vs = (size_t)from * nr;  // V(:, i)
+    for (int i = from; i < to; ++i) {
+        if (E[i - 1] <= 1e-15) return;  // AMSED_EXIT_ZERO
+        ++actual;
+        spmv_host(L.E, V.data() + vs, ut.data());
+        amsed_block_solve_host(S, level, ut.data());
+        std::fill(u.begin(), u.end(), 0.0);
+        spmv_t_add_host(L.E, ut.data(), u.data());
+        for (uint32_t j = 0; j < nr; ++j) u[j] = u[j] + (-1.0 * E[i - 1]) * Z[vs - nr + j];
+        D[i] = dot_host(nr, u.data(), V.data() + vs);
+        for (uint32_t j = 0; j < nr; ++j) u[j] = u[j] + (-1.0 * D[i]) * Z[vs + j];
+        size_t ro = 0;
+        for (int q = 0; q <= i; ++q) {  // full reorthogonalization: u -= Z(:, 1:i) (V(:, 1:i)' u)
+            const double coef = dot_host(nr, V.data() + ro, u.data());
+            for (uint32_t j = 0; j < nr; ++j) u[j] = u[j] + (-1.0 * coef) * Z[ro + j];
+            ro += nr;
+        }
+        w = u;
+        amsed_c_solve_host(S, level, w.data(), nr);
+        E[i] = dot_host(nr, w.data(), u.data());
+        if (E[i] < 0) {  // inexact B and C solves: stop
+            E[i] = 1e-15;
+            break;
+        }
+        E[i] = std::sqrt(E[i]);
+        if (E[i] <= 1e-15) break;
+        const double inv = 1.0 / E[i];
+        for (uint32_t j = 0; j < nr; ++j) {
+            V[vs + nr + j] = w[j] * inv;
+            Z[vs + nr + j] = u[j] * inv;
+        }
+        vs += nr;
+    }
+}
+
+// implicitRestartKrylovSchurLanczosForGeneralizedEigenvaluesProblem
+// (AMSEDPrecondition.cpp:1010-1274): 2r Lanczos steps, then up to three restarts, each
+// expanding to 4r steps, keeping the 2r largest Ritz pairs and bringing their
+// tridiagonal form back with Givens rotations (convertDiagonal2TriDiagonal, :1381-1468;
+// the rotations are applied as the reference applies them, each one to the rotated
+// columns' values before any rotation, transposedGivensApplied2Columns, :1470-1490).
+template <typename Low>
+void restart_lanczos(AmsedSetup<Low>& S, int level, const AmsedOptions& opt, unsigned seed) {
+    AmsedLevel<Low>& L = S.levels[level];
+    const uint32_t n_local = S.lev_ptr[level + 1] - S.lev_ptr[level];
+    const uint32_t nr = S.n - S.lev_ptr[level + 1];
+    const int ms = opt.low_rank * 2, ks = opt.low_rank * 4, restarts = 3, maxs = opt.low_rank * 5;
+    L.rank = 0;
+    L.H.clear();
+    L.W.clear();
+    if (L.E.nnz() == 0) return;
+    std::vector<double> D(maxs, 0.0), E(maxs, 0.0), V((size_t)nr * maxs, 0.0), auxV((size_t)nr * maxs, 0.0),
+        Z((size_t)nr * maxs, 0.0), auxZ((size_t)nr * maxs, 0.0), Y((size_t)maxs * maxs, 0.0), mu(maxs, 0.0);
+    std::vector<double> u(nr, 0.0), w(nr), ut(n_local), lastY(ms);
+    {
+        // generateArrayRandom1D, seeded as in the classic process
+        std::default_random_engine gen(seed);
+        std::uniform_real_distribution<float> dist(-1.0, 1.0);
+        for (uint32_t i = 0; i < nr; ++i) V[i] = dist(gen);
+    }
+    {  // v1 = v / sqrt(v' C v)  (CSRMatrix::getMatrixNorm)
+        double sum = 0.0;
+        for (uint32_t r = 0; r < nr; ++r) {
+            double cs = 0.0;
+            for (uint32_t k = L.C.rowptr[r]; k < L.C.rowptr[r + 1]; ++k) cs += L.C.val[k] * V[L.C.col[k]];
+            sum += V[r] * cs;
+        }
+        const double scale = 1.0 / std::sqrt(sum);
+        for (uint32_t i = 0; i < nr; ++i) V[i] *= scale;
+    }
+    spmv_host(L.C, V.data(), Z.data());  // z1 = C v1
+    spmv_host(L.E, V.data(), ut.data());
+    amsed_block_solve_host(S, level, ut.data());
+    spmv_t_add_host(L.E, ut.data(), u.data());
+    D[0] = dot_host(nr, u.data(), V.data());
+    for (uint32_t j = 0; j < nr; ++j) u[j] = u[j] + (-1.0 * D[0]) * Z[j];
+    const double co = dot_host(nr, u.data(), V.data());
+    for (uint32_t j = 0; j < nr; ++j) u[j] = u[j] + (-1.0 * co) * Z[j];
+    w = u;
+    amsed_c_solve_host(S, level, w.data(), nr);
+    E[0] = std::sqrt(dot_host(nr, w.data(), u.data()));
+    {
+        const double inv = 1.0 / E[0];
+        for (uint32_t j = 0; j < nr; ++j) {
+            V[nr + j] = w[j] * inv;
+            Z[nr + j] = u[j] * inv;
+        }
+    }
+    int actual = 0;
+    expand_lanczos(S, level, D, E, V, Z, 1, ms, actual);
+    for (int rs = 0; rs < restarts; ++rs) {
+        if (actual < ms) {  // ended early: no restart
+            tridiag_eig(actual, D.data(), E.data(), mu.data(), Y.data(), true);
+            break;
+        }
+        expand_lanczos(S, level, D, E, V, Z, ms, ks, actual);
+        const int last = actual - 1;
+        const double betak = E[last];
+        tridiag_eig(actual, D.data(), E.data(), mu.data(), Y.data(), true);
+        if (std::fabs(betak) * std::fabs(Y[(size_t)last * actual + last]) <= 1e-30 || rs == restarts - 1) break;
+        // eigenpairs in descending order
+        for (int e = 0; e < actual / 2; ++e) {
+            const int p = actual - 1 - e;
+            std::swap(mu[e], mu[p]);
+            for (int q = 0; q < actual; ++q) std::swap(Y[(size_t)e * actual + q], Y[(size_t)p * actual + q]);
+        }
+        // auxV = V(:, 1:k) Y(:, 1:m), auxZ likewise
+        if (rs > 0) {
+            std::fill(auxV.begin(), auxV.end(), 0.0);
+            std::fill(auxZ.begin(), auxZ.end(), 0.0);
+        }
+        for (int i = 0; i < ms; ++i) {
+            double* av = auxV.data() + (size_t)i * nr;
+            double* az = auxZ.data() + (size_t)i * nr;
+            const double* yc = Y.data() + (size_t)i * actual;
+            for (int c = 0; c < actual; ++c) {
+                const size_t b = (size_t)c * nr;
+                const double yv = yc[c];
+                for (uint32_t r = 0; r < nr; ++r) {
+                    av[r] += V[b + r] * yv;
+                    az[r] += Z[b + r] * yv;
+                }
+            }
+        }
+        for (int st = 0; st < ms; ++st) lastY[st] = Y[(size_t)st * actual + last];
+        // convertDiagonal2TriDiagonal: D = mu(1:m), E = 0, then Givens rotations; each one
+        // reads columns of auxV / auxZ and writes the same columns of V / Z
+        auto rotate = [&](double c, double s, int c1, int c2) {
+            const size_t p1 = (size_t)c1 * nr, p2 = (size_t)c2 * nr;
+            for (uint32_t r = 0; r < nr; ++r) {
+                V[p1 + r] = auxV[p1 + r] * c + auxV[p2 + r] * s;
+                Z[p1 + r] = auxZ[p1 + r] * c + auxZ[p2 + r] * s;
+                V[p2 + r] = -1.0 * auxV[p1 + r] * s + auxV[p2 + r] * c;
+                Z[p2 + r] = -1.0 * auxZ[p1 + r] * s + auxZ[p2 + r] * c;
+            }
+        };
+        std::copy(mu.begin(), mu.begin() + ms, D.begin());
+        std::fill(E.begin(), E.begin() + (ms - 1), 0.0);
+        for (int i = 0; i < ms - 1; ++i) {
+            const double zi = lastY[i], zi1 = lastY[i + 1];
+            const double delta = std::sqrt(zi * zi + zi1 * zi1);
+            double c = zi1 * 1.0 / delta, s = -1.0 * zi / delta;
+            lastY[i + 1] = delta;
+            lastY[i] = 0;
+            double sc = c * c, ss = s * s, cs = c * s;
+            const double ai = D[i], bi = E[i], ai1 = D[i + 1], tr = 2 * cs * bi;
+            D[i] = sc * ai + tr + ss * ai1;
+            E[i] = -1.0 * cs * ai + (sc - ss) * bi + cs * ai1;
+            D[i + 1] = ss * ai - tr + sc * ai1;
+            rotate(c, s, i, i + 1);
+            if (i > 0) {
+                double gamma = -1.0 * s * E[i - 1];
+                E[i - 1] *= c;
+                for (int r = i; r >= 1; --r) {
+                    const double arm = D[r - 1], brm = E[r - 1], br = E[r], ar = D[r];
+                    const double sigma = std::sqrt(gamma * gamma + br * br);
+                    c = br * 1.0 / sigma;
+                    s = -1.0 * gamma / sigma;
+                    sc = c * c;
+                    ss = s * s;
+                    cs = c * s;
+                    const double t2 = 2 * cs * brm;
+                    D[r - 1] = sc * arm + t2 + ss * ar;
+                    E[r - 1] = -1.0 * cs * arm + (sc - ss) * brm + cs * ar;
+                    D[r] = ss * arm - t2 + sc * ar;
+                    E[r] = sigma;
+                    if (r > 1) {
+                        gamma = -1.0 * s * E[r - 2];
+                        E[r - 2] *= c;
+                    }
+                    rotate(c, s, r - 1, r);
+                }
+            }
+        }
+        E[ms - 1] = lastY[ms - 1] * betak;
+        // v_{k+1} and z_{k+1} become columns m + 1
+        std::copy(V.begin() + (size_t)actual * nr, V.begin() + (size_t)(actual + 1) * nr, V.begin() + (size_t)ms * nr);
+        std::copy(Z.begin() + (size_t)actual * nr, Z.begin() + (size_t)(actual + 1) * nr, Z.begin() + (size_t)ms * nr);
+    }
+    S.lanczos_steps_done[level] = actual;
+    lowrank_from_ritz(S, L, opt, nr, actual, mu, Y, V);
+}
 }  // namespace
 
 template <typename Low>
@@ -639,8 +995,8 @@ int amsed_setup(const CsrHost& A, const AmsedOptions& opt, AmsedSetup<Low>& S, s
         return SETUP_BAD_INPUT;
     }
     const bool gmslr = opt.family == 4;
-    if (!gmslr && opt.lanczos_type != 0) {
-        if (err) *err = "only the classic generalized Lanczos (UseClassicLanczos) is provided";
+    if (!gmslr && opt.lanczos_type != 0 && opt.lanczos_type != 1) {
+        if (err) *err = "lanczos_type must be 0 (UseClassicLanczos) or 1 (UseRestartLanczos)";
         return SETUP_BAD_INPUT;
     }
     if (opt.reorder != 0 && opt.reorder != 2) {
@@ -770,7 +1126,8 @@ int amsed_setup(const CsrHost& A, const AmsedOptions& opt, AmsedSetup<Low>& S, s
             S.mnnz += m;
             S.incomp_nnz += m;
         }
-        classic_lanczos(S, level, opt, (unsigned)(opt.seed + call));
+        if (opt.lanczos_type == 1) restart_lanczos(S, level, opt, (unsigned)(opt.seed + call));
+        else classic_lanczos(S, level, opt, (unsigned)(opt.seed + call));
         ++call;
     }
     return SETUP_OK;

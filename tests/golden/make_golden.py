@@ -50,11 +50,14 @@ CASES = [
 ]
 SEED = 20241116
 AMSED_SEED = 20241116
-# (name, grid, levels, lanczos steps, low rank, lowrank type (0 MSLR, 1 deflation), FP32 factors)
+# (name, grid, levels, lanczos steps, low rank, lowrank type (0 MSLR, 1 deflation), FP32 factors,
+#  Lanczos type (0 classic, 1 restarted Krylov-Schur))
 AMSED_CASES = [
-    ("amsed_12c_mslr", (12, 12, 12), 3, 30, 16, 0, False),
-    ("amsed_16c_defl32", (16, 16, 16), 3, 40, 20, 1, True),
-    ("amsed_40sq_l4", (40, 40, 1), 4, 30, 16, 0, False),
+    ("amsed_12c_mslr", (12, 12, 12), 3, 30, 16, 0, False, 0),
+    ("amsed_16c_defl32", (16, 16, 16), 3, 40, 20, 1, True, 0),
+    ("amsed_40sq_l4", (40, 40, 1), 4, 30, 16, 0, False, 0),
+    ("amsed_14x11x9_restart", (14, 11, 9), 3, 30, 16, 0, False, 1),
+    ("amsed_20c_defl_restart32", (20, 20, 20), 3, 30, 16, 1, True, 1),
 ]
 # (name, grid with convection, levels, lanczos steps, low rank, FP32 factors)
 GMSLR_CASES = [
@@ -164,15 +167,15 @@ def basic(manifest):
 def amsed_section(manifest):
     """AMSED / MSLR (reference AMSEDPrecondition behind the METIS stand-in)."""
     amsed = {}
-    for name, grid, levels, steps, rank, ltype, low in AMSED_CASES:
+    for name, grid, levels, steps, rank, ltype, low, lanczos in AMSED_CASES:
         A = ref.RefCSR.laplacian(*grid)
         rp, ci, v = A.arrays()
         n = len(rp) - 1
-        R = ref.RefAmsed(A, levels, steps, rank, 0.8, 2, ltype, 0, low, seed=AMSED_SEED)
+        R = ref.RefAmsed(A, levels, steps, rank, 0.8, 2, ltype, lanczos, low, seed=AMSED_SEED)
         assert R.setup() == 0
         inf = R.info()
         entry = {"grid": grid, "levels": levels, "lanczos_steps": steps, "low_rank": rank, "lowrank_type": ltype,
-                 "fp32": low, "seed": AMSED_SEED, "nlev": inf["nlev"], "lev_ptr": inf["lev_ptr"].tolist(),
+                 "lanczos_type": lanczos, "fp32": low, "seed": AMSED_SEED, "nlev": inf["nlev"], "lev_ptr": inf["lev_ptr"].tolist(),
                  "ncomps": inf["ncomps"].tolist(), "ranks": inf["ranks"].tolist(), "mnnz": inf["mnnz"],
                  "perm_sha": digest(R.perm()), "blocks": {}}
         for lv in range(inf["nlev"]):

@@ -11,7 +11,7 @@ import prispack_b200 as P
 from oracle import oracle as orc
 from oracle import ref
 
-CASES = ["amsed_12c_mslr", "amsed_16c_defl32", "amsed_40sq_l4"]
+CASES = ["amsed_12c_mslr", "amsed_16c_defl32", "amsed_40sq_l4", "amsed_14x11x9_restart", "amsed_20c_defl_restart32"]
 
 
 def sha(*arrays):
@@ -24,7 +24,7 @@ def sha(*arrays):
 def build(entry):
     A = P.CSRMatrix.laplacian(*entry["grid"])
     H = P.HostAmsed(A, levels=entry["levels"], lanczos_steps=entry["lanczos_steps"], low_rank=entry["low_rank"],
-                    lowrank_type=entry["lowrank_type"], seed=entry["seed"],
+                    lowrank_type=entry["lowrank_type"], lanczos_type=entry.get("lanczos_type", 0), seed=entry["seed"],
                     precision=P.PRISM_FP32 if entry["fp32"] else P.PRISM_FP64)
     return A, H
 
@@ -105,7 +105,54 @@ def test_live_reference_amsed(grid, levels, lt, low):
             assert all(np.array_equal(x, y) for x, y in zip(a[:3], c[:3]))
     v = np.random.default_rng(4).standard_normal(A.n)
     ra = R.apply(v)
-    # W comes from each side's own tridiagonal eigen-solver (LAPACK dstevx vs the product's QL):
-    # within clusters of close Ritz values the eigenvectors may rotate, so the apply agrees to
-    # the accuracy of the Ritz pairs rather than to rounding.
+    # W comes from each side's own tridiagonal eigen-solver (LAPACK dstevx vs the product's QL
+    # eigenvalues with inverse-iteration eigenvectors): within clusters of close Ritz values the
+    # eigenvectors may rotate, so the apply agrees to the accuracy of the Ritz pairs rather than
+    # to rounding.
     assert np.abs(orc.Amsed(H).apply(v) - ra).max() / np.abs(ra).max() < 1e-8
+
+
+def random_spd(nx, ny, nz, seed):
+    """A 7-point pattern with symmetric random off-diagonal weights: no symmetric degeneracy."""
+    A = P.CSRMatrix.laplacian(nx, ny, nz)
+    rng = np.random.default_rng(seed)
+    rows = np.repeat(np.arange(A.n), np.diff(A.rowptr))
+    v = A.val.copy()
+    off = rows != A.col
+    key = np.minimum(rows, A.col).astype(np.int64) * A.n + np.maximum(rows, A.col)
+    uniq, inv = np.unique(key, return_inverse=True)
+    v[off] *= rng.uniform(0.3, 1.0, len(uniq))[inv][off]
+    return P.CSRMatrix(A.rowptr, A.col, v)
+
+
+@pytest.mark.skipif(not ref.available(), reason="reference build (oracle/_ref) not present")
+@pytest.mark.parametrize("grid,levels,lt,low,rand", [((14, 11, 9), 3, 0, False, True), ((30, 30, 1), 3, 1, False, True),
+                                                      ((20, 20, 20), 3, 1, True, False),
+                                                      ((64, 48, 1), 5, 0, False, True),
+                                                      ((64, 48, 1), 5, 0, False, False)])
+def test_live_reference_restarted_lanczos(grid, levels, lt, low, rand):
+    """UseRestartLanczos (AMSEDPrecondition.cpp:1010-1274) against the reference build.
+
+    The reference applies each Givens rotation of its restart to the Ritz vectors as they
+    were before any rotation (transposedGivensApplied2Columns reads the other buffer), so its
+    low-rank W depends on the last components of converged Ritz vectors (1e-20 and below):
+    the product computes those by inverse iteration, as dstevx does, and the low-rank terms,
+    level by level, and the apply agree to rounding."""
+    A = random_spd(*grid, 3) if rand else P.CSRMatrix.laplacian(*grid)
+    H = P.HostAmsed(A, levels=levels, lanczos_steps=30, low_rank=16, lowrank_type=lt, lanczos_type=1,
+                    precision=P.PRISM_FP32 if low else P.PRISM_FP64)
+    R = ref.RefAmsed(ref.RefCSR.from_arrays(A.rowptr, A.col, A.val), levels, 30, 16, 0.8, 2, lt, 1, low)
+    assert R.setup() == 0
+    ri, pi = R.info(), H.info()
+    assert np.array_equal(ri["ranks"], pi["ranks"]) and ri["mnnz"] == pi["mnnz"]
+    assert ri["ranks"].max() > 0
+    for lv in range(ri["nlev"] - 1):
+        (rw, rh), (hw, hh) = R.lowrank(lv), H.lowrank(lv)
+        if len(rh) == 0:
+            continue
+        np.testing.assert_allclose(np.sort(hh), np.sort(rh), rtol=1e-12, atol=1e-14 * np.abs(rh).max())
+        Mr, Mh = (rw * rh) @ rw.T, (hw * hh) @ hw.T
+        assert np.abs(Mh - Mr).max() <= 1e-11 * np.abs(Mr).max(), lv
+    v = np.random.default_rng(4).standard_normal(A.n)
+    ra = R.apply(v)
+    assert np.abs(orc.Amsed(H).apply(v) - ra).max() <= 1e-11 * np.abs(ra).max()

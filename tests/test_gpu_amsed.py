@@ -12,7 +12,8 @@ from oracle import oracle as orc
 
 pytestmark = pytest.mark.gpu
 
-CASES = ["amsed_12c_mslr", "amsed_16c_defl32", "amsed_40sq_l4"]
+# the last two build their low-rank terms with the restarted (Krylov-Schur) Lanczos
+CASES = ["amsed_12c_mslr", "amsed_16c_defl32", "amsed_40sq_l4", "amsed_14x11x9_restart", "amsed_20c_defl_restart32"]
 
 
 def rel_err(a, b):
@@ -22,7 +23,7 @@ def rel_err(a, b):
 def build(e):
     A = P.CSRMatrix.laplacian(*e["grid"])
     H = P.HostAmsed(A, levels=e["levels"], lanczos_steps=e["lanczos_steps"], low_rank=e["low_rank"],
-                    lowrank_type=e["lowrank_type"], seed=e["seed"],
+                    lowrank_type=e["lowrank_type"], lanczos_type=e.get("lanczos_type", 0), seed=e["seed"],
                     precision=P.PRISM_FP32 if e["fp32"] else P.PRISM_FP64)
     return A, H
 
