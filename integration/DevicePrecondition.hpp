@@ -99,6 +99,16 @@ class DevicePrecondition : public BasePrecondition<T> {
               vecOUT.getLength());
     }
 
+    // A's values changed on the same pattern (a new time step, a new coefficient
+    // field): copy them to the device and recompute the IC / ILDLT factor there on
+    // its own pattern (prism_refactor), instead of a new host setup.  The reference
+    // has no counterpart: it builds a new preconditioner object.
+    void refactor() {
+        setup();
+        check(prism_update_values(h_, A_->getCSRValuesPtr(0)));
+        check(prism_refactor(h_));
+    }
+
     prism_handle handle() const { return h_; }
 
   private:

@@ -11,6 +11,8 @@
 //   ic.reference   HOST::CG<double> FlexibleCG + HOST::IncompleteCholesky<double,double>(1e-3)
 //   ic.device      the same HOST::CG<double> with DevicePrecondition (IC 1e-3, FP64 factors)
 //   ic.solver      DeviceSolver (the whole FCG on the device), same preconditioner
+//   refactor.reference / refactor.device   A scaled by 1.5 on the same pattern: a new
+//                  IncompleteCholesky setup against DevicePrecondition::refactor()
 //   amsed.reference / amsed.device   the same with AMSEDPrecondition<double,double>
 //                  (3 levels, 32 Lanczos steps, rank 16, MSLR, natural local order)
 // with iteration counts, true relative residuals and the relative difference
@@ -20,7 +22,9 @@
 
 #include <cmath>
 #include <cstdio>
+#include <algorithm>
 #include <random>
+#include <vector>
 #include <string>
 
 #include "MatrixClass/CSRMatrix.h"
@@ -121,6 +125,22 @@ int main(int argc, char** argv) {
         }
         std::snprintf(buf, sizeof buf, ", \"overloads_max_diff\": [%.3e, %.3e, %.3e]", d1, d2, d3);
         out += buf;
+        // ---- new values on the same pattern (A scaled by 1.5, so IC(1e-3) keeps its pattern):
+        // a new reference setup against DevicePrecondition::refactor on the device
+        {
+            const UINT32 nnz = A->getNNZnum(0, n - 1);
+            FLOAT64* av = A->getCSRValuesPtr(0);
+            std::vector<FLOAT64> saved(av, av + nnz);
+            for (UINT32 k = 0; k < nnz; ++k) av[k] *= 1.5;
+            Vec xr2(n, memoryBase), xd2(n, memoryBase);
+            auto ic2 = std::make_shared<IncompleteCholesky<FLOAT64, FLOAT64>>(A, 1e-3);
+            out += ", " + run_cg("refactor.reference", A, ic2, *b, *xr2, nullptr);
+            dev->refactor();
+            out += ", " + run_cg("refactor.device", A, dev, *b, *xd2, &*xr2);
+            out += ", \"refactor.mnnz\": [" + std::to_string(ic2->getPreconditionNonZeroCount()) + ", " +
+                   std::to_string(dev->getPreconditionNonZeroCount()) + "]";
+            std::copy(saved.begin(), saved.end(), av);
+        }
         // ---- AMSED / MSLR
         ref_set_seed(20241116u);
         auto am = std::make_shared<AMSEDPrecondition<FLOAT64, FLOAT64>>(A, 3, 32, 16, 0.8, MatrixReorderNo,

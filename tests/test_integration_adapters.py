@@ -60,6 +60,10 @@ def test_reference_cg_with_device_preconditioner():
     assert ic_dev["true_rel_residual"] <= 1.5e-10 and ic_sol["true_rel_residual"] <= 1.5e-10
     # MInvSolve(in, out), MInvSolve(vec), MInvSolve(vec, offset), MInvSolve(in, off, out, off) agree
     assert max(d["overloads_max_diff"]) == 0.0
+    # new values on the same pattern: the device refactorisation against a new reference setup
+    rf_ref, rf_dev = d["refactor.reference"], d["refactor.device"]
+    assert rf_ref["converged"] and rf_dev["converged"] and d["refactor.mnnz"][0] == d["refactor.mnnz"][1]
+    assert abs(rf_dev["iters"] - rf_ref["iters"]) <= 1 and rf_dev["diff"] <= 1e-10
     am_ref, am_dev = d["amsed.reference"], d["amsed.device"]
     assert am_ref["converged"] and am_dev["converged"]
     assert abs(am_dev["iters"] - am_ref["iters"]) <= 1
