@@ -463,8 +463,8 @@ def bench_adjoint(args, local):
                         "1e-13; grad wrt kappa and b by the adjoint",
             "ms": round(ms, 3), "unit": "ms forward + adjoint",
             "refactor_each_step": {"ms": round(ms_rf, 3),
-                                   "grad_equal_to_factored_once": bool(np.array_equal(grads_rf[-1].cpu().numpy(),
-                                                                                      grad))},
+                                   "grad_rel_diff_to_factored_once": float(
+                                       np.abs(grads_rf[-1].cpu().numpy() - grad).max() / np.abs(grad).max())},
             "refactor": {"what": "IC(1e-3) factor of the 64^3 operator",
                          "host_factorisation_ms": round(host_factor_ms, 1), "device_refactorisation_ms": round(rf_ms, 3),
                          "speedup": round(host_factor_ms / rf_ms, 1)},

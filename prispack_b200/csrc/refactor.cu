@@ -45,7 +45,7 @@ __device__ __forceinline__ void st_release_u32(uint32_t* p, uint32_t v) {
 }
 
 struct RfArgs {
-    uint32_t n, max_col, epoch;
+    uint32_t n, max_col, smax, epoch;
     const uint32_t* lt_rowptr;
     const uint32_t* lt_col;
     const uint32_t* a_col;
@@ -55,26 +55,90 @@ struct RfArgs {
     const uint32_t* up_ptr;
     const uint32_t* up_k;
     const uint32_t* up_start;
+    const uint32_t* sched;   // the columns in order of their depth in the dependency graph
+    const uint64_t* uo;      // per column: offset of its first update entry in `slot`
+    const uint16_t* slot;    // per update entry: its row's slot in the column, or kRfDrop
     uint32_t* done;     // per column: the epoch that finished it
     int* status;        // 0, PRISM_ERR_NOT_SPD, PRISM_ERR_ZERO_PIVOT or PRISM_ERR_TIMEOUT
     int* bad_col;       // the first column that raised it
     unsigned long long wait_ns;
 };
+constexpr uint16_t kRfDrop = 0xFFFFu;  // an update entry whose row is not in the column
 
-// Column j of the factor (warp per column).  Slot 0 of the warp's shared arrays is row j
-// (the pivot); slots 1.. are the column's off-diagonal rows in increasing order.
+// Per-warp shared memory of k_refactor: the column's accumulators and rows (max_col each),
+// a chunk's products and their slots (smax each), and per update of the chunk its L_jk,
+// D_k, start and first product.
+__host__ __device__ inline size_t rf_warp_bytes(uint32_t max_col, uint32_t smax) {
+    return ((size_t)max_col * (8 + 4) + (size_t)smax * (8 + 2) + 32 * (8 + 8 + 4 + 4) + 15) & ~(size_t)15;
+}
+
+// The column of each slot's row (slot 0: row j), in increasing order, and binary search.
+struct RfCol {
+    const uint32_t* rows;
+    uint32_t m;
+    __device__ int find(uint32_t i) const {
+        uint32_t lo = 0, hi = m;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (rows[mid] < i) lo = mid + 1;
+            else hi = mid;
+        }
+        return (lo < m && rows[lo] == i) ? (int)lo : -1;
+    }
+};
+
+// Once per pattern: the slot in column j of every entry an update brings in (the entries
+// of column k from row j down), laid out column after column, update after update.
+__global__ void __launch_bounds__(kBlock) k_rf_slots(const RfArgs a, int ldlt) {
+    extern __shared__ __align__(16) unsigned char rf_smem[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint32_t* rows = reinterpret_cast<uint32_t*>(rf_smem) + (size_t)wid * a.max_col;
+    const uint32_t nwarps = gridDim.x * kRfWarps;
+    for (uint32_t j = blockIdx.x * kRfWarps + wid; j < a.n; j += nwarps) {
+        const uint32_t b = a.lt_rowptr[j], e = a.lt_rowptr[j + 1];
+        const uint32_t m = ldlt ? e - b + 1 : e - b, off0 = ldlt ? b - 1 : b;
+        for (uint32_t s = lane; s < m; s += 32) rows[s] = s == 0 ? j : a.lt_col[off0 + s];
+        __syncwarp();
+        const RfCol col{rows, m};
+        uint64_t f = a.uo[j];
+        for (uint32_t u = a.up_ptr[j]; u < a.up_ptr[j + 1]; ++u) {
+            const uint32_t k = a.up_k[u], st = a.up_start[u], c = a.lt_rowptr[k + 1] - st;
+            for (uint32_t t = lane; t < c; t += 32) {
+                const int s = col.find(a.lt_col[st + t]);
+                const_cast<uint16_t*>(a.slot)[f + t] = s < 0 ? kRfDrop : (uint16_t)s;
+            }
+            f += c;
+        }
+        __syncwarp();
+    }
+}
+
+// Column j of the factor, one warp per column, columns taken in the order of `sched`
+// (by depth in the dependency graph: a column's updates come from shallower columns, so
+// the columns in flight at any time span a few levels of the graph, not a few planes of
+// the natural order).  The updates are taken in chunks of up to
+// 32 (the lanes wait for their columns k and load L_jk, D_k in parallel) whose entries fit
+// `smax`: first every product L_ik L_jk (D_k) of the chunk into shared memory, all loads
+// independent, then the subtractions in the host's update order.
 template <typename Low, bool LDLT>
 __global__ void __launch_bounds__(kBlock) k_refactor(const RfArgs a, Low* __restrict__ lt, double* __restrict__ D) {
     extern __shared__ __align__(16) unsigned char rf_smem[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    double* acc = reinterpret_cast<double*>(rf_smem) + (size_t)wid * a.max_col;
-    uint32_t* rows = reinterpret_cast<uint32_t*>(reinterpret_cast<double*>(rf_smem) + (size_t)kRfWarps * a.max_col) +
-                     (size_t)wid * a.max_col;
+    unsigned char* base = rf_smem + (size_t)wid * rf_warp_bytes(a.max_col, a.smax);
+    double* acc = reinterpret_cast<double*>(base);
+    double* tv = acc + a.max_col;
+    double* cL = tv + a.smax;
+    double* cD = cL + 32;
+    uint32_t* rows = reinterpret_cast<uint32_t*>(cD + 32);
+    uint32_t* cst = rows + a.max_col;
+    uint32_t* coff = cst + 32;
+    uint16_t* tsl = reinterpret_cast<uint16_t*>(coff + 32);
     const uint32_t nwarps = gridDim.x * kRfWarps;
     auto fail = [&](int code, uint32_t col) {
         if (atomicCAS(a.status, 0, code) == 0) *a.bad_col = (int)col;
     };
-    for (uint32_t j = blockIdx.x * kRfWarps + wid; j < a.n; j += nwarps) {
+    for (uint32_t w = blockIdx.x * kRfWarps + wid; w < a.n; w += nwarps) {
+        const uint32_t j = a.sched[w];
         const uint32_t b = a.lt_rowptr[j], e = a.lt_rowptr[j + 1];
         // IC: the column's first entry is its diagonal; ILDLT stores none (slot 0 is row j anyway)
         const uint32_t m = LDLT ? e - b + 1 : e - b;
@@ -84,55 +148,91 @@ __global__ void __launch_bounds__(kBlock) k_refactor(const RfArgs a, Low* __rest
             acc[s] = 0.0;
         }
         __syncwarp();
-        auto find = [&](uint32_t i) -> int {
-            uint32_t lo = 0, hi = m;
-            while (lo < hi) {
-                const uint32_t mid = (lo + hi) >> 1;
-                if (rows[mid] < i) lo = mid + 1;
-                else hi = mid;
-            }
-            return (lo < m && rows[lo] == i) ? (int)lo : -1;
-        };
+        const RfCol col{rows, m};
         // the matrix entries of row j at or below the diagonal, in stored order (duplicates add up)
         if (lane == 0) {
             for (uint32_t q = a.a_ptr[j]; q < a.a_ptr[j + 1]; ++q) {
                 const uint32_t p = a.a_pos[q];
-                const int s = find(a.a_col[p]);
+                const int s = col.find(a.a_col[p]);
                 if (s >= 0) acc[s] = __dadd_rn(acc[s], a.a_val[p]);
             }
         }
         __syncwarp();
-        // the finished columns, in the host's order; each row appears once per column k
         bool ok = __all_sync(0xFFFFFFFFu, ld_relaxed_s32(a.status) == 0);  // the same in every lane
-        for (uint32_t u = a.up_ptr[j]; u < a.up_ptr[j + 1] && ok; ++u) {
-            const uint32_t k = a.up_k[u], st = a.up_start[u];
-            if (ld_acquire_u32(a.done + k) != a.epoch) {
-                const unsigned long long t0 = globaltimer_ns();
-                unsigned spins = 0;
-                while (ld_acquire_u32(a.done + k) != a.epoch) {
-                    if ((++spins & 15u) == 0u &&
-                        (ld_relaxed_s32(a.status) != 0 || globaltimer_ns() - t0 > a.wait_ns)) {
-                        ok = false;
-                        break;
+        uint64_t f0 = a.uo[j];
+        const uint32_t uend = a.up_ptr[j + 1];
+        for (uint32_t u0 = a.up_ptr[j]; u0 < uend && ok;) {
+            const uint32_t u = u0 + lane;
+            uint32_t c = 0, st = 0;
+            double L = 0.0, dk = 0.0;
+            bool mine = true;
+            if (u < uend) {
+                const uint32_t k = a.up_k[u];
+                st = a.up_start[u];
+                c = a.lt_rowptr[k + 1] - st;
+                if (ld_acquire_u32(a.done + k) != a.epoch) {
+                    const unsigned long long t0 = globaltimer_ns();
+                    unsigned spins = 0;
+                    while (ld_acquire_u32(a.done + k) != a.epoch) {
+                        if ((++spins & 15u) == 0u &&
+                            (ld_relaxed_s32(a.status) != 0 || globaltimer_ns() - t0 > a.wait_ns)) {
+                            mine = false;
+                            break;
+                        }
                     }
                 }
+                if (mine) {
+                    L = (double)lt[st];
+                    if (LDLT) dk = D[k];
+                }
             }
-            if (!__all_sync(0xFFFFFFFFu, ok)) {
+            if (!__all_sync(0xFFFFFFFFu, mine)) {
                 ok = false;
                 break;
             }
-            const double Ljk = (double)lt[st];
-            const double dk = LDLT ? D[k] : 0.0;
-            const uint32_t stop = a.lt_rowptr[k + 1];
-            for (uint32_t p = st + lane; p < stop; p += 32) {
-                const int s = find(a.lt_col[p]);
-                if (s >= 0) {
-                    const double Lik = (double)lt[p];
-                    const double t = LDLT ? __dmul_rn(__dmul_rn(Lik, Ljk), dk) : __dmul_rn(Lik, Ljk);
-                    acc[s] = __dsub_rn(acc[s], t);
-                }
+            // the chunk: the longest prefix of these updates whose entries fit smax (each
+            // update alone does: c <= max_col <= smax)
+            uint32_t incl = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+                if (lane >= o) incl += t;
+            }
+            const unsigned fit = __ballot_sync(0xFFFFFFFFu, u < uend && incl <= a.smax);
+            const int nu = __popc(fit);
+            const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, nu - 1);
+            if (lane < nu) {
+                cL[lane] = L;
+                cD[lane] = dk;
+                cst[lane] = st;
+                coff[lane] = incl - c;
             }
             __syncwarp();
+            // every product of the chunk, with its slot
+#pragma unroll 4
+            for (uint32_t t = lane; t < total; t += 32) {
+                int lo = 0, hi = nu - 1;  // the update of product t: the last coff <= t
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (coff[mid] <= t) lo = mid;
+                    else hi = mid - 1;
+                }
+                const double Lik = (double)lt[cst[lo] + (t - coff[lo])];
+                tv[t] = LDLT ? __dmul_rn(__dmul_rn(Lik, cL[lo]), cD[lo]) : __dmul_rn(Lik, cL[lo]);
+                tsl[t] = a.slot[f0 + t];
+            }
+            __syncwarp();
+            // the subtractions, update after update (a row appears once per update)
+            for (int q = 0; q < nu; ++q) {
+                const uint32_t b0 = coff[q], b1 = q + 1 < nu ? coff[q + 1] : total;
+                for (uint32_t t = b0 + lane; t < b1; t += 32) {
+                    const uint16_t sl = tsl[t];
+                    if (sl != kRfDrop) acc[sl] = __dsub_rn(acc[sl], tv[t]);
+                }
+                __syncwarp();
+            }
+            u0 += nu;
+            f0 += total;
         }
         if (!ok) {
             if (lane == 0) fail(PRISM_ERR_TIMEOUT, j);
@@ -209,6 +309,10 @@ struct SweepValueMap {
 struct RefactorState {
     uint32_t epoch = 0;
     DevBuf<uint32_t> lt_rowptr, lt_col, a_ptr, a_pos, up_ptr, up_k, up_start, done;
+    DevBuf<uint32_t> sched;   // columns by depth in the dependency graph
+    DevBuf<uint64_t> uo;      // per column: its first update entry
+    DevBuf<uint16_t> slot;    // per update entry: the slot of its row in the column
+    uint32_t smax = 0;
     DevBuf<float> lt32;
     DevBuf<double> lt64, D;
     DevBuf<int> status;       // [status, first bad column]
@@ -352,6 +456,32 @@ void TriangularPrecond::refactor() {
         R.up_start.upload(P.up_start.data(), std::max<size_t>(P.up_start.size(), 1), st);
         R.done.alloc(P.n);
         PRISM_CUDA(cudaMemsetAsync(R.done.get(), 0, (size_t)P.n * sizeof(uint32_t), st));
+        // where each column's update entries start, and (on the device, once) their slots
+        std::vector<uint64_t> uo((size_t)P.n + 1, 0);
+        for (uint32_t j = 0; j < P.n; ++j) {
+            uint64_t c = 0;
+            for (uint32_t u = P.up_ptr[j]; u < P.up_ptr[j + 1]; ++u)
+                c += F.f0.rowptr[P.up_k[u] + 1] - P.up_start[u];
+            uo[j + 1] = uo[j] + c;
+        }
+        R.uo.upload(uo.data(), uo.size(), st);
+        // depth of each column in the dependency graph (its updates come from columns k < j),
+        // and the columns ordered by depth, then index
+        std::vector<uint32_t> depth(P.n, 0), sched(std::max<uint32_t>(P.n, 1), 0);
+        uint32_t maxd = 0;
+        for (uint32_t j = 0; j < P.n; ++j) {
+            uint32_t d = 0;
+            for (uint32_t u = P.up_ptr[j]; u < P.up_ptr[j + 1]; ++u) d = std::max(d, depth[P.up_k[u]] + 1);
+            depth[j] = d;
+            maxd = std::max(maxd, d);
+        }
+        std::vector<uint32_t> start((size_t)maxd + 2, 0);
+        for (uint32_t j = 0; j < P.n; ++j) ++start[depth[j] + 1];
+        for (uint32_t d = 0; d <= maxd; ++d) start[d + 1] += start[d];
+        for (uint32_t j = 0; j < P.n; ++j) sched[start[depth[j]]++] = j;
+        R.sched.upload(sched.data(), sched.size(), st);
+        R.slot.alloc(std::max<uint64_t>(uo[P.n], 1));
+        R.smax = std::max<uint32_t>(512, (P.max_col + 31) / 32 * 32);
         const size_t nnz = std::max<size_t>(F.f0.col.size(), 1);
         if (F.fp32) R.lt32.alloc(nnz);
         else R.lt64.alloc(nnz);
@@ -370,12 +500,13 @@ void TriangularPrecond::refactor() {
         PRISM_CUDA(cudaStreamSynchronize(st));
     }
     RefactorState& R = *rf_;
-    ++R.epoch;
-    PRISM_CUDA(cudaMemsetAsync(R.status.get(), 0, 2 * sizeof(int), st));
     RfArgs a;
     a.n = P.n;
     a.max_col = std::max<uint32_t>(P.max_col, 1);
-    a.epoch = R.epoch;
+    a.smax = R.smax;
+    a.sched = R.sched.get();
+    a.uo = R.uo.get();
+    a.slot = R.slot.get();
     a.lt_rowptr = R.lt_rowptr.get();
     a.lt_col = R.lt_col.get();
     a.a_col = h_.A.col.get();
@@ -389,7 +520,19 @@ void TriangularPrecond::refactor() {
     a.status = R.status.get();
     a.bad_col = R.status.get() + 1;
     a.wait_ns = kRfWaitNs;
-    const size_t smem = (size_t)kRfWarps * a.max_col * (sizeof(double) + sizeof(uint32_t));
+    if (R.epoch == 0) {  // the slots, once per pattern
+        const size_t ssm = (size_t)kRfWarps * a.max_col * sizeof(uint32_t);
+        PRISM_CUDA(cudaFuncSetAttribute(k_rf_slots, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssm));
+        const uint64_t want = ((uint64_t)P.n + kRfWarps - 1) / kRfWarps;
+        const int g = (int)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)h_.info.sms * 4));
+        k_rf_slots<<<g, kBlock, ssm, st>>>(a, ldlt ? 1 : 0);
+        PRISM_LAUNCHED();
+        PRISM_CUDA(cudaStreamSynchronize(st));
+    }
+    ++R.epoch;
+    a.epoch = R.epoch;
+    PRISM_CUDA(cudaMemsetAsync(R.status.get(), 0, 2 * sizeof(int), st));
+    const size_t smem = (size_t)kRfWarps * rf_warp_bytes(a.max_col, a.smax);
     void* fn = F.fp32 ? (ldlt ? (void*)k_refactor<float, true> : (void*)k_refactor<float, false>)
                       : (ldlt ? (void*)k_refactor<double, true> : (void*)k_refactor<double, false>);
     PRISM_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

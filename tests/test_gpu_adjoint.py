@@ -121,7 +121,9 @@ def test_autograd_with_device_refactorisation():
     """SolveSpec(refactor="device"): each forward call recomputes the IC factor on the
     device from the new coefficients (prism_refactor) instead of a new host setup.  The
     loss and gradients equal those of a fresh host factorisation within the solve
-    tolerance, and the second call with the same coefficients is bit-identical."""
+    tolerance, and the second call with the same coefficients gives the same loss to the
+    last bit (the gradient wrt kappa passes through torch's scatter-add, whose atomic
+    order varies between runs: equal to 1e-12)."""
     import torch
     D = DiffusionPattern(10, 9, 8)
     g = gaussian_random_field(D.shape, 1.0, 2.0, seed=5)
@@ -139,7 +141,7 @@ def test_autograd_with_device_refactorisation():
 
     l1, g1 = run(SolveSpec(tol=1e-13, refactor="device"), S)
     l2, g2 = run(SolveSpec(tol=1e-13, refactor="device"), S)
-    assert l1 == l2 and np.array_equal(g1, g2)
+    assert l1 == l2 and rel_err(g1, g2) < 1e-12
     S2 = P.DeviceSystem(D.matrix(np.ones(D.n)))
     l3, g3 = run(SolveSpec(tol=1e-13, refactor=True), S2)
     assert abs(l1 - l3) <= 1e-10 * abs(l3)
