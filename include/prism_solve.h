@@ -191,6 +191,20 @@ int32_t prism_stream_sweep_order(uint32_t n, const uint32_t* rowptr, const uint3
                                  double* kcoef);
 /* Runs the streamed sweep kernel alone on `device` for the same sweep and
  * slabs as prism_stream_sweep_order (host in and out): out = T^{-1} in. */
+/* Wavefront pairing of a gather-form sweep (host only): the same solve in
+ * about half as many wavefronts.  A row on an odd wavefront 2R+1 has its
+ * dependencies on wavefront 2R substituted by their own rows, so the paired
+ * sweep T' (prow/pcol/pval, gather form, the rows' dependencies in increasing
+ * order) and the right-hand side map M (mptr/mdep/mcoef) satisfy
+ *   T^{-1} b = T'^{-1} b',  b'_r = b_r - sum m b_dep, in stored order, one
+ * fused multiply-add each, in double.  *pnnz and *mnnz receive the sizes; pass
+ * NULL arrays to query them.  The values are computed in double and rounded to
+ * the precision's value type (float unless PRISM_FP64).  No reference
+ * counterpart: the reference's sweeps run row by row. */
+int32_t prism_stream_sweep_pair(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val,
+                                const double* diag, int32_t op, int32_t lower, int32_t precision, uint64_t* pnnz,
+                                uint32_t* prow, uint32_t* pcol, double* pval, uint64_t* mnnz, uint32_t* mptr,
+                                uint32_t* mdep, double* mcoef);
 int32_t prism_stream_sweep_run(int32_t device, uint32_t n, const uint32_t* rowptr, const uint32_t* col,
                                const double* val, const double* diag, int32_t op, int32_t lower, int32_t precision,
                                uint32_t num_ctas, const double* in, double* out);
@@ -371,6 +385,12 @@ int32_t prism_precond_sweep_info(prism_handle h, int32_t sweep, uint32_t* n, uin
 int32_t prism_precond_sweep_order(prism_handle h, int32_t sweep, uint32_t* n, uint32_t* eptr, uint32_t* edep,
                                   double* ecoef, uint32_t* kptr, uint32_t* kdep, double* kcoef, double* diag,
                                   int32_t* op, int32_t* lower);
+/* The right-hand side map of a streamed sweep the autotuner kept paired (see
+ * prism_stream_sweep_pair; the order above is then the paired sweep's):
+ * *paired 1 or 0, *mnnz its entries (0 when not paired), mptr (n + 1), mdep and
+ * mcoef filled when not NULL. */
+int32_t prism_precond_sweep_rhs_map(prism_handle h, int32_t sweep, int32_t* paired, uint64_t* mnnz, uint32_t* mptr,
+                                    uint32_t* mdep, double* mcoef);
 
 /* ---- solvers ------------------------------------------------------------- */
 /* x is the in/out initial guess, as BaseSolver::solve (BaseSolver.h:16). */

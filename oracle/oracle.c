@@ -88,6 +88,18 @@ void orc_sweep_f32(uint32_t n, const uint32_t* rowptr, const uint32_t* col, cons
     free(x);
 }
 
+/* The right-hand side of a paired sweep (the library's wavefront pairing, no
+ * reference counterpart): out[r] = in[r] - sum m in[dep] over [mptr[r],
+ * mptr[r+1]), in stored order, each step one fused multiply-add in double. */
+void orc_pair_rhs(uint32_t n, const uint32_t* mptr, const uint32_t* mdep, const double* mcoef, const double* in,
+                  double* out) {
+    for (uint32_t r = 0; r < n; r++) {
+        double v = in[r];
+        for (uint32_t q = mptr[r]; q < mptr[r + 1]; q++) v = fma(-mcoef[q], in[mdep[q]], v);
+        out[r] = v;
+    }
+}
+
 /* One triangular sweep in gather form in the summation order of the library's
  * streamed sweep kernel (no reference counterpart: the reference sums each row
  * in stored order).  For row r, [eptr[r], eptr[r+1]) of edep/ecoef are its
@@ -287,11 +299,25 @@ static void ilut_inplace(uint32_t n, const uint32_t* lrp, const uint32_t* lci, c
 static void amsed_ordered_block_solve(const orc_amsed* S, const orc_amsed_level* L, double* x) {
     const orc_sweep_order* lo = L->sweep_lo;
     const orc_sweep_order* up = L->sweep_up;
-    double* t = malloc((size_t)(lo->n ? lo->n : 1) * sizeof(double));
+    const uint32_t nb = lo->n > up->n ? lo->n : up->n;
+    double* t = malloc((size_t)(nb ? nb : 1) * sizeof(double));
+    double* b = malloc((size_t)(nb ? nb : 1) * sizeof(double));
+    /* a paired sweep's right-hand side first (mptr NULL: not paired) */
+    const double* in = x;
+    if (lo->mptr) {
+        orc_pair_rhs(lo->n, lo->mptr, lo->mdep, lo->mcoef, x, b);
+        in = b;
+    }
     orc_sweep_ordered(lo->n, S->single, lo->op, lo->lower, lo->eptr, lo->edep, lo->ecoef, lo->kptr, lo->kdep,
-                      lo->kcoef, lo->diag, x, t);
+                      lo->kcoef, lo->diag, in, t);
+    in = t;
+    if (up->mptr) {
+        orc_pair_rhs(up->n, up->mptr, up->mdep, up->mcoef, t, b);
+        in = b;
+    }
     orc_sweep_ordered(up->n, S->single, up->op, up->lower, up->eptr, up->edep, up->ecoef, up->kptr, up->kdep,
-                      up->kcoef, up->diag, t, x);
+                      up->kcoef, up->diag, in, x);
+    free(b);
     free(t);
 }
 

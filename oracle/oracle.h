@@ -25,6 +25,9 @@ typedef struct orc_sweep_order {
     const uint32_t* kdep;
     const double* kcoef;
     const double* diag;
+    const uint32_t* mptr;   /* paired sweep: right-hand side map (orc_pair_rhs), else NULL */
+    const uint32_t* mdep;
+    const double* mcoef;
 } orc_sweep_order;
 
 /* One level of an AMSED/MSLR hierarchy (LevelStructure,
@@ -89,6 +92,8 @@ void orc_spmv(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const dou
 void orc_sweep_f32(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val,
                    const double* diag, int op, int lower, const double* in, double* out);
 /* a gather-form triangular sweep in the streamed kernel's summation order (see oracle.c) */
+void orc_pair_rhs(uint32_t n, const uint32_t* mptr, const uint32_t* mdep, const double* mcoef, const double* in,
+                  double* out);
 void orc_sweep_ordered(uint32_t n, int single, int op, int lower, const uint32_t* eptr, const uint32_t* edep,
                        const double* ecoef, const uint32_t* kptr, const uint32_t* kdep, const double* kcoef,
                        const double* diag, const double* in, double* out);

@@ -30,7 +30,8 @@ class _AmsedLevel(C.Structure):
 class _SweepOrder(C.Structure):
     _fields_ = [("n", C.c_uint32), ("op", C.c_int), ("lower", C.c_int),
                 ("eptr", C.c_void_p), ("edep", C.c_void_p), ("ecoef", C.c_void_p),
-                ("kptr", C.c_void_p), ("kdep", C.c_void_p), ("kcoef", C.c_void_p), ("diag", C.c_void_p)]
+                ("kptr", C.c_void_p), ("kdep", C.c_void_p), ("kcoef", C.c_void_p), ("diag", C.c_void_p),
+                ("mptr", C.c_void_p), ("mdep", C.c_void_p), ("mcoef", C.c_void_p)]
 
 
 class _Amsed(C.Structure):
@@ -62,6 +63,7 @@ def lib() -> C.CDLL:
                                        C.c_double, _u32p, _u32p, _f64p]
         _LIB.orc_spmv.argtypes = [C.c_uint32, _u32p, _u32p, _f64p, _f64p, _f64p]
         _LIB.orc_sweep_f32.argtypes = [C.c_uint32, _u32p, _u32p, _f64p, C.c_void_p, C.c_int, C.c_int, _f64p, _f64p]
+        _LIB.orc_pair_rhs.argtypes = [C.c_uint32, _u32p, _u32p, _f64p, _f64p, _f64p]
         _LIB.orc_sweep_ordered.argtypes = [C.c_uint32, C.c_int, C.c_int, C.c_int, _u32p, _u32p, _f64p, _u32p, _u32p,
                                            _f64p, C.c_void_p, _f64p, _f64p]
         _LIB.orc_precond_apply.argtypes = [C.POINTER(_Precond), _f64p]
@@ -120,11 +122,24 @@ def refactor(kind, A_rowptr, A_col, A_val, lt_rowptr, lt_col, *, single=False):
     return rc, lt_val[:len(lt_col)], D[:n]
 
 
+def pair_rhs(mptr, mdep, mcoef, b):
+    """A paired sweep's right-hand side: b_r - sum m b_dep in stored order, one fma each."""
+    n = len(mptr) - 1
+    out = np.zeros(n)
+    u = lambda a: np.ascontiguousarray(a if len(a) else np.zeros(1), np.uint32)
+    f = lambda a: np.ascontiguousarray(a if len(a) else np.zeros(1), np.float64)
+    lib().orc_pair_rhs(n, u(mptr), u(mdep), f(mcoef), np.ascontiguousarray(b, np.float64), out)
+    return out
+
+
 def sweep_ordered(order, b, *, diag=None, op=2, lower=True, single=True):
     """Gather-form triangular sweep in the streamed kernel's summation order.  `order`
     carries eptr/edep/ecoef and kptr/kdep/kcoef (per row: early then late positions,
-    padding 0xFFFFFFFF); float arithmetic when single, else double."""
+    padding 0xFFFFFFFF); float arithmetic when single, else double.  An order of a paired
+    sweep (paired true, with mptr/mdep/mcoef) maps the right-hand side first (pair_rhs)."""
     n = len(order.eptr) - 1
+    if getattr(order, "paired", False):
+        b = pair_rhs(order.mptr, order.mdep, order.mcoef, b)
     out = np.zeros(n)
     d = np.ascontiguousarray(diag, np.float64) if diag is not None else None
     u = lambda a: np.ascontiguousarray(a if len(a) else np.zeros(1), np.uint32)
@@ -267,6 +282,8 @@ class Amsed:
                 so.eptr, so.edep, so.ecoef = arr(o.eptr, np.uint32), arr(o.edep, np.uint32), arr(o.ecoef, np.float64)
                 so.kptr, so.kdep, so.kcoef = arr(o.kptr, np.uint32), arr(o.kdep, np.uint32), arr(o.kcoef, np.float64)
                 so.diag = arr(o.diag, np.float64)
+                if getattr(o, "paired", False):
+                    so.mptr, so.mdep, so.mcoef = arr(o.mptr, np.uint32), arr(o.mdep, np.uint32), arr(o.mcoef, np.float64)
                 self.keep.append(so)
                 setattr(self.levels[l], which, C.cast(C.pointer(so), C.c_void_p).value)
         self.s.single = int(bool(single))

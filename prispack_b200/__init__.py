@@ -85,6 +85,11 @@ _SIGS = {
                                            C.c_int32, C.c_uint32, _f64p, _f64p]),
     "prism_precond_sweep_order": (C.c_int32, [_vp, C.c_int32, C.POINTER(C.c_uint32), _vp, _vp, _vp, _vp, _vp,
                                               _vp, _vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "prism_precond_sweep_rhs_map": (C.c_int32, [_vp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_uint64), _vp,
+                                                _vp, _vp]),
+    "prism_stream_sweep_pair": (C.c_int32, [C.c_uint32, _u32p, _u32p, _f64p, _vp, C.c_int32, C.c_int32, C.c_int32,
+                                            C.POINTER(C.c_uint64), _vp, _vp, _vp, C.POINTER(C.c_uint64), _vp, _vp,
+                                            _vp]),
     "prism_mtx_read": (C.c_int32, [C.c_char_p, C.c_int32, C.c_int32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
                                    C.POINTER(C.c_uint64), _vp, _vp, _vp]),
     "prism_mtx_read_dense": (C.c_int32, [C.c_char_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), _vp]),
@@ -273,6 +278,32 @@ def stream_sweep_run(rowptr, col, val, in_, *, diag=None, op: int = 2, lower: bo
                                          d.ctypes.data if d is not None else None, op, int(lower), precision,
                                          num_ctas, np.ascontiguousarray(in_, np.float64), out))
     return out
+
+
+def stream_sweep_pair(rowptr, col, val, *, diag=None, op: int = 2, lower: bool = True, precision: int = 0):
+    """Wavefront pairing of a gather-form sweep (prism_stream_sweep_pair, host only): the
+    paired sweep (rowptr, col, val) and its right-hand side map (mptr, mdep, mcoef), with
+    T^{-1} b = T'^{-1} (b - M b)."""
+    rp = np.ascontiguousarray(rowptr, np.uint32)
+    ci = np.ascontiguousarray(col, np.uint32)
+    v = np.ascontiguousarray(val, np.float64)
+    d = np.ascontiguousarray(diag, np.float64) if diag is not None else None
+    n = len(rp) - 1
+    lib = load()
+    pn, mn = C.c_uint64(), C.c_uint64()
+    dp = d.ctypes.data if d is not None else None
+    _check(lib.prism_stream_sweep_pair(n, rp, ci, v, dp, op, int(lower), precision, C.byref(pn), None, None, None,
+                                       C.byref(mn), None, None, None))
+    prow = np.zeros(n + 1, np.uint32)
+    pcol = np.zeros(max(pn.value, 1), np.uint32)
+    pval = np.zeros(max(pn.value, 1))
+    mptr = np.zeros(n + 1, np.uint32)
+    mdep = np.zeros(max(mn.value, 1), np.uint32)
+    mcoef = np.zeros(max(mn.value, 1))
+    _check(lib.prism_stream_sweep_pair(n, rp, ci, v, dp, op, int(lower), precision, C.byref(pn), prow.ctypes.data,
+                                       pcol.ctypes.data, pval.ctypes.data, C.byref(mn), mptr.ctypes.data,
+                                       mdep.ctypes.data, mcoef.ctypes.data))
+    return prow, pcol[:pn.value], pval[:pn.value], mptr, mdep[:mn.value], mcoef[:mn.value]
 
 
 def read_mtx_dense(path: str):
@@ -698,6 +729,17 @@ class DeviceSystem:
         o = _fill_order(lambda ep, ed, ec, kp, kd, kc: lib.prism_precond_sweep_order(
             h, sweep, C.byref(n), ep, ed, ec, kp, kd, kc, diag.ctypes.data, C.byref(op), C.byref(lower)), n.value)
         o.diag, o.op, o.lower = diag[:n.value], op.value, bool(lower.value)
+        # a paired sweep's right-hand side map (empty when the sweep runs unpaired)
+        paired, mn = C.c_int32(), C.c_uint64()
+        _check(lib.prism_precond_sweep_rhs_map(h, sweep, C.byref(paired), C.byref(mn), None, None, None))
+        o.mptr = np.zeros(n.value + 1, np.uint32)
+        o.mdep = np.zeros(max(mn.value, 1), np.uint32)
+        o.mcoef = np.zeros(max(mn.value, 1))
+        if paired.value:
+            _check(lib.prism_precond_sweep_rhs_map(h, sweep, C.byref(paired), C.byref(mn), o.mptr.ctypes.data,
+                                                   o.mdep.ctypes.data, o.mcoef.ctypes.data))
+        o.mdep, o.mcoef = o.mdep[:mn.value], o.mcoef[:mn.value]
+        o.paired = bool(paired.value)
         return o
 
     def apply(self, vec):

@@ -138,8 +138,9 @@ void AmsedPrecond::build(const AmsedSetup<Low>& S) {
         Sweep<Low> lo, up;
         level_sweeps<Low>(S, l, lo, up);
         D.nfac = l + 1 == nlev_ ? L.B[0].n : D.nb;  // the last level factors block 0 only
-        tune_sweep<Low>(h_, D.lower, lo, a_->apply32);
-        tune_sweep<Low>(h_, D.upper, up, a_->apply32);
+        // the streamed kernel may run the level's sweeps paired (half the wavefronts)
+        tune_sweep<Low>(h_, D.lower, lo, a_->apply32, true);
+        tune_sweep<Low>(h_, D.upper, up, a_->apply32, true);
         if (l + 1 < nlev_) {
             upload_csr(D.E, L.E.n, L.E.rowptr, L.E.col, L.E.val, st);
             if (gmslr_) {

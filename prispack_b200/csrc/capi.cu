@@ -261,6 +261,75 @@ int32_t prism_stream_sweep_run(int32_t device, uint32_t n, const uint32_t* rowpt
     });
 }
 
+int32_t prism_stream_sweep_pair(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val,
+                                const double* diag, int32_t op, int32_t lower, int32_t precision, uint64_t* pnnz,
+                                uint32_t* prow, uint32_t* pcol, double* pval, uint64_t* mnnz, uint32_t* mptr,
+                                uint32_t* mdep, double* mcoef) {
+    if (!rowptr || !col || !val || !pnnz || !mnnz || n == 0) return fail(PRISM_ERR_ARG, "null array or empty sweep");
+    if (op < 0 || op > 3 || (op != 2 && !diag)) return fail(PRISM_ERR_ARG, "bad op / missing diagonal");
+    if (!valid_precision(precision)) return fail(PRISM_ERR_ARG, "bad precision");
+    return guarded([&]() -> int {
+        int rc = check_gather_form(n, rowptr, col, lower);
+        if (rc) return rc;
+        auto emit = [&](auto& s) {
+            using S = std::decay_t<decltype(s)>;
+            S ps;
+            prism::PairMap pm;
+            prism::pair_sweep(s, ps, pm);
+            *pnnz = ps.col.size();
+            *mnnz = pm.dep.size();
+            if (prow) {  // gather form by row
+                std::vector<uint32_t> pos(n);
+                for (uint32_t p = 0; p < n; ++p) pos[ps.order[p]] = p;
+                prow[0] = 0;
+                for (uint32_t r = 0; r < n; ++r) {
+                    const uint32_t p = pos[r], len = ps.rowptr[p + 1] - ps.rowptr[p];
+                    prow[r + 1] = prow[r] + len;
+                    for (uint32_t t = 0; t < len; ++t) {
+                        if (pcol) pcol[prow[r] + t] = ps.col[ps.rowptr[p] + t];
+                        if (pval) pval[prow[r] + t] = (double)ps.val[ps.rowptr[p] + t];
+                    }
+                }
+            }
+            if (mptr) std::copy(pm.ptr.begin(), pm.ptr.end(), mptr);
+            if (mdep) std::copy(pm.dep.begin(), pm.dep.end(), mdep);
+            if (mcoef) std::copy(pm.coef.begin(), pm.coef.end(), mcoef);
+        };
+        if (precision != PRISM_FP64) {
+            prism::Sweep<float> s;
+            gather_sweep<float>(n, rowptr, col, val, diag, op, lower != 0, s);
+            emit(s);
+        } else {
+            prism::Sweep<double> s;
+            gather_sweep<double>(n, rowptr, col, val, diag, op, lower != 0, s);
+            emit(s);
+        }
+        return PRISM_OK;
+    });
+}
+
+int32_t prism_precond_sweep_rhs_map(prism_handle h, int32_t sweep, int32_t* paired, uint64_t* mnnz, uint32_t* mptr,
+                                    uint32_t* mdep, double* mcoef) {
+    if (!h || !paired || !mnnz) return fail(PRISM_ERR_ARG, "null handle or output");
+    if (!h->P) return fail(PRISM_ERR_NOT_READY, "no preconditioner");
+    return guarded([&]() -> int {
+        uint32_t rows = 0;
+        if (!h->P->sweep_info(sweep, &rows, nullptr, nullptr, nullptr, nullptr))
+            return fail(PRISM_ERR_ARG, "no such sweep");
+        prism::StreamOrder o;
+        if (!h->P->sweep_order(sweep, o)) return fail(PRISM_ERR_UNSUPPORTED, "the sweep does not run the streamed kernel");
+        *paired = o.mptr.empty() ? 0 : 1;
+        *mnnz = o.mdep.size();
+        if (mptr) {
+            if (o.mptr.empty()) std::fill(mptr, mptr + rows + 1, 0u);
+            else std::copy(o.mptr.begin(), o.mptr.end(), mptr);
+        }
+        if (mdep) std::copy(o.mdep.begin(), o.mdep.end(), mdep);
+        if (mcoef) std::copy(o.mcoef.begin(), o.mcoef.end(), mcoef);
+        return PRISM_OK;
+    });
+}
+
 int32_t prism_precond_sweep_order(prism_handle h, int32_t sweep, uint32_t* n, uint32_t* eptr, uint32_t* edep,
                                   double* ecoef, uint32_t* kptr, uint32_t* kdep, double* kcoef, double* diag,
                                   int32_t* op, int32_t* lower) {

@@ -460,6 +460,77 @@ void build_sweep(uint32_t n, const std::vector<uint32_t>& rowptr, const std::vec
 }
 
 template <typename Low>
+void pair_sweep(const Sweep<Low>& s, Sweep<Low>& out, PairMap& m) {
+    const uint32_t n = s.n;
+    std::vector<uint32_t> pos(n);  // row -> position
+    for (uint32_t p = 0; p < n; ++p) pos[s.order[p]] = p;
+    auto g_of = [&](uint32_t row) -> double {
+        const double d = s.diag[pos[row]];
+        switch (s.op) {
+            case SWEEP_DIV:
+            case SWEEP_PREDIV: return 1.0 / d;
+            case SWEEP_MUL: return d;
+            default: return 1.0;
+        }
+    };
+    std::vector<uint32_t> rp((size_t)n + 1, 0), ci;
+    std::vector<Low> cv;
+    std::vector<double> diag(n, 1.0);
+    m.ptr.assign((size_t)n + 1, 0);
+    m.dep.clear();
+    m.coef.clear();
+    std::vector<int64_t> slot(n, -1);  // dependency row -> index in the row being built
+    std::vector<uint32_t> deps;
+    std::vector<double> acc;
+    for (uint32_t r = 0; r < n; ++r) {
+        const uint32_t p = pos[r], lk = s.level[r];
+        diag[r] = s.diag[p];
+        deps.clear();
+        acc.clear();
+        auto add = [&](uint32_t j, double v) {
+            if (slot[j] < 0) {
+                slot[j] = (int64_t)deps.size();
+                deps.push_back(j);
+                acc.push_back(v);
+            } else {
+                acc[(size_t)slot[j]] = acc[(size_t)slot[j]] + v;
+            }
+        };
+        const bool odd = (lk & 1u) != 0;
+        // the row's own entries that stay, in stored order
+        for (uint32_t k = s.rowptr[p]; k < s.rowptr[p + 1]; ++k) {
+            const uint32_t j = s.col[k];
+            if (!(odd && s.level[j] + 1 == lk)) add(j, (double)s.val[k]);
+        }
+        if (odd) {
+            const double gk = g_of(r);
+            for (uint32_t k = s.rowptr[p]; k < s.rowptr[p + 1]; ++k) {
+                const uint32_t i = s.col[k];
+                if (s.level[i] + 1 != lk) continue;
+                const double lki = (double)s.val[k], gi = g_of(i);
+                const double f = lki * (s.op == SWEEP_PREDIV ? 1.0 : gi);
+                const uint32_t pi = pos[i];
+                for (uint32_t q = s.rowptr[pi]; q < s.rowptr[pi + 1]; ++q) add(s.col[q], -(f * (double)s.val[q]));
+                m.dep.push_back(i);
+                m.coef.push_back(s.op == SWEEP_PREDIV ? lki * gi / gk : lki * gi);
+            }
+        }
+        m.ptr[r + 1] = (uint32_t)m.dep.size();
+        // the row's entries, dependencies in increasing order
+        std::vector<uint32_t> idx(deps.size());
+        std::iota(idx.begin(), idx.end(), 0u);
+        std::sort(idx.begin(), idx.end(), [&](uint32_t a, uint32_t b) { return deps[a] < deps[b]; });
+        for (uint32_t t : idx) {
+            ci.push_back(deps[t]);
+            cv.push_back((Low)acc[t]);
+        }
+        rp[r + 1] = (uint32_t)ci.size();
+        for (uint32_t j : deps) slot[j] = -1;
+    }
+    build_sweep<Low>(n, rp, ci, cv, &diag, s.op, s.lower, out);
+}
+
+template <typename Low>
 void slab_layout_ranges(const Sweep<Low>& s, const std::vector<uint32_t>& start, std::vector<uint32_t>& cta_pos,
                         Sweep<Low>& out) {
     const uint32_t n = s.n;
@@ -779,7 +850,8 @@ void bank_order(const std::vector<std::vector<std::pair<uint32_t, uint32_t>>>& r
 
 template <typename Low>
 bool stream_layout(const Sweep<Low>& s, const std::vector<uint32_t>& start, uint32_t max_slots, uint32_t slot_bytes,
-                   StreamLayout& out, std::string* why, StreamOrder* order, std::vector<uint32_t>* coef_map) {
+                   StreamLayout& out, std::string* why, StreamOrder* order, std::vector<uint32_t>* coef_map,
+                   uint32_t max_round_bytes) {
     auto fail = [&](const std::string& m) {
         if (why) *why = m;
         return false;
@@ -863,17 +935,34 @@ bool stream_layout(const Sweep<Low>& s, const std::vector<uint32_t>& start, uint
         const uint32_t P0 = cpos[b], P1 = cpos[b + 1];
         std::vector<Round> R;
         // 1. rounds: consecutive positions, at most kRoundRows, no dependency inside a round.
+        // With a record cap, each row's early and late entries are counted as step 4 will
+        // (late: slab rows of the kStreamLate rounds before) and the record's size
+        // (round_rec) is checked before the row joins.
+        const uint32_t vbytes = (uint32_t)sizeof(Low);
         for (uint32_t p = P0; p < P1;) {
             Round rd;
             rd.p0 = p;
             const uint32_t id = (uint32_t)R.size();
+            uint32_t maxE = 0, maxK = 0;
             while (p < P1 && p - rd.p0 < kRoundRows) {
                 bool clash = false;
+                uint32_t e = 0, kk = 0;
                 for (uint32_t k = sl.rowptr[p]; k < sl.rowptr[p + 1] && !clash; ++k) {
                     const uint32_t d = sl.col[k];
-                    clash = d >= rb && d < re && round_of[d] == id;
+                    const bool in_slab = d >= rb && d < re;
+                    clash = in_slab && round_of[d] == id;
+                    if (in_slab && round_of[d] < id && round_of[d] + kStreamLate >= id) ++kk;
+                    else ++e;
                 }
                 if (clash) break;
+                const uint32_t E2 = std::max(maxE, e), K2 = std::max(maxK, kk);
+                if (max_round_bytes && p > rd.p0) {
+                    const uint32_t Eg = std::max((E2 + 3) / 4, stream_early_groups(slot_bytes));
+                    const uint32_t Kg = std::max<uint32_t>((K2 + 3) / 4, 1);
+                    if (round_rec(p - rd.p0 + 1, Eg, Kg, vbytes, slot_bytes).bytes > max_round_bytes) break;
+                }
+                maxE = E2;
+                maxK = K2;
                 round_of[sl.order[p]] = id;
                 ++p;
             }
@@ -1345,12 +1434,14 @@ template void slab_layout<float>(const Sweep<float>&, uint32_t, uint32_t, std::v
 template std::vector<uint32_t> slab_ranges<double>(const Sweep<double>&, uint32_t);
 template std::vector<uint32_t> slab_ranges<float>(const Sweep<float>&, uint32_t);
 template bool stream_layout<double>(const Sweep<double>&, const std::vector<uint32_t>&, uint32_t, uint32_t,
-                                    StreamLayout&, std::string*, StreamOrder*, std::vector<uint32_t>*);
+                                    StreamLayout&, std::string*, StreamOrder*, std::vector<uint32_t>*, uint32_t);
 template bool stream_layout<float>(const Sweep<float>&, const std::vector<uint32_t>&, uint32_t, uint32_t,
-                                   StreamLayout&, std::string*, StreamOrder*, std::vector<uint32_t>*);
+                                   StreamLayout&, std::string*, StreamOrder*, std::vector<uint32_t>*, uint32_t);
 template std::string stream_layout_replay<double>(const Sweep<double>&, const StreamLayout&, const double*,
                                                   double*);
 template std::string stream_layout_replay<float>(const Sweep<float>&, const StreamLayout&, const double*, double*);
+template void pair_sweep<double>(const Sweep<double>&, Sweep<double>&, PairMap&);
+template void pair_sweep<float>(const Sweep<float>&, Sweep<float>&, PairMap&);
 template void build_sweep<double>(uint32_t, const std::vector<uint32_t>&, const std::vector<uint32_t>&,
                                   const std::vector<double>&, const std::vector<double>*, int, bool, Sweep<double>&);
 template void build_sweep<float>(uint32_t, const std::vector<uint32_t>&, const std::vector<uint32_t>&,

@@ -239,6 +239,9 @@ struct StreamOrder {
     std::vector<double> diag;                      // per row: the sweep's diagonal (as given, not inverted)
     int op = 0;                                    // SweepOp
     bool lower = true;
+    // a paired sweep's right-hand side map (see PairMap), empty otherwise
+    std::vector<uint32_t> mptr, mdep;
+    std::vector<double> mcoef;
 };
 // Slab boundaries for num_ctas CTAs (num_ctas + 1 entries, empty slabs
 // dropped): rows are first split where no dependency crosses (independent
@@ -254,10 +257,12 @@ std::vector<uint32_t> slab_ranges(const Sweep<Low>& s, uint32_t num_ctas);
 // value slots in one slab.  `order`, when given, receives the summation order.
 // `coef_map`, when given, receives one pair per coefficient written from the sweep:
 // (position in the blob in units of the factor value, index of the sweep entry).
+// `max_round_bytes` (0: none) ends a round early where its record, with the row
+// about to join, could grow beyond that many bytes (rows of many entries).
 template <typename Low>
 bool stream_layout(const Sweep<Low>& s, const std::vector<uint32_t>& start, uint32_t max_slots, uint32_t slot_bytes,
                    StreamLayout& out, std::string* why, StreamOrder* order = nullptr,
-                   std::vector<uint32_t>* coef_map = nullptr);
+                   std::vector<uint32_t>* coef_map = nullptr, uint32_t max_round_bytes = 0);
 // Replays k_sweep_stream on the host, in its arithmetic (float for 4-byte
 // slots): stages `in` as the prep kernel does and runs each slab's rounds in
 // the kernel's pipeline order -- round r's late entries and round r + 1's
@@ -278,6 +283,26 @@ template <typename Low>
 void build_sweep(uint32_t n, const std::vector<uint32_t>& rowptr, const std::vector<uint32_t>& col,
                  const std::vector<Low>& val, const std::vector<double>* diag, int op, bool lower,
                  Sweep<Low>& out);
+
+// Wavefront pairing: the same triangular solve in half as many wavefronts.  A
+// row k on an odd level 2R+1 depends on rows i of level 2R; substituting
+// x_i = g_i (b_i - sum_j l_ij x_j) (g_i = 1 / d_i for SWEEP_DIV, d_i for
+// SWEEP_MUL, 1 for SWEEP_NONE; for SWEEP_PREDIV x_i = g_i b_i - sum_j l_ij x_j,
+// g_i = 1 / d_i) leaves k depending on levels <= 2R-1 only, so that the paired
+// sweep's level of every row is half its old one:
+//   x_k = op_k(b'_k, sum_j c_kj x_j),  c_kj = l_kj - sum_i l_ki f_i l_ij,
+//   b'_k = b_k - sum_i m_ki b_i,
+// with f_i = g_i and m_ki = l_ki g_i (DIV, MUL, NONE), or f_i = 1 and
+// m_ki = l_ki g_i / g_k (PREDIV).  c is computed in double and stored in the
+// sweep's value type; m (double) is applied to the right-hand side before the
+// sweep (the streamed kernel's prep): per row r, in stored order,
+//   v = b_r;  v = fma(-m, b_dep, v) over [ptr[r], ptr[r+1]).
+struct PairMap {
+    std::vector<uint32_t> ptr, dep;  // by row (n + 1 / entries)
+    std::vector<double> coef;
+};
+template <typename Low>
+void pair_sweep(const Sweep<Low>& s, Sweep<Low>& out, PairMap& m);
 
 // Transpose of a CSR (pattern + values), keeping, inside every output row, the
 // increasing order of source rows.  Used to turn the reference's column

@@ -344,7 +344,7 @@ void build_map(const DevSweep& d, const Sweep<Low>& s, const Sweep<double>& idx,
         std::vector<uint32_t> cmap;
         std::string why;
         if (!stream_layout<Low>(s, slab_ranges<Low>(s, d.str_ctas_req), kNoSlot, d.str_slot_bytes, L, &why, nullptr,
-                                &cmap))
+                                &cmap, d.str_round_cap))
             throw Error(PRISM_ERR_CUDA, "streamed layout could not be rebuilt: " + why);
         cd.reserve(cmap.size() / 2);
         cs.reserve(cmap.size() / 2);

@@ -3,6 +3,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <future>
 
 #include "../../include/prism_solve.h"
 #include "kernels.cuh"
@@ -84,6 +85,21 @@ void launch_sweep_prepare(const Handle& h, cudaStream_t st, const DevSweep& s, c
     if (!s.n) return;
     if (s.layout != LAYOUT_STREAM) {
         launch_fill(st, h, s.n, out);
+        return;
+    }
+    if (s.paired) {
+        // the prep reads other rows of `in`: when in == out, the outputs are marked afterwards
+        const int mark = in != out ? 1 : 0;
+        if (s.acc32)
+            k_stream_prep_pair<float><<<vec_grid(h, s.n), kBlock, 0, st>>>(
+                s.n, s.str_in_slot.get(), s.pair_ptr.get(), s.pair_dep.get(), s.pair_coef.get(), in,
+                reinterpret_cast<float*>(s.str_blob.get()), reinterpret_cast<unsigned long long*>(out), mark);
+        else
+            k_stream_prep_pair<double><<<vec_grid(h, s.n), kBlock, 0, st>>>(
+                s.n, s.str_in_slot.get(), s.pair_ptr.get(), s.pair_dep.get(), s.pair_coef.get(), in,
+                reinterpret_cast<double*>(s.str_blob.get()), reinterpret_cast<unsigned long long*>(out), mark);
+        PRISM_LAUNCHED();
+        if (!mark) launch_fill(st, h, s.n, out);
         return;
     }
     if (s.acc32)
@@ -276,6 +292,10 @@ void init_device_info(DeviceInfo& info, int device) {
     if (info.slab_min_rows < 32) info.slab_min_rows = 32;
     // the slab kernel runs one 1024-thread CTA per SM with up to the whole opt-in shared memory
     if (const char* e = std::getenv("PRISM_STREAM_MIN_ROWS")) info.stream_min_rows = (uint32_t)std::atoi(e);
+    if (const char* e = std::getenv("PRISM_STREAM_PAIR")) {  // 0 never, 1 the tuner decides, 2 always
+        const int v = std::atoi(e);
+        info.stream_pair = v < 0 ? 0 : (v > 2 ? 2 : v);
+    }
     if (info.stream_min_rows < 32) info.stream_min_rows = 32;
     for (bool f32 : {false, true})
         for (int op = 0; op < 4; ++op) {
@@ -343,65 +363,121 @@ void DevSweep::release() {
     num_ctas = rows_per_cta = smem_rows = 0;
     str_ctas = str_ring = str_meta_slots = str_slots = str_rounds = str_smem = 0;
     str_nnz = 0;
+    str_round_cap = 0;
+    pair_ptr.release(); pair_dep.release(); pair_coef.release();
+    paired = false;
     n = num_levels = 0;  // empty: nothing launches on a released sweep
 }
 
 template <typename Low>
-bool DevSweep::upload(const Sweep<Low>& s0, const DeviceInfo& info, int lay, cudaStream_t st) {
+StreamPlan plan_stream(const Sweep<Low>& sweep, const DeviceInfo& info, bool acc32, bool pair) {
+    // One persistent CTA per SM (fewer for small sweeps); shared memory holds the
+    // round table, the value slots and, in what is left, the ring the round
+    // records stream through.
+    StreamPlan P;
+    const uint32_t nn = sweep.n;
+    if (nn == 0) return P;
+    Sweep<Low> ps;
+    if (pair) pair_sweep<Low>(sweep, ps, P.pm);
+    const Sweep<Low>& s0 = pair ? ps : sweep;
+    const uint32_t ctas_req = stream_slab_count(nn, (uint32_t)info.sms, info.stream_min_rows);
+    const std::vector<uint32_t> start = slab_ranges<Low>(s0, ctas_req);
+    const uint64_t smem = (uint64_t)info.max_smem_optin;
+    StreamLayout& L = P.L;
+    const bool a32 = acc32 && std::is_same<Low, float>::value;
+    const uint32_t slot_bytes = a32 ? 4 : 8;  // one value slot
+    const uint32_t vb = (uint32_t)sizeof(Low);
+    const uint64_t base_smem = stream_smem(0, 0, slot_bytes, vb, 0).total;  // everything but table and slots
+    if (smem <= base_smem) return P;
+    const uint32_t slot_cap = (uint32_t)std::min<uint64_t>(kNoSlot, (smem - base_smem) / slot_bytes / 2);
+    // While round i is computed the row threads hold rounds i and i + 1 and wait for
+    // round i + 2's record: two live records and room for a third, which a circular ring
+    // of four of the largest records always has in one piece.  Where a round's record
+    // is too large for that (rows of many entries), the rounds are cut shorter.
+    uint32_t cap = 0;
+    uint64_t fixed = 0;
+    bool fits = false;
+    for (int attempt = 0; attempt < 4 && !fits; ++attempt) {
+        L = StreamLayout();
+        if (!stream_layout<Low>(s0, start, slot_cap, slot_bytes, L, nullptr, nullptr, nullptr, cap)) return P;
+        if (L.max_rounds_per_cta > smem / 16 || L.slots > kNoSlot) return P;
+        fixed = stream_smem(L.max_rounds_per_cta, L.slots, slot_bytes, vb, 0).total;
+        fits = fixed + 4ull * L.max_round_bytes <= smem;
+        if (!fits) {
+            if (fixed + 4096 >= smem) return P;
+            const uint64_t room = (smem - fixed) / 4 * 7 / 8 >> attempt;  // margin for rounds and slots
+            cap = (uint32_t)std::max<uint64_t>(room & ~15ull, 1024);
+        }
+    }
+    if (!fits) return P;
+    P.ok = true;
+    P.paired = pair;
+    P.fp32 = std::is_same<Low, float>::value;
+    P.a32 = a32;
+    P.n = s0.n;
+    P.num_levels = s0.num_levels;
+    P.op = s0.op;
+    P.ctas = (uint32_t)start.size() - 1;
+    P.ctas_req = ctas_req;
+    P.slot_bytes = slot_bytes;
+    P.cap = cap;
+    P.ring = (uint32_t)((smem - fixed) & ~15ull);
+    P.smem = stream_smem(L.max_rounds_per_cta, L.slots, slot_bytes, vb, P.ring).total;  // <= smem
+    P.nnz = s0.val.size();
+    return P;
+}
+template StreamPlan plan_stream<double>(const Sweep<double>&, const DeviceInfo&, bool, bool);
+template StreamPlan plan_stream<float>(const Sweep<float>&, const DeviceInfo&, bool, bool);
+
+void DevSweep::commit_stream(StreamPlan&& P, cudaStream_t st) {
+    const StreamLayout& L = P.L;
+    release();
+    n = P.n;
+    num_levels = P.num_levels;
+    op = P.op;
+    fp32 = P.fp32;
+    acc32 = P.a32;
+    layout = LAYOUT_STREAM;
+    str_ctas = P.ctas;
+    str_ctas_req = P.ctas_req;
+    str_slot_bytes = P.slot_bytes;
+    str_round_cap = P.cap;
+    str_ring = P.ring;
+    str_meta_slots = L.max_rounds_per_cta;
+    str_slots = L.slots;
+    str_rounds = L.num_rounds;
+    str_smem = P.smem;
+    str_nnz = P.nnz;
+    str_blob.upload(L.blob.data(), L.blob.size(), st);
+    str_meta.upload(L.meta.data(), L.meta.size(), st);
+    str_cta_round.upload(L.cta_round.data(), L.cta_round.size(), st);
+    str_slab_start.upload(L.slab_start.data(), L.slab_start.size(), st);
+    str_in_slot.upload(L.in_slot.data(), L.in_slot.size(), st);
+    str_halo_ptr.upload(L.halo_ptr.data(), L.halo_ptr.size(), st);
+    str_halo_row.upload(L.halo_row.data(), L.halo_row.size(), st);
+    str_halo_sw.upload(L.halo_sw.data(), L.halo_sw.size(), st);
+    if (str_halo_row.size() == 0) str_halo_row.alloc(1);  // valid pointers for the kernel
+    if (str_halo_sw.size() == 0) str_halo_sw.alloc(1);
+    if (P.paired) {
+        paired = true;
+        pair_ptr.upload(P.pm.ptr.data(), P.pm.ptr.size(), st);
+        pair_dep.upload(P.pm.dep.data(), P.pm.dep.size(), st);
+        pair_coef.upload(P.pm.coef.data(), P.pm.coef.size(), st);
+        if (pair_dep.size() == 0) pair_dep.alloc(1);  // valid pointers for the prep
+        if (pair_coef.size() == 0) pair_coef.alloc(1);
+    }
+    PRISM_CUDA(cudaStreamSynchronize(st));
+}
+
+template <typename Low>
+bool DevSweep::upload(const Sweep<Low>& sweep, const DeviceInfo& info, int lay, cudaStream_t st, bool pair) {
     if (lay == LAYOUT_STREAM) {
-        // One persistent CTA per SM (fewer for small sweeps); shared memory holds the
-        // round table, the value slots and, in what is left, the ring the round
-        // records stream through.
-        const uint32_t nn = s0.n;
-        if (nn == 0) return false;
-        const uint32_t ctas_req = stream_slab_count(nn, (uint32_t)info.sms, info.stream_min_rows);
-        const std::vector<uint32_t> start = slab_ranges<Low>(s0, ctas_req);
-        const uint32_t ctas = (uint32_t)start.size() - 1;
-        const uint64_t smem = (uint64_t)info.max_smem_optin;
-        StreamLayout L;
-        const bool a32 = acc32 && std::is_same<Low, float>::value;
-        const uint32_t slot_bytes = a32 ? 4 : 8;  // one value slot
-        const uint32_t vb = (uint32_t)sizeof(Low);
-        const uint64_t base_smem = stream_smem(0, 0, slot_bytes, vb, 0).total;  // everything but table and slots
-        if (smem <= base_smem) return false;
-        const uint32_t slot_cap = (uint32_t)std::min<uint64_t>(kNoSlot, (smem - base_smem) / slot_bytes / 2);
-        if (!stream_layout<Low>(s0, start, slot_cap, slot_bytes, L, nullptr)) return false;
-        if (L.max_rounds_per_cta > smem / 16 || L.slots > kNoSlot) return false;
-        const uint64_t fixed = stream_smem(L.max_rounds_per_cta, L.slots, slot_bytes, vb, 0).total;
-        // While round i is computed the row threads hold rounds i and i + 1 and wait for
-        // round i + 2's record: two live records and room for a third, which a circular ring
-        // of four of the largest records always has in one piece.
-        if (fixed + 4ull * L.max_round_bytes > smem) return false;
-        const uint32_t ring = (uint32_t)((smem - fixed) & ~15ull);
-        release();
-        n = s0.n;
-        num_levels = s0.num_levels;
-        op = s0.op;
-        fp32 = std::is_same<Low, float>::value;
-        acc32 = a32;
-        layout = LAYOUT_STREAM;
-        str_ctas = ctas;
-        str_ctas_req = ctas_req;
-        str_slot_bytes = slot_bytes;
-        str_ring = ring;
-        str_meta_slots = L.max_rounds_per_cta;
-        str_slots = L.slots;
-        str_rounds = L.num_rounds;
-        str_smem = stream_smem(L.max_rounds_per_cta, L.slots, slot_bytes, vb, ring).total;  // <= smem
-        str_nnz = s0.val.size();
-        str_blob.upload(L.blob.data(), L.blob.size(), st);
-        str_meta.upload(L.meta.data(), L.meta.size(), st);
-        str_cta_round.upload(L.cta_round.data(), L.cta_round.size(), st);
-        str_slab_start.upload(L.slab_start.data(), L.slab_start.size(), st);
-        str_in_slot.upload(L.in_slot.data(), L.in_slot.size(), st);
-        str_halo_ptr.upload(L.halo_ptr.data(), L.halo_ptr.size(), st);
-        str_halo_row.upload(L.halo_row.data(), L.halo_row.size(), st);
-        str_halo_sw.upload(L.halo_sw.data(), L.halo_sw.size(), st);
-        if (str_halo_row.size() == 0) str_halo_row.alloc(1);  // valid pointers for the kernel
-        if (str_halo_sw.size() == 0) str_halo_sw.alloc(1);
-        PRISM_CUDA(cudaStreamSynchronize(st));
+        StreamPlan P = plan_stream<Low>(sweep, info, acc32, pair);
+        if (!P.ok) return false;
+        commit_stream(std::move(P), st);
         return true;
     }
+    const Sweep<Low>& s0 = sweep;
     release();
     layout = lay;
     n = s0.n;
@@ -451,12 +527,22 @@ uint32_t stream_slab_count(uint32_t n, uint32_t num_ctas, uint32_t min_rows) {
 }
 
 template <typename Low>
-bool DevSweep::stream_order(const Sweep<Low>& s, StreamOrder& o) const {
-    if (layout != LAYOUT_STREAM || s.n != n) return false;
+bool DevSweep::stream_order(const Sweep<Low>& sweep, StreamOrder& o) const {
+    if (layout != LAYOUT_STREAM || sweep.n != n) return false;
+    Sweep<Low> ps;
+    PairMap pm;
+    if (paired) pair_sweep<Low>(sweep, ps, pm);
+    const Sweep<Low>& s = paired ? ps : sweep;
     StreamLayout L;
     std::string why;
-    if (!stream_layout<Low>(s, slab_ranges<Low>(s, str_ctas_req), kNoSlot, str_slot_bytes, L, &why, &o))
+    if (!stream_layout<Low>(s, slab_ranges<Low>(s, str_ctas_req), kNoSlot, str_slot_bytes, L, &why, &o, nullptr,
+                            str_round_cap))
         throw Error(PRISM_ERR_CUDA, "streamed layout could not be rebuilt: " + why);
+    if (paired) {
+        o.mptr = std::move(pm.ptr);
+        o.mdep = std::move(pm.dep);
+        o.mcoef = std::move(pm.coef);
+    }
     return true;
 }
 template bool DevSweep::stream_order<double>(const Sweep<double>&, StreamOrder&) const;
@@ -493,22 +579,33 @@ template void stream_sweep_run<float>(int, const Sweep<float>&, bool, uint32_t, 
 // kernel wins depends on how many rows a wavefront holds and how far
 // dependencies reach.
 template <typename Low>
-void tune_sweep(Handle& h, DevSweep& d, const Sweep<Low>& s, bool acc32) {
+void tune_sweep(Handle& h, DevSweep& d, const Sweep<Low>& s, bool acc32, bool pair) {
     const int mode = h.info.sweep_kernel;
     d.acc32 = acc32 && std::is_same<Low, float>::value;
+    // Pairing keeps the arithmetic's precision class only where the derived coefficients are
+    // stored in the arithmetic's own type: double values (FP64) or float values with float
+    // arithmetic; float values with double arithmetic (<float,double>) stay unpaired.
+    const bool pp = pair && h.info.stream_pair != 0 && (d.acc32 || std::is_same<Low, double>::value);
     if (s.n == 0) {
         d.upload(s, h.info, LAYOUT_LEVEL, h.stream);
         return;
     }
-    // single-precision arithmetic: only the streamed kernel has it (the other layouts, where
-    // the streamed one does not fit, compute in double)
-    if (d.acc32) {
-        if (!d.upload(s, h.info, LAYOUT_STREAM, h.stream)) d.upload(s, h.info, LAYOUT_LEVEL, h.stream);
-        return;
+    // candidates: {layout, paired}.  Single-precision arithmetic: only the streamed kernel
+    // has it (the other layouts, where the streamed one does not fit, compute in double).
+    std::vector<std::pair<int, bool>> cand;
+    if (pp && h.info.stream_pair == 2) {  // paired where it fits
+        cand.push_back({LAYOUT_STREAM, true});
+    } else if (d.acc32 || mode == 3) {
+        cand.push_back({LAYOUT_STREAM, false});
+        if (pp) cand.push_back({LAYOUT_STREAM, true});
+    } else if (mode != 0) {
+        cand.push_back({mode == 2 ? LAYOUT_SLAB : LAYOUT_LEVEL, false});
+    } else {
+        cand = {{LAYOUT_LEVEL, false}, {LAYOUT_SLAB, false}, {LAYOUT_STREAM, false}};
+        if (pp) cand.push_back({LAYOUT_STREAM, true});
     }
-    if (mode != 0) {
-        const int want = mode == 2 ? LAYOUT_SLAB : (mode == 3 ? LAYOUT_STREAM : LAYOUT_LEVEL);
-        if (!d.upload(s, h.info, want, h.stream)) d.upload(s, h.info, LAYOUT_LEVEL, h.stream);
+    if (cand.size() == 1) {
+        if (!d.upload(s, h.info, cand[0].first, h.stream, cand[0].second)) d.upload(s, h.info, LAYOUT_LEVEL, h.stream);
         return;
     }
     DevBuf<double> in(s.n), out(s.n);
@@ -519,14 +616,30 @@ void tune_sweep(Handle& h, DevSweep& d, const Sweep<Low>& s, bool acc32) {
     PRISM_CUDA(cudaEventCreate(&e0));
     PRISM_CUDA(cudaEventCreate(&e1));
     float best = 0.f;
-    int best_layout = -1;
-    for (int lay : {LAYOUT_LEVEL, LAYOUT_SLAB, LAYOUT_STREAM}) {
-        if (!d.upload(s, h.info, lay, h.stream)) continue;
+    int best_c = -1;
+    // the streamed candidates' host layouts are built concurrently
+    std::vector<std::future<StreamPlan>> plans(cand.size());
+    for (int c = 0; c < (int)cand.size(); ++c)
+        if (cand[c].first == LAYOUT_STREAM) {
+            const bool pc = cand[c].second, a32 = d.acc32;
+            plans[c] = std::async(std::launch::async, [&s, &h, a32, pc] { return plan_stream<Low>(s, h.info, a32, pc); });
+        }
+    DevSweep kept;  // the fastest candidate so far, kept uploaded
+    for (int c = 0; c < (int)cand.size(); ++c) {
+        DevSweep t;
+        t.acc32 = d.acc32;
+        if (cand[c].first == LAYOUT_STREAM) {
+            StreamPlan P = plans[c].get();
+            if (!P.ok) continue;
+            t.commit_stream(std::move(P), h.stream);
+        } else if (!t.upload(s, h.info, cand[c].first, h.stream, cand[c].second)) {
+            continue;
+        }
         float tot = 0.f;
         for (int it = 0; it < 4; ++it) {
             PRISM_CUDA(cudaEventRecord(e0, h.stream));
-            launch_sweep_prepare(h, h.stream, d, in.get(), out.get());
-            launch_sweep_kernel(h, h.stream, d, in.get(), out.get());
+            launch_sweep_prepare(h, h.stream, t, in.get(), out.get());
+            launch_sweep_kernel(h, h.stream, t, in.get(), out.get());
             PRISM_CUDA(cudaEventRecord(e1, h.stream));
             PRISM_CUDA(cudaEventSynchronize(e1));
             float ms = 0.f;
@@ -534,18 +647,23 @@ void tune_sweep(Handle& h, DevSweep& d, const Sweep<Low>& s, bool acc32) {
             if (it > 0) tot += ms;  // first launch is a warm-up
         }
         h.check_status();
-        if (best_layout < 0 || tot < best) {
+        if (best_c < 0 || tot < best) {
             best = tot;
-            best_layout = lay;
+            best_c = c;
+            kept = std::move(t);
         }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    if (d.layout != best_layout) d.upload(s, h.info, best_layout, h.stream);
+    if (best_c < 0) {  // nothing fitted (streamed layouts only): level order, double arithmetic
+        d.upload(s, h.info, LAYOUT_LEVEL, h.stream);
+        return;
+    }
+    d = std::move(kept);
     d.tuned_ms = best / 3.f;
 }
-template void tune_sweep<double>(Handle&, DevSweep&, const Sweep<double>&, bool);
-template void tune_sweep<float>(Handle&, DevSweep&, const Sweep<float>&, bool);
+template void tune_sweep<double>(Handle&, DevSweep&, const Sweep<double>&, bool, bool);
+template void tune_sweep<float>(Handle&, DevSweep&, const Sweep<float>&, bool, bool);
 
 namespace {
 std::atomic<uint64_t> g_precond_uid{0};

@@ -24,6 +24,7 @@ struct DeviceInfo {
     uint32_t slab_min_rows = 2048; // smallest slab (small systems use fewer CTAs)
     uint32_t slab_max_rows = 1u << 30;  // largest slab (default: what shared memory holds)
     uint32_t stream_min_rows = 1024;    // smallest streamed slab (small systems use fewer CTAs)
+    int stream_pair = 1;           // where asked: 0 never paired, 1 the tuner decides, 2 paired (pair_sweep)
 };
 
 // Reduction scratch shared by all kernels of one stream (they run serially).
@@ -59,6 +60,20 @@ struct DeviceCsr {
 enum SweepLayout : int { LAYOUT_LEVEL = 0, LAYOUT_SLAB = 1, LAYOUT_STREAM = 2 };
 
 // One triangular sweep resident on the device (see build_sweep for the layout).
+// The host part of a streamed upload (pairing, layout, launch shape; no CUDA calls), which
+// DevSweep::commit_stream uploads.  ok false: the sweep does not fit the streamed layout.
+struct StreamPlan {
+    bool ok = false, paired = false, fp32 = false, a32 = false;
+    StreamLayout L;
+    PairMap pm;
+    uint32_t n = 0, num_levels = 0;
+    int op = 0;
+    uint32_t ctas = 0, ctas_req = 0, slot_bytes = 0, cap = 0, ring = 0, smem = 0;
+    uint64_t nnz = 0;
+};
+template <typename Low>
+StreamPlan plan_stream(const Sweep<Low>& sweep, const DeviceInfo& info, bool acc32, bool pair);
+
 struct DevSweep {
     uint32_t n = 0, num_levels = 0;
     int op = SWEEP_NONE;
@@ -77,10 +92,18 @@ struct DevSweep {
     DevBuf<uint32_t> str_meta, str_cta_round, str_slab_start, str_in_slot;
     DevBuf<uint32_t> str_halo_ptr, str_halo_row, str_halo_sw;
     uint32_t str_ctas_req = 0, str_slot_bytes = 0;  // what the layout was built with (for its export)
+    uint32_t str_round_cap = 0;                     // ... and its record cap (0: none)
+    // LAYOUT_STREAM built from the paired sweep (pair_sweep): the right-hand side map the prep
+    // applies before the kernel
+    bool paired = false;
+    DevBuf<uint32_t> pair_ptr, pair_dep;
+    DevBuf<double> pair_coef;
     // Uploads the sweep in the given layout; false (nothing uploaded) when the
-    // layout does not fit the sweep (stream layout only).
+    // layout does not fit the sweep (stream layout only).  pair: the streamed layout
+    // of the paired sweep (half the wavefronts; other layouts ignore it).
     template <typename Low>
-    bool upload(const Sweep<Low>& s, const DeviceInfo& info, int layout, cudaStream_t st);
+    bool upload(const Sweep<Low>& s, const DeviceInfo& info, int layout, cudaStream_t st, bool pair = false);
+    void commit_stream(StreamPlan&& plan, cudaStream_t st);
     // the stream layout marks its own output pending; the others need launch_fill first
     bool self_filling() const { return layout == LAYOUT_STREAM; }
     uint64_t entries() const { return layout == LAYOUT_STREAM ? str_nnz : (fp32 ? val32.size() : val64.size()); }
@@ -294,9 +317,10 @@ void launch_sweep_kernel(const Handle& h, cudaStream_t st, const DevSweep& s, co
 void launch_spmv(const Handle& h, cudaStream_t st, uint32_t nrows, const uint32_t* rowptr, const uint32_t* col,
                  const double* val, const double* x, double* y, int sub);
 // uploads a sweep, choosing its kernel by timing the layouts (see solve.cu);
-// acc32 (float values only): single-precision arithmetic, streamed layout only
+// acc32 (float values only): single-precision arithmetic, streamed layout only;
+// pair: the paired streamed layout (pair_sweep) is one more candidate
 template <typename Low>
-void tune_sweep(Handle& h, DevSweep& d, const Sweep<Low>& s, bool acc32 = false);
+void tune_sweep(Handle& h, DevSweep& d, const Sweep<Low>& s, bool acc32 = false, bool pair = false);
 
 // grad[k] = -lambda[row(k)] * x[col(k)] over A's stored entries
 void launch_adjoint_outer(const Handle& h, cudaStream_t st, const double* lambda, const double* x, double* grad);

@@ -244,6 +244,25 @@ static __global__ void __launch_bounds__(kBlock) k_stream_prep(uint32_t n, const
     }
 }
 
+// Prep of a paired sweep: each row's right-hand side b'_r = b_r - sum m b_dep (one fused
+// multiply-add per entry, in stored order, in double) into its record; the output marked
+// pending when mark (not when in == out: rows read other rows of `in`).
+template <typename Acc>
+static __global__ void __launch_bounds__(kBlock) k_stream_prep_pair(uint32_t n, const uint32_t* __restrict__ in_slot,
+                                                                    const uint32_t* __restrict__ mptr,
+                                                                    const uint32_t* __restrict__ mdep,
+                                                                    const double* __restrict__ mcoef,
+                                                                    const double* in, Acc* __restrict__ blob,
+                                                                    unsigned long long* out, int mark) {
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        double v = in[r];
+        for (uint32_t q = __ldg(mptr + r); q < __ldg(mptr + r + 1); ++q)
+            v = __fma_rn(-__ldg(mcoef + q), in[__ldg(mdep + q)], v);
+        blob[__ldg(in_slot + r)] = (Acc)v;
+        if (mark) out[r] = kPending;
+    }
+}
+
 // Low: factor value type; Acc: the arithmetic type of the sweep (double; float for the
 // single-precision apply, whose value slots, products and sums are float and whose
 // results are widened to double).

@@ -12,6 +12,8 @@ coupling and low-rank products whose summation order differs from the
 oracle's, so it is compared within a stated tolerance."""
 from __future__ import annotations
 
+import os
+
 import numpy as np
 import pytest
 
@@ -47,6 +49,47 @@ def test_random_sweeps_match_ordered_oracle_bitwise(precision, lower, op):
         assert bitwise_equal(got, ref), (ctas, float(np.abs(got - ref).max()))
         tol = 1e-4 if SINGLE[precision] else 1e-12
         assert np.abs(got - want).max() <= tol * np.abs(want).max()
+
+
+@pytest.mark.parametrize("precision", [P.PRISM_FP32_APPLY, P.PRISM_FP64])
+@pytest.mark.parametrize("lower", [True, False])
+@pytest.mark.parametrize("op", [0, 1, 2, 3])
+def test_paired_random_sweeps_match_ordered_oracle_bitwise(precision, lower, op):
+    """Wavefront pairing (prism_stream_sweep_pair): the paired sweep through the kernel
+    equals the ordered oracle bit for bit on the mapped right-hand side, and the paired
+    solve equals the unpaired substitution within rounding."""
+    rng = np.random.default_rng(2000 + 10 * op + lower)
+    n = 3000
+    rp, ci, v = random_triangular(n, lower, rng, near=10, far=3, long_rows=(37, 1400, 2650))
+    if precision != P.PRISM_FP64:
+        v = v.astype(np.float32).astype(np.float64)
+    d = rng.uniform(1.0, 2.0, n)
+    b = rng.standard_normal(n)
+    want = substitute(rp, ci, v, d, op, lower, b)
+    prow, pcol, pval, mptr, mdep, mcoef = P.stream_sweep_pair(rp, ci, v, diag=d, op=op, lower=lower,
+                                                              precision=precision)
+    bp = orc.pair_rhs(mptr, mdep, mcoef, b)
+    for ctas in (1, 7, 148):
+        order = P.stream_sweep_order(prow, pcol, pval, diag=d, op=op, lower=lower, precision=precision,
+                                     num_ctas=ctas)
+        ref = orc.sweep_ordered(order, bp, diag=d, op=op, lower=lower, single=SINGLE[precision])
+        got = P.stream_sweep_run(prow, pcol, pval, bp, diag=d, op=op, lower=lower, precision=precision,
+                                 num_ctas=ctas)
+        assert bitwise_equal(got, ref), (ctas, float(np.abs(got - ref).max()))
+        tol = 1e-4 if SINGLE[precision] else 1e-11
+        assert np.abs(got - want).max() <= tol * np.abs(want).max()
+
+
+@pytest.fixture(params=["0", "2"], ids=["unpaired", "paired"])
+def pairing(request):
+    """PRISM_STREAM_PAIR for the handles a test builds: 0 never paired, 2 paired where it fits."""
+    old = os.environ.get("PRISM_STREAM_PAIR")
+    os.environ["PRISM_STREAM_PAIR"] = request.param
+    yield request.param == "2"
+    if old is None:
+        del os.environ["PRISM_STREAM_PAIR"]
+    else:
+        os.environ["PRISM_STREAM_PAIR"] = old
 
 
 def _handle_sweep_check(S, sweep, single, rng):
@@ -107,9 +150,10 @@ def test_double_arithmetic_streamed_sweeps_bitwise(precision):
 AMSED_OPTS = dict(levels=3, lanczos_steps=32, low_rank=16, lowrank_type=0, reorder=0)
 
 
-def test_amsed_level_sweeps_bitwise_and_apply_against_oracle():
-    """AMSED/MSLR on 3D Poisson 32^3 with the single-precision apply: every
-    level's block sweeps equal the kernel-order oracle bit for bit; the whole
+def test_amsed_level_sweeps_bitwise_and_apply_against_oracle(pairing):
+    """AMSED/MSLR on 3D Poisson 32^3 with the single-precision apply, the level
+    sweeps paired or not: every level's block sweeps (a paired one with its
+    right-hand side map) equal the kernel-order oracle bit for bit; the whole
     apply equals the oracle's AMSED apply (orc_amsed_apply with kernel-order
     float sweeps, double elsewhere) to within 1e-6 relative in the max norm,
     the room left for the coupling and low-rank products, which sum in
@@ -122,6 +166,7 @@ def test_amsed_level_sweeps_bitwise_and_apply_against_oracle():
     S.attach(F)
     nlev = int(F.info()["nlev"])
     orders = [_handle_sweep_check(S, sw, True, rng) for sw in range(2 * nlev)]
+    assert all(o.paired == pairing for o in orders)
     O = orc.Amsed(F)
     O.use_sweep_orders(orders, single=True)
     for seed in (1, 2, 3):
@@ -130,7 +175,7 @@ def test_amsed_level_sweeps_bitwise_and_apply_against_oracle():
         assert np.abs(got - ref).max() <= 1e-6 * np.abs(ref).max()
 
 
-def test_amsed_fp32_apply_solve_matches_oracle_fcg():
+def test_amsed_fp32_apply_solve_matches_oracle_fcg(pairing):
     """FCG + AMSED with the single-precision apply on the device against the
     oracle's FCG with the same (kernel-order, float-sweep) AMSED apply: the
     same iteration count within 1 and solutions within 1e-9 relative."""
