@@ -4,8 +4,11 @@
 
 #include <algorithm>
 #include <cmath>
+#include <atomic>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
+#include <thread>
 #include <type_traits>
 
 namespace prism {
@@ -924,13 +927,34 @@ bool stream_layout(const Sweep<Low>& s, const std::vector<uint32_t>& start, uint
         std::vector<uint32_t> xrow, xslot, xwait;
     };
     constexpr uint32_t kNone = 0xFFFFFFFFu;
-    std::vector<uint32_t> round_of(n, kNone);   // by row: round of the slab being laid out
-    std::vector<uint32_t> seen(n, kNone);       // by row: slab that last read it ...
-    std::vector<int64_t> last_use(n, -1);       // ... and the last round of that slab reading it
-    std::vector<uint32_t> slot_of(n, kNoSlot);  // by row: its value slot in the slab being laid out
-    std::vector<uint32_t> slot_in(n, kNone);    // by row: slab that slot_of refers to
+    std::vector<uint32_t> round_of(n, kNone);  // by row: its round in its slab (each slab reads its own rows only)
+    // Per-thread scratch: rows a slab reads include other slabs' (halo) rows, so what a slab
+    // records about a row lives in its thread's arrays, tagged with the slab.
+    struct Scratch {
+        std::vector<uint32_t> seen;      // by row: slab that last read it ...
+        std::vector<int64_t> last_use;   // ... and the last round of that slab reading it
+        std::vector<uint32_t> slot_of;   // by row: its value slot in the slab being laid out
+        std::vector<uint32_t> slot_in;   // by row: slab that slot_of refers to
+    };
+    // What one slab contributes, with blob positions relative to its own records; the slabs
+    // are then concatenated in order, so the layout does not depend on the threads.
+    struct SlabOut {
+        std::string err;
+        std::vector<uint8_t> blob;
+        std::vector<uint32_t> meta, halo_row, halo_sw, halo_cnt, cmap;
+        uint32_t rounds = 0, slots = 0, max_round_bytes = 0;
+    };
+    std::vector<SlabOut> parts(num_ctas);
     const uint32_t G = slot_bytes == 4 ? 32u : 16u;  // rows one wavefront serves
-    for (uint32_t b = 0; b < num_ctas; ++b) {
+    auto lay_slab = [&](uint32_t b, Scratch& sc, SlabOut& so) -> bool {
+        auto fail = [&](const std::string& m) {
+            so.err = m;
+            return false;
+        };
+        std::vector<uint32_t>& seen = sc.seen;
+        std::vector<int64_t>& last_use = sc.last_use;
+        std::vector<uint32_t>& slot_of = sc.slot_of;
+        std::vector<uint32_t>& slot_in = sc.slot_in;
         const uint32_t rb = start[b], re = start[b + 1];
         const uint32_t P0 = cpos[b], P1 = cpos[b + 1];
         std::vector<Round> R;
@@ -1036,9 +1060,8 @@ bool stream_layout(const Sweep<Low>& s, const std::vector<uint32_t>& start, uint
                 }
             }
         }
-        out.slots = std::max<uint32_t>(out.slots, (uint32_t)slot_last.size());
-        out.cta_round[b + 1] = out.cta_round[b] + (uint32_t)R.size();
-        out.max_rounds_per_cta = std::max<uint32_t>(out.max_rounds_per_cta, (uint32_t)R.size());
+        so.slots = (uint32_t)slot_last.size();
+        so.rounds = (uint32_t)R.size();
         // 4. records of this slab's rounds
         for (uint32_t r = 0; r < R.size(); ++r) {
             const Round& rd = R[r];
@@ -1062,11 +1085,9 @@ bool stream_layout(const Sweep<Low>& s, const std::vector<uint32_t>& start, uint
             const uint32_t Kg = std::max<uint32_t>((K + 3) / 4, 1);
             if (Eg > 255 || Kg > 255) return fail("a row with more than 1020 entries");
             const RoundRec rec = round_rec(nr, Eg, Kg, vb, slot_bytes);
-            const uint64_t off = out.blob.size();
-            if ((off + rec.bytes) / 16 > 0xFFFFFFFFull || (off + rec.bytes) / slot_bytes > 0xFFFFFFFFull)
-                return fail("round records beyond the addressable blob");
-            out.blob.resize(off + rec.bytes, 0);
-            uint8_t* base = out.blob.data() + off;
+            const uint64_t off = so.blob.size();  // relative to the slab's records until assembled
+            so.blob.resize(off + rec.bytes, 0);
+            uint8_t* base = so.blob.data() + off;
             for (uint32_t p = rd.p0; p < rd.p1; ++p) {
                 const uint32_t j = p - rd.p0, row = sl.order[p];
                 const uint32_t os = seen[row] == b && slot_in[row] == b && last_use[row] > (int64_t)r ? slot_of[row]
@@ -1109,8 +1130,8 @@ bool stream_layout(const Sweep<Low>& s, const std::vector<uint32_t>& start, uint
                                 dep = sl.col[pr.second];
                                 if (coef_map) {
                                     const uint64_t at = off + sec_c + 4u * vb * ((size_t)(u / 4) * rec.m + j) + vb * (u % 4);
-                                    coef_map->push_back((uint32_t)(at / vb));
-                                    coef_map->push_back(sweep_entry[pr.second]);
+                                    so.cmap.push_back((uint32_t)(at / vb));
+                                    so.cmap.push_back(sweep_entry[pr.second]);
                                 }
                             } else {
                                 slot = (uint16_t)(-1 - e);
@@ -1128,16 +1149,73 @@ bool stream_layout(const Sweep<Low>& s, const std::vector<uint32_t>& start, uint
             place(lat, Kg, rec.ls, rec.lc, order ? &ord_k : nullptr);
             const uint32_t X = (uint32_t)rd.xrow.size();
             for (uint32_t x = 0; x < X; ++x) {
-                out.halo_row.push_back(rd.xrow[x]);
-                out.halo_sw.push_back(rd.xslot[x] | (rd.xwait[x] << 16));
+                so.halo_row.push_back(rd.xrow[x]);
+                so.halo_sw.push_back(rd.xslot[x] | (rd.xwait[x] << 16));
+            }
+            so.halo_cnt.push_back(X);
+            so.meta.push_back((uint32_t)(off / 16));
+            so.meta.push_back(rec.bytes);
+            so.meta.push_back(nr | (Eg << 8) | (Kg << 16) | ((X > 0 ? 1u : 0u) << 24));
+            so.meta.push_back(0);
+            so.max_round_bytes = std::max(so.max_round_bytes, rec.bytes);
+        }
+        return true;
+    };
+    // the slabs on a few host threads, each with its own scratch
+    {
+        unsigned hc = std::max(1u, std::thread::hardware_concurrency());
+        if (const char* e = std::getenv("PRISM_LAYOUT_THREADS")) hc = (unsigned)std::max(1, std::atoi(e));
+        const unsigned T = num_ctas < 8 ? 1u : std::min<unsigned>(std::min(hc, 16u), num_ctas);
+        std::atomic<uint32_t> next{0};
+        auto worker = [&]() {
+            Scratch sc;
+            sc.seen.assign(n, kNone);
+            sc.last_use.assign(n, -1);
+            sc.slot_of.assign(n, kNoSlot);
+            sc.slot_in.assign(n, kNone);
+            for (uint32_t b = next++; b < num_ctas; b = next++) lay_slab(b, sc, parts[b]);
+        };
+        if (T == 1) {
+            worker();
+        } else {
+            std::vector<std::thread> pool;
+            for (unsigned t = 0; t < T; ++t) pool.emplace_back(worker);
+            for (auto& th : pool) th.join();
+        }
+    }
+    // assembly, slab by slab
+    for (uint32_t b = 0; b < num_ctas; ++b) {
+        SlabOut& so = parts[b];
+        if (!so.err.empty()) return fail(so.err);
+        const uint64_t base = out.blob.size();
+        if ((base + so.blob.size()) / 16 > 0xFFFFFFFFull || (base + so.blob.size()) / slot_bytes > 0xFFFFFFFFull)
+            return fail("round records beyond the addressable blob");
+        out.blob.insert(out.blob.end(), so.blob.begin(), so.blob.end());
+        for (size_t t = 0; t < so.meta.size(); t += 4) {
+            out.meta.push_back(so.meta[t] + (uint32_t)(base / 16));
+            out.meta.push_back(so.meta[t + 1]);
+            out.meta.push_back(so.meta[t + 2]);
+            out.meta.push_back(so.meta[t + 3]);
+        }
+        size_t h = 0;
+        for (uint32_t c : so.halo_cnt) {
+            for (uint32_t x = 0; x < c; ++x, ++h) {
+                out.halo_row.push_back(so.halo_row[h]);
+                out.halo_sw.push_back(so.halo_sw[h]);
             }
             out.halo_ptr.push_back((uint32_t)out.halo_row.size());
-            out.meta.push_back((uint32_t)(off / 16));
-            out.meta.push_back(rec.bytes);
-            out.meta.push_back(nr | (Eg << 8) | (Kg << 16) | ((X > 0 ? 1u : 0u) << 24));
-            out.meta.push_back(0);
-            out.max_round_bytes = std::max(out.max_round_bytes, rec.bytes);
         }
+        for (uint32_t row = start[b]; row < start[b + 1]; ++row) out.in_slot[row] += (uint32_t)(base / slot_bytes);
+        if (coef_map)
+            for (size_t t = 0; t < so.cmap.size(); t += 2) {
+                coef_map->push_back(so.cmap[t] + (uint32_t)(base / vb));
+                coef_map->push_back(so.cmap[t + 1]);
+            }
+        out.slots = std::max(out.slots, so.slots);
+        out.cta_round[b + 1] = out.cta_round[b] + so.rounds;
+        out.max_rounds_per_cta = std::max(out.max_rounds_per_cta, so.rounds);
+        out.max_round_bytes = std::max(out.max_round_bytes, so.max_round_bytes);
+        SlabOut().blob.swap(so.blob);  // release the slab's copy
     }
     out.num_rounds = out.cta_round[num_ctas];
     if (order) {

@@ -151,3 +151,24 @@ def test_replay_block_diagonal_slabs_follow_the_blocks():
     for ctas in (4, 7, 19):
         got = P.selftest_stream_layout(rp, ci, v, b, diag=d, op=0, lower=True, num_ctas=ctas, rows_per_cta=0)
         np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-12)
+
+
+def test_layout_does_not_depend_on_host_threads(monkeypatch):
+    """The streamed layout is built slab by slab on several host threads and assembled in
+    slab order: one thread and several give the same summation order and the same replay."""
+    rng = np.random.default_rng(77)
+    n = 6000
+    rp, ci, v = random_triangular(n, True, rng, near=12, far=4, long_rows=(100, 3000))
+    d = rng.uniform(1.0, 2.0, n)
+    b = rng.standard_normal(n)
+    got = []
+    for threads in ("1", "5"):
+        monkeypatch.setenv("PRISM_LAYOUT_THREADS", threads)
+        o = P.stream_sweep_order(rp, ci, v, diag=d, op=0, lower=True, precision=P.PRISM_FP32_APPLY, num_ctas=40)
+        x = P.selftest_stream_layout(rp, ci, v, b, diag=d, op=0, lower=True, precision=P.PRISM_FP32_APPLY,
+                                     num_ctas=40)
+        got.append((o, x))
+    (o1, x1), (o2, x2) = got
+    for f in ("eptr", "edep", "ecoef", "kptr", "kdep", "kcoef"):
+        assert np.array_equal(getattr(o1, f), getattr(o2, f)), f
+    assert np.array_equal(x1, x2)
