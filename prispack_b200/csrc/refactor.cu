@@ -444,6 +444,17 @@ void TriangularPrecond::refactor() {
         throw Error(PRISM_ERR_UNSUPPORTED, "a factor column longer than " + std::to_string(kRfMaxCol) + " entries");
     cudaStream_t st = h_.stream;
     const bool ldlt = F.kind == 3;
+    // A paired sweep's coefficients combine several factor entries, which the value maps
+    // below cannot rebuild: such sweeps are tuned again without pairing first.
+    if (!rf_ && (lower_.paired || upper_.paired)) {
+        if (F.fp32) {
+            if (lower_.paired) tune_sweep(h_, lower_, F.lower32, F.apply32, false);
+            if (upper_.paired) tune_sweep(h_, upper_, F.upper32, F.apply32, false);
+        } else {
+            if (lower_.paired) tune_sweep(h_, lower_, F.lower64, false, false);
+            if (upper_.paired) tune_sweep(h_, upper_, F.upper64, false, false);
+        }
+    }
     if (!rf_) {
         rf_.reset(new RefactorState());
         RefactorState& R = *rf_;

@@ -671,12 +671,13 @@ std::atomic<uint64_t> g_precond_uid{0};
 Precond::Precond() : uid(++g_precond_uid) {}
 
 TriangularPrecond::TriangularPrecond(Handle& h, std::shared_ptr<const HostFactor> f) : h_(h), f_(std::move(f)) {
+    // the streamed kernel may run the sweeps paired (refactor() tunes them again unpaired)
     if (f_->fp32) {
-        tune_sweep(h_, lower_, f_->lower32, f_->apply32);
-        tune_sweep(h_, upper_, f_->upper32, f_->apply32);
+        tune_sweep(h_, lower_, f_->lower32, f_->apply32, true);
+        tune_sweep(h_, upper_, f_->upper32, f_->apply32, true);
     } else {
-        tune_sweep(h_, lower_, f_->lower64);
-        tune_sweep(h_, upper_, f_->upper64);
+        tune_sweep(h_, lower_, f_->lower64, false, true);
+        tune_sweep(h_, upper_, f_->upper64, false, true);
     }
     tmp_.alloc(h_.A.n);  // here rather than at the first apply, which may be under graph capture
 }

@@ -27,15 +27,27 @@ CASES = [(P.PRECOND_IC, P.PRISM_FP64), (P.PRECOND_IC, P.PRISM_FP32), (P.PRECOND_
          (P.PRECOND_ILDLT, P.PRISM_FP64), (P.PRECOND_ILDLT, P.PRISM_FP32)]
 
 
+def _set_env(**kv):
+    old = {k: os.environ.get(k) for k in kv}
+    os.environ.update(kv)
+    return old
+
+
+def _restore_env(old):
+    for k, v in old.items():
+        if v is None:
+            del os.environ[k]
+        else:
+            os.environ[k] = v
+
+
 @pytest.fixture(params=["global", "slab", "stream"])
 def layout(request):
-    old = os.environ.get("PRISM_SWEEP_KERNEL")
-    os.environ["PRISM_SWEEP_KERNEL"] = request.param
+    """The sweep kernel, unpaired (a paired sweep is tuned again unpaired at the first
+    refactorisation: test_refactor_of_paired_sweeps)."""
+    old = _set_env(PRISM_SWEEP_KERNEL=request.param, PRISM_STREAM_PAIR="0")
     yield request.param
-    if old is None:
-        del os.environ["PRISM_SWEEP_KERNEL"]
-    else:
-        os.environ["PRISM_SWEEP_KERNEL"] = old
+    _restore_env(old)
 
 
 def new_values(A, seed=5):
@@ -140,3 +152,36 @@ def test_refactor_is_refused_where_it_does_not_exist():
     with pytest.raises(P.PrismError) as e:
         S.refactor()
     assert e.value.status == 9  # PRISM_ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("kind,precision", [(P.PRECOND_IC, P.PRISM_FP64), (P.PRECOND_ILDLT, P.PRISM_FP32_APPLY)])
+def test_refactor_of_paired_sweeps(kind, precision):
+    """Streamed sweeps running paired (wavefront pairing): the first refactorisation tunes
+    them again unpaired, whose value maps it fills; the factor is the oracle's bit for bit
+    and the apply matches the oracle's as for unpaired sweeps."""
+    old = _set_env(PRISM_SWEEP_KERNEL="stream", PRISM_STREAM_PAIR="2")
+    try:
+        A = P.CSRMatrix.laplacian(14, 12, 10)
+        S = P.DeviceSystem(A)
+        S.set_precond(kind, tol=1e-3, precision=precision)
+        assert S.sweep_order(0).paired and S.sweep_order(1).paired
+        rp, ci, _, _ = S.precond_factor(0)
+        val2 = new_values(A, seed=12)
+        S.update_values(val2)
+        S.refactor()
+        assert not S.sweep_order(0).paired and not S.sweep_order(1).paired
+        rc, lv, D = orc.refactor(kind, A.rowptr, A.col, val2, rp, ci, single=precision != P.PRISM_FP64)
+        assert rc == 0
+        _, _, dv, dd = S.precond_factor(0)
+        assert np.array_equal(dv, lv)
+        v = np.random.default_rng(2).standard_normal(A.n)
+        got = S.apply(v)
+        ref = oracle_precond(kind, A.n, rp, ci, lv, D).apply(v.copy())
+        if precision == P.PRISM_FP32_APPLY:
+            assert np.linalg.norm(got - ref) <= 1e-5 * np.linalg.norm(ref)
+        else:
+            assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
+        x, st = S.solve(np.random.default_rng(3).standard_normal(A.n), tol=1e-10, max_iter=500)
+        assert st.converged and st.true_rel_residual < 1e-9
+    finally:
+        _restore_env(old)
