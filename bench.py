@@ -909,7 +909,7 @@ def main():
                                                           for i, b_ in zip(sweep_infos, sweep_bytes))),
                          "traffic_source": TRAFFIC_SOURCE},
             "spmv": {"ms": round(statistics.median(spmv_ms), 4), "bytes": spmv_bytes, "GB/s": round(spmv_gbs, 1),
-                     "frac": round(spmv_gbs / peak, 4)},
+                     "frac": round(spmv_gbs / peak, 4), "shape": list(S.spmv_shape())},
             "fp64_factor": fp64,
             "fp32_storage": fp32_storage,
             "parity_vs_reference_fp64": parity,

@@ -267,6 +267,12 @@ int32_t prism_dims(prism_handle h, uint32_t* n, uint64_t* nnz);
 /* y = A x on device pointers / host pointers */
 int32_t prism_spmv_device(prism_handle h, const double* x_d, double* y_d);
 int32_t prism_spmv(prism_handle h, const double* x, double* y);
+/* The shape of the handle's SpMV kernel, which prism_create chose by timing each
+ * shape on A (PRISM_SPMV_SHAPE = 0..5 names one instead): lanes that share a
+ * row and rows each group of lanes takes per pass.  The shape decides only the
+ * order of each row's sum.  No reference counterpart (CSRMatrix::MatPVec,
+ * include/MatrixClass/CSRMatrix.h:360-395, runs one row per thread). */
+int32_t prism_spmv_shape(prism_handle h, int32_t* lanes_per_row, int32_t* rows_per_pass);
 
 /* ---- preconditioners (host setup, bit-exact with the reference; then uploaded) -- */
 int32_t prism_set_precond_none(prism_handle h);

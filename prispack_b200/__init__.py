@@ -101,6 +101,7 @@ _SIGS = {
     "prism_set_stream": (C.c_int32, [_vp, _vp]),
     "prism_dims": (C.c_int32, [_vp, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]),
     "prism_spmv_device": (C.c_int32, [_vp, _vp, _vp]),
+    "prism_spmv_shape": (C.c_int32, [_vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "prism_spmv": (C.c_int32, [_vp, _f64p, _f64p]),
     "prism_set_precond_none": (C.c_int32, [_vp]),
     "prism_set_precond_ic": (C.c_int32, [_vp, C.c_double, C.c_int32]),
@@ -658,6 +659,12 @@ class DeviceSystem:
         y = np.zeros(self.n)
         _check(self.lib.prism_spmv(self.h, x, y))
         return y
+
+    def spmv_shape(self) -> tuple:
+        """(lanes per row, rows per pass) of the SpMV kernel the handle chose at creation."""
+        g, u = C.c_int32(), C.c_int32()
+        _check(self.lib.prism_spmv_shape(self.h, C.byref(g), C.byref(u)))
+        return g.value, u.value
 
     def spmv_into(self, x, y):
         """y = A x on CUDA tensors (y preallocated; no allocation in the call)."""

@@ -464,6 +464,7 @@ int32_t prism_create(uint32_t n, const uint32_t* rowptr, const uint32_t* col, co
                                        h->stream));
             PRISM_CUDA(cudaMemsetAsync(h->status.get(), 0, sizeof(int), h->stream));
             PRISM_CUDA(cudaStreamSynchronize(h->stream));
+            h->tune_spmv();
         } catch (...) {
             delete h;
             throw;
@@ -511,6 +512,15 @@ int32_t prism_spmv_device(prism_handle h, const double* x_d, double* y_d) {
         PRISM_CUDA(cudaStreamSynchronize(h->stream));
         return PRISM_OK;
     });
+}
+
+int32_t prism_spmv_shape(prism_handle h, int32_t* lanes_per_row, int32_t* rows_per_pass) {
+    if (!h || !lanes_per_row || !rows_per_pass) return fail(PRISM_ERR_ARG, "null handle or output");
+    int g = 0, u = 0;
+    h->spmv_shape_of(&g, &u);
+    *lanes_per_row = g;
+    *rows_per_pass = u;
+    return PRISM_OK;
 }
 
 int32_t prism_spmv(prism_handle h, const double* x, double* y) {

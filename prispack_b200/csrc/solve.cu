@@ -21,6 +21,11 @@ namespace {
 constexpr unsigned long long kWaitNs = 1000000000ull;  // 1 s per dependency wait
 constexpr int kSpmvSubG = 8;                           // lanes per row in k_spmv_sub
 constexpr int kSpmvG = 1, kSpmvU = 2;                  // k_spmv: lanes per row, rows per group and pass
+// the shapes A's SpMV may take (lanes per row, rows per group and pass): one lane per row
+// suits short rows such as stencils, a group of lanes per row longer ones
+constexpr int kSpmvShapes = 6;
+constexpr int kSpmvShapeG[kSpmvShapes] = {1, 1, 2, 4, 8, 16};
+constexpr int kSpmvShapeU[kSpmvShapes] = {2, 4, 2, 1, 1, 1};
 }  // namespace
 
 int vec_grid(const Handle& h, uint32_t n) {
@@ -324,22 +329,75 @@ void Handle::ensure_workspace() {
     }
 }
 
-void Handle::spmv(const double* x, double* yout, int ndot, const double* z, const double* q, int scalar) {
-    const uint32_t n = A.n;
-    if (!n) return;
-    const long rows_per_block = (long)(kBlock / 32) * (32 / kSpmvG) * kSpmvU;
+namespace {
+template <int G, int U>
+void spmv_shape_launch(const Handle& h, const double* x, double* yout, int ndot, const double* z, const double* q,
+                       ReduceSlot slot) {
+    const uint32_t n = h.A.n;
+    const long rows_per_block = (long)(kBlock / 32) * (32 / G) * U;
     long want = ((long)n + rows_per_block - 1) / rows_per_block;
-    long cap = (long)info.sms * 8;
+    long cap = (long)h.info.sms * 8;
     int grid = (int)(want < cap ? want : cap);
     if (grid > Reducer::kMaxGrid) grid = Reducer::kMaxGrid;
-    ReduceSlot slot = red.slot(scalar);
-    const uint32_t* rp = A.rowptr.get();
-    const uint32_t* ci = A.col.get();
-    const double* va = A.val.get();
-    if (ndot == 0) k_spmv<kSpmvG, kSpmvU, 0><<<grid, kBlock, 0, stream>>>(n, rp, ci, va, x, yout, z, q, slot);
-    else if (ndot == 1) k_spmv<kSpmvG, kSpmvU, 1><<<grid, kBlock, 0, stream>>>(n, rp, ci, va, x, yout, z, q, slot);
-    else k_spmv<kSpmvG, kSpmvU, 2><<<grid, kBlock, 0, stream>>>(n, rp, ci, va, x, yout, z, q, slot);
+    const uint32_t* rp = h.A.rowptr.get();
+    const uint32_t* ci = h.A.col.get();
+    const double* va = h.A.val.get();
+    if (ndot == 0) k_spmv<G, U, 0><<<grid, kBlock, 0, h.stream>>>(n, rp, ci, va, x, yout, z, q, slot);
+    else if (ndot == 1) k_spmv<G, U, 1><<<grid, kBlock, 0, h.stream>>>(n, rp, ci, va, x, yout, z, q, slot);
+    else k_spmv<G, U, 2><<<grid, kBlock, 0, h.stream>>>(n, rp, ci, va, x, yout, z, q, slot);
     PRISM_LAUNCHED();
+}
+}  // namespace
+
+void Handle::spmv(const double* x, double* yout, int ndot, const double* z, const double* q, int scalar) {
+    if (!A.n) return;
+    const ReduceSlot slot = red.slot(scalar);
+    switch (spmv_shape) {
+        case 1: spmv_shape_launch<kSpmvShapeG[1], kSpmvShapeU[1]>(*this, x, yout, ndot, z, q, slot); break;
+        case 2: spmv_shape_launch<kSpmvShapeG[2], kSpmvShapeU[2]>(*this, x, yout, ndot, z, q, slot); break;
+        case 3: spmv_shape_launch<kSpmvShapeG[3], kSpmvShapeU[3]>(*this, x, yout, ndot, z, q, slot); break;
+        case 4: spmv_shape_launch<kSpmvShapeG[4], kSpmvShapeU[4]>(*this, x, yout, ndot, z, q, slot); break;
+        case 5: spmv_shape_launch<kSpmvShapeG[5], kSpmvShapeU[5]>(*this, x, yout, ndot, z, q, slot); break;
+        default: spmv_shape_launch<kSpmvShapeG[0], kSpmvShapeU[0]>(*this, x, yout, ndot, z, q, slot); break;
+    }
+}
+
+void Handle::spmv_shape_of(int* lanes_per_row, int* rows_per_pass) const {
+    const int s = spmv_shape >= 0 && spmv_shape < kSpmvShapes ? spmv_shape : 0;
+    if (lanes_per_row) *lanes_per_row = kSpmvShapeG[s];
+    if (rows_per_pass) *rows_per_pass = kSpmvShapeU[s];
+}
+
+// Times A x with each shape (one warm-up and three timed launches, the plain product
+// without fused dot products) and keeps the fastest; PRISM_SPMV_SHAPE (0..5) forces one.
+void Handle::tune_spmv() {
+    spmv_shape = 0;
+    if (const char* e = std::getenv("PRISM_SPMV_SHAPE")) {
+        const int v = std::atoi(e);
+        spmv_shape = v >= 0 && v < kSpmvShapes ? v : 0;
+        return;
+    }
+    if (A.n == 0) return;
+    DevBuf<double> x(A.n), y(A.n);
+    std::vector<double> ones(A.n, 1.0);
+    x.upload(ones.data(), A.n, stream);
+    float best = 0.f;
+    int best_s = 0;
+    for (int s = 0; s < kSpmvShapes; ++s) {
+        spmv_shape = s;
+        spmv(x.get(), y.get());
+        PRISM_CUDA(cudaEventRecord(ev0, stream));
+        for (int it = 0; it < 3; ++it) spmv(x.get(), y.get());
+        PRISM_CUDA(cudaEventRecord(ev1, stream));
+        PRISM_CUDA(cudaEventSynchronize(ev1));
+        float ms = 0.f;
+        PRISM_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+        if (s == 0 || ms < best) {
+            best = ms;
+            best_s = s;
+        }
+    }
+    spmv_shape = best_s;
 }
 
 void Handle::check_status() {

@@ -298,6 +298,11 @@ struct Handle {
     ~Handle();
     void spmv(const double* x, double* y, int ndot = 0, const double* z = nullptr, const double* q = nullptr,
               int scalar = 0);
+    // the shape of A's SpMV kernel (index into the shape table in solve.cu), chosen at
+    // creation by timing each shape (tune_spmv) unless PRISM_SPMV_SHAPE names one
+    int spmv_shape = 0;
+    void tune_spmv();
+    void spmv_shape_of(int* lanes_per_row, int* rows_per_pass) const;
     void check_status();           // synchronises; throws on a raised device status
     void ensure_workspace();
 };
