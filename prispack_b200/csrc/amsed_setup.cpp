@@ -5,10 +5,12 @@
 #include "amsed_setup.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <limits>
 #include <numeric>
 #include <random>
+#include <thread>
 
 extern "C" int64_t prism_graph_bisect(int32_t n, const int32_t* xadj, const int32_t* adjncy, int32_t* part);
 
@@ -589,18 +591,40 @@ void tridiag_eig(int m, const double* d_in, const double* e_in, double* mu, doub
 // ============================================================================
 // Host applies of the partial preconditioner
 // ============================================================================
+// fn(i) for i in [0, count) on up to `threads` host threads (the items are independent:
+// the results do not depend on the thread count)
+template <typename F>
+void host_parallel_for(uint32_t count, unsigned threads, F&& fn) {
+    threads = std::min<unsigned>(threads, count);
+    if (threads <= 1) {
+        for (uint32_t i = 0; i < count; ++i) fn(i);
+        return;
+    }
+    std::atomic<uint32_t> next{0};
+    std::vector<std::thread> pool;
+    for (unsigned t = 0; t < threads; ++t)
+        pool.emplace_back([&] {
+            for (uint32_t i = next++; i < count; i = next++) fn(i);
+        });
+    for (auto& th : pool) th.join();
+}
+unsigned host_threads() { return std::max(1u, std::min(std::thread::hardware_concurrency(), 16u)); }
+
 template <typename Low>
 void amsed_block_solve_host(const AmsedSetup<Low>& S, int level, double* x) {
     const AmsedLevel<Low>& L = S.levels[level];
     const bool last = level == (int)S.nlev - 1;
-    for (uint32_t b = 0; b < L.ncomps; ++b) {
+    auto block = [&](uint32_t b) {
         double* seg = x + (L.dom_ptr[b] - L.dom_ptr[0]);
         if (last) {
             if (b == 0) ic_apply(L.Lt[0], seg);  // only block 0 carries a factor on the last level
         } else {
             ildlt_apply(L.Lt[b], L.D[b], seg);
         }
-    }
+    };
+    // the blocks are independent: large levels solve them on several host threads
+    const uint32_t rows = L.dom_ptr[L.ncomps] - L.dom_ptr[0];
+    host_parallel_for(L.ncomps, !last && rows >= 65536 ? host_threads() : 1u, block);
 }
 
 // levelCInvRecursiveSolve(level, x, 0) with x the C block of `level` (length len)
@@ -1085,9 +1109,17 @@ int amsed_setup(const CsrHost& A, const AmsedOptions& opt, AmsedSetup<Low>& S, s
             L.Lt.resize(nblk);
             L.U.resize(nblk);
             L.Dinv.resize(nblk);
+            std::vector<int> rcs(nblk, 0);
+            std::vector<std::string> errs(nblk);
+            host_parallel_for(nblk, host_threads(), [&](uint32_t b) {
+                rcs[b] = ilut_factor<Low>(L.B[b], lfill, opt.factor_tol, L.Lt[b], L.U[b], L.Dinv[b],
+                                          err ? &errs[b] : nullptr);
+            });
             for (uint32_t b = 0; b < nblk; ++b) {
-                int rc = ilut_factor<Low>(L.B[b], lfill, opt.factor_tol, L.Lt[b], L.U[b], L.Dinv[b], err);
-                if (rc) return rc;
+                if (rcs[b]) {
+                    if (err) *err = errs[b];
+                    return rcs[b];
+                }
                 const uint64_t m = L.Lt[b].nnz() + L.U[b].nnz() + L.B[b].n;
                 S.mnnz += m;
                 S.incomp_nnz += m;
@@ -1119,9 +1151,18 @@ int amsed_setup(const CsrHost& A, const AmsedOptions& opt, AmsedSetup<Low>& S, s
         AmsedLevel<Low>& L = S.levels[level];
         L.Lt.resize(L.ncomps);
         L.D.resize(L.ncomps);
+        // the blocks' factorisations are independent: several host threads, results and the
+        // first failing block (in block order) as one thread would give them
+        std::vector<int> rcs(L.ncomps, 0);
+        std::vector<std::string> errs(L.ncomps);
+        host_parallel_for(L.ncomps, host_threads(), [&](uint32_t b) {
+            rcs[b] = ildlt_factor<Low>(L.B[b], opt.factor_tol, L.Lt[b], L.D[b], err ? &errs[b] : nullptr);
+        });
         for (uint32_t b = 0; b < L.ncomps; ++b) {
-            int rc = ildlt_factor<Low>(L.B[b], opt.factor_tol, L.Lt[b], L.D[b], err);
-            if (rc) return rc;
+            if (rcs[b]) {
+                if (err) *err = errs[b];
+                return rcs[b];
+            }
             const uint64_t m = L.Lt[b].nnz() * 2 + L.B[b].n;
             S.mnnz += m;
             S.incomp_nnz += m;
