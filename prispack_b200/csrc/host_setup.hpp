@@ -151,10 +151,11 @@ void slab_layout(const Sweep<Low>& s, uint32_t num_ctas, uint32_t rows_per_cta, 
 // pad short rows.
 //
 // The dependencies of a row of round r split in two: "late" ones, rows of the
-// slab computed in round r - 1, and "early" ones, everything else (rows of
-// rounds <= r - 2 and halo rows).  The kernel sums a round's early entries
-// while the round before it is still being computed, so only the late ones
-// (two or three per row on 3D stencils) sit on the chain of rounds.  Inside
+// slab computed in the kStreamLate rounds before r, and "early" ones,
+// everything else (rows of earlier rounds and halo rows).  The kernel sums a
+// round's early entries while the rounds before it are still being computed,
+// so only the late ones (about a quarter of a row's entries on 3D stencils)
+// sit on the chain of rounds.  Inside
 // each group of rows that one shared-memory wavefront serves (32 rows for
 // 4-byte slots, 16 for 8-byte ones) the entries of every row are ordered so
 // that, position by position, the rows read slots of distinct banks where the
@@ -192,7 +193,7 @@ constexpr uint32_t kRoundRows = 128;
 // A dependency of a row of round r is "late" when it is a row of the slab computed in one of
 // the kStreamLate rounds before r; every other dependency (rounds <= r - kStreamLate - 1,
 // halo rows) is "early" and is summed before round r starts.
-constexpr uint32_t kStreamLate = 2;
+constexpr uint32_t kStreamLate = 3;
 constexpr uint32_t kNoSlot = 0xFFFFu;
 struct RoundRec {
     uint32_t m, fld, lo, es, ec, ls, lc, bytes;

@@ -75,7 +75,7 @@ constexpr int kStrPrefetch0 = kStrRowWarps + kStrHelperWarps;
 constexpr int kStrProducer = kStrPrefetch0 + kStrPrefetchWarps;
 constexpr int kStrThreads = 32 * (kStrProducer + 1);
 constexpr uint32_t kStrMaxRounds = 64;                 // rounds in flight (ring table and halo flag slots)
-constexpr uint32_t kStrPackets = 3;                    // rounds of packets in shared memory
+constexpr uint32_t kStrPackets = 4;                    // rounds of packets in shared memory
 static_assert(kStrPackets > kStreamLate, "a packet slot is refilled only after its round is done");
 // copy barriers, halo flags, ring offsets, words, packet flags [4], packet round info [4]
 static_assert(kStrPackets <= 4, "packet flag space");

@@ -1,8 +1,9 @@
 """The streamed sweep kernel against the oracle, bit for bit.
 
 The kernel sums each row in its own order: the "early" entries in four
-interleaved fused multiply-add chains, then the "late" ones (the rows of the
-round just before) one by one (prism_stream_sweep_order states the order).
+interleaved fused multiply-add chains, then the "late" ones (the slab's rows of
+the three rounds just before) one by one (prism_stream_sweep_order states the
+order).
 oracle.sweep_ordered restates that arithmetic in plain C from the exported
 order alone, so the GPU results must equal it to the last bit, in float for
 the single-precision apply (PRISM_FP32_APPLY) and in double otherwise; the

@@ -65,8 +65,9 @@ def test_order_is_a_permutation_of_each_row():
 
 
 def test_late_entries_are_few_on_a_3d_factor():
-    """On an IC factor of 3D Poisson most of a row's entries are summed a round
-    ahead: the late ones (rows of the round just before) are a small part."""
+    """On an IC factor of 3D Poisson most of a row's entries are summed ahead of
+    their round: the late ones (slab rows of the kStreamLate = 3 rounds just
+    before) are under a third of them."""
     A = P.CSRMatrix.laplacian(16, 16, 16)
     F = P.HostFactor(A, P.PRECOND_IC, tol=1e-3)
     rp, ci, v, _ = F.arrays(0)
@@ -79,4 +80,4 @@ def test_late_entries_are_few_on_a_3d_factor():
     late = int((o.kdep != P.SweepOrder.PAD).sum())
     early = int((o.edep != P.SweepOrder.PAD).sum())
     assert late + early == int(off.sum())
-    assert late < 0.25 * (late + early)
+    assert late < 0.3 * (late + early)
