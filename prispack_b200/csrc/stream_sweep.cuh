@@ -77,9 +77,10 @@ constexpr int kStrThreads = 32 * (kStrProducer + 1);
 constexpr uint32_t kStrMaxRounds = 64;                 // rounds in flight (ring table and halo flag slots)
 constexpr uint32_t kStrPackets = 4;                    // rounds of packets in shared memory
 static_assert(kStrPackets > kStreamLate, "a packet slot is refilled only after its round is done");
-// copy barriers, halo flags, ring offsets, words, packet flags [4], packet round info [4]
-static_assert(kStrPackets <= 4, "packet flag space");
-constexpr uint32_t kStrFixedSmem = 64 * 8 + 64 * 4 + 64 * 4 + 32 + 4 * 4 + 4 * 8 + 16;
+// copy barriers, halo flags, ring offsets, words, packet flags [kStrPkSlots], packet round
+// info [kStrPkSlots]
+constexpr uint32_t kStrPkSlots = (kStrPackets + 3u) & ~3u;
+constexpr uint32_t kStrFixedSmem = 64 * 8 + 64 * 4 + 64 * 4 + 32 + kStrPkSlots * 4 + kStrPkSlots * 8 + 16;
 constexpr unsigned long long kStrDrainNs = 2000000000ull;  // bound of the final wait for copies in flight
 static_assert(kStrThreads <= 1024, "warp roles");
 static_assert(kStrFixedSmem % 16 == 0, "round table alignment");
@@ -274,7 +275,7 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
     uint32_t* ring_off = hflag + 64;                                           // [64]
     uint32_t* words = ring_off + 64;                                           // landed, rounds done, abort
     uint32_t* pflag = words + 8;                                               // [kStrPackets] round q's packets: q + 1
-    uint2* pinfo = reinterpret_cast<uint2*>(pflag + 4);                        // [kStrPackets] {ring offset, shape}
+    uint2* pinfo = reinterpret_cast<uint2*>(pflag + kStrPkSlots);              // [kStrPackets] {ring offset, shape}
     constexpr uint32_t vb = sizeof(Low), ab = sizeof(Acc);
     constexpr uint32_t PW = stream_packet_words(vb, ab);
     const StrSmem lay = stream_smem(a.meta_slots, a.slots, ab, vb, a.ring_bytes);
