@@ -27,7 +27,7 @@
 // warps.  The setup orders every row's entries so that the 32 (16 for 8-byte
 // slots) rows one wavefront serves read distinct banks.
 //
-// Roles (384 threads, three warps per SM sub-partition):
+// Roles (416 threads, 13 warps):
 //   warps 0..3    row threads: thread j computes row j of each round.  Round i:
 //                 wait for its packets, load the late values, add them to P one
 //                 fused multiply-add at a time, the result into its slot and into
@@ -38,11 +38,11 @@
 //                 <= q - kStreamLate - 1 are done, round q's record has landed and
 //                 its halo is in, then sums the early entries of every row of round
 //                 q (slices of 32 rows) and publishes the round's packets.
-//   warps 8..10   prefetchers: warp 8+k handles the halo of rounds k, k+3, ...:
+//   warps 8..11   prefetchers: warp 8+k handles the halo of rounds k, k+4, ...:
 //                 polls each halo row in global memory until it is finished,
 //                 waits until the slot's previous value has had its last reader,
 //                 writes the slot and raises the round's halo flag.
-//   warp 11       producer: issues the bulk copies of the records into the ring
+//   warp 12       producer: issues the bulk copies of the records into the ring
 //                 in order, publishes how many have landed, and recycles the ring
 //                 space of finished rounds.
 //
@@ -70,7 +70,7 @@ namespace prism {
 
 constexpr int kStrRowWarps = (int)kRoundRows / 32;     // row threads: one per row of a round
 constexpr int kStrHelperWarps = 4;                     // early sums: warps kStrRowWarps ..
-constexpr int kStrPrefetchWarps = 3;                   // halo copies
+constexpr int kStrPrefetchWarps = 4;                   // halo copies
 constexpr int kStrPrefetch0 = kStrRowWarps + kStrHelperWarps;
 constexpr int kStrProducer = kStrPrefetch0 + kStrPrefetchWarps;
 constexpr int kStrThreads = 32 * (kStrProducer + 1);
@@ -402,7 +402,8 @@ static __global__ void __launch_bounds__(kStrThreads, 1) k_sweep_stream(const St
 
     if (warp >= kStrPrefetch0) {
         // ------------------------------------------------------------------ prefetchers
-        // Warp k copies in the halo of rounds k, k + 3, ... and raises each round's flag.
+        // Warp k copies in the halo of rounds k, k + kStrPrefetchWarps, ... and raises each
+        // round's flag.
         // Round q's halo is read by its helper once rounds <= q - kStreamLate - 1 are done;
         // each slot's wait (<= q - kStreamLate) lets the copy happen by then.
         for (uint32_t q = (uint32_t)(warp - kStrPrefetch0); q < R; q += kStrPrefetchWarps) {
