@@ -476,59 +476,97 @@ void pair_sweep(const Sweep<Low>& s, Sweep<Low>& out, PairMap& m) {
             default: return 1.0;
         }
     };
+    std::vector<double> diag(n, 1.0);
+    // Rows are independent: contiguous chunks of rows on host threads, each with its own
+    // scratch, concatenated in row order (the result does not depend on the threads).
+    struct Chunk {
+        std::vector<uint32_t> len, mlen, ci, dep;
+        std::vector<Low> cv;
+        std::vector<double> coef;
+    };
+    unsigned hc = std::max(1u, std::thread::hardware_concurrency());
+    if (const char* e = std::getenv("PRISM_LAYOUT_THREADS")) hc = (unsigned)std::max(1, std::atoi(e));
+    const uint32_t T = n < 65536 ? 1u : std::min<uint32_t>(std::min(hc, 16u), n);
+    std::vector<Chunk> parts(T);
+    auto work = [&](uint32_t t) {
+        Chunk& c = parts[t];
+        const uint32_t r0 = (uint32_t)((uint64_t)n * t / T), r1 = (uint32_t)((uint64_t)n * (t + 1) / T);
+        std::vector<int32_t> slot(n, -1);  // dependency row -> index in the row being built
+        std::vector<uint32_t> deps, idx;
+        std::vector<double> acc;
+        for (uint32_t r = r0; r < r1; ++r) {
+            const uint32_t p = pos[r], lk = s.level[r];
+            diag[r] = s.diag[p];
+            deps.clear();
+            acc.clear();
+            auto add = [&](uint32_t j, double v) {
+                if (slot[j] < 0) {
+                    slot[j] = (int32_t)deps.size();
+                    deps.push_back(j);
+                    acc.push_back(v);
+                } else {
+                    acc[(size_t)slot[j]] = acc[(size_t)slot[j]] + v;
+                }
+            };
+            const bool odd = (lk & 1u) != 0;
+            uint32_t mcount = 0;
+            // the row's own entries that stay, in stored order
+            for (uint32_t k = s.rowptr[p]; k < s.rowptr[p + 1]; ++k) {
+                const uint32_t j = s.col[k];
+                if (!(odd && s.level[j] + 1 == lk)) add(j, (double)s.val[k]);
+            }
+            if (odd) {
+                const double gk = g_of(r);
+                for (uint32_t k = s.rowptr[p]; k < s.rowptr[p + 1]; ++k) {
+                    const uint32_t i = s.col[k];
+                    if (s.level[i] + 1 != lk) continue;
+                    const double lki = (double)s.val[k], gi = g_of(i);
+                    const double f = lki * (s.op == SWEEP_PREDIV ? 1.0 : gi);
+                    const uint32_t pi = pos[i];
+                    for (uint32_t q = s.rowptr[pi]; q < s.rowptr[pi + 1]; ++q) add(s.col[q], -(f * (double)s.val[q]));
+                    c.dep.push_back(i);
+                    c.coef.push_back(s.op == SWEEP_PREDIV ? lki * gi / gk : lki * gi);
+                    ++mcount;
+                }
+            }
+            c.mlen.push_back(mcount);
+            // the row's entries, dependencies in increasing order
+            idx.resize(deps.size());
+            std::iota(idx.begin(), idx.end(), 0u);
+            std::sort(idx.begin(), idx.end(), [&](uint32_t x, uint32_t y) { return deps[x] < deps[y]; });
+            for (uint32_t t2 : idx) {
+                c.ci.push_back(deps[t2]);
+                c.cv.push_back((Low)acc[t2]);
+            }
+            c.len.push_back((uint32_t)deps.size());
+            for (uint32_t j : deps) slot[j] = -1;
+        }
+    };
+    if (T == 1) {
+        work(0);
+    } else {
+        std::vector<std::thread> pool;
+        for (uint32_t t = 0; t < T; ++t) pool.emplace_back(work, t);
+        for (auto& th : pool) th.join();
+    }
     std::vector<uint32_t> rp((size_t)n + 1, 0), ci;
     std::vector<Low> cv;
-    std::vector<double> diag(n, 1.0);
     m.ptr.assign((size_t)n + 1, 0);
     m.dep.clear();
     m.coef.clear();
-    std::vector<int64_t> slot(n, -1);  // dependency row -> index in the row being built
-    std::vector<uint32_t> deps;
-    std::vector<double> acc;
-    for (uint32_t r = 0; r < n; ++r) {
-        const uint32_t p = pos[r], lk = s.level[r];
-        diag[r] = s.diag[p];
-        deps.clear();
-        acc.clear();
-        auto add = [&](uint32_t j, double v) {
-            if (slot[j] < 0) {
-                slot[j] = (int64_t)deps.size();
-                deps.push_back(j);
-                acc.push_back(v);
-            } else {
-                acc[(size_t)slot[j]] = acc[(size_t)slot[j]] + v;
-            }
-        };
-        const bool odd = (lk & 1u) != 0;
-        // the row's own entries that stay, in stored order
-        for (uint32_t k = s.rowptr[p]; k < s.rowptr[p + 1]; ++k) {
-            const uint32_t j = s.col[k];
-            if (!(odd && s.level[j] + 1 == lk)) add(j, (double)s.val[k]);
+    uint32_t r = 0;
+    for (uint32_t t = 0; t < T; ++t) {
+        Chunk& c = parts[t];
+        for (size_t u = 0; u < c.len.size(); ++u, ++r) {
+            rp[r + 1] = rp[r] + c.len[u];
+            m.ptr[r + 1] = m.ptr[r] + c.mlen[u];
         }
-        if (odd) {
-            const double gk = g_of(r);
-            for (uint32_t k = s.rowptr[p]; k < s.rowptr[p + 1]; ++k) {
-                const uint32_t i = s.col[k];
-                if (s.level[i] + 1 != lk) continue;
-                const double lki = (double)s.val[k], gi = g_of(i);
-                const double f = lki * (s.op == SWEEP_PREDIV ? 1.0 : gi);
-                const uint32_t pi = pos[i];
-                for (uint32_t q = s.rowptr[pi]; q < s.rowptr[pi + 1]; ++q) add(s.col[q], -(f * (double)s.val[q]));
-                m.dep.push_back(i);
-                m.coef.push_back(s.op == SWEEP_PREDIV ? lki * gi / gk : lki * gi);
-            }
-        }
-        m.ptr[r + 1] = (uint32_t)m.dep.size();
-        // the row's entries, dependencies in increasing order
-        std::vector<uint32_t> idx(deps.size());
-        std::iota(idx.begin(), idx.end(), 0u);
-        std::sort(idx.begin(), idx.end(), [&](uint32_t a, uint32_t b) { return deps[a] < deps[b]; });
-        for (uint32_t t : idx) {
-            ci.push_back(deps[t]);
-            cv.push_back((Low)acc[t]);
-        }
-        rp[r + 1] = (uint32_t)ci.size();
-        for (uint32_t j : deps) slot[j] = -1;
+        ci.insert(ci.end(), c.ci.begin(), c.ci.end());
+        cv.insert(cv.end(), c.cv.begin(), c.cv.end());
+        m.dep.insert(m.dep.end(), c.dep.begin(), c.dep.end());
+        m.coef.insert(m.coef.end(), c.coef.begin(), c.coef.end());
+        Chunk().ci.swap(c.ci);  // release as we go
+        Chunk().cv.swap(c.cv);
     }
     build_sweep<Low>(n, rp, ci, cv, &diag, s.op, s.lower, out);
 }

@@ -103,3 +103,24 @@ def test_paired_sweep_with_single_precision_values():
     x = substitute(rp, ci, v.astype(np.float32).astype(np.float64), d, 0, True, b)
     xp = substitute(prow, pcol, pval, d, 0, True, apply_map(mptr, mdep, mcoef, b))
     assert np.abs(xp - x).max() <= 1e-5 * np.abs(x).max()
+
+
+def test_pairing_does_not_depend_on_host_threads(monkeypatch):
+    """Large sweeps are paired on several host threads, rows in contiguous chunks, and
+    assembled in row order: one thread and several give the same arrays to the bit."""
+    n = 90000
+    offs = np.array([1, 7, 50, 2500])
+    rows = np.repeat(np.arange(n), len(offs))
+    cols = rows - np.tile(offs, n)
+    keep = cols >= 0
+    rows, cols = rows[keep], cols[keep]
+    rp = np.concatenate([[0], np.cumsum(np.bincount(rows, minlength=n))]).astype(np.uint32)
+    ci = cols.astype(np.uint32)
+    v = np.random.default_rng(8).uniform(-0.2, 0.2, len(ci))
+    d = np.random.default_rng(9).uniform(1.5, 3.0, n)
+    got = []
+    for threads in ("1", "6"):
+        monkeypatch.setenv("PRISM_LAYOUT_THREADS", threads)
+        got.append(P.stream_sweep_pair(rp, ci, v, diag=d, op=0, lower=True, precision=P.PRISM_FP64))
+    for a, b in zip(*got):
+        assert np.array_equal(a, b)
