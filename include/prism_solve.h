@@ -156,6 +156,15 @@ int32_t prism_selftest_wait_timeout(int32_t device, uint64_t wait_ns, int32_t* d
 int32_t prism_selftest_stream_layout(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val,
                                      const double* diag, int32_t op, int32_t lower, int32_t precision,
                                      uint32_t num_ctas, uint32_t rows_per_cta, const double* in, double* out);
+/* The same with rounds cut short where their record would exceed
+ * max_round_bytes (0: no cap), as the device layout does when four of its
+ * largest records do not fit the ring; *record_bytes (may be NULL) receives
+ * the largest record of the layout. */
+int32_t prism_selftest_stream_layout_capped(uint32_t n, const uint32_t* rowptr, const uint32_t* col,
+                                            const double* val, const double* diag, int32_t op, int32_t lower,
+                                            int32_t precision, uint32_t num_ctas, uint32_t rows_per_cta,
+                                            uint32_t max_round_bytes, const double* in, double* out,
+                                            uint32_t* record_bytes);
 
 /* The low-rank correction of an AMSED / MSLR level on a block of k <= 64
  * right-hand sides, alone on `device` with host arrays: Y += W (H o (W^T X)),

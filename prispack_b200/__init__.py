@@ -77,6 +77,9 @@ _SIGS = {
     "prism_selftest_wait_timeout": (C.c_int32, [C.c_int32, C.c_uint64, C.POINTER(C.c_int32)]),
     "prism_lowrank_block_run": (C.c_int32, [C.c_int32, C.c_uint32, C.c_uint32, C.c_uint32, _f64p, _f64p, _f64p, _f64p,
                                             C.c_int32]),
+    "prism_selftest_stream_layout_capped": (C.c_int32, [C.c_uint32, _u32p, _u32p, _f64p, _vp, C.c_int32, C.c_int32,
+                                                        C.c_int32, C.c_uint32, C.c_uint32, C.c_uint32, _f64p,
+                                                        _f64p, C.POINTER(C.c_uint32)]),
     "prism_selftest_stream_layout": (C.c_int32, [C.c_uint32, _u32p, _u32p, _f64p, _vp, C.c_int32, C.c_int32,
                                                  C.c_int32, C.c_uint32, C.c_uint32, _f64p, _f64p]),
     "prism_stream_sweep_order": (C.c_int32, [C.c_uint32, _u32p, _u32p, _f64p, _vp, C.c_int32, C.c_int32, C.c_int32,
@@ -208,6 +211,23 @@ def lowrank_block_run(W, H, X, Y, *, tensor: bool, device: int = 0):
     _check(load().prism_lowrank_block_run(device, nrem, rank, X.shape[1], np.ascontiguousarray(W.T),
                                           np.ascontiguousarray(H, np.float64), X, out, int(bool(tensor))))
     return out
+
+
+def selftest_stream_layout_capped(rowptr, col, val, in_, *, max_round_bytes: int, diag=None, op: int = 2,
+                                  lower: bool = True, precision: int = 0, num_ctas: int = 4):
+    """selftest_stream_layout with rounds cut short at max_round_bytes (the device layout's
+    record cap; slab boundaries as the device layout chooses): (solution, largest record)."""
+    rp = np.ascontiguousarray(rowptr, np.uint32)
+    n = len(rp) - 1
+    out = np.zeros(n)
+    rec = C.c_uint32()
+    d = np.ascontiguousarray(diag, np.float64) if diag is not None else None
+    _check(load().prism_selftest_stream_layout_capped(n, rp, np.ascontiguousarray(col, np.uint32),
+                                                      np.ascontiguousarray(val, np.float64),
+                                                      d.ctypes.data if d is not None else None, op, int(lower),
+                                                      precision, num_ctas, 0, max_round_bytes,
+                                                      np.ascontiguousarray(in_, np.float64), out, C.byref(rec)))
+    return out, rec.value
 
 
 def selftest_stream_layout(rowptr, col, val, in_, *, diag=None, op: int = 2, lower: bool = True,

@@ -149,7 +149,8 @@ static int copy_order(const prism::StreamOrder& o, uint32_t n, uint32_t* eptr, u
 template <typename Low>
 static int stream_selftest(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val,
                            const double* diag, int op, bool lower, uint32_t num_ctas, uint32_t rows_per_cta,
-                           uint32_t slot_bytes, const double* in, double* out) {
+                           uint32_t slot_bytes, const double* in, double* out, uint32_t max_round_bytes = 0,
+                           uint32_t* record_bytes = nullptr) {
     const uint64_t nnz = rowptr[n];
     std::vector<uint32_t> rp(rowptr, rowptr + n + 1), ci(col, col + nnz);
     std::vector<Low> v(nnz);
@@ -169,8 +170,9 @@ static int stream_selftest(uint32_t n, const uint32_t* rowptr, const uint32_t* c
     }
     prism::StreamLayout L;
     std::string why;
-    if (!prism::stream_layout<Low>(s, start, prism::kNoSlot, slot_bytes, L, &why))
+    if (!prism::stream_layout<Low>(s, start, prism::kNoSlot, slot_bytes, L, &why, nullptr, nullptr, max_round_bytes))
         return fail(PRISM_ERR_UNSUPPORTED, why);
+    if (record_bytes) *record_bytes = L.max_round_bytes;
     why = prism::stream_layout_replay<Low>(s, L, in, out);
     if (!why.empty()) return fail(PRISM_ERR_ARG, "stream layout: " + why);
     return PRISM_OK;
@@ -354,6 +356,15 @@ int32_t prism_precond_sweep_order(prism_handle h, int32_t sweep, uint32_t* n, ui
 int32_t prism_selftest_stream_layout(uint32_t n, const uint32_t* rowptr, const uint32_t* col, const double* val,
                                      const double* diag, int32_t op, int32_t lower, int32_t precision,
                                      uint32_t num_ctas, uint32_t rows_per_cta, const double* in, double* out) {
+    return prism_selftest_stream_layout_capped(n, rowptr, col, val, diag, op, lower, precision, num_ctas,
+                                               rows_per_cta, 0, in, out, nullptr);
+}
+
+int32_t prism_selftest_stream_layout_capped(uint32_t n, const uint32_t* rowptr, const uint32_t* col,
+                                            const double* val, const double* diag, int32_t op, int32_t lower,
+                                            int32_t precision, uint32_t num_ctas, uint32_t rows_per_cta,
+                                            uint32_t max_round_bytes, const double* in, double* out,
+                                            uint32_t* record_bytes) {
     if (!rowptr || !col || !val || !in || !out) return fail(PRISM_ERR_ARG, "null array");
     if (op < 0 || op > 3 || (op != 2 && !diag)) return fail(PRISM_ERR_ARG, "bad op / missing diagonal");
     return guarded([&]() -> int {
@@ -364,9 +375,9 @@ int32_t prism_selftest_stream_layout(uint32_t n, const uint32_t* rowptr, const u
         const uint32_t slot_bytes = precision == PRISM_FP32_APPLY ? 4 : 8;
         if (precision != PRISM_FP64)
             return stream_selftest<float>(n, rowptr, col, val, diag, op, lower != 0, num_ctas, rows_per_cta,
-                                          slot_bytes, in, out);
+                                          slot_bytes, in, out, max_round_bytes, record_bytes);
         return stream_selftest<double>(n, rowptr, col, val, diag, op, lower != 0, num_ctas, rows_per_cta, 8, in,
-                                       out);
+                                       out, max_round_bytes, record_bytes);
     });
 }
 

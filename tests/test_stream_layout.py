@@ -172,3 +172,26 @@ def test_layout_does_not_depend_on_host_threads(monkeypatch):
     for f in ("eptr", "edep", "ecoef", "kptr", "kdep", "kcoef"):
         assert np.array_equal(getattr(o1, f), getattr(o2, f)), f
     assert np.array_equal(x1, x2)
+
+
+@pytest.mark.parametrize("precision", [P.PRISM_FP32_APPLY, P.PRISM_FP64])
+def test_capped_rounds_replay_and_respect_the_cap(precision):
+    """Rounds cut short where their record would pass a byte cap (what the device layout
+    does when four of its largest records would not fit the ring): the records stay within
+    half of the uncapped layout's largest, and the replay still solves the sweep.  (A round
+    keeps at least one row, so a cap below one row's record cannot hold.)"""
+    rng = np.random.default_rng(33)
+    n = 4000
+    rp, ci, v = random_triangular(n, True, rng, near=24, far=6)
+    d = rng.uniform(1.0, 2.0, n)
+    b = rng.standard_normal(n)
+    want = substitute(rp, ci, v, d, 0, True, b)
+    free, rec_free = P.selftest_stream_layout_capped(rp, ci, v, b, max_round_bytes=0, diag=d, op=0,
+                                                     precision=precision, num_ctas=6)
+    cap = rec_free // 2 // 16 * 16
+    got, rec = P.selftest_stream_layout_capped(rp, ci, v, b, max_round_bytes=cap, diag=d, op=0,
+                                               precision=precision, num_ctas=6)
+    assert rec <= cap
+    tol = 1e-4 if precision == P.PRISM_FP32_APPLY else 1e-12
+    for x in (free, got):
+        assert np.abs(x - want).max() <= tol * np.abs(want).max()
